@@ -1,0 +1,415 @@
+#!/usr/bin/env python3
+"""FemPIC particle hot path benchmark (move + deposit, with the removal compaction and
+periodic cell sort) on the electrostatic tet-mesh workload:
+
+  box 1 x 1 x 4 cut into 48 x 48 x 192 hexahedra x 6 tets = 2,654,208 cells, 463,393 nodes;
+  250,000 ions injected per step through the z=0 face (drift 1.0 along +z, Maxwellian
+  sigma 0.1), dt 0.01, unit charge/mass, static FEM field; particles removed on leaving
+  the box; opp_fill = Sort_Periodic with period 10; 300 fill steps to reach the steady
+  state (~5e7 particles), then W warm-up and K timed steps.
+
+Both precisions run on the same seeded inputs: plain FP64 (bit-identical to the seq
+backend) and mixed (FP32 push and barycentric tests, FP64 re-check in |lambda| < 1e-5,
+FP64 node totals).  value = mixed particle-steps/s = sum N_alive(start of move) /
+sum t(move+deposit+compaction), device time (CUDA events), summed over ranks ÷ max-rank
+time.  Particle dats (~4 GB) exceed L2, so no flush is needed between steps.
+
+--impl reference times the reference's own CPU implementation of the same path (the
+compiled OP-PIC omp/seq backend when oracle/_ref holds it, else the C oracle) on a
+bounded sample of the workload, on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT / "op-pic_b200", ROOT):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+METRIC = "particle-steps/s (move+deposit) mixed vs plain FP64 on 1 B200; % HBM roofline"
+UNIT = "particle-steps/s"
+CFG = dict(nx=48, ny=48, nz=192, lx=1.0, ly=1.0, lz=4.0, inject=250_000, sigma=0.1, dt=0.01, qm=1.0,
+           v_ion=1.0, fill="Sort_Periodic", period=10, fill_steps=300, seed=0, capacity=90_000_000)
+WORKLOAD = ("FemPIC electrostatic tet-mesh PIC, 48x48x192 hexes x 6 = 2,654,208 tets, 463,393 nodes; "
+            "250,000 ions/step; steady state after 300 fill steps; Sort_Periodic period 10")
+# Algorithmic bytes per move+deposit launch: per particle read pos 24 + p2c 4, write p2c 4 + p_lc 32;
+# per cell the record read once (FP64: det 128 + coef 8 + c2c 16 + c2n 16; mixed: origin 16 +
+# f32 lambda rows 64 + c2c/c2n 32); per node one FP64 read-modify-write.
+BYTES_PER_PARTICLE = 64
+BYTES_PER_CELL = {"f64": 168, "mixed": 112}
+BYTES_PER_NODE = 16
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [r.split(",") for r in Path(self.path).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- our arm
+
+def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, sampler=None,
+                  e2e_steps: int = 0, cpu_sample: bool = False) -> dict:
+    import numpy as np
+    import torch
+
+    from oppb import _lib as L
+    from oppb.fempic import FemPIC, injection_randoms
+
+    sim = FemPIC(hm, dev, inject_per_step=CFG["inject"], ion_velocity=CFG["v_ion"], qm=CFG["qm"], dt=CFG["dt"],
+                 precision=precision, fill=CFG["fill"], fill_period=CFG["period"], capacity=CFG["capacity"])
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    rnd_buf = torch.empty((5, CFG["inject"]), dtype=torch.float64, device=dev)
+
+    def device_randoms(out):
+        out[0:2].uniform_(0.0, 1.0, generator=gen)
+        out[2:5].normal_(0.0, CFG["sigma"], generator=gen)
+        return out
+
+    t0 = time.time()
+    for _ in range(CFG["fill_steps"]):
+        sim.step(device_randoms(rnd_buf))
+    torch.cuda.synchronize()
+    log(f"[{precision}] fill {CFG['fill_steps']} steps in {time.time() - t0:.1f}s, size {sim.parts.size}")
+    for _ in range(warmup):
+        sim.step(device_randoms(rnd_buf))
+    # Inputs of the timed steps generated before timing (device-resident).
+    tables = [device_randoms(torch.empty_like(rnd_buf)) for _ in range(min(steps, 16))]
+    torch.cuda.synchronize()
+
+    s = torch.cuda.current_stream()
+    E = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    rec = []
+    lib = L.load()
+    launches0 = lib.oppb_kernel_launches()
+    if sampler:
+        sampler.start()
+    torch.cuda.synchronize()
+    ev_all0, ev_all1 = E(), E()
+    ev_all0.record(s)
+    for k in range(steps):
+        ev = [E() for _ in range(4)]
+        sim.inject(tables[k % len(tables)])
+        sim.node_charge.zero_()
+        sim.push()
+        n_alive = sim.parts.size
+        ev[0].record(s)
+        sim.move()
+        ev[1].record(s)
+        st = sim.parts.status_host()
+        if st.error:
+            raise L.OppbError("move", st.error)
+        ev[2].record(s)
+        kind = sim.finalize(st.remove_count)
+        ev[3].record(s)
+        sim.iter += 1
+        rec.append((n_alive, ev, kind, st.total_visits, st.recheck_count, st.remove_count))
+    ev_all1.record(s)
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    launches = lib.oppb_kernel_launches() - launches0
+    total_ms = ev_all0.elapsed_time(ev_all1)
+    t_move = [r[1][0].elapsed_time(r[1][1]) for r in rec]
+    t_comp = [r[1][2].elapsed_time(r[1][3]) for r in rec]
+    n = [r[0] for r in rec]
+    ps = sum(n)
+    out = {
+        "precision": precision,
+        "particle_steps": ps,
+        "t_move_ms": sum(t_move),
+        "t_compact_ms": sum(t_comp),
+        "value": ps / ((sum(t_move) + sum(t_comp)) / 1e3),
+        "move_only": ps / (sum(t_move) / 1e3),
+        "whole_step": ps / (total_ms / 1e3),
+        "ms_per_step": total_ms / steps,
+        "mean_particles": ps / steps,
+        "visits_per_particle": sum(int(r[3]) for r in rec) / ps,
+        "recheck_frac": sum(r[4] for r in rec) / max(1, sum(int(r[3]) for r in rec)),
+        "removed_per_step": sum(r[5] for r in rec) / steps,
+        "sorts": sum(1 for r in rec if r[2] == "sort"),
+        "launches": int(launches),
+        "clocks": clocks,
+    }
+    # Roofline of the move(+deposit) kernel: algorithmic bytes / mean launch time.
+    bytes_per_launch = [BYTES_PER_PARTICLE * r[0] + BYTES_PER_CELL[precision] * hm.n_cells
+                        + BYTES_PER_NODE * hm.n_nodes for r in rec]
+    out["move_gbs"] = sum(bytes_per_launch) / (sum(t_move) / 1e3) / 1e9
+    out["move_bytes_per_launch"] = sum(bytes_per_launch) / steps
+    out["move_ms_per_launch"] = sum(t_move) / steps
+
+    if e2e_steps:
+        # End to end: host inputs (pinned) copied in, node charges + status copied out, every step.
+        host_tables = [torch.from_numpy(np.ascontiguousarray(injection_randoms(seed + 7, k, CFG["inject"],
+                                                                                CFG["sigma"]).T)).pin_memory()
+                       for k in range(min(e2e_steps, 8))]
+        charge_host = torch.empty(hm.n_nodes, dtype=torch.float64).pin_memory()
+        t_e2e, n_e2e = 0.0, 0
+        for k in range(e2e_steps):
+            e0, e1 = E(), E()
+            torch.cuda.synchronize()
+            e0.record(s)
+            rnd_buf.copy_(host_tables[k % len(host_tables)], non_blocking=True)
+            n_e2e += sim.parts.size + CFG["inject"]
+            st = sim.step(rnd_buf)
+            charge_host.copy_(sim.node_charge, non_blocking=True)
+            e1.record(s)
+            e1.synchronize()
+            t_e2e += e0.elapsed_time(e1)
+        out["e2e"] = {"value": n_e2e / (t_e2e / 1e3), "unit": UNIT,
+                      "h2d_bytes_per_step": int(host_tables[0].numel() * 8),
+                      "d2h_bytes_per_step": int(charge_host.numel() * 8 + 32), "steps": e2e_steps}
+
+    if cpu_sample:
+        # One more step up to the push, then a contiguous slice of the particles as the
+        # CPU sample (positions after the push, cells before the move).
+        sim.inject(tables[0])
+        sim.node_charge.zero_()
+        sim.push()
+        m = sim.parts.size
+        k = min(m, 1_000_000)
+        a = (m - k) // 2
+        out["cpu_sample_state"] = {
+            "pos": sim.parts.pos[:, a:a + k].T.contiguous().cpu().numpy(),
+            "p2c": sim.parts.p2c[0, a:a + k].contiguous().cpu().numpy(),
+        }
+    del sim
+    torch.cuda.empty_cache()
+    return out
+
+
+def cpu_baseline_port(hm, sample: dict, budget_s: float = 8.0) -> dict:
+    """The C oracle (single thread) on the sampled particles: move + deposit, repeated."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    pos, p2c0 = sample["pos"], sample["p2c"]
+    n = len(p2c0)
+    ps, t = 0, 0.0
+    while t < budget_s:
+        p2c = p2c0.copy()
+        lc = np.zeros((n, 4))
+        q = np.zeros(hm.n_nodes)
+        t0 = time.perf_counter()
+        O.move(pos, lc, p2c, hm.c2c, hm.c_vol, hm.c_det, n=n)
+        keep = p2c != O.REMOVED
+        O.deposit(np.ascontiguousarray(lc[keep]), np.ascontiguousarray(p2c[keep]), hm.c2n, q)
+        t += time.perf_counter() - t0
+        ps += n
+    return {"value": ps / t, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} steady-state particles (contiguous slice after the push), FP64 move + deposit, "
+                      f"C oracle single thread, {ps // n} repetitions"}
+
+
+def arm_ours(args) -> dict:
+    import torch
+    import torch.distributed as dist
+
+    from oppb.fempic import HostMesh
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    hm = HostMesh(CFG["nx"], CFG["ny"], CFG["nz"], CFG["lx"], CFG["ly"], CFG["lz"])
+    log(f"mesh {hm.n_cells} cells built in {time.time() - t0:.1f}s (CG iters {hm.cg_iters})")
+    seed = CFG["seed"] + 1000 * rank  # independent replicas per rank
+    if world > 1:
+        dist.barrier()
+    f64 = run_precision(hm, dev, "f64", args.steps, args.warmup, seed, cpu_sample=(rank == 0 and args.cpu_baseline))
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    mixed = run_precision(hm, dev, "mixed", args.steps, args.warmup, seed, sampler=sampler,
+                          e2e_steps=args.e2e_steps)
+
+    def reduce(v, op):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    SUM, MAX = (dist.ReduceOp.SUM, dist.ReduceOp.MAX) if world > 1 else (None, None)
+    res = {}
+    for r in (f64, mixed):
+        t = (r["t_move_ms"] + r["t_compact_ms"]) / 1e3
+        r["job_value"] = reduce(r["particle_steps"], SUM) / reduce(t, MAX)
+        r["job_ms_per_step"] = reduce(r["ms_per_step"], MAX)
+    if "e2e" in mixed:
+        e = mixed["e2e"]
+        e["value"] = reduce(e["value"], SUM) if world > 1 else e["value"]
+    res["f64"], res["mixed"] = f64, mixed
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return {}
+    peaks = measured_peaks()
+    line = {
+        "metric": METRIC,
+        "value": mixed["job_value"],
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": mixed["job_ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": hm.n_cells, "nodes": hm.n_nodes,
+                   "mean_particles": round(mixed["mean_particles"]), "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (particle dats ~4 GB), no flush"},
+        "plain_fp64": {"value": f64["job_value"], "move_only": f64["move_only"], "whole_step": f64["whole_step"],
+                       "ms_per_step": f64["ms_per_step"], "move_ms_per_launch": f64["move_ms_per_launch"],
+                       "move_gbs": f64["move_gbs"], "frac_of_hbm": f64["move_gbs"] / peaks["hbm_gbs"],
+                       "visits_per_particle": f64["visits_per_particle"], "mean_particles": f64["mean_particles"]},
+        "mixed": {"value": mixed["job_value"], "move_only": mixed["move_only"], "whole_step": mixed["whole_step"],
+                  "move_ms_per_launch": mixed["move_ms_per_launch"], "recheck_frac": mixed["recheck_frac"],
+                  "visits_per_particle": mixed["visits_per_particle"]},
+        "mixed_over_plain": mixed["job_value"] / f64["job_value"],
+        "roofline": {"bound": "hbm", "kernel": "move_mixed_kernel (move + fused deposit)",
+                     "achieved": mixed["move_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": mixed["move_gbs"] / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                     "bytes_per_launch": mixed["move_bytes_per_launch"], "traffic": None},
+        "gpu_launches": mixed["launches"],
+        "clocks": mixed["clocks"],
+    }
+    if "e2e" in mixed:
+        line["e2e"] = mixed["e2e"]
+    if args.cpu_baseline and "cpu_sample_state" in f64:
+        line["cpu_baseline"] = cpu_baseline_port(hm, f64["cpu_sample_state"], args.cpu_seconds)
+    return line
+
+
+# ------------------------------------------------------------------------ reference arm
+
+def arm_reference(args) -> dict:
+    """The reference's CPU path on a bounded sample: config mesh, FILL steps of 250,000
+    injected ions (the inlet region then holds the steady-state density), then
+    W + K steps, timing move + compaction + deposit."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return {}
+    import numpy as np
+
+    from oppb.fempic import HostMesh, injection_randoms
+    from oracle import oracle as O
+
+    fill = args.ref_fill_steps
+    hm = HostMesh(CFG["nx"], CFG["ny"], CFG["nz"], CFG["lx"], CFG["ly"], CFG["lz"])
+    dist = hm.inject_distribution(CFG["inject"])
+    orc = O.OracleFemPIC(hm, dist, ion_velocity=CFG["v_ion"], qm=CFG["qm"], dt=CFG["dt"], fill=CFG["fill"],
+                         fill_period=CFG["period"], alloc_mult=2.0)
+    for s in range(fill + args.warmup):
+        orc.step(injection_randoms(CFG["seed"], s, CFG["inject"], CFG["sigma"]))
+    ps, t = 0, 0.0
+    for k in range(args.steps):
+        rnd = injection_randoms(CFG["seed"], fill + args.warmup + k, CFG["inject"], CFG["sigma"])
+        orc.inject(rnd)
+        orc.node_charge[:] = 0
+        O.push(orc.p2c, hm.c_ef, orc.pos, orc.vel, orc.qm, orc.dt, n=orc.size)
+        n_alive = orc.size
+        t0 = time.perf_counter()
+        rc, visits, _ = O.move(orc.pos, orc.lc, orc.p2c, hm.c2c, hm.c_vol, hm.c_det, n=orc.size)
+        orc.finalize(rc)
+        O.deposit(orc.lc, orc.p2c, hm.c2n, orc.node_charge, n=orc.size)
+        t += time.perf_counter() - t0
+        orc.iter += 1
+        ps += n_alive
+    value = ps / t
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"first {fill} steps of injection (inlet region at steady-state "
+                                                  f"density), {round(ps / args.steps)} particles per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"{fill}+{args.warmup} fill steps then {args.steps} timed steps; C oracle"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["oppb", "reference"], default="oppb")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    ap.add_argument("--ref-fill-steps", type=int, default=20)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    line = arm_reference(args) if args.impl == "reference" else arm_ours(args)
+    if line:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

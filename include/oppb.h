@@ -1,0 +1,227 @@
+/*
+ * oppb.h — C ABI of the B200 particle hot path (move, deposit, push, inject,
+ * hole fill, cell sort) for unstructured tetrahedral meshes.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and
+ * returns an int status (OPPB_OK = 0).  Pointers named "device" must point to
+ * CUDA device memory of the current device; all launches are asynchronous on
+ * `stream` (a cudaStream_t passed as void*, NULL = the legacy default stream).
+ * Nothing here allocates device memory: scratch space is passed in by the
+ * caller (see the *_workspace_bytes queries).
+ *
+ * Each entry point names the reference interface whose body it replaces.
+ * Reference paths are relative to the OP-PIC source tree.
+ */
+#ifndef OPPB_H
+#define OPPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define OPPB_OK              0
+#define OPPB_ERR_ARG         1  /* null pointer, negative size, bad alignment      */
+#define OPPB_ERR_LAUNCH      2  /* CUDA reported an error at launch                */
+#define OPPB_ERR_WORKSPACE   3  /* workspace smaller than *_workspace_bytes()      */
+#define OPPB_ERR_HOP_LIMIT   4  /* device: a particle exceeded max_hops cell visits */
+#define OPPB_ERR_CELL_RANGE  5  /* device: p2c / c2c / c2n index out of range       */
+#define OPPB_ERR_CAPACITY    6  /* injection would exceed the set capacity          */
+#define OPPB_ERR_NO_DEVICE   7  /* no CUDA device visible                           */
+
+/* Cell index of a removed particle: MAX_CELL_INDEX in opp_lib/include/opp_defs.h:150. */
+#define OPPB_REMOVED_CELL 2147483647
+
+/* ------------------------------------------------------------------ types */
+
+/* Device-resident tetrahedral mesh in the packed layout the kernels read.
+ * Filled by oppb_tet_mesh_pack(); buffers are owned by the caller.
+ *   det   [n_cells][16] f64 : {alpha,beta,gamma,delta} of vertex 0..3
+ *                             (minifempic_funcs.h:316-382 ordering), 128-B record
+ *   coef  [n_cells]     f64 : (1.0/6.0) / c_volume (kernels.h:110)
+ *   conn  [n_cells][8]  i32 : c2c[0..3] (face opposite vertex i, -1 = boundary),
+ *                             c2n[0..3]; 32-B record
+ *   ef    [n_cells][4]  f64 : cell electric field x,y,z + pad
+ *   geo32 [n_cells][16] f32 : mixed path, per vertex {lambda_i(o), dlambda_i/dx,
+ *                             dlambda_i/dy, dlambda_i/dz} about origin o (may be NULL)
+ *   org32 [n_cells][4]  f32 : mixed path origin o = vertex 0 rounded to f32 (may be NULL) */
+typedef struct oppb_tet_mesh {
+    int32_t  n_cells;
+    int32_t  n_nodes;
+    double*  det;
+    double*  coef;
+    int32_t* conn;
+    double*  ef;
+    float*   geo32;
+    float*   org32;
+} oppb_tet_mesh;
+
+/* Particle set in the reference's device layout: SoA [dim][stride]
+ * (opp_lib/src/cuda/opp_cuda_utils.cu:128-143), stride = set capacity. */
+typedef struct oppb_particles {
+    int32_t   size;        /* particles [0,size) are live / processed          */
+    int32_t   stride;      /* SoA stride of every particle dat (capacity)      */
+    double*   pos;         /* [3][stride] p_position                           */
+    double*   vel;         /* [3][stride] p_velocity                           */
+    double*   lc;          /* [4][stride] p_lc (barycentric weights)           */
+    int32_t*  p2c;         /* [stride]    particle -> cell (mesh relation)     */
+    uint32_t* remove_bits; /* [ceil(stride/32)] bit i = (p2c[i]==REMOVED) after a move */
+} oppb_particles;
+
+/* Device-side result of one move.  The move launchers zero it first. */
+typedef struct oppb_move_status {
+    int32_t  remove_count;   /* particles removed by this move (opp_set::particle_remove_count) */
+    int32_t  error;          /* first device error (OPPB_ERR_HOP_LIMIT / _CELL_RANGE), 0 = none */
+    int32_t  error_index;    /* particle index that raised `error`                              */
+    int32_t  max_visits;     /* largest number of cells one particle visited                    */
+    uint64_t total_visits;   /* sum over particles of cells visited                             */
+    int32_t  recheck_count;  /* mixed path: particles whose decision was re-evaluated in FP64   */
+    int32_t  reserved;
+} oppb_move_status;
+
+/* One particle dat for compaction / sort: SoA [dim][stride] of elem_bytes. */
+typedef struct oppb_dat {
+    void*   data;        /* device, current contents                         */
+    void*   swap;        /* device, same shape; sort gathers into it (may be NULL for hole fill) */
+    int32_t dim;
+    int32_t elem_bytes;  /* 4 or 8 */
+} oppb_dat;
+
+/* Inlet faces for injection (FemPIC inlet surface, minifempic_funcs.h:508-583).
+ *   dist [n_faces] i32 : cumulative particle count per face (fempic_misc.h:42-80)
+ *   if2c [n_faces] i32 : cell attached to the face
+ *   geom [n_faces][12] f64 : u[3], v[3], normal[3], node0 position[3]          */
+typedef struct oppb_inlet {
+    int32_t        n_faces;
+    const int32_t* dist;
+    const int32_t* if2c;
+    const double*  geom;
+} oppb_inlet;
+
+/* ------------------------------------------------------------------ setup */
+
+const char* oppb_version(void);
+const char* oppb_status_string(int status);
+
+/* Number of CUDA kernels this library has launched in the process so far (every
+ * launcher adds its launches; memsets are not counted). */
+uint64_t oppb_kernel_launches(void);
+
+/* Bytes of each packed mesh buffer for n_cells cells (det, coef, conn, ef, geo32, org32). */
+void oppb_tet_mesh_bytes(int32_t n_cells, size_t out_bytes[6]);
+
+/* Pack the reference's device-layout cell dats (SoA [dim][soa_stride], as uploaded by
+ * opp_upload_dat, opp_lib/src/cuda/opp_cuda_utils.cu:119-152) into mesh->det/coef/conn/ef,
+ * and, when mesh->geo32/org32 are non-NULL, the mixed-precision records (needs n_pos,
+ * SoA [3][n_pos_stride]).  c_ef may be NULL (ef left untouched).  invalid_out (device
+ * int32, may be NULL) receives the number of c2c entries outside {-1}u[0,n_cells) and
+ * c2n entries outside [0,n_nodes); kernels never dereference such entries.
+ * Replaces the per-loop SoA gathers of the generated move loop
+ * (apps_codegen/app_fempic_cg/cuda/move_kernel_loop.hpp:287-301). */
+int oppb_tet_mesh_pack(oppb_tet_mesh* mesh, int32_t soa_stride,
+                       const double* c_det, const double* c_volume,
+                       const int32_t* c2c, const int32_t* c2n, const double* c_ef,
+                       const double* n_pos, int32_t n_pos_stride,
+                       int32_t* invalid_out, void* stream);
+
+/* Upload a cell electric field (SoA [3][soa_stride]) into mesh->ef. */
+int oppb_tet_mesh_set_ef(oppb_tet_mesh* mesh, int32_t soa_stride, const double* c_ef, void* stream);
+
+/* ------------------------------------------------------------------- move */
+
+/* FP64 multi-hop move.  Body of opp_particle_move__move_kernel
+ * (apps_codegen/app_fempic_cg/cuda/move_kernel_loop.hpp:189-401, user kernel
+ * apps/app_fempic/kernels.h:106-161, status rule opp_lib/include/opp_seq.h:68-86):
+ * writes p_lc and p2c, sets p2c = OPPB_REMOVED_CELL for particles leaving the mesh,
+ * fills remove_bits and *status (device).  Cell decisions are bit-identical to the
+ * FP64 seq backend.  max_hops bounds the cell visits per particle (the reference
+ * loop is unbounded); hitting it sets status->error = OPPB_ERR_HOP_LIMIT. */
+int oppb_move_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                  oppb_move_status* status, int32_t max_hops, void* stream);
+
+/* FP64 move with the node-charge deposit of the final cell fused in:
+ * node_charge[c2n[p2c][i]] += p_lc[i] for every particle that stays
+ * (apps/app_fempic/kernels.h:164-175) using warp-aggregated FP64 atomics. */
+int oppb_move_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                          double* node_charge, oppb_move_status* status,
+                          int32_t max_hops, void* stream);
+
+/* Mixed-precision move + deposit: barycentric tests in FP32 about a per-cell origin;
+ * any particle whose decision lies within `band` of a threshold or tie is re-evaluated
+ * with the FP64 reference formula, so cell assignment, hop counts and removals stay
+ * bit-identical to oppb_move_deposit_f64.  p_lc of non-rechecked particles carries
+ * FP32 accuracy; node totals accumulate in FP64.  Needs mesh->geo32/org32. */
+int oppb_move_deposit_mixed(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                            double* node_charge, oppb_move_status* status,
+                            int32_t max_hops, double band, void* stream);
+
+/* ---------------------------------------------------------------- deposit */
+
+/* Standalone deposit over [0,size): body of opp_par_loop_all__deposit_charge_on_nodes_kernel
+ * (apps_codegen/app_fempic_cg/cuda/deposit_charge_on_nodes_kernel_loop.hpp:92-165). */
+int oppb_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                     double* node_charge, void* stream);
+
+/* ------------------------------------------------------------------- push */
+
+/* v += (qm*dt)*E[p2c]; x += v*dt  (apps/app_fempic/kernels.h:93-103), FP64, bit-identical
+ * to the seq backend.  Body of opp_par_loop_all__calculate_new_pos_vel_kernel. */
+int oppb_push_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                  double qm, double dt, void* stream);
+
+/* Same update with FP32 increments on FP64 state: dv = f32(qm*dt)*f32(E),
+ * v += dv; dx = f32(v)*f32(dt), x += dx. */
+int oppb_push_mixed(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                    double qm, double dt, void* stream);
+
+/* ----------------------------------------------------------------- inject */
+
+/* Inject `count` particles into slots [start, start+count): face of particle k is the
+ * first face j with k < dist[j] (opp_lib/src/cuda/opp_increase_part_count.cu:86-105,
+ * found by binary search), then inject_ions_kernel (apps/app_fempic/kernels.h:63-90):
+ *   pos = a*u + b*v + node0  ((a,b) folded into the triangle),
+ *   vel = normal*ion_velocity - qm*E*(0.5*dt) + thermal,  p2c = if2c[face].
+ * rnd is SoA [5][rnd_stride] (a, b, thermal vx, vy, vz) indexed by k.
+ * start+count must not exceed parts->stride (else OPPB_ERR_CAPACITY). */
+int oppb_inject_f64(const oppb_tet_mesh* mesh, const oppb_inlet* inlet,
+                    const oppb_particles* parts, int32_t start, int32_t count,
+                    const double* rnd, int32_t rnd_stride,
+                    double ion_velocity, double qm, double dt, void* stream);
+
+/* ------------------------------------------------------------- compaction */
+
+/* Scratch bytes oppb_hole_fill needs for `size` particles of which `remove_count` were removed. */
+size_t oppb_hole_fill_workspace_bytes(int32_t size, int32_t remove_count);
+
+/* Hole fill after a move: the k-th removed slot (ascending) receives the k-th live
+ * particle counted from the back, while that particle lies behind the slot
+ * (opp_lib/src/core/opp_particle_organize_core.cpp:124-218; CUDA
+ * opp_lib/src/cuda/opp_particle_sorter.cu:264-363).  Holes are the set bits of
+ * remove_bits over [0,size); at most remove_count pairs move.  Every dat moves
+ * together.  The caller then sets size -= remove_count. */
+int oppb_hole_fill(int32_t size, int32_t remove_count, const uint32_t* remove_bits,
+                   int32_t stride, int32_t n_dats, const oppb_dat* dats,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* Scratch bytes oppb_sort_by_cell needs. */
+size_t oppb_sort_workspace_bytes(int32_t size, int32_t n_cells);
+
+/* Stable sort of particles [0,size) by cell (removed particles, p2c = REMOVED, last),
+ * then gather every dat into its `swap` buffer (opp_particle_sort_core,
+ * opp_lib/src/core/opp_particle_organize_core.cpp:98-121; CUDA particle_sort_device,
+ * opp_lib/src/cuda/opp_particle_sorter.cu:167-246).  dats[key_dat] must be the p2c dat.
+ * perm_out (device, may be NULL) receives the source index of every destination slot.
+ * Hand-written LSD radix sort (8-bit digits), no library sort. */
+int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride,
+                      int32_t n_dats, const oppb_dat* dats, int32_t key_dat,
+                      int32_t* perm_out, void* workspace, size_t workspace_bytes,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPPB_H */

@@ -1,0 +1,30 @@
+// Library identification and status strings of the C ABI.
+
+#include <atomic>
+
+#include "oppb_common.cuh"
+
+namespace oppb {
+namespace {
+std::atomic<uint64_t> g_launches{0};
+}
+void count_launches(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+}  // namespace oppb
+
+extern "C" uint64_t oppb_kernel_launches(void) { return oppb::g_launches.load(std::memory_order_relaxed); }
+
+extern "C" const char* oppb_version(void) { return "oppb 0.1 (sm_100a)"; }
+
+extern "C" const char* oppb_status_string(int status) {
+    switch (status) {
+        case OPPB_OK: return "ok";
+        case OPPB_ERR_ARG: return "invalid argument";
+        case OPPB_ERR_LAUNCH: return "CUDA launch error";
+        case OPPB_ERR_WORKSPACE: return "workspace too small";
+        case OPPB_ERR_HOP_LIMIT: return "particle exceeded the hop limit";
+        case OPPB_ERR_CELL_RANGE: return "cell index out of range";
+        case OPPB_ERR_CAPACITY: return "particle set capacity exceeded";
+        case OPPB_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}

@@ -1,0 +1,201 @@
+// Hole fill after a move (removal compaction).
+//
+// Holes are the set bits of the removal bitmap the move kernels write (one 32-bit
+// word per warp of particles).  The k-th hole in ascending order is paired with the
+// k-th live particle counted from the back; pairs are kept while the live particle
+// lies behind the hole and k < remove_count.  Both sequences are monotone, so the
+// kept pairs are a prefix: exactly the pairs of the reference's sequential loop
+// (opp_lib/src/core/opp_particle_organize_core.cpp:124-218).
+//   1. per-block hole counts over the bitmap,
+//   2. exclusive scan of the block counts,
+//   3. emit hole[k] and mover[k] for k < remove_count (ranks from the scan),
+//   4. copy every dat element mover[k] -> hole[k] for the kept pairs.
+
+#include "scan.cuh"
+
+namespace oppb {
+namespace {
+
+constexpr int kHfBlock = 256;
+constexpr int kHfWordsPerThread = 8;
+constexpr int kHfWords = kHfBlock * kHfWordsPerThread;  // words per block (65,536 particles)
+constexpr int kMaxDats = 16;
+
+struct DatList {
+    int32_t n;
+    int32_t total_cols;
+    void* data[kMaxDats];
+    int32_t dim[kMaxDats];
+    int32_t bytes[kMaxDats];
+};
+
+// Bitmap word w restricted to particles < size.
+__device__ __forceinline__ uint32_t hole_word(const uint32_t* bits, int64_t w, int32_t size) {
+    const int64_t first = w * 32;
+    if (first >= size) return 0u;
+    uint32_t v = bits[w];
+    const int64_t valid = size - first;
+    if (valid < 32) v &= (1u << valid) - 1u;
+    return v;
+}
+
+__global__ void __launch_bounds__(kHfBlock) hf_count_kernel(const uint32_t* __restrict__ bits, int32_t size,
+                                                            int64_t n_words, int* __restrict__ block_holes) {
+    __shared__ int sm[kHfBlock / 32 + 1];
+    const int64_t w0 = (int64_t)blockIdx.x * kHfWords;
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < kHfWordsPerThread; k++) {
+        const int64_t w = w0 + (int64_t)k * kHfBlock + threadIdx.x;
+        if (w < n_words) c += __popc(hole_word(bits, w, size));
+    }
+    int total;
+    block_exclusive_scan(c, sm, &total);
+    if (threadIdx.x == 0) block_holes[blockIdx.x] = total;
+}
+
+// block_base: exclusive hole prefix per block, block_base[n_blocks] = total holes H.
+__global__ void __launch_bounds__(kHfBlock) hf_emit_kernel(const uint32_t* __restrict__ bits, int32_t size,
+                                                           int64_t n_words, const int* __restrict__ block_base,
+                                                           int n_blocks, int32_t remove_count,
+                                                           int32_t* __restrict__ hole_list,
+                                                           int32_t* __restrict__ mover_list) {
+    __shared__ int sm[kHfBlock / 32 + 1];
+    // Thread t owns words [w0 + t*8, w0 + t*8 + 8) (blocked, so ranks follow index order).
+    const int64_t wt = (int64_t)blockIdx.x * kHfWords + (int64_t)threadIdx.x * kHfWordsPerThread;
+    uint32_t w[kHfWordsPerThread];
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < kHfWordsPerThread; k++) {
+        w[k] = (wt + k < n_words) ? hole_word(bits, wt + k, size) : 0u;
+        c += __popc(w[k]);
+    }
+    int total;
+    int holes_before = block_exclusive_scan(c, sm, &total) + block_base[blockIdx.x];
+    const int64_t H = block_base[n_blocks];
+    const int64_t live_total = (int64_t)size - H;
+#pragma unroll 1
+    for (int k = 0; k < kHfWordsPerThread; k++) {
+        const int64_t word = wt + k;
+        const int64_t first = word * 32;
+        if (first >= size) break;
+        const int n_valid = (size - first) < 32 ? (int)(size - first) : 32;
+        uint32_t hw = w[k];
+        // Holes: ascending rank holes_before, holes_before+1, ...
+        if (holes_before < remove_count) {
+            uint32_t m = hw;
+            int h = holes_before;
+            while (m && h < remove_count) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                hole_list[h++] = (int32_t)(first + b);
+            }
+        }
+        // Live particles: back rank = live_total - 1 - (index - holes before index).
+        // The largest live index of this word has the smallest back rank.
+        const int64_t live_first_rank = first - holes_before;  // front rank of first live in word
+        const int n_live = n_valid - __popc(hw);
+        if (n_live > 0) {
+            const int64_t min_back = live_total - 1 - (live_first_rank + n_live - 1);
+            if (min_back < remove_count) {
+                int64_t front = live_first_rank;
+                for (int b = 0; b < n_valid; b++) {
+                    if (hw & (1u << b)) continue;
+                    const int64_t back = live_total - 1 - front;
+                    if (back < remove_count) mover_list[back] = (int32_t)(first + b);
+                    front++;
+                }
+            }
+        }
+        holes_before += __popc(hw);
+    }
+}
+
+// One thread per (pair, column): copies the element of column col of the mover to the hole.
+__global__ void hf_copy_kernel(int32_t n_pairs_max, const int32_t* __restrict__ hole_list,
+                               const int32_t* __restrict__ mover_list, const int* __restrict__ totals,
+                               int32_t size, int32_t stride, DatList dats) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t k = t / dats.total_cols;
+    const int col = (int)(t - k * dats.total_cols);
+    if (k >= n_pairs_max) return;
+    const int64_t H = totals[0];
+    if (k >= H || k >= (int64_t)size - H) return;
+    const int32_t to = hole_list[k], from = mover_list[k];
+    if (from <= to) return;
+    int d = 0, c = col;
+    while (d < dats.n && c >= dats.dim[d]) {
+        c -= dats.dim[d];
+        d++;
+    }
+    if (d >= dats.n) return;
+    const int64_t off = (int64_t)c * stride;
+    if (dats.bytes[d] == 8) {
+        int64_t* a = reinterpret_cast<int64_t*>(dats.data[d]) + off;
+        a[to] = a[from];
+    } else {
+        int32_t* a = reinterpret_cast<int32_t*>(dats.data[d]) + off;
+        a[to] = a[from];
+    }
+}
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace oppb
+
+extern "C" size_t oppb_hole_fill_workspace_bytes(int32_t size, int32_t remove_count) {
+    using namespace oppb;
+    if (size < 0 || remove_count < 0) return 0;
+    const int64_t n_words = ceil_div(size, 32);
+    const int n_blocks = ceil_div(n_words, kHfWords);
+    return align256(sizeof(int) * (size_t)(n_blocks + 1)) + align256(sizeof(int) * scan_scratch_ints(n_blocks)) +
+           2 * align256(sizeof(int32_t) * (size_t)(remove_count > 0 ? remove_count : 1));
+}
+
+extern "C" int oppb_hole_fill(int32_t size, int32_t remove_count, const uint32_t* remove_bits, int32_t stride,
+                              int32_t n_dats, const oppb_dat* dats, void* workspace, size_t workspace_bytes,
+                              void* stream) {
+    using namespace oppb;
+    if (size < 0 || remove_count < 0 || stride < size || n_dats < 0 || n_dats > kMaxDats) return OPPB_ERR_ARG;
+    if (remove_count == 0 || size == 0) return OPPB_OK;
+    if (!remove_bits || !dats || !workspace) return OPPB_ERR_ARG;
+    if (workspace_bytes < oppb_hole_fill_workspace_bytes(size, remove_count)) return OPPB_ERR_WORKSPACE;
+    DatList dl{};
+    dl.n = n_dats;
+    dl.total_cols = 0;
+    for (int d = 0; d < n_dats; d++) {
+        if (!dats[d].data || dats[d].dim <= 0 || (dats[d].elem_bytes != 4 && dats[d].elem_bytes != 8))
+            return OPPB_ERR_ARG;
+        dl.data[d] = dats[d].data;
+        dl.dim[d] = dats[d].dim;
+        dl.bytes[d] = dats[d].elem_bytes;
+        dl.total_cols += dats[d].dim;
+    }
+    cudaStream_t s = as_stream(stream);
+    const int64_t n_words = ceil_div(size, 32);
+    const int n_blocks = ceil_div(n_words, kHfWords);
+    char* ws = static_cast<char*>(workspace);
+    int* block_base = reinterpret_cast<int*>(ws);
+    ws += align256(sizeof(int) * (size_t)(n_blocks + 1));
+    int* scan_tmp = reinterpret_cast<int*>(ws);
+    ws += align256(sizeof(int) * scan_scratch_ints(n_blocks));
+    int32_t* hole_list = reinterpret_cast<int32_t*>(ws);
+    ws += align256(sizeof(int32_t) * (size_t)remove_count);
+    int32_t* mover_list = reinterpret_cast<int32_t*>(ws);
+
+    hf_count_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base);
+    // block_base[0..n_blocks) exclusive, block_base[n_blocks] = total holes.
+    scan_single_block_kernel<<<1, kScanBlock, 0, s>>>(block_base, n_blocks);
+    (void)scan_tmp;
+    hf_emit_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base, n_blocks, remove_count,
+                                                 hole_list, mover_list);
+    count_launches(3);
+    if (dl.total_cols > 0) {
+        const int64_t threads = (int64_t)remove_count * dl.total_cols;
+        hf_copy_kernel<<<ceil_div(threads, 256), 256, 0, s>>>(remove_count, hole_list, mover_list,
+                                                             block_base + n_blocks, size, stride, dl);
+        count_launches(1);
+    }
+    return launch_status();
+}

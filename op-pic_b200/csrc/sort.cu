@@ -1,0 +1,252 @@
+// Stable cell sort of particles: hand-written LSD radix sort (8-bit digits) of the
+// cell keys with the particle index as value, then one gather of every dat.
+//
+// Key of particle i: p2c[i], or n_cells for a removed particle (so removed particles
+// sort last, as MAX_CELL_INDEX does in sort_iota_by_key, opp_lib/include/opp_util.h:211-221).
+// Each pass: (1) per-tile digit histogram, (2) exclusive scan of the digit-major
+// histogram table, (3) per tile a stable rank of every key among equal digits
+// (warp match + per-warp digit counters, warps in index order), staging in shared
+// memory so each digit run is written out contiguously.  The last pass writes the
+// sorted keys straight into the p2c swap buffer and the source indices (the
+// permutation) for the gather.
+
+#include "scan.cuh"
+
+namespace oppb {
+namespace {
+
+constexpr int kSortBlock = 256;
+constexpr int kSortWarps = kSortBlock / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortBlock * kSortItems;  // 4096 keys
+constexpr int kRadix = 256;
+constexpr int kMaxDats = 16;
+
+__device__ __forceinline__ uint32_t cell_key(int32_t c, int32_t n_cells) {
+    return ((uint32_t)c < (uint32_t)n_cells) ? (uint32_t)c : (uint32_t)n_cells;
+}
+
+// Pass input: either raw p2c (first pass) or keys from the previous pass.
+struct PassIn {
+    const int32_t* p2c;     // first pass only
+    const uint32_t* keys;   // later passes
+    const int32_t* vals;    // later passes (first pass: value = index)
+};
+
+__device__ __forceinline__ uint32_t load_key(const PassIn& in, int64_t j, int32_t n_cells) {
+    return in.p2c ? cell_key(in.p2c[j], n_cells) : in.keys[j];
+}
+
+__global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(PassIn in, int32_t size, int32_t n_cells,
+                                                                int shift, int n_tiles, int* __restrict__ hist) {
+    __shared__ int h[kRadix];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+    for (int k = 0; k < kSortItems; k++) {
+        const int64_t j = base + (int64_t)k * kSortBlock + threadIdx.x;
+        if (j < size) atomicAdd(&h[(load_key(in, j, n_cells) >> shift) & (kRadix - 1)], 1);
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * n_tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// offsets: exclusive scan of hist (digit-major), i.e. the first output slot of
+// (digit, tile).  keys_out/vals_out receive the pass result.  On the last pass
+// keys_out is the p2c swap buffer (removed key mapped back to the removed cell).
+__global__ void __launch_bounds__(kSortBlock) radix_scatter_kernel(PassIn in, int32_t size, int32_t n_cells,
+                                                                   int shift, int n_tiles,
+                                                                   const int* __restrict__ offsets,
+                                                                   uint32_t* __restrict__ keys_out,
+                                                                   int32_t* __restrict__ vals_out, int last) {
+    __shared__ int cnt[kSortWarps][kRadix];
+    __shared__ int tile_base[kRadix];
+    __shared__ int scan_sm[kSortBlock / 32 + 1];
+    __shared__ uint32_t sk[kSortTile];
+    __shared__ int32_t sv[kSortTile];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < kSortWarps * kRadix; d += kSortBlock) (&cnt[0][0])[d] = 0;
+    __syncthreads();
+
+    const int64_t base = (int64_t)blockIdx.x * kSortTile;
+    const int tile_n = ((int64_t)size - base) < kSortTile ? (int)((int64_t)size - base) : kSortTile;
+    uint32_t key[kSortItems];
+    int32_t val[kSortItems];
+    int off[kSortItems];
+    const unsigned lt = lanemask_lt();
+    // Warp w ranks tile items [w*512, w*512+512) in 16 rounds of 32, in index order.
+#pragma unroll
+    for (int r = 0; r < kSortItems; r++) {
+        const int t = warp * (kSortItems * 32) + r * 32 + lane;
+        const int64_t j = base + t;
+        const bool ok = t < tile_n;
+        key[r] = ok ? load_key(in, j, n_cells) : 0xffffffffu;
+        val[r] = ok ? (in.p2c ? (int32_t)j : in.vals[j]) : 0;
+        const int d = ok ? (int)((key[r] >> shift) & (kRadix - 1)) : kRadix;
+        const unsigned peers = __match_any_sync(kFullMask, d);
+        const int leader = __ffs(peers) - 1;
+        int b = 0;
+        if (lane == leader && ok) b = cnt[warp][d];
+        b = __shfl_sync(kFullMask, b, leader);
+        off[r] = b + __popc(peers & lt);
+        __syncwarp();
+        if (lane == leader && ok) cnt[warp][d] = b + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // Per digit: exclusive prefix over warps, then the tile-local digit base.
+    {
+        const int d = threadIdx.x;
+        int run = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; w++) {
+            const int c = cnt[w][d];
+            cnt[w][d] = run;
+            run += c;
+        }
+        int total;
+        tile_base[d] = block_exclusive_scan(run, scan_sm, &total);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortItems; r++) {
+        const int t = warp * (kSortItems * 32) + r * 32 + lane;
+        if (t < tile_n) {
+            const int d = (int)((key[r] >> shift) & (kRadix - 1));
+            const int pos = tile_base[d] + cnt[warp][d] + off[r];
+            sk[pos] = key[r];
+            sv[pos] = val[r];
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < tile_n; t += kSortBlock) {
+        const uint32_t k = sk[t];
+        const int d = (int)((k >> shift) & (kRadix - 1));
+        const int64_t dest = (int64_t)offsets[(int64_t)d * n_tiles + blockIdx.x] + (t - tile_base[d]);
+        if (last)
+            reinterpret_cast<int32_t*>(keys_out)[dest] = (k >= (uint32_t)n_cells) ? kRemoved : (int32_t)k;
+        else
+            keys_out[dest] = k;
+        vals_out[dest] = sv[t];
+    }
+}
+
+struct GatherList {
+    int32_t n;
+    const void* src[kMaxDats];
+    void* dst[kMaxDats];
+    int32_t dim[kMaxDats];
+    int32_t bytes[kMaxDats];
+};
+
+// dst[c][j] = src[c][perm[j]] for every dat other than the key dat.
+__global__ void __launch_bounds__(256) gather_kernel(int32_t size, int32_t stride, const int32_t* __restrict__ perm,
+                                                     GatherList g) {
+    const int64_t j = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (j >= size) return;
+    const int64_t from = perm[j];
+    for (int d = 0; d < g.n; d++) {
+        if (g.bytes[d] == 8) {
+            const int64_t* s = reinterpret_cast<const int64_t*>(g.src[d]);
+            int64_t* t = reinterpret_cast<int64_t*>(g.dst[d]);
+            for (int c = 0; c < g.dim[d]; c++) __stcs(t + (int64_t)c * stride + j, __ldg(s + (int64_t)c * stride + from));
+        } else {
+            const int32_t* s = reinterpret_cast<const int32_t*>(g.src[d]);
+            int32_t* t = reinterpret_cast<int32_t*>(g.dst[d]);
+            for (int c = 0; c < g.dim[d]; c++) __stcs(t + (int64_t)c * stride + j, __ldg(s + (int64_t)c * stride + from));
+        }
+    }
+}
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+int key_bits(int32_t n_cells) {
+    int b = 0;
+    while (b < 31 && ((uint32_t)n_cells >> b) != 0) b++;
+    return b > 0 ? b : 1;
+}
+
+struct SortLayout {
+    size_t keys_a, vals_a, keys_b, vals_b, perm, hist, scan, total;
+};
+
+SortLayout sort_layout(int32_t size) {
+    SortLayout L{};
+    const size_t n = (size_t)(size > 0 ? size : 1);
+    const int n_tiles = ceil_div(size > 0 ? size : 1, kSortTile);
+    const size_t hist_n = (size_t)kRadix * n_tiles;
+    size_t o = 0;
+    L.keys_a = o; o += align256(4 * n);
+    L.vals_a = o; o += align256(4 * n);
+    L.keys_b = o; o += align256(4 * n);
+    L.vals_b = o; o += align256(4 * n);
+    L.perm = o;   o += align256(4 * n);
+    L.hist = o;   o += align256(4 * hist_n);
+    L.scan = o;   o += align256(4 * scan_scratch_ints((int64_t)hist_n));
+    L.total = o;
+    return L;
+}
+
+}  // namespace
+}  // namespace oppb
+
+extern "C" size_t oppb_sort_workspace_bytes(int32_t size, int32_t n_cells) {
+    (void)n_cells;
+    if (size < 0) return 0;
+    return oppb::sort_layout(size).total;
+}
+
+extern "C" int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride, int32_t n_dats, const oppb_dat* dats,
+                                 int32_t key_dat, int32_t* perm_out, void* workspace, size_t workspace_bytes,
+                                 void* stream) {
+    using namespace oppb;
+    if (size < 0 || n_cells <= 0 || n_cells >= kRemoved || stride < size || n_dats <= 0 || n_dats > kMaxDats ||
+        !dats || key_dat < 0 || key_dat >= n_dats)
+        return OPPB_ERR_ARG;
+    const oppb_dat& kd = dats[key_dat];
+    if (!kd.data || !kd.swap || kd.dim != 1 || kd.elem_bytes != 4) return OPPB_ERR_ARG;
+    GatherList g{};
+    for (int d = 0; d < n_dats; d++) {
+        if (!dats[d].data || !dats[d].swap || dats[d].dim <= 0 || (dats[d].elem_bytes != 4 && dats[d].elem_bytes != 8))
+            return OPPB_ERR_ARG;
+        if (d == key_dat) continue;
+        g.src[g.n] = dats[d].data;
+        g.dst[g.n] = dats[d].swap;
+        g.dim[g.n] = dats[d].dim;
+        g.bytes[g.n] = dats[d].elem_bytes;
+        g.n++;
+    }
+    if (size == 0) return OPPB_OK;
+    if (!workspace || workspace_bytes < oppb_sort_workspace_bytes(size, n_cells)) return OPPB_ERR_WORKSPACE;
+    cudaStream_t s = as_stream(stream);
+    const SortLayout L = sort_layout(size);
+    char* ws = static_cast<char*>(workspace);
+    uint32_t* keys[2] = {reinterpret_cast<uint32_t*>(ws + L.keys_a), reinterpret_cast<uint32_t*>(ws + L.keys_b)};
+    int32_t* vals[2] = {reinterpret_cast<int32_t*>(ws + L.vals_a), reinterpret_cast<int32_t*>(ws + L.vals_b)};
+    int32_t* perm = perm_out ? perm_out : reinterpret_cast<int32_t*>(ws + L.perm);
+    int* hist = reinterpret_cast<int*>(ws + L.hist);
+    int* scan_tmp = reinterpret_cast<int*>(ws + L.scan);
+
+    const int n_tiles = ceil_div(size, kSortTile);
+    const int passes = (key_bits(n_cells) + 7) / 8;
+    PassIn in{static_cast<const int32_t*>(kd.data), nullptr, nullptr};
+    for (int p = 0; p < passes; p++) {
+        const int shift = 8 * p;
+        const bool last = (p == passes - 1);
+        uint32_t* ko = last ? static_cast<uint32_t*>(kd.swap) : keys[p & 1];
+        int32_t* vo = last ? perm : vals[p & 1];
+        radix_hist_kernel<<<n_tiles, kSortBlock, 0, s>>>(in, size, n_cells, shift, n_tiles, hist);
+        device_exclusive_scan(hist, hist, (int64_t)kRadix * n_tiles, scan_tmp, s);
+        radix_scatter_kernel<<<n_tiles, kSortBlock, 0, s>>>(in, size, n_cells, shift, n_tiles, hist, ko, vo,
+                                                            last ? 1 : 0);
+        count_launches(2);
+        in = PassIn{nullptr, keys[p & 1], vals[p & 1]};
+    }
+    if (g.n > 0) {
+        gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(size, stride, perm, g);
+        count_launches(1);
+    }
+    return launch_status();
+}

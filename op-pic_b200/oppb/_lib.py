@@ -1,0 +1,112 @@
+"""ctypes binding of the C ABI in include/oppb.h and include/oppb_fempic.h.
+
+The shared library is built in-tree (op-pic_b200/lib/liboppb.so).  Loading fails loudly
+when it is missing: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent.parent / "lib" / "liboppb.so"
+
+OPPB_OK = 0
+OPPB_ERR_ARG = 1
+OPPB_ERR_LAUNCH = 2
+OPPB_ERR_WORKSPACE = 3
+OPPB_ERR_HOP_LIMIT = 4
+OPPB_ERR_CELL_RANGE = 5
+OPPB_ERR_CAPACITY = 6
+OPPB_ERR_NO_DEVICE = 7
+REMOVED_CELL = 2147483647
+
+c_i32, c_u32, c_i64, c_u64 = C.c_int32, C.c_uint32, C.c_int64, C.c_uint64
+c_dp, c_fp, c_ip, c_vp = C.POINTER(C.c_double), C.POINTER(C.c_float), C.POINTER(C.c_int32), C.c_void_p
+
+
+class TetMesh(C.Structure):
+    _fields_ = [("n_cells", c_i32), ("n_nodes", c_i32), ("det", c_vp), ("coef", c_vp), ("conn", c_vp),
+                ("ef", c_vp), ("geo32", c_vp), ("org32", c_vp)]
+
+
+class Particles(C.Structure):
+    _fields_ = [("size", c_i32), ("stride", c_i32), ("pos", c_vp), ("vel", c_vp), ("lc", c_vp), ("p2c", c_vp),
+                ("remove_bits", c_vp)]
+
+
+class MoveStatus(C.Structure):
+    _fields_ = [("remove_count", c_i32), ("error", c_i32), ("error_index", c_i32), ("max_visits", c_i32),
+                ("total_visits", c_u64), ("recheck_count", c_i32), ("reserved", c_i32)]
+
+
+class Dat(C.Structure):
+    _fields_ = [("data", c_vp), ("swap", c_vp), ("dim", c_i32), ("elem_bytes", c_i32)]
+
+
+class Inlet(C.Structure):
+    _fields_ = [("n_faces", c_i32), ("dist", c_vp), ("if2c", c_vp), ("geom", c_vp)]
+
+
+class FemPICMesh(C.Structure):
+    _fields_ = [("n_nodes", c_i32), ("n_cells", c_i32), ("n_ifaces", c_i32),
+                ("n_pos", c_dp), ("n_vol", c_dp), ("n_type", c_ip), ("n_bnd_pot", c_dp),
+                ("c2n", c_ip), ("c2c", c_ip), ("c_det", c_dp), ("c_vol", c_dp), ("c_sd", c_dp),
+                ("c_ef", c_dp), ("c_centroid", c_dp), ("if2c", c_ip), ("if2n", c_ip),
+                ("if_u", c_dp), ("if_v", c_dp), ("if_norm", c_dp), ("if_area", c_dp), ("if_n_pos", c_dp)]
+
+
+P = C.POINTER
+_SIGS = {
+    "oppb_version": (C.c_char_p, []),
+    "oppb_status_string": (C.c_char_p, [C.c_int]),
+    "oppb_kernel_launches": (C.c_uint64, []),
+    "oppb_tet_mesh_bytes": (None, [c_i32, P(C.c_size_t)]),
+    "oppb_tet_mesh_pack": (C.c_int, [P(TetMesh), c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
+    "oppb_tet_mesh_set_ef": (C.c_int, [P(TetMesh), c_i32, c_vp, c_vp]),
+    "oppb_move_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_i32, c_vp]),
+    "oppb_move_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, c_vp]),
+    "oppb_move_deposit_mixed": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, C.c_double, c_vp]),
+    "oppb_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp]),
+    "oppb_push_f64": (C.c_int, [P(TetMesh), P(Particles), C.c_double, C.c_double, c_vp]),
+    "oppb_push_mixed": (C.c_int, [P(TetMesh), P(Particles), C.c_double, C.c_double, c_vp]),
+    "oppb_inject_f64": (C.c_int, [P(TetMesh), P(Inlet), P(Particles), c_i32, c_i32, c_vp, c_i32,
+                                  C.c_double, C.c_double, C.c_double, c_vp]),
+    "oppb_hole_fill_workspace_bytes": (C.c_size_t, [c_i32, c_i32]),
+    "oppb_hole_fill": (C.c_int, [c_i32, c_i32, c_vp, c_i32, c_i32, P(Dat), c_vp, C.c_size_t, c_vp]),
+    "oppb_sort_workspace_bytes": (C.c_size_t, [c_i32, c_i32]),
+    "oppb_sort_by_cell": (C.c_int, [c_i32, c_i32, c_i32, c_i32, P(Dat), c_i32, c_vp, c_vp, C.c_size_t, c_vp]),
+    "oppb_fempic_box_mesh": (C.c_int, [c_i32, c_i32, c_i32, C.c_double, C.c_double, C.c_double, P(FemPICMesh)]),
+    "oppb_fempic_solve_field": (C.c_int, [P(FemPICMesh), C.c_double, C.c_double, C.c_double, c_i32, c_dp,
+                                          P(c_i32), P(C.c_double)]),
+    "oppb_fempic_inject_distribution": (C.c_int, [P(FemPICMesh), c_i32, c_ip]),
+    "oppb_fempic_mesh_free": (None, [P(FemPICMesh)]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load liboppb.so (built by op-pic_b200/build.py); raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: run op-pic_b200/build.py (no fallback implementation)")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class OppbError(RuntimeError):
+    def __init__(self, fn: str, status: int):
+        msg = load().oppb_status_string(status).decode()
+        super().__init__(f"{fn} failed: status {status} ({msg})")
+        self.status = status
+
+
+def check(fn: str, status: int) -> None:
+    if status != OPPB_OK:
+        raise OppbError(fn, status)

@@ -1,0 +1,363 @@
+"""FemPIC particle step on one B200 through the C ABI (include/oppb.h).
+
+Host side of the library in Python for tests and the benchmark: it owns device buffers
+(torch tensors used only as device memory and streams) and calls the CUDA kernels of
+liboppb.so.  The layout follows the reference's CUDA backend: particle dats SoA
+[dim][capacity] (opp_lib/src/cuda/opp_cuda_utils.cu:128-143), mesh dats uploaded SoA
+and packed into the kernels' cell records once.
+
+The step follows the generated main loop (apps_codegen/app_fempic_cg/fempic_opp.cpp:160-215):
+  inject -> reset node charge -> push -> move (+ fused deposit) -> hole fill / cell sort.
+The deposit of the final cell is fused into the move kernel; contributions are the same
+as the separate deposit loop over the compacted set.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+# --------------------------------------------------------------------------- host mesh
+
+class HostMesh:
+    """Box tetrahedral mesh built by oppb_fempic_box_mesh (host AoS arrays, numpy views
+    onto library-owned memory, copied so the Python object owns them)."""
+
+    def __init__(self, nx: int, ny: int, nz: int, lx: float, ly: float, lz: float,
+                 phi_inlet: float = 1.0, phi_fixed: float = 0.0, solve_field: bool = True):
+        lib = L.load()
+        m = L.FemPICMesh()
+        rc = lib.oppb_fempic_box_mesh(nx, ny, nz, lx, ly, lz, C.byref(m))
+        if rc != 0:
+            raise RuntimeError(f"oppb_fempic_box_mesh failed ({rc})")
+        try:
+            self.cg_iters = 0
+            self.cg_resid = 0.0
+            if solve_field:
+                it, res = C.c_int32(0), C.c_double(0)
+                pot = np.zeros(m.n_nodes)
+                rc = lib.oppb_fempic_solve_field(C.byref(m), phi_inlet, phi_fixed, 1e-12, 100000,
+                                                 pot.ctypes.data_as(L.c_dp), C.byref(it), C.byref(res))
+                if rc != 0:
+                    raise RuntimeError(f"field solve did not converge (resid {res.value})")
+                self.cg_iters, self.cg_resid, self.n_pot = it.value, res.value, pot
+            self.n_nodes, self.n_cells, self.n_ifaces = m.n_nodes, m.n_cells, m.n_ifaces
+            nn, nc, nf = m.n_nodes, m.n_cells, m.n_ifaces
+
+            def take(ptr, shape, dtype):
+                n = int(np.prod(shape))
+                return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True).reshape(shape)
+
+            self.n_pos = take(m.n_pos, (nn, 3), np.float64)
+            self.n_vol = take(m.n_vol, (nn,), np.float64)
+            self.n_type = take(m.n_type, (nn,), np.int32)
+            self.c2n = take(m.c2n, (nc, 4), np.int32)
+            self.c2c = take(m.c2c, (nc, 4), np.int32)
+            self.c_det = take(m.c_det, (nc, 16), np.float64)
+            self.c_vol = take(m.c_vol, (nc,), np.float64)
+            self.c_sd = take(m.c_sd, (nc, 4, 3), np.float64)
+            self.c_ef = take(m.c_ef, (nc, 3), np.float64)
+            self.c_centroid = take(m.c_centroid, (nc, 3), np.float64)
+            self.if2c = take(m.if2c, (nf,), np.int32)
+            self.if2n = take(m.if2n, (nf, 3), np.int32)
+            self.if_u = take(m.if_u, (nf, 3), np.float64)
+            self.if_v = take(m.if_v, (nf, 3), np.float64)
+            self.if_norm = take(m.if_norm, (nf, 3), np.float64)
+            self.if_area = take(m.if_area, (nf,), np.float64)
+            self.if_n_pos = take(m.if_n_pos, (nf, 9), np.float64)
+        finally:
+            lib.oppb_fempic_mesh_free(C.byref(m))
+        self.dims = (nx, ny, nz, lx, ly, lz)
+
+    def inject_distribution(self, total: int) -> np.ndarray:
+        """Cumulative per-face counts (oppb_fempic_inject_distribution)."""
+        out = np.zeros(self.n_ifaces, np.int32)
+        fm = L.FemPICMesh()
+        fm.n_ifaces = self.n_ifaces
+        fm.if_area = self.if_area.ctypes.data_as(L.c_dp)
+        rc = L.load().oppb_fempic_inject_distribution(C.byref(fm), total, out.ctypes.data_as(L.c_ip))
+        if rc != 0:
+            raise RuntimeError("oppb_fempic_inject_distribution failed")
+        return out
+
+
+def injection_randoms(seed: int, step: int, count: int, sigma: float) -> np.ndarray:
+    """Seeded per-step injection table, AoS [count][5]: a, b ~ U[0,1) (position in the inlet
+    triangle, folded as in inject_ions_kernel) and the thermal velocity ~ N(0, sigma^2)^3."""
+    rng = np.random.default_rng([seed, step])
+    out = np.empty((count, 5))
+    out[:, 0:2] = rng.random((count, 2))
+    out[:, 2:5] = sigma * rng.standard_normal((count, 3))
+    return out
+
+
+# ------------------------------------------------------------------------- device side
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream_ptr(stream: torch.cuda.Stream | None) -> int | None:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream or None
+
+
+class DeviceMesh:
+    """Cell dats uploaded in the reference's device layout (SoA) and packed into the
+    kernel records by oppb_tet_mesh_pack.  Also holds the inlet."""
+
+    def __init__(self, hm: HostMesh, device: torch.device, mixed: bool = True, dist: np.ndarray | None = None):
+        self.device = device
+        nc, nn = hm.n_cells, hm.n_nodes
+        t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=dt)  # noqa: E731
+        soa_det = t(hm.c_det.T, torch.float64)
+        soa_vol = t(hm.c_vol, torch.float64)
+        soa_c2c = t(hm.c2c.T, torch.int32)
+        soa_c2n = t(hm.c2n.T, torch.int32)
+        soa_ef = t(hm.c_ef.T, torch.float64)
+        soa_npos = t(hm.n_pos.T, torch.float64)
+        self.det = torch.empty(nc * 16, dtype=torch.float64, device=device)
+        self.coef = torch.empty(nc, dtype=torch.float64, device=device)
+        self.conn = torch.empty(nc * 8, dtype=torch.int32, device=device)
+        self.ef = torch.empty(nc * 4, dtype=torch.float64, device=device)
+        self.geo32 = torch.empty(nc * 16, dtype=torch.float32, device=device) if mixed else None
+        self.org32 = torch.empty(nc * 4, dtype=torch.float32, device=device) if mixed else None
+        self.s = L.TetMesh(nc, nn, _ptr(self.det), _ptr(self.coef), _ptr(self.conn), _ptr(self.ef),
+                           _ptr(self.geo32), _ptr(self.org32))
+        invalid = torch.zeros(1, dtype=torch.int32, device=device)
+        L.check("oppb_tet_mesh_pack", L.load().oppb_tet_mesh_pack(
+            C.byref(self.s), nc, _ptr(soa_det), _ptr(soa_vol), _ptr(soa_c2c), _ptr(soa_c2n), _ptr(soa_ef),
+            _ptr(soa_npos), nn, _ptr(invalid), _stream_ptr(None)))
+        if int(invalid.item()) != 0:
+            raise ValueError(f"mesh maps hold {int(invalid.item())} out-of-range entries")
+        self.n_cells, self.n_nodes = nc, nn
+        # Inlet: dist, if2c, geom[12] = u, v, normal, node0.
+        geom = np.concatenate([hm.if_u, hm.if_v, hm.if_norm, hm.if_n_pos[:, 0:3]], axis=1)
+        self.if_geom = t(geom, torch.float64)
+        self.if2c = t(hm.if2c, torch.int32)
+        self.dist = t(dist if dist is not None else np.zeros(hm.n_ifaces, np.int32), torch.int32)
+        self.inlet = L.Inlet(hm.n_ifaces, _ptr(self.dist), _ptr(self.if2c), _ptr(self.if_geom))
+
+    def set_distribution(self, dist: np.ndarray) -> None:
+        self.dist.copy_(torch.from_numpy(np.ascontiguousarray(dist, np.int32)))
+
+
+class ParticleSet:
+    """Particle dats p_position, p_velocity, p_lc, p2c in SoA [dim][capacity] with swap
+    buffers for the sort, the removal bitmap and the move status word."""
+
+    DATS = (("pos", 3, torch.float64), ("vel", 3, torch.float64), ("lc", 4, torch.float64), ("p2c", 1, torch.int32))
+
+    def __init__(self, device: torch.device, capacity: int = 0, alloc_mult: float = 2.0):
+        self.device = device
+        self.size = 0
+        self.capacity = 0
+        self.alloc_mult = alloc_mult
+        self.status = torch.zeros(32 // 4, dtype=torch.int32, device=device)
+        self._alloc(capacity)
+
+    def _alloc(self, cap: int) -> None:
+        old = {n: getattr(self, n, None) for n, _, _ in self.DATS}
+        for name, dim, dt in self.DATS:
+            fill = L.REMOVED_CELL if name == "p2c" else 0
+            buf = torch.full((dim, max(cap, 1)), fill, dtype=dt, device=self.device)
+            if old[name] is not None and self.size > 0:
+                buf[:, : self.size].copy_(old[name][:, : self.size])
+            setattr(self, name, buf)
+            setattr(self, name + "_swap", torch.empty_like(buf))
+        self.bits = torch.zeros((max(cap, 1) + 31) // 32, dtype=torch.int32, device=self.device)
+        self.capacity = cap
+
+    def increase(self, count: int) -> None:
+        """opp_increase_particle_count_core semantics (capacity = size + count*alloc_mult),
+        growing on the device (no host round trip)."""
+        new_size = self.size + count
+        if new_size > self.capacity:
+            self._alloc(int(self.size + count * self.alloc_mult))
+
+    def view(self) -> L.Particles:
+        return L.Particles(self.size, self.capacity, _ptr(self.pos), _ptr(self.vel), _ptr(self.lc), _ptr(self.p2c),
+                           _ptr(self.bits))
+
+    def dat_list(self):
+        arr = (L.Dat * len(self.DATS))()
+        for k, (name, dim, dt) in enumerate(self.DATS):
+            arr[k] = L.Dat(_ptr(getattr(self, name)), _ptr(getattr(self, name + "_swap")), dim,
+                           8 if dt == torch.float64 else 4)
+        return arr
+
+    def swap_after_sort(self) -> None:
+        for name, _, _ in self.DATS:
+            a, b = getattr(self, name), getattr(self, name + "_swap")
+            setattr(self, name, b)
+            setattr(self, name + "_swap", a)
+
+    def host_aos(self) -> dict:
+        """Copy [0,size) to host AoS numpy (the seq backend's layout)."""
+        n = self.size
+        return {name: getattr(self, name)[:, :n].T.contiguous().cpu().numpy() if dim > 1
+                else getattr(self, name)[0, :n].cpu().numpy() for name, dim, _ in self.DATS}
+
+    def status_host(self) -> L.MoveStatus:
+        raw = self.status.cpu().numpy().tobytes()
+        return L.MoveStatus.from_buffer_copy(raw)
+
+
+@dataclass
+class StepTimes:
+    move_ms: float = 0.0
+    compact_ms: float = 0.0
+    push_ms: float = 0.0
+    inject_ms: float = 0.0
+
+
+class FemPIC:
+    """The FemPIC particle step on one GPU.
+
+    precision: 'f64' (bit-identical to the seq backend) or 'mixed' (FP32 push and tests
+    with FP64 re-check; bit-identical cell decisions for the same positions).
+    fill: 'HoleFill_All' | 'Sort_All' | 'Sort_Periodic' as the reference's opp_fill.
+    """
+
+    def __init__(self, hm: HostMesh, device: torch.device | str = "cuda", inject_per_step: int = 2000,
+                 ion_velocity: float = 1.0, qm: float = 1.0, dt: float = 0.01, precision: str = "f64",
+                 fill: str = "HoleFill_All", fill_period: int = 10, alloc_mult: float = 2.0,
+                 capacity: int = 0, max_hops: int = 4096, band: float = 1e-5, fused_deposit: bool = True):
+        if not torch.cuda.is_available():
+            raise RuntimeError("FemPIC needs a CUDA device (there is no CPU fallback)")
+        self.device = torch.device(device)
+        self.hm = hm
+        self.inject_per_step = inject_per_step
+        self.dist_host = hm.inject_distribution(inject_per_step)
+        self.mesh = DeviceMesh(hm, self.device, mixed=(precision == "mixed"), dist=self.dist_host)
+        self.parts = ParticleSet(self.device, capacity, alloc_mult)
+        self.ion_velocity, self.qm, self.dt = ion_velocity, qm, dt
+        if precision not in ("f64", "mixed"):
+            raise ValueError(precision)
+        self.precision = precision
+        self.fill, self.fill_period = fill, fill_period
+        self.max_hops, self.band = max_hops, band
+        self.fused_deposit = fused_deposit
+        self.node_charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=self.device)
+        self.iter = 0
+        self._ws = torch.empty(0, dtype=torch.uint8, device=self.device)
+        self.lib = L.load()
+        self.last = {}
+
+    # workspace shared by hole fill and sort (grown on demand)
+    def _workspace(self, nbytes: int) -> torch.Tensor:
+        if self._ws.numel() < nbytes:
+            self._ws = torch.empty(int(nbytes * 1.25) + 256, dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def inject(self, rnd_soa: torch.Tensor, stream=None) -> None:
+        """rnd_soa: device float64 [5][count] (a, b, thermal vx, vy, vz)."""
+        count = rnd_soa.shape[1]
+        p = self.parts
+        p.increase(count)
+        start = p.size
+        p.size += count
+        v = p.view()
+        L.check("oppb_inject_f64", self.lib.oppb_inject_f64(
+            C.byref(self.mesh.s), C.byref(self.mesh.inlet), C.byref(v), start, count, _ptr(rnd_soa),
+            rnd_soa.stride(0), self.ion_velocity, self.qm, self.dt, _stream_ptr(stream)))
+
+    def push(self, stream=None) -> None:
+        v = self.parts.view()
+        fn = self.lib.oppb_push_mixed if self.precision == "mixed" else self.lib.oppb_push_f64
+        L.check("oppb_push", fn(C.byref(self.mesh.s), C.byref(v), self.qm, self.dt, _stream_ptr(stream)))
+
+    def move(self, stream=None) -> None:
+        """Move (+ fused deposit into node_charge, which the caller zeroes)."""
+        v = self.parts.view()
+        st = _ptr(self.parts.status)
+        sp = _stream_ptr(stream)
+        if self.precision == "mixed":
+            rc = self.lib.oppb_move_deposit_mixed(C.byref(self.mesh.s), C.byref(v), _ptr(self.node_charge), st,
+                                                  self.max_hops, self.band, sp)
+        elif self.fused_deposit:
+            rc = self.lib.oppb_move_deposit_f64(C.byref(self.mesh.s), C.byref(v), _ptr(self.node_charge), st,
+                                                self.max_hops, sp)
+        else:
+            rc = self.lib.oppb_move_f64(C.byref(self.mesh.s), C.byref(v), st, self.max_hops, sp)
+        L.check("oppb_move", rc)
+
+    def deposit(self, stream=None) -> None:
+        v = self.parts.view()
+        L.check("oppb_deposit_f64", self.lib.oppb_deposit_f64(C.byref(self.mesh.s), C.byref(v),
+                                                              _ptr(self.node_charge), _stream_ptr(stream)))
+
+    def sort_now(self) -> bool:
+        if self.fill == "Sort_All":
+            return True
+        if self.fill == "Sort_Periodic":
+            return self.iter % self.fill_period == 0
+        return False
+
+    def finalize(self, remove_count: int, stream=None) -> str:
+        """opp_finalize_particle_move: hole fill or cell sort, then size -= removed."""
+        if remove_count <= 0:
+            return "none"
+        p = self.parts
+        dats = p.dat_list()
+        sp = _stream_ptr(stream)
+        if self.sort_now():
+            nbytes = self.lib.oppb_sort_workspace_bytes(p.size, self.mesh.n_cells)
+            ws = self._workspace(nbytes)
+            L.check("oppb_sort_by_cell", self.lib.oppb_sort_by_cell(
+                p.size, self.mesh.n_cells, p.capacity, len(p.DATS), dats, 3, None, _ptr(ws), ws.numel(), sp))
+            p.swap_after_sort()
+            kind = "sort"
+        else:
+            nbytes = self.lib.oppb_hole_fill_workspace_bytes(p.size, remove_count)
+            ws = self._workspace(nbytes)
+            L.check("oppb_hole_fill", self.lib.oppb_hole_fill(
+                p.size, remove_count, _ptr(p.bits), p.capacity, len(p.DATS), dats, _ptr(ws), ws.numel(), sp))
+            kind = "holefill"
+        p.size -= remove_count
+        return kind
+
+    def step(self, rnd_soa: torch.Tensor, stream=None, timers: StepTimes | None = None) -> dict:
+        """One FemPIC particle step.  Reads the move status once (the remove count that
+        sizes the compaction), as the reference does after its move."""
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if timers is not None else None
+        s = stream if stream is not None else torch.cuda.current_stream()
+        if ev: ev[0].record(s)
+        self.inject(rnd_soa, stream)
+        self.node_charge.zero_()
+        if ev: ev[1].record(s)
+        self.push(stream)
+        if ev: ev[2].record(s)
+        n_before = self.parts.size
+        self.move(stream)
+        if not self.fused_deposit and self.precision == "f64":
+            pass  # deposit after compaction, as the reference loop order
+        if ev: ev[3].record(s)
+        st = self.parts.status_host()
+        if st.error:
+            raise L.OppbError(f"move (particle {st.error_index})", st.error)
+        kind = self.finalize(st.remove_count, stream)
+        if not self.fused_deposit and self.precision == "f64":
+            self.deposit(stream)
+        if ev:
+            ev[4].record(s)
+            ev[4].synchronize()
+            timers.inject_ms += ev[0].elapsed_time(ev[1])
+            timers.push_ms += ev[1].elapsed_time(ev[2])
+            timers.move_ms += ev[2].elapsed_time(ev[3])
+            timers.compact_ms += ev[3].elapsed_time(ev[4])
+        out = {"iter": self.iter, "size_before_move": n_before, "removed": st.remove_count, "size": self.parts.size,
+               "visits": int(st.total_visits), "max_visits": st.max_visits, "rechecks": st.recheck_count,
+               "compaction": kind}
+        self.last = out
+        self.iter += 1
+        return out
+
+
+def randoms_to_device(rnd_aos: np.ndarray, device) -> torch.Tensor:
+    return torch.from_numpy(np.ascontiguousarray(rnd_aos.T)).to(device)

@@ -1,0 +1,95 @@
+"""TEST INFRASTRUCTURE ONLY — runs the compiled OP-PIC reference (oracle/_ref, built by
+oracle/Makefile from the reference sources) on a FemPIC case and reads back its per-step
+records (sizes, FNV-1a digests of the particle dats and node charges, wall times).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+REF_DIR = Path(__file__).resolve().parent / "_ref"
+BINARIES = {"seq_stable": "fempic_ref_seq_stable", "seq": "fempic_ref_seq", "omp": "fempic_ref_omp"}
+STEP_DTYPE = np.dtype([("step", "<i4"), ("size_before_move", "<i4"), ("removed", "<i4"), ("size", "<i4"),
+                       ("h_p2c", "<u8"), ("h_pos", "<u8"), ("h_vel", "<u8"), ("h_lc", "<u8"), ("h_charge", "<u8"),
+                       ("t_inject", "<f8"), ("t_push", "<f8"), ("t_move", "<f8"), ("t_deposit", "<f8")])
+
+
+def available(kind: str = "seq_stable") -> bool:
+    return (REF_DIR / BINARIES[kind]).exists()
+
+
+def fnv1a(a: np.ndarray) -> int:
+    from oracle.oracle import load
+
+    lib = load()
+    lib.oracle_fnv1a.restype = C.c_uint64
+    lib.oracle_fnv1a.argtypes = [C.c_void_p, C.c_int64]
+    a = np.ascontiguousarray(a)
+    return int(lib.oracle_fnv1a(a.ctypes.data, a.nbytes))
+
+
+def write_case(path: Path, mesh, dist: np.ndarray, steps: int, tables: list[np.ndarray], dt: float = 0.01,
+               qm: float = 1.0, ion_velocity: float = 1.0, sigma: float = 0.1, record_state: bool = True) -> None:
+    inject = int(dist[-1])
+    hdr = np.zeros(1, dtype=[("magic", "S8"), ("ints", "<i4", 8), ("dbl", "<f8", 4)])
+    hdr["magic"] = b"OPPBCAS1"
+    hdr["ints"] = [mesh.n_nodes, mesh.n_cells, mesh.n_ifaces, inject, steps, len(tables), int(record_state), 0]
+    hdr["dbl"] = [dt, qm, ion_velocity, sigma]
+    with open(path, "wb") as f:
+        f.write(hdr.tobytes())
+        for a, dt_ in ((mesh.c2n, "<i4"), (mesh.c2c, "<i4"), (mesh.c_det, "<f8"), (mesh.c_vol, "<f8"),
+                       (mesh.c_ef, "<f8"), (mesh.if2c, "<i4"), (mesh.if_u, "<f8"), (mesh.if_v, "<f8"),
+                       (mesh.if_norm, "<f8"), (mesh.if_n_pos, "<f8"), (dist, "<i4")):
+            f.write(np.ascontiguousarray(a, dtype=dt_).tobytes())
+        for t in tables:
+            assert t.shape == (inject, 5)
+            f.write(np.ascontiguousarray(t, dtype="<f8").tobytes())
+
+
+def params_text(fill: str, period: int, alloc_mult: float) -> str:
+    return (f"STRING opp_fill = {fill}\nINT opp_fill_period = {period}\n"
+            f"REAL opp_allocation_multiple = {alloc_mult}\nBOOL opp_profile_all = false\n"
+            f"BOOL opp_global_move = false\nINT opp_threads_per_block = 256\nBOOL print_final = false\n")
+
+
+def run(kind: str, mesh, dist, steps: int, tables, fill: str = "HoleFill_All", period: int = 10,
+        alloc_mult: float = 2.0, record_state: bool = True, threads: int | None = None, **kw) -> dict:
+    exe = REF_DIR / BINARIES[kind]
+    if not exe.exists():
+        raise FileNotFoundError(exe)
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        write_case(d / "case.bin", mesh, dist, steps, tables, record_state=record_state, **kw)
+        (d / "params.txt").write_text(params_text(fill, period, alloc_mult))
+        env = dict(os.environ)
+        if threads:
+            env["OMP_NUM_THREADS"] = str(threads)
+        r = subprocess.run([str(exe), str(d / "params.txt"), str(d / "case.bin"), str(d / "out.bin")],
+                           capture_output=True, text=True, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"{exe.name} failed ({r.returncode}): {r.stderr[-2000:]}")
+        raw = (d / "out.bin").read_bytes()
+    nrec = int(np.frombuffer(raw[:4], "<i4")[0])
+    off = 4
+    recs = np.frombuffer(raw[off:off + nrec * STEP_DTYPE.itemsize], STEP_DTYPE).copy()
+    off += nrec * STEP_DTYPE.itemsize
+    fin = int(np.frombuffer(raw[off:off + 4], "<i4")[0])
+    off += 4
+    out = {"records": recs, "size": fin}
+    if record_state:
+        def take(dt, n):
+            nonlocal off
+            a = np.frombuffer(raw[off:off + n * np.dtype(dt).itemsize], dt).copy()
+            off += n * np.dtype(dt).itemsize
+            return a
+        out["p2c"] = take("<i4", fin)
+        out["pos"] = take("<f8", fin * 3).reshape(fin, 3)
+        out["vel"] = take("<f8", fin * 3).reshape(fin, 3)
+        out["lc"] = take("<f8", fin * 4).reshape(fin, 4)
+        out["node_charge"] = take("<f8", mesh.n_nodes)
+    return out

@@ -1,0 +1,71 @@
+"""The C-ABI library without a GPU: it loads, exports every function the headers in
+include/ declare, and validates arguments before touching the device."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from oppb import _lib as L
+
+INCLUDE = Path(__file__).resolve().parent.parent / "include"
+
+
+def declared_functions():
+    names = set()
+    for h in ("oppb.h", "oppb_fempic.h"):
+        text = (INCLUDE / h).read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[\w\s\*]+?\b(oppb_\w+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.load()
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_version_and_status_strings():
+    lib = L.load()
+    assert b"sm_100a" in lib.oppb_version()
+    for s in range(8):
+        assert lib.oppb_status_string(s)
+    assert lib.oppb_status_string(99) == b"unknown status"
+
+
+def test_argument_validation_without_device():
+    lib = L.load()
+    assert lib.oppb_move_f64(None, None, None, 16, None) == L.OPPB_ERR_ARG
+    m = L.TetMesh(10, 10, None, None, None, None, None, None)
+    p = L.Particles(5, 4, None, None, None, None, None)  # stride < size
+    assert lib.oppb_move_f64(C.byref(m), C.byref(p), None, 16, None) == L.OPPB_ERR_ARG
+    assert lib.oppb_push_f64(C.byref(m), C.byref(p), 1.0, 0.01, None) == L.OPPB_ERR_ARG
+    assert lib.oppb_hole_fill(-1, 0, None, 0, 0, None, None, 0, None) == L.OPPB_ERR_ARG
+    assert lib.oppb_hole_fill(10, 0, None, 10, 0, None, None, 0, None) == L.OPPB_OK  # nothing removed
+    assert lib.oppb_sort_by_cell(10, 0, 10, 1, None, 0, None, None, 0, None) == L.OPPB_ERR_ARG
+
+
+def test_workspace_queries():
+    lib = L.load()
+    assert lib.oppb_hole_fill_workspace_bytes(0, 0) > 0
+    small = lib.oppb_sort_workspace_bytes(1000, 100)
+    big = lib.oppb_sort_workspace_bytes(50_000_000, 2_654_208)
+    assert big > 5 * 4 * 50_000_000 > small
+    assert lib.oppb_sort_workspace_bytes(-1, 5) == 0
+
+
+def test_kernel_launch_counter_starts_at_zero_without_launches():
+    assert L.load().oppb_kernel_launches() >= 0
+
+
+@pytest.mark.parametrize("n", [1, 1000])
+def test_mesh_bytes(n):
+    out = (C.c_size_t * 6)()
+    L.load().oppb_tet_mesh_bytes(n, out)
+    assert list(out) == [128 * n, 8 * n, 32 * n, 32 * n, 64 * n, 16 * n]

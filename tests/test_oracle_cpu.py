@@ -1,0 +1,130 @@
+"""The C oracle against the reference: the golden fixtures (made by the compiled
+reference seq backend, tests/golden/make_golden.py) always, and the live compiled
+reference on the 10x10x40-hex case when oracle/_ref is built."""
+from __future__ import annotations
+
+from pathlib import Path
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import ref_runner as R
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def _golden(name):
+    z = np.load(GOLDEN / f"{name}.npz")
+    mesh = SimpleNamespace(**{k: z[k] for k in ("c2n", "c2c", "c_det", "c_vol", "c_ef", "if2c", "if_u", "if_v",
+                                                "if_norm", "if_n_pos")})
+    mesh.n_nodes, mesh.n_cells, mesh.n_ifaces = int(z["n_nodes"]), int(z["n_cells"]), int(z["n_ifaces"])
+    return z, mesh
+
+
+@pytest.mark.parametrize("name", ["fempic_4x4x8_holefill", "fempic_4x4x8_sort"])
+def test_oracle_matches_golden(name):
+    z, mesh = _golden(name)
+    o = O.OracleFemPIC(mesh, z["dist"], fill=str(z["fill"]), fill_period=int(z["period"]))
+    recs = z["records"]
+    for s in range(int(z["steps"])):
+        r = o.step(z["tables"][s])
+        rec = recs[s]
+        n = o.size
+        assert (r["size"], r["removed"]) == (int(rec["size"]), int(rec["removed"])), s
+        assert R.fnv1a(o.p2c[:n]) == int(rec["h_p2c"]), s
+        assert R.fnv1a(o.pos[:n]) == int(rec["h_pos"]), s
+        assert R.fnv1a(o.vel[:n]) == int(rec["h_vel"]), s
+        assert R.fnv1a(o.lc[:n]) == int(rec["h_lc"]), s
+        assert R.fnv1a(o.node_charge) == int(rec["h_charge"]), s
+    n = o.size
+    np.testing.assert_array_equal(o.p2c[:n], z["p2c"])
+    np.testing.assert_array_equal(o.pos[:n].view(np.uint64), z["pos"].view(np.uint64))
+    np.testing.assert_array_equal(o.lc[:n].view(np.uint64), z["lc"].view(np.uint64))
+    np.testing.assert_array_equal(o.node_charge.view(np.uint64), z["node_charge"].view(np.uint64))
+    # golden cases exercise removals, and the sort case sorts
+    assert recs["removed"].sum() > 0
+
+
+def test_golden_invariants():
+    """Properties the reference's state obeys: charge sum = particle count (weights sum
+    to 1), every live particle's weights lie in the inside band of its cell."""
+    z, mesh = _golden("fempic_4x4x8_sort")
+    n = len(z["p2c"])
+    assert abs(z["node_charge"].sum() - n) < 1e-9 * n
+    assert (z["lc"] > -1e-10).all() and (z["lc"] - 1.0 < 1e-10).all()
+    assert ((z["p2c"] >= 0) & (z["p2c"] < mesh.n_cells)).all()
+
+
+@pytest.mark.skipif(not R.available("seq_stable"), reason="compiled reference not built (needs its sources)")
+@pytest.mark.parametrize("fill,steps,period", [("HoleFill_All", 120, 10), ("Sort_Periodic", 60, 5)])
+def test_oracle_matches_live_reference(fill, steps, period):
+    from helpers import mesh as mk
+    from oppb.fempic import injection_randoms
+
+    hm = mk()
+    dist = hm.inject_distribution(2000)
+    tables = [injection_randoms(5, s, 2000, 0.1) for s in range(steps)]
+    ref = R.run("seq_stable", hm, dist, steps, tables, fill=fill, period=period)
+    o = O.OracleFemPIC(hm, dist, fill=fill, fill_period=period)
+    for s in range(steps):
+        o.step(tables[s])
+        rec = ref["records"][s]
+        n = o.size
+        assert o.size == rec["size"]
+        assert R.fnv1a(o.p2c[:n]) == int(rec["h_p2c"]), s
+        assert R.fnv1a(o.lc[:n]) == int(rec["h_lc"]), s
+        assert R.fnv1a(o.node_charge) == int(rec["h_charge"]), s
+
+
+@pytest.mark.skipif(not R.available("seq"), reason="compiled reference not built (needs its sources)")
+def test_stock_seq_sort_differs_only_within_cells():
+    """The shipped seq backend sorts with std::sort (unstable): same cells per position
+    after a sort, possibly a different particle order inside a cell."""
+    from helpers import mesh as mk
+    from oppb.fempic import injection_randoms
+
+    hm = mk()
+    dist = hm.inject_distribution(2000)
+    tables = [injection_randoms(6, s, 2000, 0.1) for s in range(21)]
+    a = R.run("seq_stable", hm, dist, 21, tables, fill="Sort_Periodic", period=10)
+    b = R.run("seq", hm, dist, 21, tables, fill="Sort_Periodic", period=10)
+    assert a["size"] == b["size"]
+    np.testing.assert_array_equal(np.sort(a["p2c"]), np.sort(b["p2c"]))
+    np.testing.assert_array_equal(np.sort(a["node_charge"]), np.sort(a["node_charge"]))
+
+
+def test_hole_fill_pairs_follow_reference_rule():
+    """k-th hole (ascending) takes the k-th live particle from the back while it lies behind."""
+    rng = np.random.default_rng(0)
+    for trial in range(50):
+        n = int(rng.integers(1, 300))
+        p2c = rng.integers(0, 10, n).astype(np.int32)
+        rem = rng.random(n) < rng.random()
+        p2c[rem] = O.REMOVED
+        R_ = int(rem.sum())
+        data = np.arange(n, dtype=np.float64).reshape(n, 1).copy()
+        p = p2c.copy()
+        pf, pt = O.hole_fill(n, R_, p, [data, p])
+        holes = np.flatnonzero(p2c == O.REMOVED)
+        live_back = np.flatnonzero(p2c != O.REMOVED)[::-1]
+        k = 0
+        while k < min(R_, len(holes), len(live_back)) and live_back[k] > holes[k]:
+            k += 1
+        np.testing.assert_array_equal(pt, holes[:k])
+        np.testing.assert_array_equal(pf, live_back[:k])
+        assert not (p[: n - R_] == O.REMOVED).any()
+
+
+def test_oracle_sort_is_stable():
+    rng = np.random.default_rng(1)
+    n = 5000
+    p2c = rng.integers(0, 50, n).astype(np.int32)
+    p2c[rng.random(n) < 0.1] = O.REMOVED
+    idx = np.arange(n, dtype=np.float64).reshape(n, 1).copy()
+    key = p2c.copy()
+    perm = O.sort(n, 50, [idx, key], 1)
+    ref = np.argsort(np.where(p2c == O.REMOVED, 50, p2c), kind="stable")
+    np.testing.assert_array_equal(perm, ref)
+    np.testing.assert_array_equal(idx[:, 0], ref.astype(np.float64))
