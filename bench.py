@@ -277,12 +277,26 @@ def arm_ours(args) -> dict:
     seed = CFG["seed"] + 1000 * rank  # independent replicas per rank
     if world > 1:
         dist.barrier()
-    f64 = run_precision(hm, dev, "f64", args.steps, args.warmup, seed, cpu_sample=(rank == 0 and args.cpu_baseline))
-    sampler = ClockSampler(local)
+    f64 = mixed = None
+    if args.precision in ("both", "f64"):
+        f64 = run_precision(hm, dev, "f64", args.steps, args.warmup, seed,
+                            cpu_sample=(rank == 0 and args.cpu_baseline),
+                            sampler=ClockSampler(local) if args.precision == "f64" else None)
     if world > 1:
         dist.barrier()
-    mixed = run_precision(hm, dev, "mixed", args.steps, args.warmup, seed, sampler=sampler,
-                          e2e_steps=args.e2e_steps)
+    if args.precision in ("both", "mixed"):
+        mixed = run_precision(hm, dev, "mixed", args.steps, args.warmup, seed, sampler=ClockSampler(local),
+                              e2e_steps=args.e2e_steps)
+    if f64 is None or mixed is None:  # single-precision profiling runs: a short line, no ratio
+        r = f64 or mixed
+        if rank == 0:
+            print(json.dumps({"precision": r["precision"], "value": r["value"], "move_only": r["move_only"],
+                              "move_ms_per_launch": r["move_ms_per_launch"], "move_gbs": r["move_gbs"],
+                              "mean_particles": r["mean_particles"], "visits_per_particle": r["visits_per_particle"],
+                              "clocks": r["clocks"]}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return {}
 
     def reduce(v, op):
         if world == 1:
@@ -403,7 +417,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--ref-fill-steps", type=int, default=20)
+    ap.add_argument("--fill-steps", type=int, default=CFG["fill_steps"], help="steps to reach the steady state")
+    ap.add_argument("--capacity", type=int, default=CFG["capacity"], help="particle set capacity")
+    ap.add_argument("--precision", choices=["both", "f64", "mixed"], default="both")
     args = ap.parse_args()
+    CFG["fill_steps"], CFG["capacity"] = args.fill_steps, args.capacity
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     line = arm_reference(args) if args.impl == "reference" else arm_ours(args)

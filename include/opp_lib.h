@@ -1,0 +1,274 @@
+// opp_lib.h — the OP-PIC user API on the B200 backend (C++).
+//
+// Same names, argument meaning and error behaviour as the reference's
+// opp_lib/include/opp_lib.h and opp_defs.h, so that a generated FemPIC main compiles and
+// links against this library unchanged.  Storage: host copies AoS (as declared), device
+// copies SoA [dim][capacity] as in the reference's CUDA backend.  All compute goes through
+// the C ABI of oppb.h; errors abort through opp_abort as in the reference.
+#pragma once
+
+#include <cuda_runtime_api.h>
+
+#include <climits>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "oppb.h"
+
+typedef int OPP_INT;
+typedef double OPP_REAL;
+typedef bool OPP_BOOL;
+typedef std::string OPP_STRING;
+
+#define MAX_CELL_INDEX INT_MAX
+#define OPP_ROOT 0
+#define OPP_DBG false
+
+#define OPP_READ 0
+#define OPP_WRITE 1
+#define OPP_RW 2
+#define OPP_INC 3
+#define OPP_MIN 4
+#define OPP_MAX 5
+
+#define OPP_ARG_GBL 0
+#define OPP_ARG_DAT 1
+#define OPP_ARG_MAP 2
+
+#define OPP_RUN_ON_ROOT(command) if (OPP_rank == OPP_ROOT command)
+
+enum opp_iterate_type { OPP_ITERATE_ALL = 1, OPP_ITERATE_INJECTED };
+enum opp_move_status { OPP_MOVE_DONE = 0, OPP_NEED_MOVE, OPP_NEED_REMOVE };
+enum opp_data_type { DT_INT = 0, DT_REAL };
+enum Dirty { NotDirty = 0, Device = 1, Host = 2 };
+enum DeviceType { Device_CPU = 1, Device_GPU = 2 };
+enum opp_reset { OPP_Reset_Core = 0, OPP_Reset_Set, OPP_Reset_ieh, OPP_Reset_inh, OPP_Reset_All };
+enum opp_fill_type { OPP_HoleFill_All = 0, OPP_Sort_All, OPP_Shuffle_All, OPP_Sort_Periodic, OPP_Shuffle_Periodic };
+
+struct opp_set_core;
+typedef struct opp_set_core* opp_set;
+struct opp_map_core;
+typedef struct opp_map_core* opp_map;
+struct opp_dat_core;
+typedef struct opp_dat_core* opp_dat;
+
+typedef int opp_access;
+typedef int opp_arg_type;
+
+struct opp_arg {
+    int index;
+    opp_dat dat;         // dataset
+    opp_map map;         // indirect mapping
+    opp_dat p2c_map;     // particle -> cell dat of a double-indirect access
+    int dim;
+    int idx;
+    int size;
+    char* data;          // host data
+    char* data_d;        // device data
+    int* map_data;       // host map
+    int* map_data_d;     // device map (SoA)
+    char const* type;
+    opp_access acc;
+    opp_arg_type argtype;
+    int sent;
+    int opt;
+};
+
+struct opp_set_core {
+    int index;
+    int size;                       // elements in the set
+    char const* name;
+    int core_size;
+    int exec_size;
+    int nonexec_size;
+    bool is_particle;
+    int set_capacity;               // allocated elements (particle sets)
+    int diff;                       // particles added by the last increase
+    int particle_size;              // bytes of one particle over all its dats
+    opp_dat mesh_relation_dat = nullptr;
+    std::vector<opp_dat>* particle_dats;
+    int particle_remove_count;
+    opp_set cells_set;
+};
+
+struct opp_map_core {
+    int index;
+    opp_set from;
+    opp_set to;
+    int dim;
+    int* map;                       // host AoS [from.size][dim]
+    int* map_d;                     // device SoA [dim][from.size]
+    char const* name;
+    int user_managed;
+    opp_dat p2c_dat;                // particle maps: the mesh relation dat
+};
+
+struct opp_dat_core {
+    int index;
+    opp_set set;
+    int dim;
+    int size;                       // bytes of one element (dim * sizeof(type))
+    char* data;                     // host AoS
+    char* data_d;                   // device SoA [dim][stride]
+    char* data_swap_d;              // device SoA, target of the cell sort
+    char const* type;
+    char const* name;
+    int dirtybit;
+    Dirty dirty_hd;                 // which copy is stale
+    int user_managed;
+    bool is_cell_index;
+    opp_map p2c_map;
+    uint64_t version;               // bumped whenever the device copy is written
+};
+
+struct opp_point {
+    opp_point(double _x, double _y, double _z) : x(_x), y(_y), z(_z) {}
+    opp_point() {}
+    double x = 0.0, y = 0.0, z = 0.0;
+};
+
+constexpr double opp_zero_double16[16] = {0.0};
+constexpr int opp_zero_int16[16] = {0};
+
+namespace opp {
+
+// `TYPE key = value` parameter file (the reference's opp::Params format): INT, REAL,
+// BOOL, STRING; missing keys give INT_MAX / DBL_MAX / false / "NOT FOUND".
+class Params {
+   public:
+    explicit Params(const std::string& file);
+    Params() = default;
+    template <typename T>
+    T get(const std::string& key, bool error = true) const;
+    template <typename T>
+    void add(const std::string& key, T value);
+    void write(std::FILE* out) const;
+
+   private:
+    std::map<std::string, std::string> ints_, reals_, bools_, strings_;
+};
+
+// Named wall-clock regions; device work is synchronised at region ends by the loops.
+class Profiler {
+   public:
+    void reg(const std::string& name);
+    void start(const std::string& name);
+    void end(const std::string& name);
+    double seconds(const std::string& name) const;
+    long count(const std::string& name) const;
+    void printProfile(bool all_ranks = false) const;
+
+   private:
+    struct Entry {
+        double total = 0.0, started = 0.0;
+        long count = 0;
+    };
+    std::map<std::string, Entry> entries_;
+};
+
+}  // namespace opp
+
+extern std::unique_ptr<opp::Params> opp_params;
+extern std::unique_ptr<opp::Profiler> opp_profiler;
+
+extern int OPP_rank;
+extern int OPP_comm_size;
+extern int OPP_main_loop_iter;
+extern int OPP_comm_iteration;
+extern int OPP_fill_period;
+extern opp_fill_type OPP_fill_type;
+extern double OPP_part_alloc_mult;
+extern int OPP_iter_start;
+extern int OPP_iter_end;
+extern int OPP_move_max_hops;       // bound on cell visits per particle and move
+extern std::vector<opp_set> opp_sets;
+extern std::vector<opp_map> opp_maps;
+extern std::vector<opp_dat> opp_dats;
+
+// ------------------------------------------------------------------ lifetime
+void opp_init(int argc, char** argv);
+void opp_exit();
+void opp_abort(std::string s = "");
+void opp_printf(const char* function, const char* format, ...);
+
+// -------------------------------------------------------------- declarations
+opp_set opp_decl_set(int size, char const* name);
+opp_set opp_decl_particle_set(int size, char const* name, opp_set cells_set);
+opp_set opp_decl_particle_set(char const* name, opp_set cells_set);
+opp_map opp_decl_map(opp_set from, opp_set to, int dim, int* imap, char const* name);
+opp_dat opp_decl_dat(opp_set set, int dim, opp_data_type dtype, void* data, char const* name);
+
+void opp_decl_const_impl(int dim, int size, char* data, const char* name);
+template <typename T>
+void opp_decl_const(int dim, T* data, const char* name) {
+    opp_decl_const_impl(dim, sizeof(T), (char*)data, name);
+}
+// Value of a constant registered with opp_decl_const (abort if unknown).
+double opp_get_const(const char* name);
+
+// ------------------------------------------------------------------- args
+opp_arg opp_arg_gbl(double* data, int dim, char const* typ, opp_access acc);
+opp_arg opp_arg_gbl(int* data, int dim, char const* typ, opp_access acc);
+opp_arg opp_arg_gbl(const bool* data, int dim, char const* typ, opp_access acc);
+
+opp_arg opp_arg_dat(opp_dat dat, int idx, opp_map map, int dim, const char* typ, opp_map p2c_map, opp_access acc,
+                    bool offset = true);
+opp_arg opp_arg_dat(opp_dat dat, int idx, opp_map map, opp_map p2c_map, opp_access acc, bool offset = true);
+opp_arg opp_arg_dat(opp_dat dat, int idx, opp_map map, opp_access acc, bool offset = true);
+opp_arg opp_arg_dat(opp_dat dat, opp_map p2c_map, opp_access acc, bool offset = true);
+opp_arg opp_arg_dat(opp_dat dat, opp_access acc, bool offset = true);
+opp_arg opp_arg_dat(opp_map data_map, opp_access acc, bool offset = true);
+opp_arg opp_arg_dat(opp_map data_map, opp_map p2c_map, opp_access acc, bool offset = true);
+opp_arg opp_arg_dat(opp_map data_map, int idx, opp_map map, opp_access acc, bool offset = true);
+opp_arg opp_arg_dat(opp_map data_map, int idx, opp_map map, opp_map p2c_map, opp_access acc, bool offset = true);
+
+// -------------------------------------------------------------- particles
+void opp_increase_particle_count(opp_set part_set, int insert_count);
+void opp_inc_part_count_with_distribution(opp_set part_set, int insert_count, opp_dat part_dist,
+                                          bool calc_new = true);
+void opp_reset_num_particles_to_insert(opp_set set);
+void opp_init_particle_move(opp_set set, int nargs, opp_arg* args);
+bool opp_finalize_particle_move(opp_set set);
+void opp_particle_sort(opp_set set);
+
+void opp_reset_dat_impl(opp_dat dat, char* val, opp_reset reset = OPP_Reset_All);
+template <typename T>
+void opp_reset_dat(opp_dat dat, T* val, opp_reset reset = OPP_Reset_All) {
+    opp_reset_dat_impl(dat, (char*)val, reset);
+}
+
+// --------------------------------------------------------------- transfers
+void opp_upload_dat(opp_dat dat);
+void opp_download_dat(opp_dat dat);
+void opp_download_particle_set(opp_set set, bool force_download = false);
+void opp_upload_particle_set(opp_set set, bool realloc = false);
+template <typename T>
+T* opp_get_data(opp_dat dat) {
+    opp_download_dat(dat);
+    return (T*)dat->data;
+}
+OPP_INT* opp_get_data(opp_map map);
+void opp_print_dat_to_txtfile(opp_dat dat, const char* file_prefix, const char* file_suffix);
+
+// One-GPU build: halo exchanges and global reductions are identities.
+int opp_mpi_halo_exchanges_grouped(opp_set set, int nargs, opp_arg* args, DeviceType device);
+void opp_mpi_halo_wait_all(int nargs, opp_arg* args);
+void opp_set_dirtybit_grouped(int nargs, opp_arg* args, DeviceType device);
+inline int64_t opp_get_global_value(int64_t value) { return value; }
+
+// --------------------------------------------------------- B200 extensions
+// Device-resident packed mesh and scratch shared by the generated-loop entry points.
+namespace oppb_rt {
+cudaStream_t stream();
+const oppb_tet_mesh& tet_mesh(opp_dat c_det, opp_dat c_volume, opp_map c2c, opp_map c2n, opp_dat c_ef);
+void* workspace(size_t bytes);
+oppb_move_status* move_status();
+uint32_t* remove_bits(opp_set set);
+void mark_device_written(opp_dat dat);
+void sync_host_to_device(opp_dat dat);
+}  // namespace oppb_rt

@@ -37,26 +37,30 @@ extern "C" {
 
 /* ------------------------------------------------------------------ types */
 
-/* Device-resident tetrahedral mesh in the packed layout the kernels read.
- * Filled by oppb_tet_mesh_pack(); buffers are owned by the caller.
+/* Device-resident tetrahedral mesh in the packed layout the kernels read: one cell
+ * visit of the FP64 move is four 256-bit loads of `det` and one of `nav`; of the mixed
+ * move two of `geo32` and one of `nav32`.  Filled by oppb_tet_mesh_pack(); buffers are
+ * owned by the caller and 32-byte aligned (oppb_tet_mesh_bytes gives the sizes).
  *   det   [n_cells][16] f64 : {alpha,beta,gamma,delta} of vertex 0..3
  *                             (minifempic_funcs.h:316-382 ordering), 128-B record
- *   coef  [n_cells]     f64 : (1.0/6.0) / c_volume (kernels.h:110)
- *   conn  [n_cells][8]  i32 : c2c[0..3] (face opposite vertex i, -1 = boundary),
- *                             c2n[0..3]; 32-B record
+ *   nav   [n_cells][4] 64-bit: coef = (1.0/6.0)/c_volume (kernels.h:110), then
+ *                             c2c[0..3] as four int32 (face opposite vertex i, -1 =
+ *                             boundary), then 8 unused bytes; 32-B record
+ *   c2n   [n_cells][4]  i32 : cell -> node map (deposit)
  *   ef    [n_cells][4]  f64 : cell electric field x,y,z + pad
  *   geo32 [n_cells][16] f32 : mixed path, per vertex {lambda_i(o), dlambda_i/dx,
  *                             dlambda_i/dy, dlambda_i/dz} about origin o (may be NULL)
- *   org32 [n_cells][4]  f32 : mixed path origin o = vertex 0 rounded to f32 (may be NULL) */
+ *   nav32 [n_cells][8] 32-bit: mixed path origin o = vertex 0 rounded to f32 (3 floats),
+ *                             one unused word, c2c[0..3] as int32 (may be NULL) */
 typedef struct oppb_tet_mesh {
     int32_t  n_cells;
     int32_t  n_nodes;
     double*  det;
-    double*  coef;
-    int32_t* conn;
+    double*  nav;
+    int32_t* c2n;
     double*  ef;
     float*   geo32;
-    float*   org32;
+    float*   nav32;
 } oppb_tet_mesh;
 
 /* Particle set in the reference's device layout: SoA [dim][stride]
@@ -110,13 +114,15 @@ const char* oppb_status_string(int status);
  * launcher adds its launches; memsets are not counted). */
 uint64_t oppb_kernel_launches(void);
 
-/* Bytes of each packed mesh buffer for n_cells cells (det, coef, conn, ef, geo32, org32). */
+/* Bytes of each packed mesh buffer for n_cells cells (det, nav, c2n, ef, geo32, nav32). */
 void oppb_tet_mesh_bytes(int32_t n_cells, size_t out_bytes[6]);
 
 /* Pack the reference's device-layout cell dats (SoA [dim][soa_stride], as uploaded by
- * opp_upload_dat, opp_lib/src/cuda/opp_cuda_utils.cu:119-152) into mesh->det/coef/conn/ef,
- * and, when mesh->geo32/org32 are non-NULL, the mixed-precision records (needs n_pos,
- * SoA [3][n_pos_stride]).  c_ef may be NULL (ef left untouched).  invalid_out (device
+ * opp_upload_dat, opp_lib/src/cuda/opp_cuda_utils.cu:119-152) into the records of *mesh,
+ * and, when mesh->geo32/nav32 are non-NULL, the mixed-precision records (needs n_pos,
+ * SoA [3][n_pos_stride]).  Each input may be NULL, leaving its part of the records
+ * untouched: c_det and c_volume (det, nav coef), c2c (nav and nav32 neighbours), c2n (c2n),
+ * c_ef (ef); geo32 and the nav32 origin need c_det, c_volume, c2n and n_pos.  invalid_out (device
  * int32, may be NULL) receives the number of c2c entries outside {-1}u[0,n_cells) and
  * c2n entries outside [0,n_nodes); kernels never dereference such entries.
  * Replaces the per-loop SoA gathers of the generated move loop
@@ -184,12 +190,25 @@ int oppb_push_mixed(const oppb_tet_mesh* mesh, const oppb_particles* parts,
  * found by binary search), then inject_ions_kernel (apps/app_fempic/kernels.h:63-90):
  *   pos = a*u + b*v + node0  ((a,b) folded into the triangle),
  *   vel = normal*ion_velocity - qm*E*(0.5*dt) + thermal,  p2c = if2c[face].
- * rnd is SoA [5][rnd_stride] (a, b, thermal vx, vy, vz) indexed by k.
+ * When inlet->dist is NULL the face index is taken from p2c[start+k] instead, as left
+ * there by oppb_assign_faces (the reference's split into the two calls).
+ * rnd is SoA [rnd_dim][rnd_stride] indexed by k: a, b and, when rnd_dim == 5, the
+ * thermal velocity vx, vy, vz (rnd_dim == 2 is the reference's dummy_part_random).
  * start+count must not exceed parts->stride (else OPPB_ERR_CAPACITY). */
 int oppb_inject_f64(const oppb_tet_mesh* mesh, const oppb_inlet* inlet,
                     const oppb_particles* parts, int32_t start, int32_t count,
-                    const double* rnd, int32_t rnd_stride,
+                    const double* rnd, int32_t rnd_stride, int32_t rnd_dim,
                     double ion_velocity, double qm, double dt, void* stream);
+
+/* Face assignment of opp_inc_part_count_with_distribution: p2c[start+k] = first face j
+ * with k < dist[j], k in [0,count) (opp_lib/src/cuda/opp_increase_part_count.cu:86-105;
+ * the seq backend's rule, opp_increase_part_count_core.cpp:134-142, agrees whenever no face
+ * is empty). */
+int oppb_assign_faces(const oppb_inlet* inlet, int32_t* p2c, int32_t start, int32_t count, void* stream);
+
+/* Fill count elements of elem_bytes (4 or 8) at dst with the low bytes of `pattern`
+ * (opp_reset_dat of one component; the removed-cell fill of new particle slots). */
+int oppb_fill(void* dst, int64_t count, int32_t elem_bytes, uint64_t pattern, void* stream);
 
 /* ------------------------------------------------------------- compaction */
 

@@ -41,10 +41,14 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError(f"build command failed: {' '.join(cmd)}")
 
 
-def build_oppb(force: bool = False) -> Path:
-    """Compile csrc/*.cu and host/*.cpp into lib/liboppb.so."""
+CUDA_INC = "/usr/local/cuda/include"
+# Host sources of the C ABI library (set-up utilities) and of the C++ drop-in runtime.
+ABI_HOST = ("fempic_mesh.cpp",)
+RUNTIME_HOST = ("fempic_mesh.cpp", "opp_runtime.cpp", "fempic_loops.cpp")
+
+
+def _objects(force: bool, names) -> list[Path]:
     BUILD.mkdir(exist_ok=True)
-    LIB.mkdir(exist_ok=True)
     headers = sorted(INC.glob("*.h")) + sorted((PKG / "csrc").glob("*.cuh"))
     objs = []
     for src in sorted((PKG / "csrc").glob("*.cu")):
@@ -52,14 +56,33 @@ def build_oppb(force: bool = False) -> Path:
         if force or _newer(obj, [src] + headers):
             _run([NVCC] + NVCC_FLAGS + ["-c", str(src), "-o", str(obj)])
         objs.append(obj)
-    for src in sorted((PKG / "host").glob("*.cpp")):
+    for name in names:
+        src = PKG / "host" / name
         obj = BUILD / (src.stem + ".cpp.o")
         if force or _newer(obj, [src] + headers):
-            _run(["g++"] + CXX_FLAGS + ["-c", str(src), "-o", str(obj)])
+            _run(["g++"] + CXX_FLAGS + [f"-I{CUDA_INC}", "-c", str(src), "-o", str(obj)])
         objs.append(obj)
+    return objs
+
+
+def build_oppb(force: bool = False) -> Path:
+    """Compile csrc/*.cu and the set-up utilities into lib/liboppb.so (the C ABI), and
+    the same kernels with the opp_* runtime into lib/libopp_b200.so (the C++ drop-in),
+    plus the FemPIC app linked against the latter."""
+    LIB.mkdir(exist_ok=True)
+    objs = _objects(force, ABI_HOST)
     so = LIB / "liboppb.so"
     if force or _newer(so, objs):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", str(so)] + [str(o) for o in objs])
+    robjs = _objects(False, RUNTIME_HOST)
+    rso = LIB / "libopp_b200.so"
+    if force or _newer(rso, robjs):
+        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", str(rso)] + [str(o) for o in robjs])
+    app_src = PKG / "apps" / "fempic" / "fempic_b200.cpp"
+    app = LIB / "fempic_b200"
+    if force or _newer(app, [app_src, rso] + sorted(INC.glob("*.h"))):
+        _run(["g++"] + CXX_FLAGS + [f"-I{CUDA_INC}", str(app_src), "-o", str(app), f"-L{LIB}", "-lopp_b200",
+                                    "-Wl,-rpath,$ORIGIN"])
     return so
 
 

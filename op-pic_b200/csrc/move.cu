@@ -1,12 +1,21 @@
 // Particle move (multi-hop barycentric cell location) and node-charge deposit for
 // tetrahedral meshes, FP64 and mixed FP32/FP64.
 //
-// One thread per particle, particles in SoA (stride = capacity), cells in packed
-// records (det: 128 B, conn: 32 B, coef: 8 B) read through the read-only path.
-// The FP64 arithmetic uses explicit round-to-nearest intrinsics so nothing is
-// contracted into FMAs: each lambda_i is bit-identical to the reference expression
+// One thread per particle; particles in SoA (stride = capacity).  A cell visit reads
+// 32-byte-aligned records with 256-bit loads through the read-only path: FP64 = 4 loads
+// of the 128-B det record + 1 of the 32-B nav record {coef, c2c}; mixed = 2 loads of the
+// f32 lambda rows + 1 of {origin, c2c}.  The L1 data pipe pays one wavefront per distinct
+// cell per load instruction, so fewer, wider loads per visit is what bounds this kernel.
+//
+// The FP64 arithmetic uses explicit round-to-nearest intrinsics so nothing is contracted
+// into FMAs: each lambda_i is bit-identical to the reference expression
 //   coef * (((d0 - d1*x) + d2*y) - d3*z)          (apps/app_fempic/kernels.h:110-117)
 // and the inside test / argmin follow kernels.h:121-146 exactly.
+//
+// Deposit: lanes of a warp holding the same cell in a contiguous run are summed with a
+// segmented shuffle reduction; the run heads add into a per-CTA shared-memory table of
+// node sums (open addressing); the table is flushed with one FP64 global atomic per
+// distinct node at the end of the CTA.
 
 #include "oppb_common.cuh"
 
@@ -14,19 +23,11 @@ namespace oppb {
 namespace {
 
 constexpr int kMoveBlock = 256;
-constexpr double kTol = 1e-10;  // KERNEL_TOLERENCE, apps/app_fempic/kernels.h:44
+constexpr int kSlots = 1024;           // shared node-sum table (power of two)
+constexpr int kMaxProbe = 32;          // linear-probe bound; beyond it the sum goes straight to global
+constexpr double kTol = 1e-10;         // KERNEL_TOLERENCE, apps/app_fempic/kernels.h:44
 
 enum : int { kDone = 0, kNeedMove = 1, kNeedRemove = 2, kFailed = 3 };
-
-struct MeshArgs {
-    int32_t n_cells;
-    int32_t n_nodes;
-    const double* det;
-    const double* coef;
-    const int32_t* conn;
-    const float* geo32;
-    const float* org32;
-};
 
 struct PartArgs {
     int32_t size;
@@ -37,18 +38,34 @@ struct PartArgs {
     uint32_t* remove_bits;
 };
 
+struct NodeTable {
+    int keys[kSlots];
+    double vals[kSlots];
+};
+
 // lambda_0..3 of point (x,y,z) in cell c, evaluated exactly as the FP64 reference.
-__device__ __forceinline__ void lambda_f64(const MeshArgs& m, int32_t c, double x, double y, double z,
-                                           double l[4]) {
+// Also returns the cell's neighbours (nav record).
+__device__ __forceinline__ void visit_f64(const oppb_tet_mesh& m, int32_t c, double x, double y, double z,
+                                          double l[4], int nb[4]) {
     const double* d = m.det + (int64_t)c * 16;
-    const double coef = __ldg(m.coef + c);
+    double r[16];
+    ldg256(d, r[0], r[1], r[2], r[3]);
+    ldg256(d + 4, r[4], r[5], r[6], r[7]);
+    ldg256(d + 8, r[8], r[9], r[10], r[11]);
+    ldg256(d + 12, r[12], r[13], r[14], r[15]);
+    double coef, n01, n23, unused;
+    ldg256(m.nav + (int64_t)c * 4, coef, n01, n23, unused);
+    (void)unused;
+    const long long a = __double_as_longlong(n01), b = __double_as_longlong(n23);
+    nb[0] = (int)(a & 0xffffffffll);
+    nb[1] = (int)(a >> 32);
+    nb[2] = (int)(b & 0xffffffffll);
+    nb[3] = (int)(b >> 32);
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const double2 ab = ldg_d2(d + 4 * i);
-        const double2 gd = ldg_d2(d + 4 * i + 2);
-        double t = __dsub_rn(ab.x, __dmul_rn(ab.y, x));
-        t = __dadd_rn(t, __dmul_rn(gd.x, y));
-        t = __dsub_rn(t, __dmul_rn(gd.y, z));
+        double t = __dsub_rn(r[4 * i], __dmul_rn(r[4 * i + 1], x));
+        t = __dadd_rn(t, __dmul_rn(r[4 * i + 2], y));
+        t = __dsub_rn(t, __dmul_rn(r[4 * i + 3], z));
         l[i] = __dmul_rn(coef, t);
     }
 }
@@ -72,11 +89,14 @@ __device__ __forceinline__ int argmin4(const double l[4]) {
     return mi;
 }
 
+__device__ __forceinline__ int pick(const int nb[4], int i) {
+    return i == 0 ? nb[0] : i == 1 ? nb[1] : i == 2 ? nb[2] : nb[3];
+}
+
 // Warp-level bookkeeping shared by all move variants: removal bitmap word, remove
 // count, visit statistics.  Every lane of the warp must call it.
 __device__ __forceinline__ void warp_account(const PartArgs& p, oppb_move_status* st, int64_t i, bool active,
-                                             int32_t final_cell, bool newly_removed, int visits,
-                                             int rechecks) {
+                                             int32_t final_cell, bool newly_removed, int visits, int rechecks) {
     const int lane = threadIdx.x & 31;
     const unsigned hole = __ballot_sync(kFullMask, active && final_cell == kRemoved);
     const unsigned rem = __ballot_sync(kFullMask, newly_removed);
@@ -98,10 +118,40 @@ __device__ __forceinline__ void warp_account(const PartArgs& p, oppb_move_status
     }
 }
 
-// Warp-aggregated deposit: lanes holding the same cell in a contiguous run add
-// their weights with a segmented shuffle reduction; the run head issues four FP64
-// atomics into node_charge[c2n[cell][k]].  key < 0 = no contribution.
-__device__ __forceinline__ void warp_deposit(const MeshArgs& m, double* node_charge, int32_t key,
+__device__ __forceinline__ void table_init(NodeTable& t) {
+    for (int s = threadIdx.x; s < kSlots; s += kMoveBlock) {
+        t.keys[s] = -1;
+        t.vals[s] = 0.0;
+    }
+}
+
+// Adds v to node's slot (inserting the node), or straight to global memory when the
+// probe sequence is exhausted.
+__device__ __forceinline__ void table_add(NodeTable& t, double* node_charge, int node, double v) {
+    uint32_t h = ((uint32_t)node * 2654435761u) >> 22;  // 10 bits
+#pragma unroll 1
+    for (int probe = 0; probe < kMaxProbe; probe++) {
+        int k = *reinterpret_cast<volatile int*>(&t.keys[h]);
+        if (k == -1) k = atomicCAS(&t.keys[h], -1, node);
+        if (k == -1 || k == node) {
+            atomicAdd(&t.vals[h], v);
+            return;
+        }
+        h = (h + 1) & (kSlots - 1);
+    }
+    atomicAdd(node_charge + node, v);
+}
+
+__device__ __forceinline__ void table_flush(const NodeTable& t, double* node_charge) {
+    for (int s = threadIdx.x; s < kSlots; s += kMoveBlock) {
+        const int k = t.keys[s];
+        if (k >= 0) atomicAdd(node_charge + k, t.vals[s]);
+    }
+}
+
+// Segmented sum over contiguous lanes with equal key; run heads add the four weights to
+// the node table.  key < 0 = no contribution.  Every lane of the warp must call it.
+__device__ __forceinline__ void warp_deposit(const oppb_tet_mesh& m, NodeTable& t, double* node_charge, int32_t key,
                                              double l0, double l1, double l2, double l3) {
     const int lane = threadIdx.x & 31;
     const int32_t prev = __shfl_up_sync(kFullMask, key, 1);
@@ -123,20 +173,33 @@ __device__ __forceinline__ void warp_deposit(const MeshArgs& m, double* node_cha
         }
     }
     if (head && key >= 0) {
-        const int4 nodes = ldg_i4(m.conn + (int64_t)key * 8 + 4);
+        const int4 nodes = ldg_i4(m.c2n + (int64_t)key * 4);
         const uint32_t nn = (uint32_t)m.n_nodes;
-        if ((uint32_t)nodes.x < nn) atomicAdd(node_charge + nodes.x, l0);
-        if ((uint32_t)nodes.y < nn) atomicAdd(node_charge + nodes.y, l1);
-        if ((uint32_t)nodes.z < nn) atomicAdd(node_charge + nodes.z, l2);
-        if ((uint32_t)nodes.w < nn) atomicAdd(node_charge + nodes.w, l3);
+        if ((uint32_t)nodes.x < nn) table_add(t, node_charge, nodes.x, l0);
+        if ((uint32_t)nodes.y < nn) table_add(t, node_charge, nodes.y, l1);
+        if ((uint32_t)nodes.z < nn) table_add(t, node_charge, nodes.z, l2);
+        if ((uint32_t)nodes.w < nn) table_add(t, node_charge, nodes.w, l3);
     }
+}
+
+__device__ __forceinline__ void store_result(const PartArgs& p, int64_t i, const double l[4], int visits,
+                                             int32_t cell, int32_t cell0) {
+    if (visits > 0) {
+        st_stream(p.lc + i, l[0]);
+        st_stream(p.lc + p.stride + i, l[1]);
+        st_stream(p.lc + 2 * (int64_t)p.stride + i, l[2]);
+        st_stream(p.lc + 3 * (int64_t)p.stride + i, l[3]);
+    }
+    if (cell != cell0) st_stream(p.p2c + i, cell);
 }
 
 // ------------------------------------------------------------------ FP64 move
 
 template <bool kDeposit>
-__global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(MeshArgs m, PartArgs p, double* node_charge,
+__global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(oppb_tet_mesh m, PartArgs p, double* node_charge,
                                                               oppb_move_status* st, int32_t max_hops) {
+    __shared__ NodeTable table;
+    if (kDeposit) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
     const bool active = i < p.size;
     int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
@@ -154,39 +217,36 @@ __global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(MeshArgs m, PartAr
                 status = kFailed;
                 break;
             }
-            lambda_f64(m, cell, x, y, z, l);
+            int nb[4];
+            visit_f64(m, cell, x, y, z, l, nb);
             visits++;
             if (inside_f64(l)) {
                 status = kDone;
                 break;
             }
-            const int mi = argmin4(l);
-            const int32_t nb = __ldg(m.conn + (int64_t)cell * 8 + mi);
-            if (nb < 0) {
+            const int32_t next = pick(nb, argmin4(l));
+            if (next < 0) {
                 cell = kRemoved;
                 status = kNeedRemove;
                 break;
             }
-            cell = nb;
+            cell = next;
             if (visits >= max_hops) {
                 raise_error(st, OPPB_ERR_HOP_LIMIT, (int32_t)i);
                 status = kFailed;
                 break;
             }
         }
-        if (visits > 0) {
-            st_stream(p.lc + i, l[0]);
-            st_stream(p.lc + p.stride + i, l[1]);
-            st_stream(p.lc + 2 * (int64_t)p.stride + i, l[2]);
-            st_stream(p.lc + 3 * (int64_t)p.stride + i, l[3]);
-        }
-        if (cell != cell0) st_stream(p.p2c + i, cell);
+        store_result(p, i, l, visits, cell, cell0);
     }
     warp_account(p, st, i, active, cell, status == kNeedRemove, visits, 0);
     if (kDeposit) {
+        __syncthreads();  // table initialised by every thread
         const bool dep = active && cell0 != kRemoved && status == kDone;
-        warp_deposit(m, node_charge, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0, dep ? l[2] : 0.0,
+        warp_deposit(m, table, node_charge, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0, dep ? l[2] : 0.0,
                      dep ? l[3] : 0.0);
+        __syncthreads();
+        table_flush(table, node_charge);
     }
 }
 
@@ -202,9 +262,11 @@ __global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(MeshArgs m, PartAr
 constexpr float kMaxS = 16.0f;
 
 template <bool kDeposit>
-__global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(MeshArgs m, PartArgs p, double* node_charge,
+__global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(oppb_tet_mesh m, PartArgs p, double* node_charge,
                                                                 oppb_move_status* st, int32_t max_hops,
                                                                 float band) {
+    __shared__ NodeTable table;
+    if (kDeposit) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
     const bool active = i < p.size;
     int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
@@ -224,18 +286,22 @@ __global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(MeshArgs m, Part
                 break;
             }
             visits++;
-            const float4 o = ldg_f4(m.org32 + (int64_t)cell * 4);
-            const float dx = (float)(x - (double)o.x);
-            const float dy = (float)(y - (double)o.y);
-            const float dz = (float)(z - (double)o.z);
+            float nv[8], g0[8], g1[8];
+            ldg256(m.nav32 + (int64_t)cell * 8, nv);
+            ldg256(m.geo32 + (int64_t)cell * 16, g0);
+            ldg256(m.geo32 + (int64_t)cell * 16 + 8, g1);
+            const float dx = (float)(x - (double)nv[0]);
+            const float dy = (float)(y - (double)nv[1]);
+            const float dz = (float)(z - (double)nv[2]);
+            const float rows[16] = {g0[0], g0[1], g0[2], g0[3], g0[4], g0[5], g0[6], g0[7],
+                                    g1[0], g1[1], g1[2], g1[3], g1[4], g1[5], g1[6], g1[7]};
             float lf[4];
             float smax = 0.0f;
-            const float* g = m.geo32 + (int64_t)cell * 16;
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                const float4 r = ldg_f4(g + 4 * k);
-                lf[k] = fmaf(r.w, dz, fmaf(r.z, dy, fmaf(r.y, dx, r.x)));
-                const float s = fabsf(r.x) + fabsf(r.y) * fabsf(dx) + fabsf(r.z) * fabsf(dy) + fabsf(r.w) * fabsf(dz);
+                const float c0 = rows[4 * k], gx = rows[4 * k + 1], gy = rows[4 * k + 2], gz = rows[4 * k + 3];
+                lf[k] = fmaf(gz, dz, fmaf(gy, dy, fmaf(gx, dx, c0)));
+                const float s = fabsf(c0) + fabsf(gx) * fabsf(dx) + fabsf(gy) * fabsf(dy) + fabsf(gz) * fabsf(dz);
                 smax = fmaxf(smax, s);
             }
             // Classify in FP32.
@@ -267,7 +333,8 @@ __global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(MeshArgs m, Part
             bool in;
             if (ambiguous) {
                 rechecks++;
-                lambda_f64(m, cell, x, y, z, l);
+                int nb_unused[4];
+                visit_f64(m, cell, x, y, z, l, nb_unused);
                 in = inside_f64(l);
                 if (!in) mi = argmin4(l);
             } else {
@@ -279,38 +346,37 @@ __global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(MeshArgs m, Part
                 status = kDone;
                 break;
             }
-            const int32_t nb = __ldg(m.conn + (int64_t)cell * 8 + mi);
-            if (nb < 0) {
+            const int32_t next = __float_as_int(nv[4 + mi]);
+            if (next < 0) {
                 cell = kRemoved;
                 status = kNeedRemove;
                 break;
             }
-            cell = nb;
+            cell = next;
             if (visits >= max_hops) {
                 raise_error(st, OPPB_ERR_HOP_LIMIT, (int32_t)i);
                 status = kFailed;
                 break;
             }
         }
-        if (visits > 0) {
-            st_stream(p.lc + i, l[0]);
-            st_stream(p.lc + p.stride + i, l[1]);
-            st_stream(p.lc + 2 * (int64_t)p.stride + i, l[2]);
-            st_stream(p.lc + 3 * (int64_t)p.stride + i, l[3]);
-        }
-        if (cell != cell0) st_stream(p.p2c + i, cell);
+        store_result(p, i, l, visits, cell, cell0);
     }
     warp_account(p, st, i, active, cell, status == kNeedRemove, visits, rechecks);
     if (kDeposit) {
+        __syncthreads();
         const bool dep = active && cell0 != kRemoved && status == kDone;
-        warp_deposit(m, node_charge, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0, dep ? l[2] : 0.0,
+        warp_deposit(m, table, node_charge, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0, dep ? l[2] : 0.0,
                      dep ? l[3] : 0.0);
+        __syncthreads();
+        table_flush(table, node_charge);
     }
 }
 
 // ------------------------------------------------------------- standalone deposit
 
-__global__ void __launch_bounds__(kMoveBlock) deposit_f64_kernel(MeshArgs m, PartArgs p, double* node_charge) {
+__global__ void __launch_bounds__(kMoveBlock) deposit_f64_kernel(oppb_tet_mesh m, PartArgs p, double* node_charge) {
+    __shared__ NodeTable table;
+    table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
     const bool active = i < p.size;
     int32_t cell = active ? ld_stream(p.p2c + i) : -1;
@@ -322,14 +388,17 @@ __global__ void __launch_bounds__(kMoveBlock) deposit_f64_kernel(MeshArgs m, Par
         l2 = ld_stream(p.lc + 2 * (int64_t)p.stride + i);
         l3 = ld_stream(p.lc + 3 * (int64_t)p.stride + i);
     }
-    warp_deposit(m, node_charge, ok ? cell : -1, l0, l1, l2, l3);
+    __syncthreads();
+    warp_deposit(m, table, node_charge, ok ? cell : -1, l0, l1, l2, l3);
+    __syncthreads();
+    table_flush(table, node_charge);
 }
 
-int check_mesh(const oppb_tet_mesh* mesh, bool mixed) {
+int check_mesh(const oppb_tet_mesh* mesh, bool mixed, bool need_c2n) {
     if (!mesh || mesh->n_cells <= 0 || mesh->n_nodes <= 0) return OPPB_ERR_ARG;
-    if (!mesh->det || !mesh->coef || !mesh->conn) return OPPB_ERR_ARG;
-    if (!aligned(mesh->det, 16) || !aligned(mesh->conn, 16)) return OPPB_ERR_ARG;
-    if (mixed && (!mesh->geo32 || !mesh->org32 || !aligned(mesh->geo32, 16) || !aligned(mesh->org32, 16)))
+    if (!mesh->det || !mesh->nav || !aligned(mesh->det, 32) || !aligned(mesh->nav, 32)) return OPPB_ERR_ARG;
+    if (need_c2n && (!mesh->c2n || !aligned(mesh->c2n, 16))) return OPPB_ERR_ARG;
+    if (mixed && (!mesh->geo32 || !mesh->nav32 || !aligned(mesh->geo32, 32) || !aligned(mesh->nav32, 32)))
         return OPPB_ERR_ARG;
     return OPPB_OK;
 }
@@ -341,9 +410,6 @@ int check_parts(const oppb_particles* p, bool need_bits) {
     return OPPB_OK;
 }
 
-MeshArgs mesh_args(const oppb_tet_mesh* mesh) {
-    return MeshArgs{mesh->n_cells, mesh->n_nodes, mesh->det, mesh->coef, mesh->conn, mesh->geo32, mesh->org32};
-}
 PartArgs part_args(const oppb_particles* p) {
     return PartArgs{p->size, p->stride, p->pos, p->lc, p->p2c, p->remove_bits};
 }
@@ -351,7 +417,7 @@ PartArgs part_args(const oppb_particles* p) {
 template <int kKind>  // 0 move, 1 move+deposit, 2 mixed move+deposit
 int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
                 oppb_move_status* status, int32_t max_hops, double band, void* stream) {
-    int rc = check_mesh(mesh, kKind == 2);
+    int rc = check_mesh(mesh, kKind == 2, kKind != 0);
     if (rc) return rc;
     rc = check_parts(parts, true);
     if (rc) return rc;
@@ -361,15 +427,14 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     cudaStream_t s = as_stream(stream);
     if (cudaMemsetAsync(status, 0, sizeof(oppb_move_status), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
     if (parts->size == 0) return launch_status();
-    const MeshArgs m = mesh_args(mesh);
     const PartArgs p = part_args(parts);
     const int grid = ceil_div(parts->size, kMoveBlock);
     if (kKind == 0)
-        move_f64_kernel<false><<<grid, kMoveBlock, 0, s>>>(m, p, nullptr, status, max_hops);
+        move_f64_kernel<false><<<grid, kMoveBlock, 0, s>>>(*mesh, p, nullptr, status, max_hops);
     else if (kKind == 1)
-        move_f64_kernel<true><<<grid, kMoveBlock, 0, s>>>(m, p, node_charge, status, max_hops);
+        move_f64_kernel<true><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops);
     else
-        move_mixed_kernel<true><<<grid, kMoveBlock, 0, s>>>(m, p, node_charge, status, max_hops, (float)band);
+        move_mixed_kernel<true><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops, (float)band);
     count_launches(1);
     return launch_status();
 }
@@ -395,14 +460,14 @@ extern "C" int oppb_move_deposit_mixed(const oppb_tet_mesh* mesh, const oppb_par
 
 extern "C" int oppb_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
                                 void* stream) {
-    int rc = oppb::check_mesh(mesh, false);
-    if (rc) return rc;
+    if (!mesh || mesh->n_cells <= 0 || mesh->n_nodes <= 0 || !mesh->c2n || !oppb::aligned(mesh->c2n, 16))
+        return OPPB_ERR_ARG;
     if (!parts || parts->size < 0 || parts->stride < parts->size || !parts->lc || !parts->p2c || !node_charge)
         return OPPB_ERR_ARG;
     if (parts->size == 0) return OPPB_OK;
     const int grid = oppb::ceil_div(parts->size, oppb::kMoveBlock);
-    oppb::deposit_f64_kernel<<<grid, oppb::kMoveBlock, 0, oppb::as_stream(stream)>>>(
-        oppb::mesh_args(mesh), oppb::part_args(parts), node_charge);
+    oppb::deposit_f64_kernel<<<grid, oppb::kMoveBlock, 0, oppb::as_stream(stream)>>>(*mesh, oppb::part_args(parts),
+                                                                                    node_charge);
     oppb::count_launches(1);
     return oppb::launch_status();
 }

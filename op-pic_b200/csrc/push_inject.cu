@@ -2,6 +2,8 @@
 // surface.  FP64 arithmetic uses explicit round-to-nearest intrinsics so the results
 // are bit-identical to the seq backend's scalar expressions.
 
+#include <algorithm>
+
 #include "oppb_common.cuh"
 
 namespace oppb {
@@ -57,6 +59,31 @@ __global__ void __launch_bounds__(kPushBlock) push_mixed_kernel(int32_t size, in
     }
 }
 
+// First inlet face j with k < dist[j] (the last face if none).
+__device__ __forceinline__ int face_of(const int32_t* __restrict__ dist, int32_t n_faces, int64_t k) {
+    int lo = 0, hi = n_faces;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (k < __ldg(dist + mid))
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return lo < n_faces ? lo : n_faces - 1;
+}
+
+__global__ void __launch_bounds__(kPushBlock) assign_faces_kernel(int32_t start, int32_t count, int32_t n_faces,
+                                                                  const int32_t* __restrict__ dist, int32_t* p2c) {
+    const int64_t k = (int64_t)blockIdx.x * kPushBlock + threadIdx.x;
+    if (k < count) p2c[(int64_t)start + k] = face_of(dist, n_faces, k);
+}
+
+template <typename T>
+__global__ void fill_kernel(T* dst, int64_t count, T value) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = value;
+}
+
 // Injection: face of injected particle k = first j with k < dist[j]; then
 // inject_ions_kernel (apps/app_fempic/kernels.h:63-90) plus the thermal velocity.
 __global__ void __launch_bounds__(kPushBlock) inject_kernel(int32_t start, int32_t count, int32_t stride,
@@ -66,19 +93,16 @@ __global__ void __launch_bounds__(kPushBlock) inject_kernel(int32_t start, int32
                                                             const double* __restrict__ geom,
                                                             const double* __restrict__ ef,
                                                             const double* __restrict__ rnd, int32_t rstride,
-                                                            double ion_velocity, double qm, double dt,
+                                                            int32_t rdim, double ion_velocity, double qm, double dt,
                                                             double* pos, double* vel, int32_t* p2c) {
     const int64_t k = (int64_t)blockIdx.x * kPushBlock + threadIdx.x;
     if (k >= count) return;
-    int lo = 0, hi = n_faces;  // first j in [0, n_faces) with k < dist[j]
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (k < __ldg(dist + mid))
-            hi = mid;
-        else
-            lo = mid + 1;
+    // Without a distribution the face index is already in p2c (opp_inc_part_count_with_distribution).
+    const int face = dist ? face_of(dist, n_faces, k) : p2c[(int64_t)start + k];
+    if ((uint32_t)face >= (uint32_t)n_faces) {
+        p2c[(int64_t)start + k] = kRemoved;
+        return;
     }
-    const int face = lo < n_faces ? lo : n_faces - 1;
     const int32_t cell = __ldg(if2c + face);
     if ((uint32_t)cell >= (uint32_t)n_cells) {
         p2c[(int64_t)start + k] = kRemoved;
@@ -101,7 +125,7 @@ __global__ void __launch_bounds__(kPushBlock) inject_kernel(int32_t start, int32
         const double x = __dadd_rn(__dadd_rn(__dmul_rn(a, g[d]), __dmul_rn(b, g[3 + d])), g[9 + d]);
         double v = __dmul_rn(g[6 + d], ion_velocity);
         v = __dsub_rn(v, __dmul_rn(__dmul_rn(qm, e[d]), half_dt));
-        v = __dadd_rn(v, rnd[(int64_t)(2 + d) * rstride + k]);
+        if (rdim >= 5) v = __dadd_rn(v, rnd[(int64_t)(2 + d) * rstride + k]);
         pos[(int64_t)d * stride + p] = x;
         vel[(int64_t)d * stride + p] = v;
     }
@@ -144,19 +168,44 @@ extern "C" int oppb_push_mixed(const oppb_tet_mesh* mesh, const oppb_particles* 
 }
 
 extern "C" int oppb_inject_f64(const oppb_tet_mesh* mesh, const oppb_inlet* inlet, const oppb_particles* parts,
-                               int32_t start, int32_t count, const double* rnd, int32_t rnd_stride,
+                               int32_t start, int32_t count, const double* rnd, int32_t rnd_stride, int32_t rnd_dim,
                                double ion_velocity, double qm, double dt, void* stream) {
     using namespace oppb;
-    if (!mesh || !mesh->ef || !aligned(mesh->ef, 16) || !inlet || inlet->n_faces <= 0 || !inlet->dist ||
-        !inlet->if2c || !inlet->geom)
+    if (!mesh || !mesh->ef || !aligned(mesh->ef, 16) || !inlet || inlet->n_faces <= 0 || !inlet->if2c ||
+        !inlet->geom)
         return OPPB_ERR_ARG;
     if (!parts || !parts->pos || !parts->vel || !parts->p2c || start < 0 || count < 0) return OPPB_ERR_ARG;
-    if (count > 0 && (!rnd || rnd_stride < count)) return OPPB_ERR_ARG;
+    if (count > 0 && (!rnd || rnd_stride < count || (rnd_dim != 2 && rnd_dim != 5))) return OPPB_ERR_ARG;
     if ((int64_t)start + count > parts->stride) return OPPB_ERR_CAPACITY;
     if (count == 0) return OPPB_OK;
     inject_kernel<<<ceil_div(count, kPushBlock), kPushBlock, 0, as_stream(stream)>>>(
         start, count, parts->stride, inlet->n_faces, mesh->n_cells, inlet->dist, inlet->if2c, inlet->geom, mesh->ef, rnd,
-        rnd_stride, ion_velocity, qm, dt, parts->pos, parts->vel, parts->p2c);
+        rnd_stride, rnd_dim, ion_velocity, qm, dt, parts->pos, parts->vel, parts->p2c);
+    count_launches(1);
+    return launch_status();
+}
+
+extern "C" int oppb_assign_faces(const oppb_inlet* inlet, int32_t* p2c, int32_t start, int32_t count, void* stream) {
+    using namespace oppb;
+    if (!inlet || inlet->n_faces <= 0 || !inlet->dist || !p2c || start < 0 || count < 0) return OPPB_ERR_ARG;
+    if (count == 0) return OPPB_OK;
+    assign_faces_kernel<<<ceil_div(count, kPushBlock), kPushBlock, 0, as_stream(stream)>>>(start, count, inlet->n_faces,
+                                                                                        inlet->dist, p2c);
+    count_launches(1);
+    return launch_status();
+}
+
+extern "C" int oppb_fill(void* dst, int64_t count, int32_t elem_bytes, uint64_t pattern, void* stream) {
+    using namespace oppb;
+    if (count < 0 || (count > 0 && !dst) || (elem_bytes != 4 && elem_bytes != 8)) return OPPB_ERR_ARG;
+    if (!aligned(dst, (size_t)elem_bytes)) return OPPB_ERR_ARG;
+    if (count == 0) return OPPB_OK;
+    const int grid = (int)std::min<int64_t>(ceil_div(count, 256), 148 * 16);
+    if (elem_bytes == 8)
+        fill_kernel<uint64_t><<<grid, 256, 0, as_stream(stream)>>>(static_cast<uint64_t*>(dst), count, pattern);
+    else
+        fill_kernel<uint32_t><<<grid, 256, 0, as_stream(stream)>>>(static_cast<uint32_t*>(dst), count,
+                                                                   (uint32_t)pattern);
     count_launches(1);
     return launch_status();
 }

@@ -1,0 +1,138 @@
+// The FemPIC generated-loop entry points (apps_codegen/app_fempic_cg/fempic_opp.cpp:40-49
+// declares them with C++ linkage) on the B200 backend.  Each one replaces the body of the
+// reference's generated CUDA loop with the launchers of oppb.h; argument order and access
+// modes are the generated code's.
+
+#include <cuda_runtime.h>
+
+#include "opp_lib.h"
+
+namespace {
+
+void check(int rc, const char* what) {
+    if (rc != OPPB_OK) opp_abort(std::string(what) + ": " + oppb_status_string(rc));
+}
+
+oppb_particles particles(opp_set set, opp_dat pos, opp_dat vel, opp_dat lc) {
+    oppb_particles p{};
+    p.size = set->size;
+    p.stride = set->set_capacity > 0 ? set->set_capacity : 1;
+    p.pos = pos ? reinterpret_cast<double*>(pos->data_d) : nullptr;
+    p.vel = vel ? reinterpret_cast<double*>(vel->data_d) : nullptr;
+    p.lc = lc ? reinterpret_cast<double*>(lc->data_d) : nullptr;
+    p.p2c = reinterpret_cast<int32_t*>(set->mesh_relation_dat->data_d);
+    p.remove_bits = oppb_rt::remove_bits(set);
+    return p;
+}
+
+double charge_over_mass() { return opp_get_const("CONST_charge") / opp_get_const("CONST_mass"); }
+
+// Inlet geometry record [n_faces][12] = u, v, normal, node0, packed from the iface dats.
+struct InletCache {
+    opp_dat u = nullptr, v = nullptr, n = nullptr, np = nullptr;
+    uint64_t ver = 0;
+    double* geom = nullptr;
+    int n_faces = 0;
+} g_inlet;
+
+const double* inlet_geom(opp_dat u, opp_dat v, opp_dat nrm, opp_dat npos) {
+    const uint64_t ver = u->version + v->version + nrm->version + npos->version;
+    if (g_inlet.geom && g_inlet.u == u && g_inlet.v == v && g_inlet.n == nrm && g_inlet.np == npos &&
+        g_inlet.ver == ver)
+        return g_inlet.geom;
+    opp_download_dat(u);
+    opp_download_dat(v);
+    opp_download_dat(nrm);
+    opp_download_dat(npos);
+    const int nf = u->set->size;
+    std::vector<double> h((size_t)nf * 12);
+    for (int f = 0; f < nf; f++)
+        for (int d = 0; d < 3; d++) {
+            h[(size_t)f * 12 + d] = reinterpret_cast<double*>(u->data)[f * 3 + d];
+            h[(size_t)f * 12 + 3 + d] = reinterpret_cast<double*>(v->data)[f * 3 + d];
+            h[(size_t)f * 12 + 6 + d] = reinterpret_cast<double*>(nrm->data)[f * 3 + d];
+            h[(size_t)f * 12 + 9 + d] = reinterpret_cast<double*>(npos->data)[f * 9 + d];
+        }
+    if (g_inlet.geom && g_inlet.n_faces < nf) {
+        cudaFree(g_inlet.geom);
+        g_inlet.geom = nullptr;
+    }
+    if (!g_inlet.geom && cudaMalloc(&g_inlet.geom, h.size() * sizeof(double)) != cudaSuccess)
+        opp_abort("cudaMalloc inlet");
+    if (cudaMemcpy(g_inlet.geom, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        opp_abort("inlet upload");
+    g_inlet = InletCache{u, v, nrm, npos, ver, g_inlet.geom, nf};
+    return g_inlet.geom;
+}
+
+}  // namespace
+
+// inject_ions_kernel over the injected particles [size - diff, size).
+void opp_par_loop_injected__inject_ions_kernel(opp_set set, opp_arg arg0, opp_arg arg1, opp_arg arg2, opp_arg arg3,
+                                               opp_arg arg4, opp_arg arg5, opp_arg arg6, opp_arg arg7, opp_arg arg8,
+                                               opp_arg arg9) {
+    opp_profiler->start("inject_ions_kernel");
+    (void)arg2;
+    opp_dat c_ef = arg4.dat, rnd = arg9.dat;
+    oppb_rt::sync_host_to_device(rnd);
+    const oppb_tet_mesh& mesh = oppb_rt::tet_mesh(nullptr, nullptr, nullptr, nullptr, c_ef);
+    // arg3 is the if2c map read through p2c: the face index the distribution left in p2c.
+    const oppb_inlet inlet{arg5.dat->set->size, nullptr, arg3.map_data_d ? arg3.map_data_d : nullptr,
+                           inlet_geom(arg5.dat, arg6.dat, arg7.dat, arg8.dat)};
+    if (!inlet.if2c) opp_abort("inject_ions_kernel: if2c map has no device copy");
+    oppb_particles p = particles(set, arg0.dat, arg1.dat, nullptr);
+    const int rstride = rnd->set->is_particle ? rnd->set->set_capacity : rnd->set->size;
+    check(oppb_inject_f64(&mesh, &inlet, &p, set->size - set->diff, set->diff,
+                          reinterpret_cast<const double*>(rnd->data_d), rstride, rnd->dim,
+                          opp_get_const("CONST_ion_velocity"), charge_over_mass(), opp_get_const("CONST_dt"),
+                          oppb_rt::stream()),
+          "oppb_inject_f64");
+    oppb_rt::mark_device_written(arg0.dat);
+    oppb_rt::mark_device_written(arg1.dat);
+    oppb_rt::mark_device_written(set->mesh_relation_dat);
+    opp_profiler->end("inject_ions_kernel");
+}
+
+// calculate_new_pos_vel_kernel over [0, size).
+void opp_par_loop_all__calculate_new_pos_vel_kernel(opp_set set, opp_arg arg0, opp_arg arg1, opp_arg arg2) {
+    opp_profiler->start("calculate_new_pos_vel_kernel");
+    const oppb_tet_mesh& mesh = oppb_rt::tet_mesh(nullptr, nullptr, nullptr, nullptr, arg0.dat);
+    oppb_particles p = particles(set, arg1.dat, arg2.dat, nullptr);
+    check(oppb_push_f64(&mesh, &p, charge_over_mass(), opp_get_const("CONST_dt"), oppb_rt::stream()), "oppb_push_f64");
+    oppb_rt::mark_device_written(arg1.dat);
+    oppb_rt::mark_device_written(arg2.dat);
+    opp_profiler->end("calculate_new_pos_vel_kernel");
+}
+
+// move_kernel with multi-hop, then the finalize (hole fill / sort).
+void opp_particle_move__move_kernel(opp_set set, opp_map c2c_map, opp_map p2c_map, opp_arg arg0, opp_arg arg1,
+                                    opp_arg arg2, opp_arg arg3) {
+    opp_profiler->start("move_kernel");
+    (void)p2c_map;
+    opp_init_particle_move(set, 0, nullptr);
+    const oppb_tet_mesh& mesh = oppb_rt::tet_mesh(arg3.dat, arg2.dat, c2c_map, nullptr, nullptr);
+    oppb_particles p = particles(set, arg0.dat, nullptr, arg1.dat);
+    opp_profiler->start("move_kernel_only");
+    check(oppb_move_f64(&mesh, &p, oppb_rt::move_status(), OPP_move_max_hops, oppb_rt::stream()), "oppb_move_f64");
+    oppb_rt::mark_device_written(arg1.dat);
+    oppb_rt::mark_device_written(set->mesh_relation_dat);
+    opp_profiler->end("move_kernel_only");
+    while (opp_finalize_particle_move(set)) {
+    }
+    opp_profiler->end("move_kernel");
+}
+
+// deposit_charge_on_nodes_kernel: n_charge_den[c2n[p2c][i]] += p_lc[i].
+void opp_par_loop_all__deposit_charge_on_nodes_kernel(opp_set set, opp_arg arg0, opp_arg arg1, opp_arg arg2,
+                                                      opp_arg arg3, opp_arg arg4) {
+    opp_profiler->start("deposit_charge_on_nodes_kernel");
+    (void)arg2, (void)arg3, (void)arg4;
+    oppb_rt::sync_host_to_device(arg1.dat);
+    const oppb_tet_mesh& mesh = oppb_rt::tet_mesh(nullptr, nullptr, nullptr, arg1.map, nullptr);
+    oppb_particles p = particles(set, nullptr, nullptr, arg0.dat);
+    check(oppb_deposit_f64(&mesh, &p, reinterpret_cast<double*>(arg1.dat->data_d), oppb_rt::stream()),
+          "oppb_deposit_f64");
+    oppb_rt::mark_device_written(arg1.dat);
+    if (cudaStreamSynchronize(oppb_rt::stream()) != cudaSuccess) opp_abort("deposit");
+    opp_profiler->end("deposit_charge_on_nodes_kernel");
+}

@@ -25,8 +25,8 @@ c_dp, c_fp, c_ip, c_vp = C.POINTER(C.c_double), C.POINTER(C.c_float), C.POINTER(
 
 
 class TetMesh(C.Structure):
-    _fields_ = [("n_cells", c_i32), ("n_nodes", c_i32), ("det", c_vp), ("coef", c_vp), ("conn", c_vp),
-                ("ef", c_vp), ("geo32", c_vp), ("org32", c_vp)]
+    _fields_ = [("n_cells", c_i32), ("n_nodes", c_i32), ("det", c_vp), ("nav", c_vp), ("c2n", c_vp),
+                ("ef", c_vp), ("geo32", c_vp), ("nav32", c_vp)]
 
 
 class Particles(C.Structure):
@@ -69,8 +69,10 @@ _SIGS = {
     "oppb_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp]),
     "oppb_push_f64": (C.c_int, [P(TetMesh), P(Particles), C.c_double, C.c_double, c_vp]),
     "oppb_push_mixed": (C.c_int, [P(TetMesh), P(Particles), C.c_double, C.c_double, c_vp]),
-    "oppb_inject_f64": (C.c_int, [P(TetMesh), P(Inlet), P(Particles), c_i32, c_i32, c_vp, c_i32,
+    "oppb_inject_f64": (C.c_int, [P(TetMesh), P(Inlet), P(Particles), c_i32, c_i32, c_vp, c_i32, c_i32,
                                   C.c_double, C.c_double, C.c_double, c_vp]),
+    "oppb_assign_faces": (C.c_int, [P(Inlet), c_vp, c_i32, c_i32, c_vp]),
+    "oppb_fill": (C.c_int, [c_vp, c_i64, c_i32, c_u64, c_vp]),
     "oppb_hole_fill_workspace_bytes": (C.c_size_t, [c_i32, c_i32]),
     "oppb_hole_fill": (C.c_int, [c_i32, c_i32, c_vp, c_i32, c_i32, P(Dat), c_vp, C.c_size_t, c_vp]),
     "oppb_sort_workspace_bytes": (C.c_size_t, [c_i32, c_i32]),

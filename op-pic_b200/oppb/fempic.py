@@ -122,13 +122,13 @@ class DeviceMesh:
         soa_ef = t(hm.c_ef.T, torch.float64)
         soa_npos = t(hm.n_pos.T, torch.float64)
         self.det = torch.empty(nc * 16, dtype=torch.float64, device=device)
-        self.coef = torch.empty(nc, dtype=torch.float64, device=device)
-        self.conn = torch.empty(nc * 8, dtype=torch.int32, device=device)
+        self.nav = torch.zeros(nc * 4, dtype=torch.float64, device=device)
+        self.c2n = torch.empty(nc * 4, dtype=torch.int32, device=device)
         self.ef = torch.empty(nc * 4, dtype=torch.float64, device=device)
         self.geo32 = torch.empty(nc * 16, dtype=torch.float32, device=device) if mixed else None
-        self.org32 = torch.empty(nc * 4, dtype=torch.float32, device=device) if mixed else None
-        self.s = L.TetMesh(nc, nn, _ptr(self.det), _ptr(self.coef), _ptr(self.conn), _ptr(self.ef),
-                           _ptr(self.geo32), _ptr(self.org32))
+        self.nav32 = torch.zeros(nc * 8, dtype=torch.float32, device=device) if mixed else None
+        self.s = L.TetMesh(nc, nn, _ptr(self.det), _ptr(self.nav), _ptr(self.c2n), _ptr(self.ef),
+                           _ptr(self.geo32), _ptr(self.nav32))
         invalid = torch.zeros(1, dtype=torch.int32, device=device)
         L.check("oppb_tet_mesh_pack", L.load().oppb_tet_mesh_pack(
             C.byref(self.s), nc, _ptr(soa_det), _ptr(soa_vol), _ptr(soa_c2c), _ptr(soa_c2n), _ptr(soa_ef),
@@ -265,7 +265,7 @@ class FemPIC:
         v = p.view()
         L.check("oppb_inject_f64", self.lib.oppb_inject_f64(
             C.byref(self.mesh.s), C.byref(self.mesh.inlet), C.byref(v), start, count, _ptr(rnd_soa),
-            rnd_soa.stride(0), self.ion_velocity, self.qm, self.dt, _stream_ptr(stream)))
+            rnd_soa.stride(0), rnd_soa.shape[0], self.ion_velocity, self.qm, self.dt, _stream_ptr(stream)))
 
     def push(self, stream=None) -> None:
         v = self.parts.view()

@@ -73,7 +73,13 @@ def run(kind: str, mesh, dist, steps: int, tables, fill: str = "HoleFill_All", p
                            capture_output=True, text=True, env=env)
         if r.returncode != 0:
             raise RuntimeError(f"{exe.name} failed ({r.returncode}): {r.stderr[-2000:]}")
-        raw = (d / "out.bin").read_bytes()
+        return read_output(d / "out.bin", mesh.n_nodes, record_state)
+
+
+def read_output(path: Path, n_nodes: int, record_state: bool = True) -> dict:
+    """Per-step records and final state written by the harness (and by the library's
+    FemPIC app, which uses the same layout)."""
+    raw = Path(path).read_bytes()
     nrec = int(np.frombuffer(raw[:4], "<i4")[0])
     off = 4
     recs = np.frombuffer(raw[off:off + nrec * STEP_DTYPE.itemsize], STEP_DTYPE).copy()
@@ -91,5 +97,5 @@ def run(kind: str, mesh, dist, steps: int, tables, fill: str = "HoleFill_All", p
         out["pos"] = take("<f8", fin * 3).reshape(fin, 3)
         out["vel"] = take("<f8", fin * 3).reshape(fin, 3)
         out["lc"] = take("<f8", fin * 4).reshape(fin, 4)
-        out["node_charge"] = take("<f8", mesh.n_nodes)
+        out["node_charge"] = take("<f8", n_nodes)
     return out

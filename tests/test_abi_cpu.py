@@ -68,4 +68,4 @@ def test_kernel_launch_counter_starts_at_zero_without_launches():
 def test_mesh_bytes(n):
     out = (C.c_size_t * 6)()
     L.load().oppb_tet_mesh_bytes(n, out)
-    assert list(out) == [128 * n, 8 * n, 32 * n, 32 * n, 64 * n, 16 * n]
+    assert list(out) == [128 * n, 32 * n, 16 * n, 32 * n, 64 * n, 32 * n]

@@ -138,7 +138,7 @@ def test_inject_bit_exact(count):
     rd = randoms_to_device(rnd, DEV)
     v = ps.view()
     L.check("inject", L.load().oppb_inject_f64(C.byref(dm.s), C.byref(dm.inlet), C.byref(v), 17, count,
-                                               rd.data_ptr(), rd.stride(0), 1.0, 1.0, 0.01, None))
+                                               rd.data_ptr(), rd.stride(0), 5, 1.0, 1.0, 0.01, None))
     ps.size = 17 + count
     o = O.OracleFemPIC(hm, dist)
     o._grow(count + 17)
@@ -157,7 +157,7 @@ def test_inject_capacity_error():
     rd = randoms_to_device(injection_randoms(0, 0, 100, 0.1), DEV)
     v = ps.view()
     rc = L.load().oppb_inject_f64(C.byref(dm.s), C.byref(dm.inlet), C.byref(v), 0, 100, rd.data_ptr(),
-                                  rd.stride(0), 1.0, 1.0, 0.01, None)
+                                  rd.stride(0), 5, 1.0, 1.0, 0.01, None)
     assert rc == L.OPPB_ERR_CAPACITY
 
 
