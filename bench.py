@@ -420,10 +420,16 @@ def main():
     ap.add_argument("--fill-steps", type=int, default=CFG["fill_steps"], help="steps to reach the steady state")
     ap.add_argument("--capacity", type=int, default=CFG["capacity"], help="particle set capacity")
     ap.add_argument("--precision", choices=["both", "f64", "mixed"], default="both")
+    ap.add_argument("--deposit", choices=["warp", "table"], default="warp",
+                    help="deposit strategy: warp-run FP64 atomics or per-CTA shared node table")
     args = ap.parse_args()
     CFG["fill_steps"], CFG["capacity"] = args.fill_steps, args.capacity
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.impl != "reference":
+        from oppb import _lib as L
+
+        L.set_deposit_strategy(L.DEPOSIT_CTA_TABLE if args.deposit == "table" else L.DEPOSIT_WARP_ATOMIC)
     line = arm_reference(args) if args.impl == "reference" else arm_ours(args)
     if line:
         print(json.dumps(line), flush=True)

@@ -114,6 +114,18 @@ const char* oppb_status_string(int status);
  * launcher adds its launches; memsets are not counted). */
 uint64_t oppb_kernel_launches(void);
 
+/* Launch choices of the move kernels (process-wide; the autotuner's output). */
+#define OPPB_DEPOSIT_WARP_ATOMIC 0  /* warp run aggregation, FP64 global atomics per run head */
+#define OPPB_DEPOSIT_CTA_TABLE   1  /* per-CTA shared-memory node-sum table, one global atomic per node */
+typedef struct oppb_tuning {
+    int32_t deposit;     /* OPPB_DEPOSIT_* */
+    int32_t reserved[7];
+} oppb_tuning;
+
+/* Set / read the tuning used by subsequent launches (OPPB_ERR_ARG on unknown values). */
+int oppb_set_tuning(const oppb_tuning* tuning);
+void oppb_get_tuning(oppb_tuning* out);
+
 /* Bytes of each packed mesh buffer for n_cells cells (det, nav, c2n, ef, geo32, nav32). */
 void oppb_tet_mesh_bytes(int32_t n_cells, size_t out_bytes[6]);
 

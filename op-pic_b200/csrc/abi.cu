@@ -7,11 +7,23 @@
 namespace oppb {
 namespace {
 std::atomic<uint64_t> g_launches{0};
-}
+oppb_tuning g_tuning = {OPPB_DEPOSIT_WARP_ATOMIC, {0, 0, 0, 0, 0, 0, 0}};
+}  // namespace
 void count_launches(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+const oppb_tuning& tuning() { return g_tuning; }
 }  // namespace oppb
 
 extern "C" uint64_t oppb_kernel_launches(void) { return oppb::g_launches.load(std::memory_order_relaxed); }
+
+extern "C" int oppb_set_tuning(const oppb_tuning* t) {
+    if (!t || (t->deposit != OPPB_DEPOSIT_WARP_ATOMIC && t->deposit != OPPB_DEPOSIT_CTA_TABLE)) return OPPB_ERR_ARG;
+    oppb::g_tuning = *t;
+    return OPPB_OK;
+}
+
+extern "C" void oppb_get_tuning(oppb_tuning* out) {
+    if (out) *out = oppb::g_tuning;
+}
 
 extern "C" const char* oppb_version(void) { return "oppb 0.1 (sm_100a)"; }
 

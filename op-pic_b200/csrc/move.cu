@@ -12,10 +12,10 @@
 //   coef * (((d0 - d1*x) + d2*y) - d3*z)          (apps/app_fempic/kernels.h:110-117)
 // and the inside test / argmin follow kernels.h:121-146 exactly.
 //
-// Deposit: lanes of a warp holding the same cell in a contiguous run are summed with a
-// segmented shuffle reduction; the run heads add into a per-CTA shared-memory table of
-// node sums (open addressing); the table is flushed with one FP64 global atomic per
-// distinct node at the end of the CTA.
+// Deposit (kDep): lanes of a warp holding the same cell in a contiguous run are summed
+// with a segmented shuffle reduction; the run heads then either issue four FP64 global
+// atomics (kDepWarp) or add into a per-CTA shared-memory table of node sums (open
+// addressing) that is flushed with one global atomic per distinct node (kDepTable).
 
 #include "oppb_common.cuh"
 
@@ -23,9 +23,11 @@ namespace oppb {
 namespace {
 
 constexpr int kMoveBlock = 256;
-constexpr int kSlots = 1024;           // shared node-sum table (power of two)
-constexpr int kMaxProbe = 32;          // linear-probe bound; beyond it the sum goes straight to global
+constexpr int kSlots = 256;            // shared node-sum table (power of two, one slot per thread)
+constexpr int kMaxProbe = 16;          // linear-probe bound; beyond it the sum goes straight to global
 constexpr double kTol = 1e-10;         // KERNEL_TOLERENCE, apps/app_fempic/kernels.h:44
+constexpr int kDepNone = 0, kDepWarp = 1, kDepTable = 2;
+static_assert(kSlots == kMoveBlock, "table init/flush assume one slot per thread");
 
 enum : int { kDone = 0, kNeedMove = 1, kNeedRemove = 2, kFailed = 3 };
 
@@ -119,16 +121,14 @@ __device__ __forceinline__ void warp_account(const PartArgs& p, oppb_move_status
 }
 
 __device__ __forceinline__ void table_init(NodeTable& t) {
-    for (int s = threadIdx.x; s < kSlots; s += kMoveBlock) {
-        t.keys[s] = -1;
-        t.vals[s] = 0.0;
-    }
+    t.keys[threadIdx.x] = -1;
+    t.vals[threadIdx.x] = 0.0;
 }
 
 // Adds v to node's slot (inserting the node), or straight to global memory when the
 // probe sequence is exhausted.
 __device__ __forceinline__ void table_add(NodeTable& t, double* node_charge, int node, double v) {
-    uint32_t h = ((uint32_t)node * 2654435761u) >> 22;  // 10 bits
+    uint32_t h = ((uint32_t)node * 2654435761u) >> 24;  // 8 bits
 #pragma unroll 1
     for (int probe = 0; probe < kMaxProbe; probe++) {
         int k = *reinterpret_cast<volatile int*>(&t.keys[h]);
@@ -143,14 +143,21 @@ __device__ __forceinline__ void table_add(NodeTable& t, double* node_charge, int
 }
 
 __device__ __forceinline__ void table_flush(const NodeTable& t, double* node_charge) {
-    for (int s = threadIdx.x; s < kSlots; s += kMoveBlock) {
-        const int k = t.keys[s];
-        if (k >= 0) atomicAdd(node_charge + k, t.vals[s]);
-    }
+    const int k = t.keys[threadIdx.x];
+    if (k >= 0) atomicAdd(node_charge + k, t.vals[threadIdx.x]);
+}
+
+template <int kDep>
+__device__ __forceinline__ void node_add(NodeTable& t, double* node_charge, int node, double v) {
+    if (kDep == kDepTable)
+        table_add(t, node_charge, node, v);
+    else
+        atomicAdd(node_charge + node, v);
 }
 
 // Segmented sum over contiguous lanes with equal key; run heads add the four weights to
-// the node table.  key < 0 = no contribution.  Every lane of the warp must call it.
+// the nodes.  key < 0 = no contribution.  Every lane of the warp must call it.
+template <int kDep>
 __device__ __forceinline__ void warp_deposit(const oppb_tet_mesh& m, NodeTable& t, double* node_charge, int32_t key,
                                              double l0, double l1, double l2, double l3) {
     const int lane = threadIdx.x & 31;
@@ -175,10 +182,10 @@ __device__ __forceinline__ void warp_deposit(const oppb_tet_mesh& m, NodeTable& 
     if (head && key >= 0) {
         const int4 nodes = ldg_i4(m.c2n + (int64_t)key * 4);
         const uint32_t nn = (uint32_t)m.n_nodes;
-        if ((uint32_t)nodes.x < nn) table_add(t, node_charge, nodes.x, l0);
-        if ((uint32_t)nodes.y < nn) table_add(t, node_charge, nodes.y, l1);
-        if ((uint32_t)nodes.z < nn) table_add(t, node_charge, nodes.z, l2);
-        if ((uint32_t)nodes.w < nn) table_add(t, node_charge, nodes.w, l3);
+        if ((uint32_t)nodes.x < nn) node_add<kDep>(t, node_charge, nodes.x, l0);
+        if ((uint32_t)nodes.y < nn) node_add<kDep>(t, node_charge, nodes.y, l1);
+        if ((uint32_t)nodes.z < nn) node_add<kDep>(t, node_charge, nodes.z, l2);
+        if ((uint32_t)nodes.w < nn) node_add<kDep>(t, node_charge, nodes.w, l3);
     }
 }
 
@@ -195,11 +202,25 @@ __device__ __forceinline__ void store_result(const PartArgs& p, int64_t i, const
 
 // ------------------------------------------------------------------ FP64 move
 
-template <bool kDeposit>
+// Deposit epilogue shared by the move kernels.  Every thread of the CTA must call it.
+template <int kDep>
+__device__ __forceinline__ void deposit_epilogue(const oppb_tet_mesh& m, NodeTable& table, double* node_charge,
+                                                 bool dep, int32_t cell, const double l[4]) {
+    if (kDep == kDepNone) return;
+    if (kDep == kDepTable) __syncthreads();  // table initialised by every thread
+    warp_deposit<kDep>(m, table, node_charge, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0,
+                       dep ? l[2] : 0.0, dep ? l[3] : 0.0);
+    if (kDep == kDepTable) {
+        __syncthreads();
+        table_flush(table, node_charge);
+    }
+}
+
+template <int kDep>
 __global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(oppb_tet_mesh m, PartArgs p, double* node_charge,
                                                               oppb_move_status* st, int32_t max_hops) {
     __shared__ NodeTable table;
-    if (kDeposit) table_init(table);
+    if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
     const bool active = i < p.size;
     int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
@@ -240,14 +261,7 @@ __global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(oppb_tet_mesh m, P
         store_result(p, i, l, visits, cell, cell0);
     }
     warp_account(p, st, i, active, cell, status == kNeedRemove, visits, 0);
-    if (kDeposit) {
-        __syncthreads();  // table initialised by every thread
-        const bool dep = active && cell0 != kRemoved && status == kDone;
-        warp_deposit(m, table, node_charge, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0, dep ? l[2] : 0.0,
-                     dep ? l[3] : 0.0);
-        __syncthreads();
-        table_flush(table, node_charge);
-    }
+    deposit_epilogue<kDep>(m, table, node_charge, active && cell0 != kRemoved && status == kDone, cell, l);
 }
 
 // -------------------------------------------------------- mixed FP32 / FP64 move
@@ -261,12 +275,12 @@ __global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(oppb_tet_mesh m, P
 
 constexpr float kMaxS = 16.0f;
 
-template <bool kDeposit>
+template <int kDep>
 __global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(oppb_tet_mesh m, PartArgs p, double* node_charge,
                                                                 oppb_move_status* st, int32_t max_hops,
                                                                 float band) {
     __shared__ NodeTable table;
-    if (kDeposit) table_init(table);
+    if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
     const bool active = i < p.size;
     int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
@@ -362,36 +376,27 @@ __global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(oppb_tet_mesh m,
         store_result(p, i, l, visits, cell, cell0);
     }
     warp_account(p, st, i, active, cell, status == kNeedRemove, visits, rechecks);
-    if (kDeposit) {
-        __syncthreads();
-        const bool dep = active && cell0 != kRemoved && status == kDone;
-        warp_deposit(m, table, node_charge, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0, dep ? l[2] : 0.0,
-                     dep ? l[3] : 0.0);
-        __syncthreads();
-        table_flush(table, node_charge);
-    }
+    deposit_epilogue<kDep>(m, table, node_charge, active && cell0 != kRemoved && status == kDone, cell, l);
 }
 
 // ------------------------------------------------------------- standalone deposit
 
+template <int kDep>
 __global__ void __launch_bounds__(kMoveBlock) deposit_f64_kernel(oppb_tet_mesh m, PartArgs p, double* node_charge) {
     __shared__ NodeTable table;
-    table_init(table);
+    if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
     const bool active = i < p.size;
     int32_t cell = active ? ld_stream(p.p2c + i) : -1;
     const bool ok = active && (uint32_t)cell < (uint32_t)m.n_cells;
-    double l0 = 0, l1 = 0, l2 = 0, l3 = 0;
+    double l[4] = {0.0, 0.0, 0.0, 0.0};
     if (ok) {
-        l0 = ld_stream(p.lc + i);
-        l1 = ld_stream(p.lc + p.stride + i);
-        l2 = ld_stream(p.lc + 2 * (int64_t)p.stride + i);
-        l3 = ld_stream(p.lc + 3 * (int64_t)p.stride + i);
+        l[0] = ld_stream(p.lc + i);
+        l[1] = ld_stream(p.lc + p.stride + i);
+        l[2] = ld_stream(p.lc + 2 * (int64_t)p.stride + i);
+        l[3] = ld_stream(p.lc + 3 * (int64_t)p.stride + i);
     }
-    __syncthreads();
-    warp_deposit(m, table, node_charge, ok ? cell : -1, l0, l1, l2, l3);
-    __syncthreads();
-    table_flush(table, node_charge);
+    deposit_epilogue<kDep>(m, table, node_charge, ok, cell, l);
 }
 
 int check_mesh(const oppb_tet_mesh* mesh, bool mixed, bool need_c2n) {
@@ -429,12 +434,19 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     if (parts->size == 0) return launch_status();
     const PartArgs p = part_args(parts);
     const int grid = ceil_div(parts->size, kMoveBlock);
+    const bool table = tuning().deposit == OPPB_DEPOSIT_CTA_TABLE;
     if (kKind == 0)
-        move_f64_kernel<false><<<grid, kMoveBlock, 0, s>>>(*mesh, p, nullptr, status, max_hops);
+        move_f64_kernel<kDepNone><<<grid, kMoveBlock, 0, s>>>(*mesh, p, nullptr, status, max_hops);
+    else if (kKind == 1 && table)
+        move_f64_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops);
     else if (kKind == 1)
-        move_f64_kernel<true><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops);
+        move_f64_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops);
+    else if (table)
+        move_mixed_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops,
+                                                                 (float)band);
     else
-        move_mixed_kernel<true><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops, (float)band);
+        move_mixed_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops,
+                                                                (float)band);
     count_launches(1);
     return launch_status();
 }
@@ -466,8 +478,12 @@ extern "C" int oppb_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles*
         return OPPB_ERR_ARG;
     if (parts->size == 0) return OPPB_OK;
     const int grid = oppb::ceil_div(parts->size, oppb::kMoveBlock);
-    oppb::deposit_f64_kernel<<<grid, oppb::kMoveBlock, 0, oppb::as_stream(stream)>>>(*mesh, oppb::part_args(parts),
-                                                                                    node_charge);
+    if (oppb::tuning().deposit == OPPB_DEPOSIT_CTA_TABLE)
+        oppb::deposit_f64_kernel<oppb::kDepTable><<<grid, oppb::kMoveBlock, 0, oppb::as_stream(stream)>>>(
+            *mesh, oppb::part_args(parts), node_charge);
+    else
+        oppb::deposit_f64_kernel<oppb::kDepWarp><<<grid, oppb::kMoveBlock, 0, oppb::as_stream(stream)>>>(
+            *mesh, oppb::part_args(parts), node_charge);
     oppb::count_launches(1);
     return oppb::launch_status();
 }

@@ -15,6 +15,8 @@ inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 
 // Process-wide count of kernels launched by the library (abi.cu).
 void count_launches(int n);
+// Process-wide launch choices (abi.cu).
+const oppb_tuning& tuning();
 
 inline int launch_status() {
     const cudaError_t e = cudaGetLastError();

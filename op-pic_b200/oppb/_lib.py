@@ -43,6 +43,14 @@ class Dat(C.Structure):
     _fields_ = [("data", c_vp), ("swap", c_vp), ("dim", c_i32), ("elem_bytes", c_i32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("deposit", c_i32), ("reserved", c_i32 * 7)]
+
+
+DEPOSIT_WARP_ATOMIC = 0
+DEPOSIT_CTA_TABLE = 1
+
+
 class Inlet(C.Structure):
     _fields_ = [("n_faces", c_i32), ("dist", c_vp), ("if2c", c_vp), ("geom", c_vp)]
 
@@ -60,6 +68,8 @@ _SIGS = {
     "oppb_version": (C.c_char_p, []),
     "oppb_status_string": (C.c_char_p, [C.c_int]),
     "oppb_kernel_launches": (C.c_uint64, []),
+    "oppb_set_tuning": (C.c_int, [P(Tuning)]),
+    "oppb_get_tuning": (None, [P(Tuning)]),
     "oppb_tet_mesh_bytes": (None, [c_i32, P(C.c_size_t)]),
     "oppb_tet_mesh_pack": (C.c_int, [P(TetMesh), c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
     "oppb_tet_mesh_set_ef": (C.c_int, [P(TetMesh), c_i32, c_vp, c_vp]),
@@ -112,3 +122,10 @@ class OppbError(RuntimeError):
 def check(fn: str, status: int) -> None:
     if status != OPPB_OK:
         raise OppbError(fn, status)
+
+
+def set_deposit_strategy(strategy: int) -> None:
+    t = Tuning()
+    load().oppb_get_tuning(C.byref(t))
+    t.deposit = strategy
+    check("oppb_set_tuning", load().oppb_set_tuning(C.byref(t)))

@@ -61,8 +61,15 @@ def test_move_f64_bit_exact(n, seed):
     np.testing.assert_array_equal(rebuilt, holes)
 
 
+@pytest.fixture(params=[L.DEPOSIT_WARP_ATOMIC, L.DEPOSIT_CTA_TABLE], ids=["warp", "table"])
+def deposit_strategy(request):
+    L.set_deposit_strategy(request.param)
+    yield request.param
+    L.set_deposit_strategy(L.DEPOSIT_WARP_ATOMIC)
+
+
 @pytest.mark.parametrize("n,seed", [(5000, 4), (300_001, 5)])
-def test_move_deposit_f64(n, seed):
+def test_move_deposit_f64(n, seed, deposit_strategy):
     hm = mesh()
     dm = DeviceMesh(hm, DEV, mixed=False)
     pos, p2c = random_particles(hm, n, seed)
@@ -84,7 +91,7 @@ def test_move_deposit_f64(n, seed):
     _charge_close(charge.cpu().numpy(), ref, CHARGE_RTOL)
 
 
-def test_deposit_f64_standalone():
+def test_deposit_f64_standalone(deposit_strategy):
     hm = mesh()
     dm = DeviceMesh(hm, DEV, mixed=False)
     rng = np.random.default_rng(7)
