@@ -115,11 +115,12 @@ const char* oppb_status_string(int status);
 uint64_t oppb_kernel_launches(void);
 
 /* Launch choices of the move kernels (process-wide; the autotuner's output). */
-#define OPPB_DEPOSIT_WARP_ATOMIC 0  /* warp run aggregation, FP64 global atomics per run head */
+#define OPPB_DEPOSIT_WARP_ATOMIC 0  /* lanes grouped by final cell (warp match), FP64 atomics per group */
 #define OPPB_DEPOSIT_CTA_TABLE   1  /* per-CTA shared-memory node-sum table, one global atomic per node */
 typedef struct oppb_tuning {
     int32_t deposit;     /* OPPB_DEPOSIT_* */
-    int32_t reserved[7];
+    int32_t replicas;    /* node-sum copies the deposit spreads its atomics over (1..64, default 8) */
+    int32_t reserved[6];
 } oppb_tuning;
 
 /* Set / read the tuning used by subsequent launches (OPPB_ERR_ARG on unknown values). */
@@ -160,28 +161,36 @@ int oppb_tet_mesh_set_ef(oppb_tet_mesh* mesh, int32_t soa_stride, const double* 
 int oppb_move_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
                   oppb_move_status* status, int32_t max_hops, void* stream);
 
+/* Scratch bytes a deposit (fused or standalone) can use for n_nodes nodes: the node-sum
+ * copies beyond the first for the tuned replica count.  With less (or NULL) the deposit
+ * adds straight into node_charge. */
+size_t oppb_deposit_workspace_bytes(int32_t n_nodes);
+
 /* FP64 move with the node-charge deposit of the final cell fused in:
  * node_charge[c2n[p2c][i]] += p_lc[i] for every particle that stays
- * (apps/app_fempic/kernels.h:164-175) using warp-aggregated FP64 atomics. */
+ * (apps/app_fempic/kernels.h:164-175).  Lanes of a warp ending in the same cell are
+ * summed first; the sums go to FP64 atomics spread over replica copies of the node array
+ * (in `workspace`, zeroed here) that are added into node_charge at the end, as the
+ * reference spreads its atomics over thread-level copies (opp_lib/include/opp_cuda.h:526-588). */
 int oppb_move_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
-                          double* node_charge, oppb_move_status* status,
-                          int32_t max_hops, void* stream);
+                          double* node_charge, oppb_move_status* status, int32_t max_hops,
+                          void* workspace, size_t workspace_bytes, void* stream);
 
 /* Mixed-precision move + deposit: barycentric tests in FP32 about a per-cell origin;
  * any particle whose decision lies within `band` of a threshold or tie is re-evaluated
  * with the FP64 reference formula, so cell assignment, hop counts and removals stay
  * bit-identical to oppb_move_deposit_f64.  p_lc of non-rechecked particles carries
- * FP32 accuracy; node totals accumulate in FP64.  Needs mesh->geo32/org32. */
+ * FP32 accuracy; node totals accumulate in FP64.  Needs mesh->geo32/nav32. */
 int oppb_move_deposit_mixed(const oppb_tet_mesh* mesh, const oppb_particles* parts,
-                            double* node_charge, oppb_move_status* status,
-                            int32_t max_hops, double band, void* stream);
+                            double* node_charge, oppb_move_status* status, int32_t max_hops,
+                            double band, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------- deposit */
 
 /* Standalone deposit over [0,size): body of opp_par_loop_all__deposit_charge_on_nodes_kernel
  * (apps_codegen/app_fempic_cg/cuda/deposit_charge_on_nodes_kernel_loop.hpp:92-165). */
 int oppb_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
-                     double* node_charge, void* stream);
+                     double* node_charge, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------- push */
 

@@ -1,21 +1,25 @@
 // Particle move (multi-hop barycentric cell location) and node-charge deposit for
 // tetrahedral meshes, FP64 and mixed FP32/FP64.
 //
-// One thread per particle; particles in SoA (stride = capacity).  A cell visit reads
-// 32-byte-aligned records with 256-bit loads through the read-only path: FP64 = 4 loads
-// of the 128-B det record + 1 of the 32-B nav record {coef, c2c}; mixed = 2 loads of the
-// f32 lambda rows + 1 of {origin, c2c}.  The L1 data pipe pays one wavefront per distinct
-// cell per load instruction, so fewer, wider loads per visit is what bounds this kernel.
+// One thread per particle; particles in SoA (stride = capacity).  A cell visit is a
+// dependent gather of the cell's record with 256-bit loads through the read-only path:
+// FP64 = 4 loads of the 128-B det record + 1 of the 32-B nav record {coef, c2c}; mixed =
+// 2 loads of the f32 lambda rows + 1 of {origin, c2c}.  Lanes of a warp are rarely in the
+// same cell, so every load instruction pays about one L1 sector per lane; the L1 data pipe
+// is what bounds the kernel, hence few wide loads per visit and a 32-register cap (full
+// occupancy hides the dependent-gather latency).
 //
 // The FP64 arithmetic uses explicit round-to-nearest intrinsics so nothing is contracted
 // into FMAs: each lambda_i is bit-identical to the reference expression
 //   coef * (((d0 - d1*x) + d2*y) - d3*z)          (apps/app_fempic/kernels.h:110-117)
 // and the inside test / argmin follow kernels.h:121-146 exactly.
 //
-// Deposit (kDep): lanes of a warp holding the same cell in a contiguous run are summed
-// with a segmented shuffle reduction; the run heads then either issue four FP64 global
-// atomics (kDepWarp) or add into a per-CTA shared-memory table of node sums (open
-// addressing) that is flushed with one global atomic per distinct node (kDepTable).
+// Deposit (kDep): lanes ending in the same cell are grouped with a warp match; the lowest
+// lane of a group sums the group's weights by shuffles and issues four FP64 atomics
+// (kDepWarp), or adds into a per-CTA shared-memory node table flushed once per node
+// (kDepTable).  The atomics of CTA b go to node-sum copy b % R (copy 0 = node_charge,
+// copies 1..R-1 in the caller's workspace) so that neighbouring CTAs, which deposit on the
+// same nodes, do not serialise on one address; the copies are added afterwards.
 
 #include "oppb_common.cuh"
 
@@ -23,6 +27,7 @@ namespace oppb {
 namespace {
 
 constexpr int kMoveBlock = 256;
+constexpr int kMinBlocks = 8;          // 8 x 256 threads per SM: 32 registers per thread
 constexpr int kSlots = 256;            // shared node-sum table (power of two, one slot per thread)
 constexpr int kMaxProbe = 16;          // linear-probe bound; beyond it the sum goes straight to global
 constexpr double kTol = 1e-10;         // KERNEL_TOLERENCE, apps/app_fempic/kernels.h:44
@@ -40,10 +45,22 @@ struct PartArgs {
     uint32_t* remove_bits;
 };
 
+// Node-sum target of this CTA: copy (blockIdx.x % replicas).
+struct DepositArgs {
+    double* node_charge;
+    double* copies;     // replicas - 1 arrays of n_nodes, or nullptr
+    int32_t replicas;
+};
+
 struct NodeTable {
     int keys[kSlots];
     double vals[kSlots];
 };
+
+__device__ __forceinline__ double* deposit_target(const DepositArgs& d, int32_t n_nodes) {
+    const int r = d.replicas > 1 ? (int)(blockIdx.x % (unsigned)d.replicas) : 0;
+    return r == 0 ? d.node_charge : d.copies + (int64_t)(r - 1) * n_nodes;
+}
 
 // lambda_0..3 of point (x,y,z) in cell c, evaluated exactly as the FP64 reference.
 // Also returns the cell's neighbours (nav record).
@@ -70,6 +87,14 @@ __device__ __forceinline__ void visit_f64(const oppb_tet_mesh& m, int32_t c, dou
         t = __dsub_rn(t, __dmul_rn(r[4 * i + 3], z));
         l[i] = __dmul_rn(coef, t);
     }
+}
+
+// The FP64 re-evaluation of the mixed path, kept out of line: it is rare, and inlined it
+// would raise the register count of the whole kernel.
+__device__ __noinline__ void recheck_f64(const oppb_tet_mesh& m, int32_t c, double x, double y, double z,
+                                         double* l) {
+    int nb[4];
+    visit_f64(m, c, x, y, z, l, nb);
 }
 
 // Inside test of kernels.h:121-124 and first-index argmin of kernels.h:139-146.
@@ -127,7 +152,7 @@ __device__ __forceinline__ void table_init(NodeTable& t) {
 
 // Adds v to node's slot (inserting the node), or straight to global memory when the
 // probe sequence is exhausted.
-__device__ __forceinline__ void table_add(NodeTable& t, double* node_charge, int node, double v) {
+__device__ __forceinline__ void table_add(NodeTable& t, double* target, int node, double v) {
     uint32_t h = ((uint32_t)node * 2654435761u) >> 24;  // 8 bits
 #pragma unroll 1
     for (int probe = 0; probe < kMaxProbe; probe++) {
@@ -139,53 +164,64 @@ __device__ __forceinline__ void table_add(NodeTable& t, double* node_charge, int
         }
         h = (h + 1) & (kSlots - 1);
     }
-    atomicAdd(node_charge + node, v);
-}
-
-__device__ __forceinline__ void table_flush(const NodeTable& t, double* node_charge) {
-    const int k = t.keys[threadIdx.x];
-    if (k >= 0) atomicAdd(node_charge + k, t.vals[threadIdx.x]);
+    atomicAdd(target + node, v);
 }
 
 template <int kDep>
-__device__ __forceinline__ void node_add(NodeTable& t, double* node_charge, int node, double v) {
+__device__ __forceinline__ void node_add(NodeTable& t, double* target, int node, double v) {
     if (kDep == kDepTable)
-        table_add(t, node_charge, node, v);
+        table_add(t, target, node, v);
     else
-        atomicAdd(node_charge + node, v);
+        atomicAdd(target + node, v);
 }
 
-// Segmented sum over contiguous lanes with equal key; run heads add the four weights to
-// the nodes.  key < 0 = no contribution.  Every lane of the warp must call it.
+// Lanes with equal key form a group; the group's lowest lane sums the group's weights
+// (shuffle loop over the group members) and adds them to the cell's four nodes.
+// key < 0 = no contribution.  Every lane of the warp must call it.
 template <int kDep>
-__device__ __forceinline__ void warp_deposit(const oppb_tet_mesh& m, NodeTable& t, double* node_charge, int32_t key,
+__device__ __forceinline__ void warp_deposit(const oppb_tet_mesh& m, NodeTable& t, double* target, int32_t key,
                                              double l0, double l1, double l2, double l3) {
     const int lane = threadIdx.x & 31;
-    const int32_t prev = __shfl_up_sync(kFullMask, key, 1);
-    const bool head = (lane == 0) || (prev != key);
-    const unsigned heads = __ballot_sync(kFullMask, head);
-    const unsigned later = (lane == 31) ? 0u : (heads & (~0u << (lane + 1)));
-    const int seg_end = later ? (__ffs(later) - 2) : 31;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const double a0 = __shfl_down_sync(kFullMask, l0, o);
-        const double a1 = __shfl_down_sync(kFullMask, l1, o);
-        const double a2 = __shfl_down_sync(kFullMask, l2, o);
-        const double a3 = __shfl_down_sync(kFullMask, l3, o);
-        if (lane + o <= seg_end) {
+    const unsigned peers = __match_any_sync(kFullMask, key);
+    const bool leader = (lane == __ffs(peers) - 1) && key >= 0;
+    unsigned rest = leader ? (peers & ~(1u << lane)) : 0u;
+    while (__any_sync(kFullMask, rest != 0)) {
+        const int src = rest ? __ffs(rest) - 1 : lane;
+        const double a0 = __shfl_sync(kFullMask, l0, src);
+        const double a1 = __shfl_sync(kFullMask, l1, src);
+        const double a2 = __shfl_sync(kFullMask, l2, src);
+        const double a3 = __shfl_sync(kFullMask, l3, src);
+        if (rest) {
             l0 += a0;
             l1 += a1;
             l2 += a2;
             l3 += a3;
+            rest &= rest - 1;
         }
     }
-    if (head && key >= 0) {
+    if (leader) {
         const int4 nodes = ldg_i4(m.c2n + (int64_t)key * 4);
         const uint32_t nn = (uint32_t)m.n_nodes;
-        if ((uint32_t)nodes.x < nn) node_add<kDep>(t, node_charge, nodes.x, l0);
-        if ((uint32_t)nodes.y < nn) node_add<kDep>(t, node_charge, nodes.y, l1);
-        if ((uint32_t)nodes.z < nn) node_add<kDep>(t, node_charge, nodes.z, l2);
-        if ((uint32_t)nodes.w < nn) node_add<kDep>(t, node_charge, nodes.w, l3);
+        if ((uint32_t)nodes.x < nn) node_add<kDep>(t, target, nodes.x, l0);
+        if ((uint32_t)nodes.y < nn) node_add<kDep>(t, target, nodes.y, l1);
+        if ((uint32_t)nodes.z < nn) node_add<kDep>(t, target, nodes.z, l2);
+        if ((uint32_t)nodes.w < nn) node_add<kDep>(t, target, nodes.w, l3);
+    }
+}
+
+// Deposit epilogue shared by the move kernels.  Every thread of the CTA must call it.
+template <int kDep>
+__device__ __forceinline__ void deposit_epilogue(const oppb_tet_mesh& m, NodeTable& table, const DepositArgs& d,
+                                                 bool dep, int32_t cell, const double l[4]) {
+    if (kDep == kDepNone) return;
+    double* target = deposit_target(d, m.n_nodes);
+    if (kDep == kDepTable) __syncthreads();  // table initialised by every thread
+    warp_deposit<kDep>(m, table, target, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0, dep ? l[2] : 0.0,
+                       dep ? l[3] : 0.0);
+    if (kDep == kDepTable) {
+        __syncthreads();
+        const int k = table.keys[threadIdx.x];
+        if (k >= 0) atomicAdd(target + k, table.vals[threadIdx.x]);
     }
 }
 
@@ -202,23 +238,9 @@ __device__ __forceinline__ void store_result(const PartArgs& p, int64_t i, const
 
 // ------------------------------------------------------------------ FP64 move
 
-// Deposit epilogue shared by the move kernels.  Every thread of the CTA must call it.
 template <int kDep>
-__device__ __forceinline__ void deposit_epilogue(const oppb_tet_mesh& m, NodeTable& table, double* node_charge,
-                                                 bool dep, int32_t cell, const double l[4]) {
-    if (kDep == kDepNone) return;
-    if (kDep == kDepTable) __syncthreads();  // table initialised by every thread
-    warp_deposit<kDep>(m, table, node_charge, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0,
-                       dep ? l[2] : 0.0, dep ? l[3] : 0.0);
-    if (kDep == kDepTable) {
-        __syncthreads();
-        table_flush(table, node_charge);
-    }
-}
-
-template <int kDep>
-__global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(oppb_tet_mesh m, PartArgs p, double* node_charge,
-                                                              oppb_move_status* st, int32_t max_hops) {
+__global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
+    move_f64_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops) {
     __shared__ NodeTable table;
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
@@ -261,7 +283,7 @@ __global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(oppb_tet_mesh m, P
         store_result(p, i, l, visits, cell, cell0);
     }
     warp_account(p, st, i, active, cell, status == kNeedRemove, visits, 0);
-    deposit_epilogue<kDep>(m, table, node_charge, active && cell0 != kRemoved && status == kDone, cell, l);
+    deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, l);
 }
 
 // -------------------------------------------------------- mixed FP32 / FP64 move
@@ -276,9 +298,9 @@ __global__ void __launch_bounds__(kMoveBlock) move_f64_kernel(oppb_tet_mesh m, P
 constexpr float kMaxS = 16.0f;
 
 template <int kDep>
-__global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(oppb_tet_mesh m, PartArgs p, double* node_charge,
-                                                                oppb_move_status* st, int32_t max_hops,
-                                                                float band) {
+__global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
+    move_mixed_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
+                      float band) {
     __shared__ NodeTable table;
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
@@ -347,8 +369,7 @@ __global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(oppb_tet_mesh m,
             bool in;
             if (ambiguous) {
                 rechecks++;
-                int nb_unused[4];
-                visit_f64(m, cell, x, y, z, l, nb_unused);
+                recheck_f64(m, cell, x, y, z, l);
                 in = inside_f64(l);
                 if (!in) mi = argmin4(l);
             } else {
@@ -376,13 +397,14 @@ __global__ void __launch_bounds__(kMoveBlock) move_mixed_kernel(oppb_tet_mesh m,
         store_result(p, i, l, visits, cell, cell0);
     }
     warp_account(p, st, i, active, cell, status == kNeedRemove, visits, rechecks);
-    deposit_epilogue<kDep>(m, table, node_charge, active && cell0 != kRemoved && status == kDone, cell, l);
+    deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, l);
 }
 
 // ------------------------------------------------------------- standalone deposit
 
 template <int kDep>
-__global__ void __launch_bounds__(kMoveBlock) deposit_f64_kernel(oppb_tet_mesh m, PartArgs p, double* node_charge) {
+__global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
+    deposit_f64_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep) {
     __shared__ NodeTable table;
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
@@ -396,7 +418,17 @@ __global__ void __launch_bounds__(kMoveBlock) deposit_f64_kernel(oppb_tet_mesh m
         l[2] = ld_stream(p.lc + 2 * (int64_t)p.stride + i);
         l[3] = ld_stream(p.lc + 3 * (int64_t)p.stride + i);
     }
-    deposit_epilogue<kDep>(m, table, node_charge, ok, cell, l);
+    deposit_epilogue<kDep>(m, table, dep, ok, cell, l);
+}
+
+// node_charge[n] += sum over copies r of copies[r][n].
+__global__ void __launch_bounds__(256) reduce_copies_kernel(double* node_charge, const double* copies, int32_t n,
+                                                            int32_t n_copies) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        double s = node_charge[k];
+        for (int r = 0; r < n_copies; r++) s += copies[(int64_t)r * n + k];
+        node_charge[k] = s;
+    }
 }
 
 int check_mesh(const oppb_tet_mesh* mesh, bool mixed, bool need_c2n) {
@@ -419,9 +451,40 @@ PartArgs part_args(const oppb_particles* p) {
     return PartArgs{p->size, p->stride, p->pos, p->lc, p->p2c, p->remove_bits};
 }
 
+int replicas_for(size_t workspace_bytes, const void* workspace, int32_t n_nodes) {
+    const int want = tuning().replicas > 0 ? tuning().replicas : 1;
+    if (!workspace || want <= 1 || !aligned(workspace, 8)) return 1;
+    const size_t fit = workspace_bytes / ((size_t)n_nodes * sizeof(double)) + 1;
+    return (int)(fit < (size_t)want ? fit : (size_t)want);
+}
+
+// Zeroes the copies before, and folds them into node_charge after, the deposit launch.
+struct Replicas {
+    DepositArgs args;
+    int n_nodes;
+    int begin(cudaStream_t s) {
+        if (args.replicas > 1 &&
+            cudaMemsetAsync(args.copies, 0, (size_t)(args.replicas - 1) * n_nodes * sizeof(double), s) != cudaSuccess)
+            return OPPB_ERR_LAUNCH;
+        return OPPB_OK;
+    }
+    void end(cudaStream_t s) {
+        if (args.replicas <= 1) return;
+        const int grid = ceil_div(n_nodes, 256) < 148 * 8 ? ceil_div(n_nodes, 256) : 148 * 8;
+        reduce_copies_kernel<<<grid, 256, 0, s>>>(args.node_charge, args.copies, n_nodes, args.replicas - 1);
+        count_launches(1);
+    }
+};
+
+Replicas make_replicas(double* node_charge, void* workspace, size_t workspace_bytes, int32_t n_nodes) {
+    const int r = replicas_for(workspace_bytes, workspace, n_nodes);
+    return Replicas{DepositArgs{node_charge, r > 1 ? static_cast<double*>(workspace) : nullptr, r}, n_nodes};
+}
+
 template <int kKind>  // 0 move, 1 move+deposit, 2 mixed move+deposit
 int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
-                oppb_move_status* status, int32_t max_hops, double band, void* stream) {
+                oppb_move_status* status, int32_t max_hops, double band, void* workspace, size_t ws_bytes,
+                void* stream) {
     int rc = check_mesh(mesh, kKind == 2, kKind != 0);
     if (rc) return rc;
     rc = check_parts(parts, true);
@@ -434,56 +497,69 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     if (parts->size == 0) return launch_status();
     const PartArgs p = part_args(parts);
     const int grid = ceil_div(parts->size, kMoveBlock);
+    Replicas rep = make_replicas(node_charge, kKind == 0 ? nullptr : workspace, ws_bytes, mesh->n_nodes);
+    if ((rc = rep.begin(s))) return rc;
     const bool table = tuning().deposit == OPPB_DEPOSIT_CTA_TABLE;
     if (kKind == 0)
-        move_f64_kernel<kDepNone><<<grid, kMoveBlock, 0, s>>>(*mesh, p, nullptr, status, max_hops);
+        move_f64_kernel<kDepNone><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops);
     else if (kKind == 1 && table)
-        move_f64_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops);
+        move_f64_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops);
     else if (kKind == 1)
-        move_f64_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops);
+        move_f64_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops);
     else if (table)
-        move_mixed_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops,
-                                                                 (float)band);
+        move_mixed_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, (float)band);
     else
-        move_mixed_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, node_charge, status, max_hops,
-                                                                (float)band);
+        move_mixed_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, (float)band);
     count_launches(1);
+    rep.end(s);
     return launch_status();
 }
 
 }  // namespace
 }  // namespace oppb
 
+extern "C" size_t oppb_deposit_workspace_bytes(int32_t n_nodes) {
+    const int r = oppb::tuning().replicas;
+    if (n_nodes <= 0 || r <= 1) return 0;
+    return (size_t)(r - 1) * (size_t)n_nodes * sizeof(double);
+}
+
 extern "C" int oppb_move_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts, oppb_move_status* status,
                              int32_t max_hops, void* stream) {
-    return oppb::launch_move<0>(mesh, parts, nullptr, status, max_hops, 0.0, stream);
+    return oppb::launch_move<0>(mesh, parts, nullptr, status, max_hops, 0.0, nullptr, 0, stream);
 }
 
 extern "C" int oppb_move_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
-                                     oppb_move_status* status, int32_t max_hops, void* stream) {
-    return oppb::launch_move<1>(mesh, parts, node_charge, status, max_hops, 0.0, stream);
+                                     oppb_move_status* status, int32_t max_hops, void* workspace,
+                                     size_t workspace_bytes, void* stream) {
+    return oppb::launch_move<1>(mesh, parts, node_charge, status, max_hops, 0.0, workspace, workspace_bytes, stream);
 }
 
 extern "C" int oppb_move_deposit_mixed(const oppb_tet_mesh* mesh, const oppb_particles* parts,
                                        double* node_charge, oppb_move_status* status, int32_t max_hops,
-                                       double band, void* stream) {
-    return oppb::launch_move<2>(mesh, parts, node_charge, status, max_hops, band, stream);
+                                       double band, void* workspace, size_t workspace_bytes, void* stream) {
+    return oppb::launch_move<2>(mesh, parts, node_charge, status, max_hops, band, workspace, workspace_bytes,
+                                stream);
 }
 
 extern "C" int oppb_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
-                                void* stream) {
-    if (!mesh || mesh->n_cells <= 0 || mesh->n_nodes <= 0 || !mesh->c2n || !oppb::aligned(mesh->c2n, 16))
+                                void* workspace, size_t workspace_bytes, void* stream) {
+    using namespace oppb;
+    if (!mesh || mesh->n_cells <= 0 || mesh->n_nodes <= 0 || !mesh->c2n || !aligned(mesh->c2n, 16))
         return OPPB_ERR_ARG;
     if (!parts || parts->size < 0 || parts->stride < parts->size || !parts->lc || !parts->p2c || !node_charge)
         return OPPB_ERR_ARG;
     if (parts->size == 0) return OPPB_OK;
-    const int grid = oppb::ceil_div(parts->size, oppb::kMoveBlock);
-    if (oppb::tuning().deposit == OPPB_DEPOSIT_CTA_TABLE)
-        oppb::deposit_f64_kernel<oppb::kDepTable><<<grid, oppb::kMoveBlock, 0, oppb::as_stream(stream)>>>(
-            *mesh, oppb::part_args(parts), node_charge);
+    cudaStream_t s = as_stream(stream);
+    Replicas rep = make_replicas(node_charge, workspace, workspace_bytes, mesh->n_nodes);
+    int rc = rep.begin(s);
+    if (rc) return rc;
+    const int grid = ceil_div(parts->size, kMoveBlock);
+    if (tuning().deposit == OPPB_DEPOSIT_CTA_TABLE)
+        deposit_f64_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, part_args(parts), rep.args);
     else
-        oppb::deposit_f64_kernel<oppb::kDepWarp><<<grid, oppb::kMoveBlock, 0, oppb::as_stream(stream)>>>(
-            *mesh, oppb::part_args(parts), node_charge);
-    oppb::count_launches(1);
-    return oppb::launch_status();
+        deposit_f64_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, part_args(parts), rep.args);
+    count_launches(1);
+    rep.end(s);
+    return launch_status();
 }

@@ -130,7 +130,9 @@ void opp_par_loop_all__deposit_charge_on_nodes_kernel(opp_set set, opp_arg arg0,
     oppb_rt::sync_host_to_device(arg1.dat);
     const oppb_tet_mesh& mesh = oppb_rt::tet_mesh(nullptr, nullptr, nullptr, arg1.map, nullptr);
     oppb_particles p = particles(set, nullptr, nullptr, arg0.dat);
-    check(oppb_deposit_f64(&mesh, &p, reinterpret_cast<double*>(arg1.dat->data_d), oppb_rt::stream()),
+    const size_t ws_bytes = oppb_deposit_workspace_bytes(mesh.n_nodes);
+    check(oppb_deposit_f64(&mesh, &p, reinterpret_cast<double*>(arg1.dat->data_d),
+                           ws_bytes ? oppb_rt::workspace(ws_bytes) : nullptr, ws_bytes, oppb_rt::stream()),
           "oppb_deposit_f64");
     oppb_rt::mark_device_written(arg1.dat);
     if (cudaStreamSynchronize(oppb_rt::stream()) != cudaSuccess) opp_abort("deposit");

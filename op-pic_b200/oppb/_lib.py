@@ -44,7 +44,7 @@ class Dat(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("deposit", c_i32), ("reserved", c_i32 * 7)]
+    _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("reserved", c_i32 * 6)]
 
 
 DEPOSIT_WARP_ATOMIC = 0
@@ -74,9 +74,11 @@ _SIGS = {
     "oppb_tet_mesh_pack": (C.c_int, [P(TetMesh), c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
     "oppb_tet_mesh_set_ef": (C.c_int, [P(TetMesh), c_i32, c_vp, c_vp]),
     "oppb_move_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_i32, c_vp]),
-    "oppb_move_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, c_vp]),
-    "oppb_move_deposit_mixed": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, C.c_double, c_vp]),
-    "oppb_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp]),
+    "oppb_deposit_workspace_bytes": (C.c_size_t, [c_i32]),
+    "oppb_move_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, c_vp, C.c_size_t, c_vp]),
+    "oppb_move_deposit_mixed": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, C.c_double, c_vp,
+                                          C.c_size_t, c_vp]),
+    "oppb_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, C.c_size_t, c_vp]),
     "oppb_push_f64": (C.c_int, [P(TetMesh), P(Particles), C.c_double, C.c_double, c_vp]),
     "oppb_push_mixed": (C.c_int, [P(TetMesh), P(Particles), C.c_double, C.c_double, c_vp]),
     "oppb_inject_f64": (C.c_int, [P(TetMesh), P(Inlet), P(Particles), c_i32, c_i32, c_vp, c_i32, c_i32,
@@ -124,8 +126,15 @@ def check(fn: str, status: int) -> None:
         raise OppbError(fn, status)
 
 
-def set_deposit_strategy(strategy: int) -> None:
+def set_tuning(deposit: int | None = None, replicas: int | None = None) -> None:
     t = Tuning()
     load().oppb_get_tuning(C.byref(t))
-    t.deposit = strategy
+    if deposit is not None:
+        t.deposit = deposit
+    if replicas is not None:
+        t.replicas = replicas
     check("oppb_set_tuning", load().oppb_set_tuning(C.byref(t)))
+
+
+def set_deposit_strategy(strategy: int) -> None:
+    set_tuning(deposit=strategy)

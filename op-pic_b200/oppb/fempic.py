@@ -246,6 +246,7 @@ class FemPIC:
         self.node_charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=self.device)
         self.iter = 0
         self._ws = torch.empty(0, dtype=torch.uint8, device=self.device)
+        self._dep_ws = torch.empty(0, dtype=torch.uint8, device=self.device)
         self.lib = L.load()
         self.last = {}
 
@@ -272,25 +273,34 @@ class FemPIC:
         fn = self.lib.oppb_push_mixed if self.precision == "mixed" else self.lib.oppb_push_f64
         L.check("oppb_push", fn(C.byref(self.mesh.s), C.byref(v), self.qm, self.dt, _stream_ptr(stream)))
 
+    def _deposit_ws(self) -> torch.Tensor:
+        nbytes = self.lib.oppb_deposit_workspace_bytes(self.mesh.n_nodes)
+        if self._dep_ws.numel() < nbytes:
+            self._dep_ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        return self._dep_ws
+
     def move(self, stream=None) -> None:
         """Move (+ fused deposit into node_charge, which the caller zeroes)."""
         v = self.parts.view()
         st = _ptr(self.parts.status)
         sp = _stream_ptr(stream)
+        ws = self._deposit_ws()
         if self.precision == "mixed":
             rc = self.lib.oppb_move_deposit_mixed(C.byref(self.mesh.s), C.byref(v), _ptr(self.node_charge), st,
-                                                  self.max_hops, self.band, sp)
+                                                  self.max_hops, self.band, _ptr(ws), ws.numel(), sp)
         elif self.fused_deposit:
             rc = self.lib.oppb_move_deposit_f64(C.byref(self.mesh.s), C.byref(v), _ptr(self.node_charge), st,
-                                                self.max_hops, sp)
+                                                self.max_hops, _ptr(ws), ws.numel(), sp)
         else:
             rc = self.lib.oppb_move_f64(C.byref(self.mesh.s), C.byref(v), st, self.max_hops, sp)
         L.check("oppb_move", rc)
 
     def deposit(self, stream=None) -> None:
         v = self.parts.view()
+        ws = self._deposit_ws()
         L.check("oppb_deposit_f64", self.lib.oppb_deposit_f64(C.byref(self.mesh.s), C.byref(v),
-                                                              _ptr(self.node_charge), _stream_ptr(stream)))
+                                                              _ptr(self.node_charge), _ptr(ws), ws.numel(),
+                                                              _stream_ptr(stream)))
 
     def sort_now(self) -> bool:
         if self.fill == "Sort_All":

@@ -61,11 +61,16 @@ def test_move_f64_bit_exact(n, seed):
     np.testing.assert_array_equal(rebuilt, holes)
 
 
-@pytest.fixture(params=[L.DEPOSIT_WARP_ATOMIC, L.DEPOSIT_CTA_TABLE], ids=["warp", "table"])
+def _dep_ws(n_nodes: int) -> torch.Tensor:
+    return torch.empty(max(1, L.load().oppb_deposit_workspace_bytes(n_nodes)), dtype=torch.uint8, device=DEV)
+
+
+@pytest.fixture(params=[(L.DEPOSIT_WARP_ATOMIC, 8), (L.DEPOSIT_WARP_ATOMIC, 1), (L.DEPOSIT_CTA_TABLE, 3)],
+                ids=["warp-r8", "warp-r1", "table-r3"])
 def deposit_strategy(request):
-    L.set_deposit_strategy(request.param)
+    L.set_tuning(deposit=request.param[0], replicas=request.param[1])
     yield request.param
-    L.set_deposit_strategy(L.DEPOSIT_WARP_ATOMIC)
+    L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC, replicas=8)
 
 
 @pytest.mark.parametrize("n,seed", [(5000, 4), (300_001, 5)])
@@ -77,8 +82,10 @@ def test_move_deposit_f64(n, seed, deposit_strategy):
     _set_particles(ps, pos, p2c)
     charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
     v = ps.view()
+    ws = _dep_ws(hm.n_nodes)
     L.check("move_deposit", L.load().oppb_move_deposit_f64(C.byref(dm.s), C.byref(v), charge.data_ptr(),
-                                                           ps.status.data_ptr(), 4096, None))
+                                                           ps.status.data_ptr(), 4096, ws.data_ptr(), ws.numel(),
+                                                           None))
     lc = np.zeros((n, 4))
     p2c_o = p2c.copy()
     O.move(pos, lc, p2c_o, hm.c2c, hm.c_vol, hm.c_det, n=n, max_hops=4096)
@@ -106,7 +113,9 @@ def test_deposit_f64_standalone(deposit_strategy):
     ps.lc[:, :n] = torch.from_numpy(lc.T.copy()).to(DEV)
     charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
     v = ps.view()
-    L.check("deposit", L.load().oppb_deposit_f64(C.byref(dm.s), C.byref(v), charge.data_ptr(), None))
+    ws = _dep_ws(hm.n_nodes)
+    L.check("deposit", L.load().oppb_deposit_f64(C.byref(dm.s), C.byref(v), charge.data_ptr(), ws.data_ptr(),
+                                                 ws.numel(), None))
     ref = np.zeros(hm.n_nodes)
     O.deposit(lc, p2c, hm.c2n, ref)
     _charge_close(charge.cpu().numpy(), ref, CHARGE_RTOL)
@@ -334,8 +343,10 @@ def test_move_deterministic():
         _set_particles(ps, pos, p2c)
         charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
         v = ps.view()
+        ws = _dep_ws(hm.n_nodes)
         L.check("mixed", L.load().oppb_move_deposit_mixed(C.byref(dm.s), C.byref(v), charge.data_ptr(),
-                                                          ps.status.data_ptr(), 4096, 1e-5, None))
+                                                          ps.status.data_ptr(), 4096, 1e-5, ws.data_ptr(),
+                                                          ws.numel(), None))
         outs.append(ps.host_aos())
     np.testing.assert_array_equal(outs[0]["p2c"], outs[1]["p2c"])
     np.testing.assert_array_equal(outs[0]["lc"], outs[1]["lc"])
