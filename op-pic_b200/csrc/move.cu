@@ -120,17 +120,22 @@ __device__ __forceinline__ int pick(const int nb[4], int i) {
     return i == 0 ? nb[0] : i == 1 ? nb[1] : i == 2 ? nb[2] : nb[3];
 }
 
-// Warp-level bookkeeping shared by all move variants: removal bitmap word, remove
-// count, visit statistics.  Every lane of the warp must call it.
-__device__ __forceinline__ void warp_account(const PartArgs& p, oppb_move_status* st, int64_t i, bool active,
-                                             int32_t final_cell, bool newly_removed, int visits, int rechecks) {
-    const int lane = threadIdx.x & 31;
+// Bookkeeping shared by all move variants: the warp's removal bitmap word, then the CTA's
+// remove count, visit sum, visit maximum and recheck count, reduced in shared memory and
+// added to the status with one atomic per counter per CTA.  Every CTA updates the same
+// few status words, so per-warp atomics there serialise in L2 and cost as much as a
+// large share of the move itself.  Every thread of the CTA must call it.
+__device__ __forceinline__ void cta_account(const PartArgs& p, oppb_move_status* st, int64_t i, bool active,
+                                            int32_t final_cell, bool newly_removed, int visits, int rechecks) {
+    constexpr int kWarps = kMoveBlock / 32;
+    __shared__ unsigned long long s_sum[kWarps];
+    __shared__ int s_cnt[kWarps][3];  // removed, max visits, rechecks
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned hole = __ballot_sync(kFullMask, active && final_cell == kRemoved);
     const unsigned rem = __ballot_sync(kFullMask, newly_removed);
     if (lane == 0 && i < p.size) p.remove_bits[i >> 5] = hole;
-    int vmax = visits;
-    unsigned vsum = (unsigned)visits;
-    int rsum = rechecks;
+    int vmax = visits, rsum = rechecks;
+    unsigned long long vsum = (unsigned long long)visits;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         vmax = max(vmax, __shfl_xor_sync(kFullMask, vmax, o));
@@ -138,10 +143,29 @@ __device__ __forceinline__ void warp_account(const PartArgs& p, oppb_move_status
         rsum += __shfl_xor_sync(kFullMask, rsum, o);
     }
     if (lane == 0) {
-        if (rem) atomicAdd(&st->remove_count, __popc(rem));
-        if (vsum) atomicAdd(reinterpret_cast<unsigned long long*>(&st->total_visits), (unsigned long long)vsum);
-        if (vmax) atomicMax(&st->max_visits, vmax);
-        if (rsum) atomicAdd(&st->recheck_count, rsum);
+        s_sum[warp] = vsum;
+        s_cnt[warp][0] = __popc(rem);
+        s_cnt[warp][1] = vmax;
+        s_cnt[warp][2] = rsum;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const bool mine = lane < kWarps;
+        unsigned long long s = mine ? s_sum[lane] : 0ull;
+        int r = mine ? s_cnt[lane][0] : 0, m = mine ? s_cnt[lane][1] : 0, c = mine ? s_cnt[lane][2] : 0;
+#pragma unroll
+        for (int o = kWarps / 2; o > 0; o >>= 1) {
+            s += __shfl_xor_sync(kFullMask, s, o);
+            r += __shfl_xor_sync(kFullMask, r, o);
+            m = max(m, __shfl_xor_sync(kFullMask, m, o));
+            c += __shfl_xor_sync(kFullMask, c, o);
+        }
+        if (lane == 0) {
+            if (r) atomicAdd(&st->remove_count, r);
+            if (s) atomicAdd(reinterpret_cast<unsigned long long*>(&st->total_visits), s);
+            if (m) atomicMax(&st->max_visits, m);
+            if (c) atomicAdd(&st->recheck_count, c);
+        }
     }
 }
 
@@ -249,6 +273,7 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     const int32_t cell0 = cell;
     int status = kDone;
     int visits = 0;
+    int err = 0;
     double l[4] = {0.0, 0.0, 0.0, 0.0};
     if (active && cell != kRemoved) {
         const double x = ld_stream(p.pos + i);
@@ -256,17 +281,13 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
         const double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
         for (;;) {
             if ((uint32_t)cell >= (uint32_t)m.n_cells) {
-                raise_error(st, OPPB_ERR_CELL_RANGE, (int32_t)i);
-                status = kFailed;
+                err = OPPB_ERR_CELL_RANGE;
                 break;
             }
             int nb[4];
             visit_f64(m, cell, x, y, z, l, nb);
             visits++;
-            if (inside_f64(l)) {
-                status = kDone;
-                break;
-            }
+            if (inside_f64(l)) break;
             const int32_t next = pick(nb, argmin4(l));
             if (next < 0) {
                 cell = kRemoved;
@@ -275,14 +296,17 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
             }
             cell = next;
             if (visits >= max_hops) {
-                raise_error(st, OPPB_ERR_HOP_LIMIT, (int32_t)i);
-                status = kFailed;
+                err = OPPB_ERR_HOP_LIMIT;
                 break;
             }
         }
+        if (err) {
+            raise_error(st, err, (int32_t)i);
+            status = kFailed;
+        }
         store_result(p, i, l, visits, cell, cell0);
     }
-    warp_account(p, st, i, active, cell, status == kNeedRemove, visits, 0);
+    cta_account(p, st, i, active, cell, status == kNeedRemove, visits, 0);
     deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, l);
 }
 
@@ -297,10 +321,20 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
 
 constexpr float kMaxS = 16.0f;
 
+// The band's thresholds, precomputed on the host: kernel parameters live in the constant
+// bank and are used as instruction operands without occupying registers.
+struct Band {
+    float lo;      // band
+    float neg;     // -band
+    float in_hi;   // 1 - band
+    float out_hi;  // 1 + band
+    float tie;     // 2 * band
+};
+
 template <int kDep>
 __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     move_mixed_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
-                      float band) {
+                      Band band) {
     __shared__ NodeTable table;
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
@@ -310,6 +344,7 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     int status = kDone;
     int visits = 0;
     int rechecks = 0;
+    int err = 0;
     double l[4] = {0.0, 0.0, 0.0, 0.0};
     if (active && cell != kRemoved) {
         const double x = ld_stream(p.pos + i);
@@ -317,8 +352,7 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
         const double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
         for (;;) {
             if ((uint32_t)cell >= (uint32_t)m.n_cells) {
-                raise_error(st, OPPB_ERR_CELL_RANGE, (int32_t)i);
-                status = kFailed;
+                err = OPPB_ERR_CELL_RANGE;
                 break;
             }
             visits++;
@@ -346,8 +380,8 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
             bool ambiguous = !(smax <= kMaxS);
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                clear_in = clear_in && (lf[k] >= band) && (lf[k] <= 1.0f - band);
-                clear_out = clear_out || (lf[k] <= -band) || (lf[k] >= 1.0f + band);
+                clear_in = clear_in && (lf[k] >= band.lo) && (lf[k] <= band.in_hi);
+                clear_out = clear_out || (lf[k] <= band.neg) || (lf[k] >= band.out_hi);
             }
             int mi = 0;
             if (!clear_in && !ambiguous) {
@@ -363,7 +397,7 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
                         }
 #pragma unroll
                     for (int k = 0; k < 4; k++)
-                        if (k != mi && !(lf[k] - mv > 2.0f * band)) ambiguous = true;
+                        if (k != mi && !(lf[k] - mv > band.tie)) ambiguous = true;
                 }
             }
             bool in;
@@ -377,11 +411,10 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
 #pragma unroll
                 for (int k = 0; k < 4; k++) l[k] = (double)lf[k];
             }
-            if (in) {
-                status = kDone;
-                break;
-            }
-            const int32_t next = __float_as_int(nv[4 + mi]);
+            if (in) break;
+            // Re-read c2c[mi] from the record line just loaded (L1 hit) instead of keeping the
+            // four neighbours live across the visit under the 32-register cap.
+            const int32_t next = __ldg(reinterpret_cast<const int32_t*>(m.nav32 + (int64_t)cell * 8 + 4) + mi);
             if (next < 0) {
                 cell = kRemoved;
                 status = kNeedRemove;
@@ -389,14 +422,17 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
             }
             cell = next;
             if (visits >= max_hops) {
-                raise_error(st, OPPB_ERR_HOP_LIMIT, (int32_t)i);
-                status = kFailed;
+                err = OPPB_ERR_HOP_LIMIT;
                 break;
             }
         }
+        if (err) {
+            raise_error(st, err, (int32_t)i);
+            status = kFailed;
+        }
         store_result(p, i, l, visits, cell, cell0);
     }
-    warp_account(p, st, i, active, cell, status == kNeedRemove, visits, rechecks);
+    cta_account(p, st, i, active, cell, status == kNeedRemove, visits, rechecks);
     deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, l);
 }
 
@@ -500,6 +536,8 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     Replicas rep = make_replicas(node_charge, kKind == 0 ? nullptr : workspace, ws_bytes, mesh->n_nodes);
     if ((rc = rep.begin(s))) return rc;
     const bool table = tuning().deposit == OPPB_DEPOSIT_CTA_TABLE;
+    const float bf = (float)band;
+    const Band bd{bf, -bf, 1.0f - bf, 1.0f + bf, 2.0f * bf};
     if (kKind == 0)
         move_f64_kernel<kDepNone><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops);
     else if (kKind == 1 && table)
@@ -507,9 +545,9 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     else if (kKind == 1)
         move_f64_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops);
     else if (table)
-        move_mixed_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, (float)band);
+        move_mixed_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, bd);
     else
-        move_mixed_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, (float)band);
+        move_mixed_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, bd);
     count_launches(1);
     rep.end(s);
     return launch_status();
