@@ -31,6 +31,7 @@ extern "C" {
 #define OPPB_ERR_CELL_RANGE  5  /* device: p2c / c2c / c2n index out of range       */
 #define OPPB_ERR_CAPACITY    6  /* injection would exceed the set capacity          */
 #define OPPB_ERR_NO_DEVICE   7  /* no CUDA device visible                           */
+#define OPPB_ERR_SCRATCH_LIMIT 8 /* request larger than a fixed in-library scratch  */
 
 /* Cell index of a removed particle: MAX_CELL_INDEX in opp_lib/include/opp_defs.h:150. */
 #define OPPB_REMOVED_CELL 2147483647
@@ -245,6 +246,26 @@ size_t oppb_hole_fill_workspace_bytes(int32_t size, int32_t remove_count);
 int oppb_hole_fill(int32_t size, int32_t remove_count, const uint32_t* remove_bits,
                    int32_t stride, int32_t n_dats, const oppb_dat* dats,
                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* Largest remove_count that oppb_hole_fill_static accepts. */
+#define OPPB_HOLE_FILL_STATIC_MAX_REMOVES 1048576
+
+/* oppb_hole_fill without a workspace argument and without allocating anything: no
+ * counterpart in the reference.  It is for callers that cannot call cudaMalloc at the
+ * point of the move: a plugin that holds only the particle dats' device pointers while
+ * another runtime owns all device memory through its own pool, or a step loop that must
+ * not pay cudaMalloc/cudaFree's implicit device-wide synchronisation.  Same arguments and
+ * same result as oppb_hole_fill, bit for bit.
+ *
+ * Its scratch is a fixed array inside the library, about 8.1 MiB on every GPU that loads
+ * the library, held until the process exits; remove_count above
+ * OPPB_HOLE_FILL_STATIC_MAX_REMOVES returns OPPB_ERR_SCRATCH_LIMIT and changes nothing.
+ * The first call on each device looks the array's device address up with that device
+ * current; make that first call before any stream capture begins.  All calls on a device
+ * share the one array, so calls that may overlap on the GPU (other streams, other host
+ * threads) race and must be ordered by the caller. */
+int oppb_hole_fill_static(int32_t size, int32_t remove_count, const uint32_t* remove_bits,
+                          int32_t stride, int32_t n_dats, const oppb_dat* dats, void* stream);
 
 /* Scratch bytes oppb_sort_by_cell needs. */
 size_t oppb_sort_workspace_bytes(int32_t size, int32_t n_cells);

@@ -38,6 +38,7 @@ extern "C" const char* oppb_status_string(int status) {
         case OPPB_ERR_CELL_RANGE: return "cell index out of range";
         case OPPB_ERR_CAPACITY: return "particle set capacity exceeded";
         case OPPB_ERR_NO_DEVICE: return "no CUDA device";
+        case OPPB_ERR_SCRATCH_LIMIT: return "request exceeds the fixed scratch of an allocation-free entry point";
         default: return "unknown status";
     }
 }

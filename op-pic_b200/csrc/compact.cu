@@ -11,6 +11,9 @@
 //   3. emit hole[k] and mover[k] for k < remove_count (ranks from the scan),
 //   4. copy every dat element mover[k] -> hole[k] for the kept pairs.
 
+#include <climits>
+#include <mutex>
+
 #include "scan.cuh"
 
 namespace oppb {
@@ -188,6 +191,109 @@ extern "C" int oppb_hole_fill(int32_t size, int32_t remove_count, const uint32_t
     // block_base[0..n_blocks) exclusive, block_base[n_blocks] = total holes.
     scan_single_block_kernel<<<1, kScanBlock, 0, s>>>(block_base, n_blocks);
     (void)scan_tmp;
+    hf_emit_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base, n_blocks, remove_count,
+                                                 hole_list, mover_list);
+    count_launches(3);
+    if (dl.total_cols > 0) {
+        const int64_t threads = (int64_t)remove_count * dl.total_cols;
+        hf_copy_kernel<<<ceil_div(threads, 256), 256, 0, s>>>(remove_count, hole_list, mover_list,
+                                                             block_base + n_blocks, size, stride, dl);
+        count_launches(1);
+    }
+    return launch_status();
+}
+
+// ------------------------------------------------------- allocation-free hole fill
+//
+// oppb_hole_fill_static runs the same four kernels as oppb_hole_fill with its scratch in
+// a fixed array of this library instead of a caller workspace, for callers that cannot
+// allocate device memory where they move particles (a plugin that sees only the dats'
+// device pointers while another runtime owns the memory, or a loop that cannot afford
+// the device-wide synchronisation of cudaMalloc / cudaFree).
+//
+// Layout of the array (int32 words): per-block hole counts for the largest possible
+// particle count (their scan leaves the total at [n_blocks]), then the hole list and the
+// mover list of OPPB_HOLE_FILL_STATIC_MAX_REMOVES entries each.  Every word a call reads
+// was written earlier in the same call, so nothing has to start at zero and the contents
+// left by the previous call are harmless.  All calls on a device share the array: calls
+// that overlap on the GPU race.
+
+namespace oppb {
+namespace {
+
+constexpr int64_t kStaticMaxBlocks = (((int64_t)INT_MAX + 31) / 32 + kHfWords - 1) / kHfWords;  // 32,768
+constexpr int64_t kStaticBaseWords = (kStaticMaxBlocks + 1 + 63) / 64 * 64;  // whole 256-B lines
+constexpr int64_t kStaticListWords = OPPB_HOLE_FILL_STATIC_MAX_REMOVES;
+constexpr int64_t kStaticWords = kStaticBaseWords + 2 * kStaticListWords;  // about 8.1 MiB
+
+}  // namespace
+
+// Held by every GPU that loads the library, until the process exits.
+static __device__ __align__(256) int32_t g_hole_fill_scratch[kStaticWords];
+
+namespace {
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+int32_t* g_static_addr[kStaticMaxDevices];  // device address of g_hole_fill_scratch, per device
+
+// Device address of the scratch array on the current device, looked up on the first call
+// for that device.  In host code the array's name only stands in for the symbol; a kernel
+// must be given this address instead.
+int static_scratch(int32_t** out) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return OPPB_ERR_NO_DEVICE;
+    }
+    if (dev < 0 || dev >= kStaticMaxDevices) return OPPB_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_hole_fill_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return OPPB_ERR_LAUNCH;
+        }
+        g_static_addr[dev] = static_cast<int32_t*>(p);
+    }
+    *out = g_static_addr[dev];
+    return OPPB_OK;
+}
+
+}  // namespace
+}  // namespace oppb
+
+extern "C" int oppb_hole_fill_static(int32_t size, int32_t remove_count, const uint32_t* remove_bits,
+                                     int32_t stride, int32_t n_dats, const oppb_dat* dats, void* stream) {
+    using namespace oppb;
+    if (size < 0 || remove_count < 0 || stride < size || n_dats < 0 || n_dats > kMaxDats) return OPPB_ERR_ARG;
+    if (remove_count > OPPB_HOLE_FILL_STATIC_MAX_REMOVES) return OPPB_ERR_SCRATCH_LIMIT;
+    if (remove_count == 0 || size == 0) return OPPB_OK;
+    if (!remove_bits || !dats) return OPPB_ERR_ARG;
+    DatList dl{};
+    dl.n = n_dats;
+    dl.total_cols = 0;
+    for (int d = 0; d < n_dats; d++) {
+        if (!dats[d].data || dats[d].dim <= 0 || (dats[d].elem_bytes != 4 && dats[d].elem_bytes != 8))
+            return OPPB_ERR_ARG;
+        dl.data[d] = dats[d].data;
+        dl.dim[d] = dats[d].dim;
+        dl.bytes[d] = dats[d].elem_bytes;
+        dl.total_cols += dats[d].dim;
+    }
+    int32_t* scratch = nullptr;
+    const int rc = static_scratch(&scratch);
+    if (rc != OPPB_OK) return rc;
+    const int64_t n_words = ceil_div(size, 32);
+    const int n_blocks = ceil_div(n_words, kHfWords);  // <= kStaticMaxBlocks for any int32 size
+    int* block_base = scratch;
+    int32_t* hole_list = scratch + kStaticBaseWords;
+    int32_t* mover_list = hole_list + kStaticListWords;
+
+    cudaStream_t s = as_stream(stream);
+    hf_count_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base);
+    scan_single_block_kernel<<<1, kScanBlock, 0, s>>>(block_base, n_blocks);
     hf_emit_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base, n_blocks, remove_count,
                                                  hole_list, mover_list);
     count_launches(3);

@@ -18,6 +18,8 @@ OPPB_ERR_HOP_LIMIT = 4
 OPPB_ERR_CELL_RANGE = 5
 OPPB_ERR_CAPACITY = 6
 OPPB_ERR_NO_DEVICE = 7
+OPPB_ERR_SCRATCH_LIMIT = 8
+HOLE_FILL_STATIC_MAX_REMOVES = 1048576
 REMOVED_CELL = 2147483647
 
 c_i32, c_u32, c_i64, c_u64 = C.c_int32, C.c_uint32, C.c_int64, C.c_uint64
@@ -87,6 +89,7 @@ _SIGS = {
     "oppb_fill": (C.c_int, [c_vp, c_i64, c_i32, c_u64, c_vp]),
     "oppb_hole_fill_workspace_bytes": (C.c_size_t, [c_i32, c_i32]),
     "oppb_hole_fill": (C.c_int, [c_i32, c_i32, c_vp, c_i32, c_i32, P(Dat), c_vp, C.c_size_t, c_vp]),
+    "oppb_hole_fill_static": (C.c_int, [c_i32, c_i32, c_vp, c_i32, c_i32, P(Dat), c_vp]),
     "oppb_sort_workspace_bytes": (C.c_size_t, [c_i32, c_i32]),
     "oppb_sort_by_cell": (C.c_int, [c_i32, c_i32, c_i32, c_i32, P(Dat), c_i32, c_vp, c_vp, C.c_size_t, c_vp]),
     "oppb_fempic_box_mesh": (C.c_int, [c_i32, c_i32, c_i32, C.c_double, C.c_double, C.c_double, P(FemPICMesh)]),
