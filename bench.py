@@ -361,10 +361,44 @@ def arm_ours(args) -> dict:
 
 # ------------------------------------------------------------------------ reference arm
 
+def _reference_line(args, value: float, ms_per_step: float, particles_per_step: float, kind: str, cores: int,
+                    sample: str) -> dict:
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"first {args.ref_fill_steps} steps of injection (inlet region "
+                                                  f"at steady-state density), {round(particles_per_step)} "
+                                                  f"particles per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def arm_reference_compiled(args, hm, dist) -> dict:
+    """The compiled OP-PIC omp backend with the generated FemPIC loops (oracle/_ref), on
+    every host thread: per step inject -> push -> move with its finalize -> deposit, the
+    move (with hole fill / sort) and the deposit timed by the harness."""
+    from oracle import ref_runner as R
+
+    fill = args.ref_fill_steps
+    cores = len(os.sched_getaffinity(0))
+    out = R.run("omp", hm, dist, fill + args.warmup + args.steps, [], fill=CFG["fill"], period=CFG["period"],
+                alloc_mult=2.0, record_state=False, threads=cores, dt=CFG["dt"], qm=CFG["qm"],
+                ion_velocity=CFG["v_ion"], sigma=CFG["sigma"])
+    recs = out["records"][fill + args.warmup:]
+    t = float((recs["t_move"] + recs["t_deposit"]).sum())
+    ps = float(recs["size_before_move"].sum())
+    return _reference_line(args, ps / t, 1e3 * t / args.steps, ps / args.steps, "reference", cores,
+                           f"{fill}+{args.warmup} fill steps then {args.steps} timed steps; compiled OP-PIC omp "
+                           f"backend + generated FemPIC loops, OMP_NUM_THREADS={cores}")
+
+
 def arm_reference(args) -> dict:
     """The reference's CPU path on a bounded sample: config mesh, FILL steps of 250,000
     injected ions (the inlet region then holds the steady-state density), then
-    W + K steps, timing move + compaction + deposit."""
+    W + K steps, timing move + compaction + deposit.  The compiled reference (oracle/_ref)
+    when it is present, else the C oracle."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return {}
@@ -372,10 +406,13 @@ def arm_reference(args) -> dict:
 
     from oppb.fempic import HostMesh, injection_randoms
     from oracle import oracle as O
+    from oracle import ref_runner as R
 
     fill = args.ref_fill_steps
     hm = HostMesh(CFG["nx"], CFG["ny"], CFG["nz"], CFG["lx"], CFG["ly"], CFG["lz"])
     dist = hm.inject_distribution(CFG["inject"])
+    if R.available("omp"):
+        return arm_reference_compiled(args, hm, dist)
     orc = O.OracleFemPIC(hm, dist, ion_velocity=CFG["v_ion"], qm=CFG["qm"], dt=CFG["dt"], fill=CFG["fill"],
                          fill_period=CFG["period"], alloc_mult=2.0)
     for s in range(fill + args.warmup):
@@ -394,17 +431,8 @@ def arm_reference(args) -> dict:
         t += time.perf_counter() - t0
         orc.iter += 1
         ps += n_alive
-    value = ps / t
-    return {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"first {fill} steps of injection (inlet region at steady-state "
-                                                  f"density), {round(ps / args.steps)} particles per step"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": f"{fill}+{args.warmup} fill steps then {args.steps} timed steps; C oracle"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    return _reference_line(args, ps / t, 1e3 * t / args.steps, ps / args.steps, "port", 1,
+                           f"{fill}+{args.warmup} fill steps then {args.steps} timed steps; C oracle")
 
 
 def main():

@@ -6,7 +6,8 @@
 //   opp_inc_part_count_with_distribution -> inject_ions (+ thermal velocity from the case)
 //   -> reset n_charge_den -> calculate_new_pos_vel -> move (with its finalize) -> deposit.
 // The field is the static cell field of the case (no field solve).  Per step it records
-// sizes, FNV-1a hashes of the particle dats and of the node charges, and wall times.
+// sizes and wall times and, unless the case is a timing case (record_state 0), FNV-1a
+// hashes of the particle dats and of the node charges.
 //
 //   ref_harness <opp params file> <case file> <out file>
 //
@@ -208,12 +209,14 @@ int main(int argc, char** argv) {
             r.t_push = secs(t1, t2);
             r.t_move = secs(t2, t3);
             r.t_deposit = secs(t3, t4);
-            const size_t n = (size_t)r.size;
-            r.h_p2c = fnv1a(p2c_map->p2c_dat->data, n * sizeof(int));
-            r.h_pos = fnv1a(p_pos->data, n * 3 * sizeof(double));
-            r.h_vel = fnv1a(p_vel->data, n * 3 * sizeof(double));
-            r.h_lc = fnv1a(p_lc->data, n * 4 * sizeof(double));
-            r.h_charge = fnv1a(n_charge_den->data, nn * sizeof(double));
+            if (h.record_state) {  // timing cases (record_state 0) skip the per-step digests
+                const size_t n = (size_t)r.size;
+                r.h_p2c = fnv1a(p2c_map->p2c_dat->data, n * sizeof(int));
+                r.h_pos = fnv1a(p_pos->data, n * 3 * sizeof(double));
+                r.h_vel = fnv1a(p_vel->data, n * 3 * sizeof(double));
+                r.h_lc = fnv1a(p_lc->data, n * 4 * sizeof(double));
+                r.h_charge = fnv1a(n_charge_den->data, nn * sizeof(double));
+            }
             recs.push_back(r);
         }
 
