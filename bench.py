@@ -140,6 +140,8 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     if sampler:
         sampler.start()
     torch.cuda.synchronize()
+    # Profiler range = the timed steps (for `ncu --profile-from-start off`); no effect otherwise.
+    torch.cuda.profiler.start()
     ev_all0, ev_all1 = E(), E()
     ev_all0.record(s)
     for k in range(steps):
@@ -161,6 +163,7 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
         rec.append((n_alive, ev, kind, st.total_visits, st.recheck_count, st.remove_count))
     ev_all1.record(s)
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     clocks = sampler.stop() if sampler else None
     launches = lib.oppb_kernel_launches() - launches0
     total_ms = ev_all0.elapsed_time(ev_all1)

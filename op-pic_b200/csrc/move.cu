@@ -200,48 +200,51 @@ __device__ __forceinline__ void node_add(NodeTable& t, double* target, int node,
 }
 
 // Lanes with equal key form a group; the group's lowest lane sums the group's weights
-// (shuffle loop over the group members) and adds them to the cell's four nodes.
+// (shuffle loop over the group members) in FP64 and adds them to the cell's four nodes.
+// T is the weights' type: FP32 weights (mixed path) take half the shuffles of FP64 ones.
 // key < 0 = no contribution.  Every lane of the warp must call it.
-template <int kDep>
+template <int kDep, typename T>
 __device__ __forceinline__ void warp_deposit(const oppb_tet_mesh& m, NodeTable& t, double* target, int32_t key,
-                                             double l0, double l1, double l2, double l3) {
+                                             T l0, T l1, T l2, T l3) {
     const int lane = threadIdx.x & 31;
     const unsigned peers = __match_any_sync(kFullMask, key);
     const bool leader = (lane == __ffs(peers) - 1) && key >= 0;
     unsigned rest = leader ? (peers & ~(1u << lane)) : 0u;
+    double s0 = l0, s1 = l1, s2 = l2, s3 = l3;
     while (__any_sync(kFullMask, rest != 0)) {
         const int src = rest ? __ffs(rest) - 1 : lane;
-        const double a0 = __shfl_sync(kFullMask, l0, src);
-        const double a1 = __shfl_sync(kFullMask, l1, src);
-        const double a2 = __shfl_sync(kFullMask, l2, src);
-        const double a3 = __shfl_sync(kFullMask, l3, src);
+        const T a0 = __shfl_sync(kFullMask, l0, src);
+        const T a1 = __shfl_sync(kFullMask, l1, src);
+        const T a2 = __shfl_sync(kFullMask, l2, src);
+        const T a3 = __shfl_sync(kFullMask, l3, src);
         if (rest) {
-            l0 += a0;
-            l1 += a1;
-            l2 += a2;
-            l3 += a3;
+            s0 += a0;
+            s1 += a1;
+            s2 += a2;
+            s3 += a3;
             rest &= rest - 1;
         }
     }
     if (leader) {
         const int4 nodes = ldg_i4(m.c2n + (int64_t)key * 4);
         const uint32_t nn = (uint32_t)m.n_nodes;
-        if ((uint32_t)nodes.x < nn) node_add<kDep>(t, target, nodes.x, l0);
-        if ((uint32_t)nodes.y < nn) node_add<kDep>(t, target, nodes.y, l1);
-        if ((uint32_t)nodes.z < nn) node_add<kDep>(t, target, nodes.z, l2);
-        if ((uint32_t)nodes.w < nn) node_add<kDep>(t, target, nodes.w, l3);
+        if ((uint32_t)nodes.x < nn) node_add<kDep>(t, target, nodes.x, s0);
+        if ((uint32_t)nodes.y < nn) node_add<kDep>(t, target, nodes.y, s1);
+        if ((uint32_t)nodes.z < nn) node_add<kDep>(t, target, nodes.z, s2);
+        if ((uint32_t)nodes.w < nn) node_add<kDep>(t, target, nodes.w, s3);
     }
 }
 
 // Deposit epilogue shared by the move kernels.  Every thread of the CTA must call it.
-template <int kDep>
+template <int kDep, typename T>
 __device__ __forceinline__ void deposit_epilogue(const oppb_tet_mesh& m, NodeTable& table, const DepositArgs& d,
-                                                 bool dep, int32_t cell, const double l[4]) {
+                                                 bool dep, int32_t cell, const T l[4]) {
     if (kDep == kDepNone) return;
     double* target = deposit_target(d, m.n_nodes);
     if (kDep == kDepTable) __syncthreads();  // table initialised by every thread
-    warp_deposit<kDep>(m, table, target, dep ? cell : -1, dep ? l[0] : 0.0, dep ? l[1] : 0.0, dep ? l[2] : 0.0,
-                       dep ? l[3] : 0.0);
+    const T zero = 0;
+    warp_deposit<kDep, T>(m, table, target, dep ? cell : -1, dep ? l[0] : zero, dep ? l[1] : zero,
+                          dep ? l[2] : zero, dep ? l[3] : zero);
     if (kDep == kDepTable) {
         __syncthreads();
         const int k = table.keys[threadIdx.x];
@@ -249,13 +252,14 @@ __device__ __forceinline__ void deposit_epilogue(const oppb_tet_mesh& m, NodeTab
     }
 }
 
-__device__ __forceinline__ void store_result(const PartArgs& p, int64_t i, const double l[4], int visits,
+template <typename T>
+__device__ __forceinline__ void store_result(const PartArgs& p, int64_t i, const T l[4], int visits,
                                              int32_t cell, int32_t cell0) {
     if (visits > 0) {
-        st_stream(p.lc + i, l[0]);
-        st_stream(p.lc + p.stride + i, l[1]);
-        st_stream(p.lc + 2 * (int64_t)p.stride + i, l[2]);
-        st_stream(p.lc + 3 * (int64_t)p.stride + i, l[3]);
+        st_stream(p.lc + i, (double)l[0]);
+        st_stream(p.lc + p.stride + i, (double)l[1]);
+        st_stream(p.lc + 2 * (int64_t)p.stride + i, (double)l[2]);
+        st_stream(p.lc + 3 * (int64_t)p.stride + i, (double)l[3]);
     }
     if (cell != cell0) st_stream(p.p2c + i, cell);
 }
@@ -345,16 +349,18 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     int visits = 0;
     int rechecks = 0;
     int err = 0;
-    double l[4] = {0.0, 0.0, 0.0, 0.0};
-    if (active && cell != kRemoved) {
+    // The last visit's lambdas in FP32 (stored as p_lc and deposited: the mixed path keeps
+    // cell decisions exact, weights to FP32 precision).  lr receives the rare FP64
+    // re-evaluation; it lives in local memory because the out-of-line recheck writes it,
+    // so it is touched on that path only.
+    float lf[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    double lr[4];
+    if (active && cell != kRemoved && (uint32_t)cell >= (uint32_t)m.n_cells) err = OPPB_ERR_CELL_RANGE;
+    if (active && cell != kRemoved && !err) {
         const double x = ld_stream(p.pos + i);
         const double y = ld_stream(p.pos + p.stride + i);
         const double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
         for (;;) {
-            if ((uint32_t)cell >= (uint32_t)m.n_cells) {
-                err = OPPB_ERR_CELL_RANGE;
-                break;
-            }
             visits++;
             float nv[8], g0[8], g1[8];
             ldg256(m.nav32 + (int64_t)cell * 8, nv);
@@ -365,7 +371,6 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
             const float dz = (float)(z - (double)nv[2]);
             const float rows[16] = {g0[0], g0[1], g0[2], g0[3], g0[4], g0[5], g0[6], g0[7],
                                     g1[0], g1[1], g1[2], g1[3], g1[4], g1[5], g1[6], g1[7]};
-            float lf[4];
             float smax = 0.0f;
 #pragma unroll
             for (int k = 0; k < 4; k++) {
@@ -400,16 +405,14 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
                         if (k != mi && !(lf[k] - mv > band.tie)) ambiguous = true;
                 }
             }
-            bool in;
+            bool in = clear_in;
             if (ambiguous) {
                 rechecks++;
-                recheck_f64(m, cell, x, y, z, l);
-                in = inside_f64(l);
-                if (!in) mi = argmin4(l);
-            } else {
-                in = clear_in;
+                recheck_f64(m, cell, x, y, z, lr);
+                in = inside_f64(lr);
+                if (!in) mi = argmin4(lr);
 #pragma unroll
-                for (int k = 0; k < 4; k++) l[k] = (double)lf[k];
+                for (int k = 0; k < 4; k++) lf[k] = (float)lr[k];
             }
             if (in) break;
             // Re-read c2c[mi] from the record line just loaded (L1 hit) instead of keeping the
@@ -420,20 +423,24 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
                 status = kNeedRemove;
                 break;
             }
+            if ((uint32_t)next >= (uint32_t)m.n_cells) {
+                err = OPPB_ERR_CELL_RANGE;
+                break;
+            }
             cell = next;
             if (visits >= max_hops) {
                 err = OPPB_ERR_HOP_LIMIT;
                 break;
             }
         }
-        if (err) {
-            raise_error(st, err, (int32_t)i);
-            status = kFailed;
-        }
-        store_result(p, i, l, visits, cell, cell0);
     }
+    if (err) {
+        raise_error(st, err, (int32_t)i);
+        status = kFailed;
+    }
+    if (active && cell0 != kRemoved) store_result(p, i, lf, visits, cell, cell0);
     cta_account(p, st, i, active, cell, status == kNeedRemove, visits, rechecks);
-    deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, l);
+    deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, lf);
 }
 
 // ------------------------------------------------------------- standalone deposit

@@ -304,31 +304,43 @@ def test_fempic_steps_mixed():
     assert rechecks > 0
 
 
-def test_move_hop_limit_reports_error():
+def _move_once(kind, dm, ps, max_hops, hm):
+    """One move through the f64 entry point or the mixed move+deposit entry point."""
+    v = ps.view()
+    if kind == "f64":
+        return L.load().oppb_move_f64(C.byref(dm.s), C.byref(v), ps.status.data_ptr(), max_hops, None)
+    charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
+    ws = _dep_ws(hm.n_nodes)
+    return L.load().oppb_move_deposit_mixed(C.byref(dm.s), C.byref(v), charge.data_ptr(), ps.status.data_ptr(),
+                                            max_hops, 1e-5, ws.data_ptr(), ws.numel(), None)
+
+
+@pytest.mark.parametrize("kind", ["f64", "mixed"])
+def test_move_hop_limit_reports_error(kind):
     hm = mesh()
-    dm = DeviceMesh(hm, DEV, mixed=False)
+    dm = DeviceMesh(hm, DEV, mixed=kind == "mixed")
     pos = np.array([[0.95, 0.95, 3.9]])
     p2c = np.array([0], np.int32)  # far from the point: needs many hops
     ps = ParticleSet(DEV, 1)
     _set_particles(ps, pos, p2c)
-    v = ps.view()
-    L.check("move", L.load().oppb_move_f64(C.byref(dm.s), C.byref(v), ps.status.data_ptr(), 3, None))
+    L.check("move", _move_once(kind, dm, ps, 3, hm))
     st = ps.status_host()
     assert st.error == L.OPPB_ERR_HOP_LIMIT and st.error_index == 0
-    # the context stays usable
-    L.check("move", L.load().oppb_move_f64(C.byref(dm.s), C.byref(v), ps.status.data_ptr(), 4096, None))
+    # the context stays usable and the move resumes from where it stopped
+    L.check("move", _move_once(kind, dm, ps, 4096, hm))
     assert ps.status_host().error == 0
+    assert ps.host_aos()["p2c"][0] != REMOVED
 
 
-def test_move_bad_cell_reports_error():
+@pytest.mark.parametrize("kind", ["f64", "mixed"])
+def test_move_bad_cell_reports_error(kind):
     hm = mesh()
-    dm = DeviceMesh(hm, DEV, mixed=False)
+    dm = DeviceMesh(hm, DEV, mixed=kind == "mixed")
     ps = ParticleSet(DEV, 40)
     p2c = np.zeros(40, np.int32)
     p2c[13] = hm.n_cells + 5
     _set_particles(ps, np.full((40, 3), 0.05), p2c)
-    v = ps.view()
-    L.check("move", L.load().oppb_move_f64(C.byref(dm.s), C.byref(v), ps.status.data_ptr(), 4096, None))
+    L.check("move", _move_once(kind, dm, ps, 4096, hm))
     st = ps.status_host()
     assert st.error == L.OPPB_ERR_CELL_RANGE and st.error_index == 13
 
