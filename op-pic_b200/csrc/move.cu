@@ -134,14 +134,14 @@ __device__ __forceinline__ void cta_account(const PartArgs& p, oppb_move_status*
     const unsigned hole = __ballot_sync(kFullMask, active && final_cell == kRemoved);
     const unsigned rem = __ballot_sync(kFullMask, newly_removed);
     if (lane == 0 && i < p.size) p.remove_bits[i >> 5] = hole;
-    int vmax = visits, rsum = rechecks;
-    unsigned long long vsum = (unsigned long long)visits;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        vmax = max(vmax, __shfl_xor_sync(kFullMask, vmax, o));
-        vsum += __shfl_xor_sync(kFullMask, vsum, o);
-        rsum += __shfl_xor_sync(kFullMask, rsum, o);
-    }
+    // Warp reductions in the integer reduce unit (shuffles would load the L1 data pipe the
+    // visits are bound by).  The visit sum is taken in 16-bit halves so that 32 lanes
+    // cannot overflow 32 bits whatever max_hops is.
+    const int vmax = (int)__reduce_max_sync(kFullMask, (unsigned)visits);
+    const int rsum = (int)__reduce_add_sync(kFullMask, (unsigned)rechecks);
+    const unsigned long long vsum =
+        ((unsigned long long)__reduce_add_sync(kFullMask, (unsigned)visits >> 16) << 16) +
+        __reduce_add_sync(kFullMask, (unsigned)visits & 0xffffu);
     if (lane == 0) {
         s_sum[warp] = vsum;
         s_cnt[warp][0] = __popc(rem);
