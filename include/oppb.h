@@ -40,7 +40,8 @@ extern "C" {
 
 /* Device-resident tetrahedral mesh in the packed layout the kernels read: one cell
  * visit of the FP64 move is four 256-bit loads of `det` and one of `nav`; of the mixed
- * move two of `geo32` and one of `nav32`.  Filled by oppb_tet_mesh_pack(); buffers are
+ * move two of `geo32` (64 B), plus one 16-B read of the nav32 neighbours when the
+ * particle hops on.  Filled by oppb_tet_mesh_pack(); buffers are
  * owned by the caller and 32-byte aligned (oppb_tet_mesh_bytes gives the sizes).
  *   det   [n_cells][16] f64 : {alpha,beta,gamma,delta} of vertex 0..3
  *                             (minifempic_funcs.h:316-382 ordering), 128-B record
@@ -49,10 +50,12 @@ extern "C" {
  *                             boundary), then 8 unused bytes; 32-B record
  *   c2n   [n_cells][4]  i32 : cell -> node map (deposit)
  *   ef    [n_cells][4]  f64 : cell electric field x,y,z + pad
- *   geo32 [n_cells][16] f32 : mixed path, per vertex {lambda_i(o), dlambda_i/dx,
- *                             dlambda_i/dy, dlambda_i/dz} about origin o (may be NULL)
- *   nav32 [n_cells][8] 32-bit: mixed path origin o = vertex 0 rounded to f32 (3 floats),
- *                             one unused word, c2c[0..3] as int32 (may be NULL) */
+ *   geo32 [n_cells][16] f32 : mixed path, for vertices 0..2 {lambda_i(o), dlambda_i/dx,
+ *                             dlambda_i/dy, dlambda_i/dz} about origin o, then o = vertex 0
+ *                             rounded to f32 (3 floats) and one zero word; lambda_3 is
+ *                             1 - lambda_0 - lambda_1 - lambda_2 (may be NULL)
+ *   nav32 [n_cells][8] 32-bit: mixed path origin o (3 floats), one unused word,
+ *                             c2c[0..3] as int32 (may be NULL) */
 typedef struct oppb_tet_mesh {
     int32_t  n_cells;
     int32_t  n_nodes;

@@ -64,14 +64,16 @@ __global__ void pack_kernel(PackIn in, oppb_tet_mesh m, int32_t* invalid_out) {
         }
         if (m.geo32 && in.n_pos && in.c_det && in.c2n && nd.x >= 0 && nd.x < in.n_nodes) {
             // Origin: vertex 0 rounded to f32; lambda_i(o) and grad(lambda_i) from the
-            // FP64 coefficients, lambda_i(x) = coef*(alpha - beta*x + gamma*y - delta*z).
+            // FP64 coefficients, lambda_i(x) = coef*(alpha - beta*x + gamma*y - delta*z),
+            // for vertices 0..2 (the move derives lambda_3 from their sum), then o.
             const int64_t ps = in.n_pos_stride;
             const float ox = (float)in.n_pos[nd.x];
             const float oy = (float)in.n_pos[ps + nd.x];
             const float oz = (float)in.n_pos[2 * ps + nd.x];
             reinterpret_cast<float4*>(m.nav32 + c * 8)[0] = make_float4(ox, oy, oz, 0.0f);
+            reinterpret_cast<float4*>(m.geo32 + c * 16)[3] = make_float4(ox, oy, oz, 0.0f);
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
+            for (int i = 0; i < 3; i++) {
                 const double a = d[4 * i], b = d[4 * i + 1], g = d[4 * i + 2], e = d[4 * i + 3];
                 const double li = cf * (((a - b * (double)ox) + g * (double)oy) - e * (double)oz);
                 reinterpret_cast<float4*>(m.geo32 + c * 16)[i] =

@@ -4,9 +4,10 @@
 // One thread per particle; particles in SoA (stride = capacity).  A cell visit is a
 // dependent gather of the cell's record with 256-bit loads through the read-only path:
 // FP64 = 4 loads of the 128-B det record + 1 of the 32-B nav record {coef, c2c}; mixed =
-// 2 loads of the f32 lambda rows + 1 of {origin, c2c}.  Lanes of a warp are rarely in the
-// same cell, so every load instruction pays about one L1 sector per lane; the L1 data pipe
-// is what bounds the kernel, hence few wide loads per visit and a 32-register cap (full
+// 2 loads of the 64-B f32 record {3 lambda rows, origin}, + the 16-B c2c on a hop.  Lanes
+// of a warp share cells only while the particles are still close to their sorted order,
+// so a load instruction pays up to one L1 sector per lane; the L1 data pipe is what
+// bounds the kernel, hence few wide loads per visit and a 32-register cap (full
 // occupancy hides the dependent-gather latency).
 //
 // The FP64 arithmetic uses explicit round-to-nearest intrinsics so nothing is contracted
@@ -316,12 +317,16 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
 
 // -------------------------------------------------------- mixed FP32 / FP64 move
 //
-// lambda_i(x) = c_i + g_i . (x - o) with o = f32(vertex 0), c_i, g_i in f32.  The FP32
-// evaluation error is below 6 * 2^-24 * S, S = |c_i| + sum_j |g_ij| |d_j|.  A decision
-// is taken in FP32 only when every threshold (-1e-10, 1+1e-10) and, outside the cell,
-// every argmin tie is at least `band` away and S <= kMaxS; otherwise the visit is
-// recomputed with the FP64 reference expression.  Hence every decision equals the
-// FP64 one.
+// lambda_i(x) = c_i + g_i . (x - o) for i = 0..2 with o = f32(vertex 0), c_i, g_i in f32,
+// and lambda_3 = ((1 - lambda_0) - lambda_1) - lambda_2: a visit reads one 64-B record
+// (two sectors).  With u = 2^-24, d = f32(x - o) and S_i = |c_i| + sum_j |g_ij| |d_j|, the
+// FP32 error of lambda_0..2 is below 6u S_i (rounding of c, g, d and of the three FMAs),
+// and that of lambda_3 below 6u (S_0 + S_1 + S_2) + 3u (1 + S_0 + S_1 + S_2) (the three
+// subtractions), so below 9u (1 + S) with S = S_0 + S_1 + S_2.  For S <= kMaxS = 16 every
+// error is below 9.2e-6 < band = 1e-5.  A decision is taken in FP32 only when every
+// threshold (-1e-10, 1+1e-10) and, outside the cell, every argmin tie is at least `band`
+// away and S <= kMaxS; otherwise the visit is recomputed with the FP64 reference
+// expression.  Hence every decision equals the FP64 one.
 
 constexpr float kMaxS = 16.0f;
 
@@ -362,27 +367,26 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
         const double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
         for (;;) {
             visits++;
-            float nv[8], g0[8], g1[8];
-            ldg256(m.nav32 + (int64_t)cell * 8, nv);
+            float g0[8], g1[8];  // rows 0..2, then the origin
             ldg256(m.geo32 + (int64_t)cell * 16, g0);
             ldg256(m.geo32 + (int64_t)cell * 16 + 8, g1);
-            const float dx = (float)(x - (double)nv[0]);
-            const float dy = (float)(y - (double)nv[1]);
-            const float dz = (float)(z - (double)nv[2]);
-            const float rows[16] = {g0[0], g0[1], g0[2], g0[3], g0[4], g0[5], g0[6], g0[7],
-                                    g1[0], g1[1], g1[2], g1[3], g1[4], g1[5], g1[6], g1[7]};
-            float smax = 0.0f;
+            const float dx = (float)(x - (double)g1[4]);
+            const float dy = (float)(y - (double)g1[5]);
+            const float dz = (float)(z - (double)g1[6]);
+            const float rows[12] = {g0[0], g0[1], g0[2], g0[3], g0[4], g0[5], g0[6], g0[7],
+                                    g1[0], g1[1], g1[2], g1[3]};
+            float ssum = 0.0f;
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
+            for (int k = 0; k < 3; k++) {
                 const float c0 = rows[4 * k], gx = rows[4 * k + 1], gy = rows[4 * k + 2], gz = rows[4 * k + 3];
                 lf[k] = fmaf(gz, dz, fmaf(gy, dy, fmaf(gx, dx, c0)));
-                const float s = fabsf(c0) + fabsf(gx) * fabsf(dx) + fabsf(gy) * fabsf(dy) + fabsf(gz) * fabsf(dz);
-                smax = fmaxf(smax, s);
+                ssum += fabsf(c0) + fabsf(gx) * fabsf(dx) + fabsf(gy) * fabsf(dy) + fabsf(gz) * fabsf(dz);
             }
+            lf[3] = ((1.0f - lf[0]) - lf[1]) - lf[2];
             // Classify in FP32.
-            bool clear_in = smax <= kMaxS;
+            bool clear_in = ssum <= kMaxS;
             bool clear_out = false;
-            bool ambiguous = !(smax <= kMaxS);
+            bool ambiguous = !(ssum <= kMaxS);
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 clear_in = clear_in && (lf[k] >= band.lo) && (lf[k] <= band.in_hi);
@@ -415,8 +419,8 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
                 for (int k = 0; k < 4; k++) lf[k] = (float)lr[k];
             }
             if (in) break;
-            // Re-read c2c[mi] from the record line just loaded (L1 hit) instead of keeping the
-            // four neighbours live across the visit under the 32-register cap.
+            // The neighbour is read only when the particle hops on (16 B of nav32), so the
+            // last visit of a particle costs two sectors.
             const int32_t next = __ldg(reinterpret_cast<const int32_t*>(m.nav32 + (int64_t)cell * 8 + 4) + mi);
             if (next < 0) {
                 cell = kRemoved;

@@ -362,3 +362,42 @@ def test_move_deterministic():
         outs.append(ps.host_aos())
     np.testing.assert_array_equal(outs[0]["p2c"], outs[1]["p2c"])
     np.testing.assert_array_equal(outs[0]["lc"], outs[1]["lc"])
+
+
+@pytest.mark.parametrize("face", [0, 1, 2, 3])
+def test_move_mixed_cells_exact_at_faces(face):
+    """Points at barycentric distance t from the face opposite vertex `face` of their
+    start cell, t from 0 to +-3e-5, i.e. on both sides of the mixed path's 1e-5 band: the
+    mixed kernel (lambda_3 derived from the other three in FP32) must take exactly the FP64
+    oracle's cell decisions, rechecking in FP64 inside the band."""
+    hm = mesh()
+    dm = DeviceMesh(hm, DEV, mixed=True)
+    rng = np.random.default_rng(40 + face)
+    ts = np.array([0.0, 1e-12, -1e-12, 1e-9, -1e-9, 1e-7, -1e-7, 1e-6, -1e-6, 5e-6, -5e-6, 9e-6, -9e-6,
+                   1.2e-5, -1.2e-5, 3e-5, -3e-5])
+    per_t = 2000
+    n = per_t * len(ts)
+    cells = rng.integers(0, hm.n_cells, n).astype(np.int32)
+    b = rng.random((n, 4)) + 0.05
+    b[:, face] = 0.0
+    t = np.repeat(ts, per_t)
+    b *= ((1.0 - t) / b.sum(axis=1))[:, None]
+    b[:, face] = t
+    verts = hm.n_pos[hm.c2n[cells]]  # [n, 4, 3]
+    pos = np.einsum("nk,nkd->nd", b, verts)
+    ps = ParticleSet(DEV, n)
+    _set_particles(ps, pos, cells)
+    charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
+    ws = _dep_ws(hm.n_nodes)
+    v = ps.view()
+    L.check("mixed", L.load().oppb_move_deposit_mixed(C.byref(dm.s), C.byref(v), charge.data_ptr(),
+                                                      ps.status.data_ptr(), 4096, 1e-5, ws.data_ptr(), ws.numel(),
+                                                      None))
+    st = ps.status_host()
+    lc = np.zeros((n, 4))
+    p2c_o = cells.copy()
+    rc, visits, _ = O.move(pos, lc, p2c_o, hm.c2c, hm.c_vol, hm.c_det, n=n, max_hops=4096)
+    assert st.error == 0
+    np.testing.assert_array_equal(ps.host_aos()["p2c"], p2c_o)
+    assert st.remove_count == rc and int(st.total_visits) == visits
+    assert st.recheck_count > 0
