@@ -17,8 +17,9 @@ namespace {
 
 constexpr int kSortBlock = 256;
 constexpr int kSortWarps = kSortBlock / 32;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortBlock * kSortItems;  // 4096 keys
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortBlock * kSortItems;  // 2048 keys
+constexpr int kScatterMinBlocks = 5;  // 48 registers: the scatter is latency-bound, occupancy pays
 constexpr int kRadix = 256;
 constexpr int kMaxDats = 16;
 
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(PassIn in, int32
 // offsets: exclusive scan of hist (digit-major), i.e. the first output slot of
 // (digit, tile).  keys_out/vals_out receive the pass result.  On the last pass
 // keys_out is the p2c swap buffer (removed key mapped back to the removed cell).
-__global__ void __launch_bounds__(kSortBlock) radix_scatter_kernel(PassIn in, int32_t size, int32_t n_cells,
+__global__ void __launch_bounds__(kSortBlock, kScatterMinBlocks) radix_scatter_kernel(PassIn in, int32_t size, int32_t n_cells,
                                                                    int shift, int n_tiles,
                                                                    const int* __restrict__ offsets,
                                                                    uint32_t* __restrict__ keys_out,
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(kSortBlock) radix_scatter_kernel(PassIn in, in
     int32_t val[kSortItems];
     int off[kSortItems];
     const unsigned lt = lanemask_lt();
-    // Warp w ranks tile items [w*512, w*512+512) in 16 rounds of 32, in index order.
+    // Warp w ranks tile items [w*256, w*256+256) in 8 rounds of 32, in index order.
 #pragma unroll
     for (int r = 0; r < kSortItems; r++) {
         const int t = warp * (kSortItems * 32) + r * 32 + lane;
@@ -133,29 +134,40 @@ __global__ void __launch_bounds__(kSortBlock) radix_scatter_kernel(PassIn in, in
     }
 }
 
-struct GatherList {
+constexpr int kMaxCols = 16;  // gathered columns per launch
+
+// One column of a dat: element j of column c lives at src + (c * stride + j) * bytes.
+struct GatherCols {
     int32_t n;
-    const void* src[kMaxDats];
-    void* dst[kMaxDats];
-    int32_t dim[kMaxDats];
-    int32_t bytes[kMaxDats];
+    const char* src[kMaxCols];
+    char* dst[kMaxCols];
+    int32_t bytes[kMaxCols];
 };
 
-// dst[c][j] = src[c][perm[j]] for every dat other than the key dat.
-__global__ void __launch_bounds__(256) gather_kernel(int32_t size, int32_t stride, const int32_t* __restrict__ perm,
-                                                     GatherList g) {
+// dst[c][j] = src[c][perm[j]] for every column of every dat other than the key dat.
+// All loads of a particle are issued before its stores, so each thread keeps up to
+// kMaxCols loads in flight.
+__global__ void __launch_bounds__(256) gather_kernel(int32_t size, const int32_t* __restrict__ perm, GatherCols g) {
     const int64_t j = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (j >= size) return;
     const int64_t from = perm[j];
-    for (int d = 0; d < g.n; d++) {
-        if (g.bytes[d] == 8) {
-            const int64_t* s = reinterpret_cast<const int64_t*>(g.src[d]);
-            int64_t* t = reinterpret_cast<int64_t*>(g.dst[d]);
-            for (int c = 0; c < g.dim[d]; c++) __stcs(t + (int64_t)c * stride + j, __ldg(s + (int64_t)c * stride + from));
-        } else {
-            const int32_t* s = reinterpret_cast<const int32_t*>(g.src[d]);
-            int32_t* t = reinterpret_cast<int32_t*>(g.dst[d]);
-            for (int c = 0; c < g.dim[d]; c++) __stcs(t + (int64_t)c * stride + j, __ldg(s + (int64_t)c * stride + from));
+    uint64_t v[kMaxCols];
+#pragma unroll
+    for (int c = 0; c < kMaxCols; c++) {
+        if (c < g.n) {
+            if (g.bytes[c] == 8)
+                v[c] = (uint64_t)__ldg(reinterpret_cast<const long long*>(g.src[c]) + from);
+            else
+                v[c] = (uint32_t)__ldg(reinterpret_cast<const int*>(g.src[c]) + from);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kMaxCols; c++) {
+        if (c < g.n) {
+            if (g.bytes[c] == 8)
+                __stcs(reinterpret_cast<long long*>(g.dst[c]) + j, (long long)v[c]);
+            else
+                __stcs(reinterpret_cast<int*>(g.dst[c]) + j, (int)v[c]);
         }
     }
 }
@@ -207,17 +219,9 @@ extern "C" int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride, 
         return OPPB_ERR_ARG;
     const oppb_dat& kd = dats[key_dat];
     if (!kd.data || !kd.swap || kd.dim != 1 || kd.elem_bytes != 4) return OPPB_ERR_ARG;
-    GatherList g{};
-    for (int d = 0; d < n_dats; d++) {
+    for (int d = 0; d < n_dats; d++)
         if (!dats[d].data || !dats[d].swap || dats[d].dim <= 0 || (dats[d].elem_bytes != 4 && dats[d].elem_bytes != 8))
             return OPPB_ERR_ARG;
-        if (d == key_dat) continue;
-        g.src[g.n] = dats[d].data;
-        g.dst[g.n] = dats[d].swap;
-        g.dim[g.n] = dats[d].dim;
-        g.bytes[g.n] = dats[d].elem_bytes;
-        g.n++;
-    }
     if (size == 0) return OPPB_OK;
     if (!workspace || workspace_bytes < oppb_sort_workspace_bytes(size, n_cells)) return OPPB_ERR_WORKSPACE;
     cudaStream_t s = as_stream(stream);
@@ -244,8 +248,23 @@ extern "C" int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride, 
         count_launches(2);
         in = PassIn{nullptr, keys[p & 1], vals[p & 1]};
     }
+    GatherCols g{};
+    for (int d = 0; d < n_dats; d++) {
+        if (d == key_dat) continue;
+        for (int c = 0; c < dats[d].dim; c++) {
+            const size_t off = (size_t)c * stride * dats[d].elem_bytes;
+            g.src[g.n] = static_cast<const char*>(dats[d].data) + off;
+            g.dst[g.n] = static_cast<char*>(dats[d].swap) + off;
+            g.bytes[g.n] = dats[d].elem_bytes;
+            if (++g.n == kMaxCols) {
+                gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(size, perm, g);
+                count_launches(1);
+                g.n = 0;
+            }
+        }
+    }
     if (g.n > 0) {
-        gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(size, stride, perm, g);
+        gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(size, perm, g);
         count_launches(1);
     }
     return launch_status();
