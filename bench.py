@@ -42,11 +42,16 @@ CFG = dict(nx=48, ny=48, nz=192, lx=1.0, ly=1.0, lz=4.0, inject=250_000, sigma=0
 WORKLOAD = ("FemPIC electrostatic tet-mesh PIC, 48x48x192 hexes x 6 = 2,654,208 tets, 463,393 nodes; "
             "250,000 ions/step; steady state after 300 fill steps; Sort_Periodic period 10")
 # Algorithmic bytes per move+deposit launch: per particle read pos 24 + p2c 4, write p2c 4 + p_lc 32;
-# per cell the record read once (FP64: det 128 + coef 8 + c2c 16 + c2n 16; mixed: origin 16 +
-# f32 lambda rows 64 + c2c/c2n 32); per node one FP64 read-modify-write.
+# per cell the record read once (FP64: det 128 + nav {coef, c2c, pad} 32 + c2n 16; mixed: the
+# 64-B f32 record {3 lambda rows, origin} + c2c 16 + c2n 16); per node one FP64 read-modify-write.
 BYTES_PER_PARTICLE = 64
-BYTES_PER_CELL = {"f64": 168, "mixed": 112}
+BYTES_PER_CELL = {"f64": 168, "mixed": 96}
 BYTES_PER_NODE = 16
+# DRAM bytes per particle of one move+deposit launch (dram__bytes_read.sum + dram__bytes_write.sum),
+# from an ncu capture of full-size launches of this workload: profiles/move_mixed_kernel_fempic_48x48x192.txt
+# and profiles/move_f64_kernel_fempic_48x48x192.txt.
+MEASURED_DRAM_BYTES_PER_PARTICLE = {"f64": 73.0, "mixed": 70.0}
+TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of full-size launches, per particle x particles"
 
 
 def log(*a):
@@ -351,7 +356,9 @@ def arm_ours(args) -> dict:
         "roofline": {"bound": "hbm", "kernel": "move_mixed_kernel (move + fused deposit)",
                      "achieved": mixed["move_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": mixed["move_gbs"] / peaks["hbm_gbs"], "peak_source": peaks["source"],
-                     "bytes_per_launch": mixed["move_bytes_per_launch"], "traffic": None},
+                     "bytes_per_launch": mixed["move_bytes_per_launch"],
+                     "traffic": MEASURED_DRAM_BYTES_PER_PARTICLE["mixed"] * mixed["mean_particles"],
+                     "traffic_source": TRAFFIC_SOURCE},
         "gpu_launches": mixed["launches"],
         "clocks": mixed["clocks"],
     }
