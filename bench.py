@@ -150,9 +150,10 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     ev_all0, ev_all1 = E(), E()
     ev_all0.record(s)
     for k in range(steps):
-        ev = [E() for _ in range(4)]
+        ev = [E() for _ in range(5)]
         sim.inject(tables[k % len(tables)])
         sim.node_charge.zero_()
+        ev[4].record(s)
         sim.push()
         n_alive = sim.parts.size
         ev[0].record(s)
@@ -174,6 +175,7 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     total_ms = ev_all0.elapsed_time(ev_all1)
     t_move = [r[1][0].elapsed_time(r[1][1]) for r in rec]
     t_comp = [r[1][2].elapsed_time(r[1][3]) for r in rec]
+    t_push = [r[1][4].elapsed_time(r[1][0]) for r in rec]
     n = [r[0] for r in rec]
     ps = sum(n)
     out = {
@@ -199,6 +201,33 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     out["move_gbs"] = sum(bytes_per_launch) / (sum(t_move) / 1e3) / 1e9
     out["move_bytes_per_launch"] = sum(bytes_per_launch) / steps
     out["move_ms_per_launch"] = sum(t_move) / steps
+    out["push_ms_per_launch"] = sum(t_push) / steps
+    out["push_inclusive"] = ps / ((sum(t_push) + sum(t_move) + sum(t_comp)) / 1e3)
+
+    # The push fused into the move kernel as its prologue (one launch per step): push +
+    # move + deposit + compaction, device time, on the following steps.
+    n_fused = min(steps, 20)
+    ps_f, t_f = 0, 0.0
+    for k in range(n_fused):
+        ev = [E() for _ in range(4)]
+        sim.inject(tables[k % len(tables)])
+        sim.node_charge.zero_()
+        n_alive = sim.parts.size
+        ev[0].record(s)
+        sim.push_move()
+        ev[1].record(s)
+        st = sim.parts.status_host()
+        if st.error:
+            raise L.OppbError("push_move", st.error)
+        ev[2].record(s)
+        sim.finalize(st.remove_count)
+        ev[3].record(s)
+        sim.iter += 1
+        torch.cuda.synchronize()
+        ps_f += n_alive
+        t_f += ev[0].elapsed_time(ev[1]) + ev[2].elapsed_time(ev[3])
+    out["push_inclusive_fused"] = ps_f / (t_f / 1e3)
+    out["fused_steps"] = n_fused
 
     if e2e_steps:
         # End to end: host inputs (pinned) copied in, node charges + status copied out, every step.
@@ -352,6 +381,10 @@ def arm_ours(args) -> dict:
         "mixed": {"value": mixed["job_value"], "move_only": mixed["move_only"], "whole_step": mixed["whole_step"],
                   "move_ms_per_launch": mixed["move_ms_per_launch"], "recheck_frac": mixed["recheck_frac"],
                   "visits_per_particle": mixed["visits_per_particle"]},
+        "push_inclusive": {"unit": UNIT, "what": "push + move + deposit + compaction, device time",
+                           "mixed_unfused": mixed["push_inclusive"], "mixed_fused": mixed["push_inclusive_fused"],
+                           "f64_unfused": f64["push_inclusive"], "f64_fused": f64["push_inclusive_fused"],
+                           "fused_steps": mixed["fused_steps"]},
         "mixed_over_plain": mixed["job_value"] / f64["job_value"],
         "roofline": {"bound": "hbm", "kernel": "move_mixed_kernel (move + fused deposit)",
                      "achieved": mixed["move_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",

@@ -183,11 +183,27 @@ int oppb_move_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts
 /* Mixed-precision move + deposit: barycentric tests in FP32 about a per-cell origin;
  * any particle whose decision lies within `band` of a threshold or tie is re-evaluated
  * with the FP64 reference formula, so cell assignment, hop counts and removals stay
- * bit-identical to oppb_move_deposit_f64.  p_lc of non-rechecked particles carries
- * FP32 accuracy; node totals accumulate in FP64.  Needs mesh->geo32/nav32. */
+ * bit-identical to oppb_move_deposit_f64.  p_lc carries FP32 accuracy (within 1e-5 of
+ * FP64); node totals accumulate in FP64.  Needs mesh->geo32/nav32. */
 int oppb_move_deposit_mixed(const oppb_tet_mesh* mesh, const oppb_particles* parts,
                             double* node_charge, oppb_move_status* status, int32_t max_hops,
                             double band, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Push fused into the move as its once-per-particle prologue (the OPP_DO_ONCE pattern,
+ * opp_lib/include/opp_seq.h:64): calculate_new_pos_vel_kernel (apps/app_fempic/kernels.h:93-103,
+ * replacing opp_par_loop_all__calculate_new_pos_vel_kernel) on every particle with a valid
+ * cell, then the move + deposit of the entry points above on the pushed position held in
+ * registers.  p_pos and p_vel are written; results are bit-identical to oppb_push_f64 +
+ * oppb_move_deposit_f64 (oppb_push_mixed + oppb_move_deposit_mixed for the mixed form).
+ * Needs parts->vel and mesh->ef. */
+int oppb_push_move_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                               double* node_charge, oppb_move_status* status, int32_t max_hops,
+                               double charge_over_mass, double dt,
+                               void* workspace, size_t workspace_bytes, void* stream);
+int oppb_push_move_deposit_mixed(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                                 double* node_charge, oppb_move_status* status, int32_t max_hops,
+                                 double band, double charge_over_mass, double dt,
+                                 void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------- deposit */
 

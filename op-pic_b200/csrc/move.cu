@@ -40,10 +40,19 @@ enum : int { kDone = 0, kNeedMove = 1, kNeedRemove = 2, kFailed = 3 };
 struct PartArgs {
     int32_t size;
     int32_t stride;
-    const double* pos;
+    double* pos;          // written only by the fused push
+    double* vel;          // fused push only
     double* lc;
     int32_t* p2c;
     uint32_t* remove_bits;
+};
+
+// Push prologue of the fused entry points: calculate_new_pos_vel_kernel
+// (apps/app_fempic/kernels.h:93-103) run on the particle's registers before its walk, the
+// role OPP_DO_ONCE gives a push inside a move loop (opp_lib/include/opp_seq.h:64).
+struct PushArgs {
+    double qm, dt;     // FP64 push
+    float qmdt, dtf;   // mixed push: f32(q/m*dt), f32(dt)
 };
 
 // Node-sum target of this CTA: copy (blockIdx.x % replicas).
@@ -265,11 +274,43 @@ __device__ __forceinline__ void store_result(const PartArgs& p, int64_t i, const
     if (cell != cell0) st_stream(p.p2c + i, cell);
 }
 
+// v += (q/m) dt E[cell]; x += v dt, stored back and left in x, y, z.  The operation order
+// and rounding are those of push_f64_kernel (FP64) and push_mixed_kernel (FP32 increments on
+// FP64 state), so a fused step is bit-identical to push + move.
+template <bool kMixed>
+__device__ __forceinline__ void push_prologue(const oppb_tet_mesh& m, const PartArgs& p, const PushArgs& a,
+                                              int64_t i, int32_t cell, double& x, double& y, double& z) {
+    const double2 e01 = ldg_d2(m.ef + (int64_t)cell * 4);
+    const double2 e2_ = ldg_d2(m.ef + (int64_t)cell * 4 + 2);
+    const double e[3] = {e01.x, e01.y, e2_.x};
+    double xs[3] = {x, y, z};
+    const double coefficient1 = __dmul_rn(a.qm, a.dt);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        double* vp = p.vel + (int64_t)d * p.stride + i;
+        double v;
+        if (kMixed) {
+            const float dv = __fmul_rn(a.qmdt, __double2float_rn(e[d]));
+            v = __dadd_rn(ld_stream(vp), (double)dv);
+            xs[d] = __dadd_rn(xs[d], (double)__fmul_rn(__double2float_rn(v), a.dtf));
+        } else {
+            v = __dadd_rn(ld_stream(vp), __dmul_rn(coefficient1, e[d]));
+            xs[d] = __dadd_rn(xs[d], __dmul_rn(v, a.dt));
+        }
+        st_stream(vp, v);
+        st_stream(p.pos + (int64_t)d * p.stride + i, xs[d]);
+    }
+    x = xs[0];
+    y = xs[1];
+    z = xs[2];
+}
+
 // ------------------------------------------------------------------ FP64 move
 
-template <int kDep>
+template <int kDep, bool kPush>
 __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
-    move_f64_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops) {
+    move_f64_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
+                    PushArgs push) {
     __shared__ NodeTable table;
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
@@ -281,9 +322,10 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     int err = 0;
     double l[4] = {0.0, 0.0, 0.0, 0.0};
     if (active && cell != kRemoved) {
-        const double x = ld_stream(p.pos + i);
-        const double y = ld_stream(p.pos + p.stride + i);
-        const double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
+        double x = ld_stream(p.pos + i);
+        double y = ld_stream(p.pos + p.stride + i);
+        double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
+        if (kPush && (uint32_t)cell < (uint32_t)m.n_cells) push_prologue<false>(m, p, push, i, cell, x, y, z);
         for (;;) {
             if ((uint32_t)cell >= (uint32_t)m.n_cells) {
                 err = OPPB_ERR_CELL_RANGE;
@@ -340,10 +382,10 @@ struct Band {
     float tie;     // 2 * band
 };
 
-template <int kDep>
+template <int kDep, bool kPush>
 __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     move_mixed_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
-                      Band band) {
+                      Band band, PushArgs push) {
     __shared__ NodeTable table;
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
@@ -362,9 +404,10 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     double lr[4];
     if (active && cell != kRemoved && (uint32_t)cell >= (uint32_t)m.n_cells) err = OPPB_ERR_CELL_RANGE;
     if (active && cell != kRemoved && !err) {
-        const double x = ld_stream(p.pos + i);
-        const double y = ld_stream(p.pos + p.stride + i);
-        const double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
+        double x = ld_stream(p.pos + i);
+        double y = ld_stream(p.pos + p.stride + i);
+        double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
+        if (kPush) push_prologue<true>(m, p, push, i, cell, x, y, z);
         for (;;) {
             visits++;
             float g0[8], g1[8];  // rows 0..2, then the origin
@@ -495,7 +538,7 @@ int check_parts(const oppb_particles* p, bool need_bits) {
 }
 
 PartArgs part_args(const oppb_particles* p) {
-    return PartArgs{p->size, p->stride, p->pos, p->lc, p->p2c, p->remove_bits};
+    return PartArgs{p->size, p->stride, p->pos, p->vel, p->lc, p->p2c, p->remove_bits};
 }
 
 int replicas_for(size_t workspace_bytes, const void* workspace, int32_t n_nodes) {
@@ -528,37 +571,44 @@ Replicas make_replicas(double* node_charge, void* workspace, size_t workspace_by
     return Replicas{DepositArgs{node_charge, r > 1 ? static_cast<double*>(workspace) : nullptr, r}, n_nodes};
 }
 
-template <int kKind>  // 0 move, 1 move+deposit, 2 mixed move+deposit
+enum MoveKind { kMoveOnly, kMoveDepositF64, kMoveDepositMixed };
+
+template <int kKind, bool kPush>
 int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
-                oppb_move_status* status, int32_t max_hops, double band, void* workspace, size_t ws_bytes,
-                void* stream) {
-    int rc = check_mesh(mesh, kKind == 2, kKind != 0);
+                oppb_move_status* status, int32_t max_hops, double band, const PushArgs& push, void* workspace,
+                size_t ws_bytes, void* stream) {
+    constexpr bool kMixed = kKind == kMoveDepositMixed;
+    int rc = check_mesh(mesh, kMixed, kKind != kMoveOnly);
     if (rc) return rc;
     rc = check_parts(parts, true);
     if (rc) return rc;
     if (!status || max_hops <= 0) return OPPB_ERR_ARG;
-    if (kKind != 0 && !node_charge) return OPPB_ERR_ARG;
-    if (kKind == 2 && !(band > 0.0 && band < 0.25)) return OPPB_ERR_ARG;
+    if (kKind != kMoveOnly && !node_charge) return OPPB_ERR_ARG;
+    if (kMixed && !(band > 0.0 && band < 0.25)) return OPPB_ERR_ARG;
+    if (kPush && (!parts->vel || !mesh->ef || !aligned(mesh->ef, 16))) return OPPB_ERR_ARG;
     cudaStream_t s = as_stream(stream);
     if (cudaMemsetAsync(status, 0, sizeof(oppb_move_status), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
     if (parts->size == 0) return launch_status();
     const PartArgs p = part_args(parts);
     const int grid = ceil_div(parts->size, kMoveBlock);
-    Replicas rep = make_replicas(node_charge, kKind == 0 ? nullptr : workspace, ws_bytes, mesh->n_nodes);
+    Replicas rep = make_replicas(node_charge, kKind == kMoveOnly ? nullptr : workspace, ws_bytes, mesh->n_nodes);
     if ((rc = rep.begin(s))) return rc;
     const bool table = tuning().deposit == OPPB_DEPOSIT_CTA_TABLE;
     const float bf = (float)band;
     const Band bd{bf, -bf, 1.0f - bf, 1.0f + bf, 2.0f * bf};
-    if (kKind == 0)
-        move_f64_kernel<kDepNone><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops);
-    else if (kKind == 1 && table)
-        move_f64_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops);
-    else if (kKind == 1)
-        move_f64_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops);
-    else if (table)
-        move_mixed_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, bd);
+    if constexpr (kKind == kMoveOnly)
+        move_f64_kernel<kDepNone, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, push);
+    else if constexpr (kKind == kMoveDepositF64) {
+        if (table)
+            move_f64_kernel<kDepTable, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, push);
+        else
+            move_f64_kernel<kDepWarp, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, push);
+    } else if (table)
+        move_mixed_kernel<kDepTable, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, bd,
+                                                                        push);
     else
-        move_mixed_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, bd);
+        move_mixed_kernel<kDepWarp, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, bd,
+                                                                       push);
     count_launches(1);
     rep.end(s);
     return launch_status();
@@ -575,20 +625,41 @@ extern "C" size_t oppb_deposit_workspace_bytes(int32_t n_nodes) {
 
 extern "C" int oppb_move_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts, oppb_move_status* status,
                              int32_t max_hops, void* stream) {
-    return oppb::launch_move<0>(mesh, parts, nullptr, status, max_hops, 0.0, nullptr, 0, stream);
+    return oppb::launch_move<oppb::kMoveOnly, false>(mesh, parts, nullptr, status, max_hops, 0.0, oppb::PushArgs{},
+                                                    nullptr, 0, stream);
 }
 
 extern "C" int oppb_move_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
                                      oppb_move_status* status, int32_t max_hops, void* workspace,
                                      size_t workspace_bytes, void* stream) {
-    return oppb::launch_move<1>(mesh, parts, node_charge, status, max_hops, 0.0, workspace, workspace_bytes, stream);
+    return oppb::launch_move<oppb::kMoveDepositF64, false>(mesh, parts, node_charge, status, max_hops, 0.0,
+                                                          oppb::PushArgs{}, workspace, workspace_bytes, stream);
 }
 
 extern "C" int oppb_move_deposit_mixed(const oppb_tet_mesh* mesh, const oppb_particles* parts,
                                        double* node_charge, oppb_move_status* status, int32_t max_hops,
                                        double band, void* workspace, size_t workspace_bytes, void* stream) {
-    return oppb::launch_move<2>(mesh, parts, node_charge, status, max_hops, band, workspace, workspace_bytes,
-                                stream);
+    return oppb::launch_move<oppb::kMoveDepositMixed, false>(mesh, parts, node_charge, status, max_hops, band,
+                                                            oppb::PushArgs{}, workspace, workspace_bytes, stream);
+}
+
+extern "C" int oppb_push_move_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                                          double* node_charge, oppb_move_status* status, int32_t max_hops,
+                                          double charge_over_mass, double dt, void* workspace,
+                                          size_t workspace_bytes, void* stream) {
+    const oppb::PushArgs push{charge_over_mass, dt, 0.0f, 0.0f};
+    return oppb::launch_move<oppb::kMoveDepositF64, true>(mesh, parts, node_charge, status, max_hops, 0.0, push,
+                                                         workspace, workspace_bytes, stream);
+}
+
+extern "C" int oppb_push_move_deposit_mixed(const oppb_tet_mesh* mesh, const oppb_particles* parts,
+                                            double* node_charge, oppb_move_status* status, int32_t max_hops,
+                                            double band, double charge_over_mass, double dt, void* workspace,
+                                            size_t workspace_bytes, void* stream) {
+    // The same FP32 coefficients as oppb_push_mixed: f32(q/m * dt) and f32(dt).
+    const oppb::PushArgs push{charge_over_mass, dt, (float)(charge_over_mass * dt), (float)dt};
+    return oppb::launch_move<oppb::kMoveDepositMixed, true>(mesh, parts, node_charge, status, max_hops, band, push,
+                                                           workspace, workspace_bytes, stream);
 }
 
 extern "C" int oppb_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,

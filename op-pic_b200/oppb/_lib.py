@@ -80,6 +80,10 @@ _SIGS = {
     "oppb_move_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, c_vp, C.c_size_t, c_vp]),
     "oppb_move_deposit_mixed": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, C.c_double, c_vp,
                                           C.c_size_t, c_vp]),
+    "oppb_push_move_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, C.c_double, C.c_double,
+                                             c_vp, C.c_size_t, c_vp]),
+    "oppb_push_move_deposit_mixed": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, c_i32, C.c_double, C.c_double,
+                                               C.c_double, c_vp, C.c_size_t, c_vp]),
     "oppb_deposit_f64": (C.c_int, [P(TetMesh), P(Particles), c_vp, c_vp, C.c_size_t, c_vp]),
     "oppb_push_f64": (C.c_int, [P(TetMesh), P(Particles), C.c_double, C.c_double, c_vp]),
     "oppb_push_mixed": (C.c_int, [P(TetMesh), P(Particles), C.c_double, C.c_double, c_vp]),

@@ -227,7 +227,8 @@ class FemPIC:
     def __init__(self, hm: HostMesh, device: torch.device | str = "cuda", inject_per_step: int = 2000,
                  ion_velocity: float = 1.0, qm: float = 1.0, dt: float = 0.01, precision: str = "f64",
                  fill: str = "HoleFill_All", fill_period: int = 10, alloc_mult: float = 2.0,
-                 capacity: int = 0, max_hops: int = 4096, band: float = 1e-5, fused_deposit: bool = True):
+                 capacity: int = 0, max_hops: int = 4096, band: float = 1e-5, fused_deposit: bool = True,
+                 fused_push: bool = True):
         if not torch.cuda.is_available():
             raise RuntimeError("FemPIC needs a CUDA device (there is no CPU fallback)")
         self.device = torch.device(device)
@@ -243,6 +244,8 @@ class FemPIC:
         self.fill, self.fill_period = fill, fill_period
         self.max_hops, self.band = max_hops, band
         self.fused_deposit = fused_deposit
+        # push as the prologue of the move kernel (one launch); needs the deposit fused too
+        self.fused_push = fused_push and (fused_deposit or precision == "mixed")
         self.node_charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=self.device)
         self.iter = 0
         self._ws = torch.empty(0, dtype=torch.uint8, device=self.device)
@@ -295,6 +298,22 @@ class FemPIC:
             rc = self.lib.oppb_move_f64(C.byref(self.mesh.s), C.byref(v), st, self.max_hops, sp)
         L.check("oppb_move", rc)
 
+    def push_move(self, stream=None) -> None:
+        """Push + move + deposit in one launch (the push is the move kernel's prologue);
+        bit-identical to push() followed by move()."""
+        v = self.parts.view()
+        st = _ptr(self.parts.status)
+        sp = _stream_ptr(stream)
+        ws = self._deposit_ws()
+        if self.precision == "mixed":
+            rc = self.lib.oppb_push_move_deposit_mixed(C.byref(self.mesh.s), C.byref(v), _ptr(self.node_charge), st,
+                                                       self.max_hops, self.band, self.qm, self.dt, _ptr(ws),
+                                                       ws.numel(), sp)
+        else:
+            rc = self.lib.oppb_push_move_deposit_f64(C.byref(self.mesh.s), C.byref(v), _ptr(self.node_charge), st,
+                                                     self.max_hops, self.qm, self.dt, _ptr(ws), ws.numel(), sp)
+        L.check("oppb_push_move_deposit", rc)
+
     def deposit(self, stream=None) -> None:
         v = self.parts.view()
         ws = self._deposit_ws()
@@ -341,12 +360,14 @@ class FemPIC:
         self.inject(rnd_soa, stream)
         self.node_charge.zero_()
         if ev: ev[1].record(s)
-        self.push(stream)
-        if ev: ev[2].record(s)
         n_before = self.parts.size
-        self.move(stream)
-        if not self.fused_deposit and self.precision == "f64":
-            pass  # deposit after compaction, as the reference loop order
+        if self.fused_push:
+            if ev: ev[2].record(s)
+            self.push_move(stream)  # push time is counted in move_ms
+        else:
+            self.push(stream)
+            if ev: ev[2].record(s)
+            self.move(stream)  # unfused FP64 deposit runs after the compaction, as the reference loop order
         if ev: ev[3].record(s)
         st = self.parts.status_host()
         if st.error:

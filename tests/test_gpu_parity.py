@@ -245,9 +245,10 @@ def test_sort_matches_oracle(n, n_cells, frac, seed):
         np.testing.assert_array_equal(got[name].view(np.uint8), dats[k].view(np.uint8), err_msg=name)
 
 
-def _run_both(precision, fill, steps, inject, seed=0, period=5):
+def _run_both(precision, fill, steps, inject, seed=0, period=5, fused_push=True):
     hm = mesh()
-    sim = FemPIC(hm, DEV, inject_per_step=inject, precision=precision, fill=fill, fill_period=period)
+    sim = FemPIC(hm, DEV, inject_per_step=inject, precision=precision, fill=fill, fill_period=period,
+                 fused_push=fused_push)
     orc = O.OracleFemPIC(hm, sim.dist_host, fill=fill, fill_period=period, mixed=(precision == "mixed"))
     for s in range(steps):
         rnd = injection_randoms(seed, s, inject, 0.1)
@@ -259,10 +260,11 @@ def _run_both(precision, fill, steps, inject, seed=0, period=5):
         yield s, sim, orc
 
 
+@pytest.mark.parametrize("fused_push", [True, False])
 @pytest.mark.parametrize("fill", ["HoleFill_All", "Sort_Periodic"])
-def test_fempic_steps_f64(fill):
+def test_fempic_steps_f64(fill, fused_push):
     last = None
-    for s, sim, orc in _run_both("f64", fill, 60, 2000):
+    for s, sim, orc in _run_both("f64", fill, 60, 2000, fused_push=fused_push):
         if s % 10 == 9 or s == 0:
             got = sim.parts.host_aos()
             n = orc.size
@@ -286,11 +288,12 @@ def test_fempic_steps_unfused_deposit():
     _charge_close(sim.node_charge.cpu().numpy(), orc.node_charge, CHARGE_RTOL)
 
 
-def test_fempic_steps_mixed():
+@pytest.mark.parametrize("fused_push", [True, False])
+def test_fempic_steps_mixed(fused_push):
     """Mixed precision: same cells, counts and hop totals as the oracle running the same
     FP32 push with FP64 cell decisions; weights and node charges within stated bounds."""
     rechecks = 0
-    for s, sim, orc in _run_both("mixed", "HoleFill_All", 40, 2000, seed=2):
+    for s, sim, orc in _run_both("mixed", "HoleFill_All", 40, 2000, seed=2, fused_push=fused_push):
         rechecks += sim.last["rechecks"]
         if s % 10 == 9:
             got = sim.parts.host_aos()
@@ -401,3 +404,47 @@ def test_move_mixed_cells_exact_at_faces(face):
     np.testing.assert_array_equal(ps.host_aos()["p2c"], p2c_o)
     assert st.remove_count == rc and int(st.total_visits) == visits
     assert st.recheck_count > 0
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_push_move_fused_equals_push_then_move(precision):
+    """oppb_push_move_deposit_* against oppb_push_* followed by oppb_move_deposit_* on the
+    same state: positions, velocities, weights and cells bit-identical, node charges within
+    the FP64 atomic-order tolerance."""
+    hm = mesh()
+    dm = DeviceMesh(hm, DEV, mixed=precision == "mixed")
+    pos, p2c = random_particles(hm, 300_007, 31)
+    vel = np.random.default_rng(32).normal(0.0, 0.5, (len(p2c), 3))
+    lib = L.load()
+    outs = []
+    for fused in (False, True):
+        ps = ParticleSet(DEV, len(p2c))
+        _set_particles(ps, pos, p2c, vel)
+        charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
+        ws = _dep_ws(hm.n_nodes)
+        v = ps.view()
+        if fused and precision == "f64":
+            rc = lib.oppb_push_move_deposit_f64(C.byref(dm.s), C.byref(v), charge.data_ptr(), ps.status.data_ptr(),
+                                                4096, 1.0, 0.01, ws.data_ptr(), ws.numel(), None)
+        elif fused:
+            rc = lib.oppb_push_move_deposit_mixed(C.byref(dm.s), C.byref(v), charge.data_ptr(),
+                                                  ps.status.data_ptr(), 4096, 1e-5, 1.0, 0.01, ws.data_ptr(),
+                                                  ws.numel(), None)
+        else:
+            push = lib.oppb_push_f64 if precision == "f64" else lib.oppb_push_mixed
+            L.check("push", push(C.byref(dm.s), C.byref(v), 1.0, 0.01, None))
+            if precision == "f64":
+                rc = lib.oppb_move_deposit_f64(C.byref(dm.s), C.byref(v), charge.data_ptr(), ps.status.data_ptr(),
+                                               4096, ws.data_ptr(), ws.numel(), None)
+            else:
+                rc = lib.oppb_move_deposit_mixed(C.byref(dm.s), C.byref(v), charge.data_ptr(),
+                                                 ps.status.data_ptr(), 4096, 1e-5, ws.data_ptr(), ws.numel(), None)
+        L.check("move", rc)
+        st = ps.status_host()
+        assert st.error == 0
+        outs.append((ps.host_aos(), charge.cpu().numpy(), st.remove_count, int(st.total_visits)))
+    (a, qa, ra, va), (b, qb, rb, vb) = outs
+    assert (ra, va) == (rb, vb)
+    for name in ("pos", "vel", "lc", "p2c"):
+        np.testing.assert_array_equal(a[name].view(np.uint8), b[name].view(np.uint8), err_msg=name)
+    _charge_close(qb, qa, CHARGE_RTOL)
