@@ -25,6 +25,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{INC}"]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", f"-I{INC}", "-Wall"]
+# Sources whose FP64 expressions must keep the reference's written order with one rounding
+# per operation: no FMA contraction anywhere in the file.
+PER_FILE_NVCC_FLAGS = {"cabana.cu": ["-fmad=false"]}
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:
@@ -54,7 +57,7 @@ def _objects(force: bool, names) -> list[Path]:
     for src in sorted((PKG / "csrc").glob("*.cu")):
         obj = BUILD / (src.stem + ".cu.o")
         if force or _newer(obj, [src] + headers):
-            _run([NVCC] + NVCC_FLAGS + ["-c", str(src), "-o", str(obj)])
+            _run([NVCC] + NVCC_FLAGS + PER_FILE_NVCC_FLAGS.get(src.name, []) + ["-c", str(src), "-o", str(obj)])
         objs.append(obj)
     for name in names:
         src = PKG / "host" / name
@@ -88,12 +91,13 @@ def build_oppb(force: bool = False) -> Path:
 
 def build_oracle(force: bool = False) -> Path:
     """Compile the C oracle (test infrastructure) into oracle/lib/liboppb_oracle.so."""
-    src = ROOT / "oracle" / "fempic_oracle.c"
+    srcs = [ROOT / "oracle" / "fempic_oracle.c", ROOT / "oracle" / "cabana_oracle.c"]
     out_dir = ROOT / "oracle" / "lib"
     out_dir.mkdir(exist_ok=True)
     so = out_dir / "liboppb_oracle.so"
-    if force or _newer(so, [src]):
-        _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-Wall", str(src), "-o", str(so)])
+    if force or _newer(so, srcs):
+        _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-Wall", *map(str, srcs),
+              "-o", str(so), "-lm"])
     return so
 
 

@@ -57,6 +57,19 @@ class Inlet(C.Structure):
     _fields_ = [("n_faces", c_i32), ("dist", c_vp), ("if2c", c_vp), ("geom", c_vp)]
 
 
+class HexMesh(C.Structure):
+    _fields_ = [("n_cells", c_i32), ("c2f", c_vp), ("interp", c_vp)]
+
+
+class CabanaParticles(C.Structure):
+    _fields_ = [("size", c_i32), ("stride", c_i32), ("pos", c_vp), ("vel", c_vp), ("streak_mid", c_vp),
+                ("weight", c_vp), ("p2c", c_vp)]
+
+
+class CabanaConsts(C.Structure):
+    _fields_ = [("qdt_2mc", C.c_double), ("cdt_d", C.c_double * 3), ("qsp", C.c_double)]
+
+
 class FemPICMesh(C.Structure):
     _fields_ = [("n_nodes", c_i32), ("n_cells", c_i32), ("n_ifaces", c_i32),
                 ("n_pos", c_dp), ("n_vol", c_dp), ("n_type", c_ip), ("n_bnd_pot", c_dp),
@@ -96,6 +109,9 @@ _SIGS = {
     "oppb_hole_fill_static": (C.c_int, [c_i32, c_i32, c_vp, c_i32, c_i32, P(Dat), c_vp]),
     "oppb_sort_workspace_bytes": (C.c_size_t, [c_i32, c_i32]),
     "oppb_sort_by_cell": (C.c_int, [c_i32, c_i32, c_i32, c_i32, P(Dat), c_i32, c_vp, c_vp, C.c_size_t, c_vp]),
+    "oppb_hex_mesh_pack": (C.c_int, [P(HexMesh), c_i32, c_vp, c_vp, c_vp]),
+    "oppb_cabana_move_deposit": (C.c_int, [P(HexMesh), P(CabanaParticles), P(CabanaConsts), c_vp, c_i32, c_vp,
+                                           c_i32, c_vp]),
     "oppb_fempic_box_mesh": (C.c_int, [c_i32, c_i32, c_i32, C.c_double, C.c_double, C.c_double, P(FemPICMesh)]),
     "oppb_fempic_solve_field": (C.c_int, [P(FemPICMesh), C.c_double, C.c_double, C.c_double, c_i32, c_dp,
                                           P(c_i32), P(C.c_double)]),

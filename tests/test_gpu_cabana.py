@@ -1,0 +1,129 @@
+"""Parity of the CabanaPIC move + current deposit kernel (through the C ABI) with the oracle
+and with the reference's own outputs (golden fixture): positions, momenta, streaks, cells
+and call counts bit-exact; the 12 accumulators, summed with FP64 atomics in a different
+order, within CUR_RTOL of the largest accumulator magnitude."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from oppb import _lib as L
+from oppb.cabana import CabanaDevice, Deck, HexMesh, synthetic_interp, two_stream
+from oracle import cabana as OC
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+CUR_RTOL = 1e-12
+GOLDEN = Path(__file__).resolve().parent / "golden" / "cabana_4x5x6.npz"
+
+
+class _K:
+    """Constants object for CabanaDevice.move_deposit from explicit values."""
+
+    def __init__(self, qdt_2mc, cdt_d, qsp):
+        self.qdt_2mc, self.cdt_d, self.qsp = qdt_2mc, tuple(cdt_d), qsp
+
+    def consts(self):
+        import ctypes as C
+        return L.CabanaConsts(self.qdt_2mc, (C.c_double * 3)(*self.cdt_d), self.qsp)
+
+
+def _bits_equal(a, b, name):
+    np.testing.assert_array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8), err_msg=name)
+
+
+def _acc_close(got, ref):
+    scale = max(np.abs(ref).max(), 1e-300)
+    err = np.abs(got - ref).max() / scale
+    assert err <= CUR_RTOL, f"accumulator max err {err:.2e} of max |acc|"
+
+
+def _run_gpu(mesh, interp, pos, vel, streak, w, p2c, k, calls=1, max_hops=4096):
+    dev = CabanaDevice(mesh, DEV, len(p2c))
+    dev.set_interp(interp)
+    dev.set_particles(pos, vel, streak, w, p2c)
+    for _ in range(calls):
+        dev.move_deposit(k, max_hops=max_hops)
+    torch.cuda.synchronize()
+    return dev.host(), dev.status_host()
+
+
+def _run_oracle(mesh, interp, pos, vel, streak, w, p2c, k, calls=1):
+    a = {"pos": pos.copy(), "vel": vel.copy(), "streak": streak.copy(), "p2c": p2c.copy()}
+    visits = 0
+    for _ in range(calls):
+        acc = np.zeros((mesh.n_cells, 12))
+        visits = OC.move_deposit(a["pos"], a["vel"], a["streak"], w, a["p2c"], mesh.c2ngc, interp, acc, k.qdt_2mc,
+                                 np.array(k.cdt_d), k.qsp)
+    a["acc"] = acc
+    return a, visits
+
+
+def test_matches_reference_golden():
+    z = np.load(GOLDEN)
+    mesh = HexMesh(*[int(v) for v in z["dims"]])
+    k = _K(float(z["qdt_2mc"]), z["cdt_d"], float(z["qsp"]))
+    got, st = _run_gpu(mesh, z["interp"], z["pos"], z["vel"], z["streak"], z["weight"], z["p2c"], k,
+                       calls=int(z["calls"]))
+    assert st.error == 0
+    for name in ("pos", "vel", "streak", "p2c"):
+        _bits_equal(got[name], z["ref_" + name], name)
+    _acc_close(got["acc"], z["ref_acc"])
+
+
+@pytest.mark.parametrize("n,seed,scale", [(1, 0, 2.0), (33, 1, 2.0), (5000, 2, 0.5), (200_003, 3, 2.5)])
+def test_matches_oracle_random(n, seed, scale):
+    mesh = HexMesh(6, 5, 7)
+    rng = np.random.default_rng(seed)
+    interp = synthetic_interp(mesh, seed + 100, e_scale=0.3, b_scale=0.4)
+    p2c = np.sort(rng.choice(mesh.interior, n)).astype(np.int32)
+    pos = rng.uniform(-1, 1, (n, 3))
+    vel = rng.normal(0, scale, (n, 3))
+    if n > 200:
+        pos[:60, 1] = 1.0  # on a face
+        vel[60:120, 0] = 0.0  # zero component: the 3.4e38 branch
+    w = rng.uniform(0.1, 2.0, n)
+    k = _K(-0.27, (1.4, 0.8, 2.2), -1.0)
+    streak = np.zeros((n, 3))
+    got, st = _run_gpu(mesh, interp, pos, vel, streak, w, p2c, k)
+    ref, visits = _run_oracle(mesh, interp, pos, vel, streak, w, p2c, k)
+    assert st.error == 0 and int(st.total_visits) == visits
+    for name in ("pos", "vel", "streak", "p2c"):
+        _bits_equal(got[name], ref[name], name)
+    _acc_close(got["acc"], ref["acc"])
+
+
+def test_two_stream_steps_match_oracle():
+    """The workload's own construction at small size, five successive calls."""
+    mesh = HexMesh(4, 4, 16)
+    deck = Deck(4, 4, 16, 1.0, 1.0, 4.0, nppc=64, courant_frac=0.5)
+    pos, vel, streak, w, p2c = two_stream(mesh, deck, 0.2, 0.01, seed=5)
+    interp = synthetic_interp(mesh, 6)
+    got, st = _run_gpu(mesh, interp, pos, vel, streak, w, p2c, deck, calls=5)
+    ref, visits = _run_oracle(mesh, interp, pos, vel, streak, w, p2c, deck, calls=5)
+    assert st.error == 0 and int(st.total_visits) == visits
+    for name in ("pos", "vel", "streak", "p2c"):
+        _bits_equal(got[name], ref[name], name)
+    _acc_close(got["acc"], ref["acc"])
+
+
+def test_errors_reported():
+    mesh = HexMesh(3, 3, 3)
+    interp = synthetic_interp(mesh, 1)
+    n = 64
+    rng = np.random.default_rng(3)
+    p2c = np.full(n, mesh.interior[0], np.int32)
+    p2c[17] = mesh.n_cells + 3
+    pos, vel = rng.uniform(-1, 1, (n, 3)), rng.normal(0, 0.1, (n, 3))
+    k = _K(-0.2, (0.5, 0.5, 0.5), -1.0)
+    _, st = _run_gpu(mesh, interp, pos, vel, np.zeros((n, 3)), np.ones(n), p2c, k)
+    assert st.error == L.OPPB_ERR_CELL_RANGE and st.error_index == 17
+    # a long streak with a hop bound of 2 calls
+    vel2 = np.zeros((1, 3))
+    vel2[0, 2] = 50.0
+    _, st = _run_gpu(mesh, interp, np.zeros((1, 3)), vel2, np.zeros((1, 3)), np.ones(1),
+                     np.array([mesh.interior[0]], np.int32), _K(-0.2, (3.0, 3.0, 3.0), -1.0), max_hops=2)
+    assert st.error == L.OPPB_ERR_HOP_LIMIT and st.error_index == 0
