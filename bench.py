@@ -399,7 +399,108 @@ def arm_ours(args) -> dict:
         line["e2e"] = mixed["e2e"]
     if args.cpu_baseline and "cpu_sample_state" in f64:
         line["cpu_baseline"] = cpu_baseline_port(hm, f64["cpu_sample_state"], args.cpu_seconds)
+    if args.cabana and world == 1:
+        line["cabanapic"] = run_cabana(dev, min(args.steps, 20), args.warmup, args.cpu_baseline, args.cpu_seconds)
+        line["gpu_launches_cabanapic"] = line["cabanapic"]["gpu_launches"]
     return line
+
+
+# ------------------------------------------------------------- CabanaPIC (second workload)
+
+CAB = dict(nx=32, ny=32, nz=256, lx=1.0, ly=1.0, lz=8.0, nppc=400, v0=0.2, sigma=0.01, courant=0.5, seed=3)
+CAB_WORKLOAD = ("CabanaPIC two-stream move + current deposit: 32x32x256 periodic hexes (262,144 cells + ghost "
+                "layer), 400 particles per cell (2 counter-streaming species x 200), u_z = +-0.2c gamma + "
+                "N(0, 0.01c), dt = 0.5 Courant; synthetic fixed interpolated fields")
+# Per call: read pos 24 + vel 24 + weight 8 + p2c 4, write pos 24 + vel 24 B per particle; per cell
+# the interp record 160 B + faces 32 B read and the 12 accumulators read + written (192 B).
+CAB_BYTES_PER_PARTICLE = 108
+CAB_BYTES_PER_CELL = 384
+
+
+def run_cabana(dev, steps: int, warmup: int, cpu: bool, cpu_seconds: float) -> dict:
+    """move_deposit on the config-sized two-stream state: `warmup` untimed then `steps` timed
+    calls (c_acc zeroed + kernel each, as the reference main loop between field updates)."""
+    import torch
+
+    from oppb import _lib as L
+    from oppb.cabana import CabanaDevice, Deck, HexMesh, synthetic_interp
+
+    mesh = HexMesh(CAB["nx"], CAB["ny"], CAB["nz"])
+    deck = Deck(CAB["nx"], CAB["ny"], CAB["nz"], CAB["lx"], CAB["ly"], CAB["lz"], nppc=CAB["nppc"],
+                courant_frac=CAB["courant"])
+    n = len(mesh.interior) * CAB["nppc"]
+    cd = CabanaDevice(mesh, dev, n)
+    cd.set_interp(synthetic_interp(mesh, CAB["seed"]))
+    cd.fill_two_stream(mesh, deck, CAB["v0"], CAB["sigma"], CAB["seed"])
+    lib = L.load()
+    for _ in range(warmup):
+        cd.move_deposit(deck)
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    t_ms, visits = [], 0
+    l0 = lib.oppb_kernel_launches()
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        cd.move_deposit(deck)
+        e1.record(s)
+        e1.synchronize()
+        st = cd.status_host()
+        if st.error:
+            raise L.OppbError("cabana move_deposit", st.error)
+        t_ms.append(e0.elapsed_time(e1))
+        visits += int(st.total_visits)
+    launches = lib.oppb_kernel_launches() - l0
+    t = sum(t_ms) / 1e3
+    bytes_call = CAB_BYTES_PER_PARTICLE * n + CAB_BYTES_PER_CELL * mesh.n_cells
+    peaks = measured_peaks()
+    out = {"workload": CAB_WORKLOAD, "metric": "particle-steps/s (move + current deposit)", "unit": UNIT,
+           "value": n * steps / t, "particles": n, "cells": mesh.n_cells, "steps": steps, "warmup": warmup,
+           "ms_per_step": 1e3 * t / steps, "calls_per_particle": visits / (n * steps), "dtype": "f64",
+           "gpu_launches": int(launches),
+           "roofline": {"bound": "hbm", "achieved": bytes_call / (t / steps) / 1e9, "peak": peaks["hbm_gbs"],
+                        "unit": "GB/s", "frac": bytes_call / (t / steps) / 1e9 / peaks["hbm_gbs"],
+                        "bytes_per_launch": bytes_call, "traffic": None}}
+    del cd
+    torch.cuda.empty_cache()
+    if cpu:
+        out["cpu_baseline"] = cabana_cpu_baseline(cpu_seconds)
+    return out
+
+
+def cabana_cpu_baseline(budget_s: float) -> dict:
+    """The compiled reference omp build (oracle/_ref/cabana_ref_omp, all host threads) on a
+    bounded sample of the same construction (8x8x64 cells, 400 per cell), else the C oracle."""
+    import numpy as np
+
+    from oppb.cabana import Deck, HexMesh, synthetic_interp, two_stream
+    from oracle import cabana as OC
+    from oracle import ref_runner as R
+
+    mesh = HexMesh(8, 8, 64)
+    deck = Deck(8, 8, 64, 0.25, 0.25, 2.0, nppc=CAB["nppc"], courant_frac=CAB["courant"])
+    interp = synthetic_interp(mesh, CAB["seed"])
+    pos, vel, streak, w, p2c = two_stream(mesh, deck, CAB["v0"], CAB["sigma"], CAB["seed"])
+    n = len(p2c)
+    if (R.REF_DIR / "cabana_ref_omp").exists():
+        cores = len(os.sched_getaffinity(0))
+        calls = 8
+        res = OC.run_reference("omp", mesh.c2ngc, interp, pos, vel, streak, w, p2c, deck.qdt_2mc, deck.cdt_d,
+                               deck.qsp, calls=calls, threads=cores)
+        t = float(res["times"][1:].sum())
+        return {"value": n * (calls - 1) / t, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"{n} particles (8x8x64 cells x {CAB['nppc']}), {calls - 1} timed calls after 1; "
+                          f"compiled OP-PIC omp backend + generated CabanaPIC loops"}
+    ps, t = 0, 0.0
+    while t < budget_s:
+        acc = np.zeros((mesh.n_cells, 12))
+        t0 = time.perf_counter()
+        OC.move_deposit(pos, vel, streak, w, p2c, mesh.c2ngc, interp, acc, deck.qdt_2mc, np.array(deck.cdt_d),
+                        deck.qsp)
+        t += time.perf_counter() - t0
+        ps += n
+    return {"value": ps / t, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} particles (8x8x64 cells x {CAB['nppc']}); C oracle single thread"}
 
 
 # ------------------------------------------------------------------------ reference arm
@@ -491,6 +592,11 @@ def main():
     ap.add_argument("--fill-steps", type=int, default=CFG["fill_steps"], help="steps to reach the steady state")
     ap.add_argument("--capacity", type=int, default=CFG["capacity"], help="particle set capacity")
     ap.add_argument("--precision", choices=["both", "f64", "mixed"], default="both")
+    ap.add_argument("--no-cabana", dest="cabana", action="store_false",
+                    help="skip the CabanaPIC move + current deposit measurement")
+    ap.add_argument("--cabana-only", action="store_true",
+                    help="run only the CabanaPIC measurement and print its object")
+    ap.add_argument("--cabana-dims", default=None, help="nx,ny,nz of the CabanaPIC mesh (default 32,32,256)")
     ap.add_argument("--deposit", choices=["warp", "table"], default="warp",
                     help="deposit strategy: warp-run FP64 atomics or per-CTA shared node table")
     args = ap.parse_args()
@@ -501,6 +607,15 @@ def main():
         from oppb import _lib as L
 
         L.set_deposit_strategy(L.DEPOSIT_CTA_TABLE if args.deposit == "table" else L.DEPOSIT_WARP_ATOMIC)
+    if args.cabana_dims:
+        nx, ny, nz = (int(v) for v in args.cabana_dims.split(","))
+        CAB.update(nx=nx, ny=ny, nz=nz, lx=nx / 32, ly=ny / 32, lz=nz / 32)
+    if args.cabana_only and args.impl != "reference":
+        import torch
+
+        print(json.dumps(run_cabana(torch.device("cuda:0"), args.steps, args.warmup, args.cpu_baseline,
+                                    args.cpu_seconds)), flush=True)
+        return
     line = arm_reference(args) if args.impl == "reference" else arm_ours(args)
     if line:
         print(json.dumps(line), flush=True)

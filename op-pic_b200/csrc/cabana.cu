@@ -3,10 +3,10 @@
 //
 // One thread per particle; a particle's calls of the reference kernel (the first one with the
 // push, then one per face crossing) run in a warp-wide loop so that every call's deposit goes
-// through one warp reduction: lanes whose deposits target the same cell in a run of
-// consecutive lanes are summed in shared memory and the run issues 12 FP64 atomics.  Particles
-// are initialised cell by cell and move about a tenth of a cell per step, so a warp's 32 lanes
-// usually share one cell and the reduction turns 384 atomics into 12.
+// through one warp reduction: lanes whose deposits target the same cell are summed in shared
+// memory and each such group issues 12 FP64 atomics.  Particles are initialised cell by cell
+// and move a few hundredths of a cell per step, so a warp's lanes spread over a few cells and
+// the reduction turns 384 atomics per warp into a few dozen.
 //
 // FP64 expressions are written in the reference's order and this file is compiled with
 // -fmad=false (no contraction), so positions, momenta, streaks and cells are bit-identical to
@@ -20,6 +20,7 @@ namespace {
 
 constexpr int kCabBlock = 256;
 constexpr int kCabWarps = kCabBlock / 32;
+constexpr int kSparseLanes = 4;  // at most this many depositing lanes: plain atomics, no staging
 constexpr int kStageStride = 14;  // doubles per staged row: 12 used, 16-B aligned rows
 
 struct HexArgs {
@@ -192,32 +193,44 @@ struct WarpStage {
     int32_t keys[32];
 };
 
-// Adds every lane's 12 values j to acc[k * acc_stride + key] (key < 0: nothing).  Runs of
-// consecutive lanes with the same key are summed in shared memory by lanes 0..11 (one column
-// each) and issue one atomic per column.  Every lane of the warp must call it.
+// Adds every lane's 12 values j to acc[k * acc_stride + key] (key < 0: nothing).  Lanes with
+// the same key form a group (warp match, whatever their positions: the two counter-streaming
+// species interleave lane by lane and drift apart); lanes 0..11 sum one column each over a
+// group's rows in shared memory and issue one atomic per column and group.  Every lane of
+// the warp must call it.
 __device__ __forceinline__ void warp_deposit(WarpStage& ws, double* acc, int32_t acc_stride, int32_t key,
                                              const double* j) {
     const int lane = threadIdx.x & 31;
-    const int32_t prev = __shfl_up_sync(kFullMask, key, 1);
-    const unsigned heads = __ballot_sync(kFullMask, lane == 0 || prev != key);
-    if (__ballot_sync(kFullMask, key >= 0) == 0u) return;
+    // Calls after the first one (face crossings) involve a few lanes of a warp: their
+    // deposits go straight to global atomics.
+    if (__popc(__ballot_sync(kFullMask, key >= 0)) <= kSparseLanes) {
+        if (key >= 0) {
+#pragma unroll
+            for (int c = 0; c < 12; c++) atomicAdd(acc + (int64_t)c * acc_stride + key, j[c]);
+        }
+        return;
+    }
+    const unsigned peers = __match_any_sync(kFullMask, key);
+    unsigned leaders = __ballot_sync(kFullMask, key >= 0 && lane == __ffs(peers) - 1);
+    if (leaders == 0u) return;
     __syncwarp();  // the previous call's readers are done with the stage
     double2* row = reinterpret_cast<double2*>(&ws.vals[lane][0]);
 #pragma unroll
     for (int c = 0; c < 6; c++) row[c] = make_double2(j[2 * c], j[2 * c + 1]);
     ws.keys[lane] = key;
     __syncwarp();
-    if (lane < 12) {
-        double sum = 0.0;
-#pragma unroll 8
-        for (int r = 0; r < 32; r++) {
-            sum += ws.vals[r][lane];
-            const bool run_ends = r == 31 || ((heads >> (r + 1)) & 1u);
-            if (run_ends) {
-                const int32_t k = ws.keys[r];
-                if (k >= 0) atomicAdd(acc + (int64_t)lane * acc_stride + k, sum);
-                sum = 0.0;
+    while (leaders) {  // warp-uniform
+        const int leader = __ffs(leaders) - 1;
+        leaders &= leaders - 1;
+        unsigned members = __shfl_sync(kFullMask, peers, leader);
+        if (lane < 12) {
+            double sum = 0.0;
+            while (members) {
+                const int r = __ffs(members) - 1;
+                members &= members - 1;
+                sum += ws.vals[r][lane];
             }
+            atomicAdd(acc + (int64_t)lane * acc_stride + ws.keys[leader], sum);
         }
     }
 }

@@ -162,6 +162,27 @@ class CabanaDevice:
         self.weight[:n] = torch.from_numpy(np.ascontiguousarray(weight)).to(self.device)
         self.p2c[:n] = torch.from_numpy(np.ascontiguousarray(p2c, dtype=np.int32)).to(self.device)
 
+    def fill_two_stream(self, mesh: HexMesh, deck: Deck, v0: float, sigma: float, seed: int) -> None:
+        """The two_stream construction drawn on the device (torch generator): nppc particles per
+        non-ghost cell in cell order, positions uniform in [-1,1]^3, u = N(0, sigma^2) per axis
+        plus +-v0 gamma along z alternating per particle, zero streak, weight deck.we."""
+        n = len(mesh.interior) * deck.nppc
+        if n > self.capacity or deck.nppc % 2:
+            raise ValueError("capacity exceeded or odd nppc")
+        self.size = n
+        g = torch.Generator(device=self.device)
+        g.manual_seed(seed)
+        self.pos[:, :n].uniform_(-1.0, 1.0, generator=g)
+        self.vel[:, :n].normal_(0.0, sigma, generator=g)
+        drift = v0 / math.sqrt(1.0 - v0 * v0)
+        pairs = self.vel[2, :n].view(-1, 2)
+        pairs[:, 0] += drift
+        pairs[:, 1] -= drift
+        self.streak[:, :n].zero_()
+        self.weight[:n] = deck.we
+        cells = torch.from_numpy(mesh.interior).to(self.device)
+        self.p2c[:n] = cells.repeat_interleave(deck.nppc)
+
     def view(self) -> L.CabanaParticles:
         return L.CabanaParticles(self.size, self.capacity, _ptr(self.pos), _ptr(self.vel), _ptr(self.streak),
                                  _ptr(self.weight), _ptr(self.p2c))
