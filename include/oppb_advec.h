@@ -1,0 +1,79 @@
+/* C ABI of the B200 backend for OP-PIC's NESO-advection particle path
+ * (apps_codegen/app_neso_advection_mdir_cg): the periodic position update
+ * (opp_par_loop_all__update_pos_kernel) and the axis-wise multi-hop move
+ * (opp_particle_move__move_kernel), for one instance or for a batch of independent
+ * instances of different mesh and particle counts advanced by one persistent launch.
+ *
+ * Conventions are those of oppb.h (plain pointers, int status, explicit stream, no
+ * allocation).  Particle dats of all instances are concatenated in the reference's device
+ * layout, SoA [2][stride]; p2c and the neighbour map hold instance-local cell indices.
+ */
+#ifndef OPPB_ADVEC_H
+#define OPPB_ADVEC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "oppb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One instance: its particles [part_offset, part_offset + n_parts) of the concatenated dats,
+ * its cells [cell_offset, cell_offset + n_cells) of the packed cell records, and its
+ * CONST_dt, CONST_cell_width, CONST_extents (advec_opp.cpp). */
+typedef struct oppb_advec_instance {
+    int64_t part_offset;
+    int32_t n_parts;
+    int32_t cell_offset;
+    int32_t n_cells;
+    int32_t reserved;
+    double  dt;
+    double  cell_width;
+    double  extents[2];
+} oppb_advec_instance;
+
+/* A batch.  instances: device array [n_instances].  tile_prefix: device array
+ * [n_instances + 1], the first 256-particle work item of each instance (prefix sum of
+ * ceil(n_parts / 256)).  cells: packed records [total cells][4] f64 = c_pos_ll x, y, then
+ * c2c (CellMap order xd_y, xu_y, x_yd, x_yu) as four int32; 32-byte aligned. */
+typedef struct oppb_advec_batch {
+    int32_t n_instances;
+    int32_t n_work;            /* tile_prefix[n_instances] */
+    const oppb_advec_instance* instances;
+    const int32_t* tile_prefix;
+    const double* cells;
+    int64_t stride;            /* capacity of the concatenated particle dats */
+    double*  pos;              /* p_pos  [2][stride] */
+    const double* vel;         /* p_vel  [2][stride] */
+    int32_t* mdir;             /* p_move_dir [2][stride] */
+    int32_t* p2c;              /* p2c [stride] */
+} oppb_advec_batch;
+
+/* Packs one instance's c_pos_ll (SoA [2][ld]) and c2c_map (SoA [4][ld]) into
+ * cells[cell_offset .. cell_offset + n_cells). */
+int oppb_advec_pack_cells(double* cells, int32_t cell_offset, int32_t n_cells, int32_t ld,
+                          const double* c_pos_ll, const int32_t* c2c, void* stream);
+
+/* update_pos_kernel then move_kernel for every particle of every instance, fused per
+ * particle (the position stays in registers), in one persistent launch.  Bit-identical to
+ * the seq backend running the two loops on each instance.  status is accumulated into, not
+ * cleared (zero it before a sequence of steps, e.g. one captured CUDA graph of many steps):
+ * total_visits / max_visits count move calls; the first hop-bound overrun or out-of-range
+ * cell sets error / error_index (index into the concatenated dats). */
+int oppb_advec_step(const oppb_advec_batch* batch, oppb_move_status* status, int32_t max_hops,
+                    void* stream);
+
+/* The two loops separately, as the generated main calls them:
+ * opp_par_loop_all__update_pos_kernel (apps_codegen/app_neso_advection_mdir_cg/cuda/update_pos_kernel_loop.hpp)
+ * and opp_particle_move__move_kernel (.../cuda/move_kernel_loop.hpp). */
+int oppb_advec_update_pos(const oppb_advec_batch* batch, void* stream);
+int oppb_advec_move(const oppb_advec_batch* batch, oppb_move_status* status, int32_t max_hops,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPPB_ADVEC_H */

@@ -27,7 +27,7 @@ NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", f"
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", f"-I{INC}", "-Wall"]
 # Sources whose FP64 expressions must keep the reference's written order with one rounding
 # per operation: no FMA contraction anywhere in the file.
-PER_FILE_NVCC_FLAGS = {"cabana.cu": ["-fmad=false"]}
+PER_FILE_NVCC_FLAGS = {"cabana.cu": ["-fmad=false"], "advec.cu": ["-fmad=false"]}
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:
@@ -91,7 +91,7 @@ def build_oppb(force: bool = False) -> Path:
 
 def build_oracle(force: bool = False) -> Path:
     """Compile the C oracle (test infrastructure) into oracle/lib/liboppb_oracle.so."""
-    srcs = [ROOT / "oracle" / "fempic_oracle.c", ROOT / "oracle" / "cabana_oracle.c"]
+    srcs = [ROOT / "oracle" / "fempic_oracle.c", ROOT / "oracle" / "cabana_oracle.c", ROOT / "oracle" / "advec_oracle.c"]
     out_dir = ROOT / "oracle" / "lib"
     out_dir.mkdir(exist_ok=True)
     so = out_dir / "liboppb_oracle.so"

@@ -70,6 +70,16 @@ class CabanaConsts(C.Structure):
     _fields_ = [("qdt_2mc", C.c_double), ("cdt_d", C.c_double * 3), ("qsp", C.c_double)]
 
 
+class AdvecInstance(C.Structure):
+    _fields_ = [("part_offset", c_i64), ("n_parts", c_i32), ("cell_offset", c_i32), ("n_cells", c_i32),
+                ("reserved", c_i32), ("dt", C.c_double), ("cell_width", C.c_double), ("extents", C.c_double * 2)]
+
+
+class AdvecBatch(C.Structure):
+    _fields_ = [("n_instances", c_i32), ("n_work", c_i32), ("instances", c_vp), ("tile_prefix", c_vp),
+                ("cells", c_vp), ("stride", c_i64), ("pos", c_vp), ("vel", c_vp), ("mdir", c_vp), ("p2c", c_vp)]
+
+
 class FemPICMesh(C.Structure):
     _fields_ = [("n_nodes", c_i32), ("n_cells", c_i32), ("n_ifaces", c_i32),
                 ("n_pos", c_dp), ("n_vol", c_dp), ("n_type", c_ip), ("n_bnd_pot", c_dp),
@@ -112,6 +122,10 @@ _SIGS = {
     "oppb_hex_mesh_pack": (C.c_int, [P(HexMesh), c_i32, c_vp, c_vp, c_vp]),
     "oppb_cabana_move_deposit": (C.c_int, [P(HexMesh), P(CabanaParticles), P(CabanaConsts), c_vp, c_i32, c_vp,
                                            c_i32, c_vp]),
+    "oppb_advec_pack_cells": (C.c_int, [c_vp, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp]),
+    "oppb_advec_step": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
+    "oppb_advec_update_pos": (C.c_int, [P(AdvecBatch), c_vp]),
+    "oppb_advec_move": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
     "oppb_fempic_box_mesh": (C.c_int, [c_i32, c_i32, c_i32, C.c_double, C.c_double, C.c_double, P(FemPICMesh)]),
     "oppb_fempic_solve_field": (C.c_int, [P(FemPICMesh), C.c_double, C.c_double, C.c_double, c_i32, c_dp,
                                           P(c_i32), P(C.c_double)]),
