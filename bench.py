@@ -402,6 +402,8 @@ def arm_ours(args) -> dict:
     if args.cabana and world == 1:
         line["cabanapic"] = run_cabana(dev, min(args.steps, 20), args.warmup, args.cpu_baseline, args.cpu_seconds)
         line["gpu_launches_cabanapic"] = line["cabanapic"]["gpu_launches"]
+    if args.advec and world == 1:
+        line["advec_ensemble"] = run_advec(dev, min(args.steps, 20), args.warmup, args.cpu_baseline)
     return line
 
 
@@ -503,6 +505,125 @@ def cabana_cpu_baseline(budget_s: float) -> dict:
             "sample": f"{n} particles (8x8x64 cells x {CAB['nppc']}); C oracle single thread"}
 
 
+# ------------------------------------------------- NESO-advection ensemble (third workload)
+
+ADV = dict(instances=64, side_lo=64, side_hi=512, ppc_lo=10, ppc_hi=200, cell_width=1.0, dt=0.5, v_sd=0.5,
+           v_clip=1.0, seed=5, graph_steps=10)
+ADV_WORKLOAD = ("NESO-advection ensemble: 64 independent periodic square meshes, side ~ U{64..512} cells, "
+                "10..200 particles per cell (seeded), |v dt| <= 0.5 cell per step; update_pos + move of every "
+                "instance in one persistent launch per step, captured as a CUDA graph")
+# Per step: read pos 16 + vel 16 + mdir 8 + p2c 4, write pos 16 + mdir 8 B per particle; 32 B per cell record.
+ADV_BYTES_PER_PARTICLE = 68
+ADV_BYTES_PER_CELL = 32
+
+
+def run_advec(dev, steps: int, warmup: int, cpu: bool) -> dict:
+    """The ensemble three ways on the same state: CUDA-graph replay of the batched step, the
+    batched step launched directly, and one launch per instance."""
+    import numpy as np
+    import torch
+
+    from oppb import _lib as L
+    from oppb.advec import AdvecBatchDevice, AdvecMesh
+
+    rng = np.random.default_rng(ADV["seed"])
+    sides = rng.integers(ADV["side_lo"], ADV["side_hi"] + 1, ADV["instances"])
+    ppcs = rng.integers(ADV["ppc_lo"], ADV["ppc_hi"] + 1, ADV["instances"])
+    meshes = [AdvecMesh(int(s), int(s), ADV["cell_width"]) for s in sides]
+    counts = [m.n_cells * int(p) for m, p in zip(meshes, ppcs)]
+    bd = AdvecBatchDevice(meshes, counts, [ADV["dt"]] * len(meshes), dev)
+    for k, p in enumerate(ppcs):
+        bd.fill_instance(k, int(p), ADV["v_sd"], ADV["v_clip"], ADV["seed"] * 1000 + k)
+    n = bd.n_total
+    lib = L.load()
+    for _ in range(warmup):
+        bd.step()
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    E = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(fn, reps):
+        bd.zero_status()
+        torch.cuda.synchronize()
+        e0, e1 = E(), E()
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        e1.synchronize()
+        st = bd.status_host()
+        if st.error:
+            raise L.OppbError("advec step", st.error)
+        return e0.elapsed_time(e1) / 1e3, int(st.total_visits)
+
+    # Autotune the particles in flight per thread (the kernel's work items per block pass) on
+    # this state, then capture the graph with the fastest choice.
+    sweep = {}
+    for items in (1, 2, 4):
+        L.set_tuning(advec_items=items)
+        bd.step()
+        t_k, _ = timed(bd.step, 3)
+        sweep[items] = n * 3 / t_k
+    best = max(sweep, key=sweep.get)
+    L.set_tuning(advec_items=best)
+    G = ADV["graph_steps"]
+    graph = bd.capture(G)
+    replays = max(1, steps // G)
+    l0 = lib.oppb_kernel_launches()
+    t_graph, visits = timed(graph.replay, replays)
+    graph_steps = replays * G
+    t_direct, _ = timed(bd.step, graph_steps)
+    launches = lib.oppb_kernel_launches() - l0
+    singles = bd.instance_batches()
+    t_single, _ = timed(lambda: [bd.step_batch(b) for b, _ in singles], graph_steps)
+    del graph
+    bytes_step = ADV_BYTES_PER_PARTICLE * n + ADV_BYTES_PER_CELL * sum(m.n_cells for m in meshes)
+    peaks = measured_peaks()
+    out = {"workload": ADV_WORKLOAD, "metric": "particle-steps/s (update_pos + move, all instances)", "unit": UNIT,
+           "value": n * graph_steps / t_graph, "particles": n, "instances": len(meshes),
+           "cells": int(sum(m.n_cells for m in meshes)), "steps": graph_steps, "warmup": warmup,
+           "ms_per_step": 1e3 * t_graph / graph_steps, "calls_per_particle": visits / (n * graph_steps),
+           "direct_launch_value": n * graph_steps / t_direct, "per_instance_launch_value": n * graph_steps / t_single,
+           "dtype": "f64", "gpu_launches": int(launches),
+           "autotune": {"advec_items": {str(k): v for k, v in sweep.items()}, "chosen": best},
+           "roofline": {"bound": "hbm", "achieved": bytes_step / (t_graph / graph_steps) / 1e9,
+                        "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": bytes_step / (t_graph / graph_steps) / 1e9 / peaks["hbm_gbs"],
+                        "bytes_per_launch": bytes_step, "traffic": None}}
+    del bd, singles
+    torch.cuda.empty_cache()
+    if cpu:
+        out["cpu_baseline"] = advec_cpu_baseline()
+    return out
+
+
+def advec_cpu_baseline() -> dict:
+    """The compiled reference omp build (oracle/_ref/advec_ref_omp, all host threads) on one
+    256 x 256 instance with 100 particles per cell, else the C oracle on a 128 x 128 one."""
+    from oppb.advec import AdvecMesh, particles
+    from oracle import advec as OA
+    from oracle import ref_runner as R
+
+    if (R.REF_DIR / "advec_ref_omp").exists():
+        m = AdvecMesh(256, 256, ADV["cell_width"])
+        pos, vel, mdir, p2c = particles(m, 100, ADV["v_sd"], ADV["seed"], v_clip=ADV["v_clip"])
+        cores = len(os.sched_getaffinity(0))
+        steps = 6
+        res = OA.run_reference("omp", m.nx, m.ny, m.cell_width, ADV["dt"], pos, vel, mdir, p2c, m.c2c, m.c_pos_ll,
+                               steps, threads=cores)
+        t = float(res["times"][1:].sum())
+        return {"value": len(p2c) * (steps - 1) / t, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"one 256x256 instance, {len(p2c)} particles, {steps - 1} timed steps after 1; compiled "
+                          f"OP-PIC omp backend + generated NESO-advection loops"}
+    m = AdvecMesh(128, 128, ADV["cell_width"])
+    pos, vel, mdir, p2c = particles(m, 100, ADV["v_sd"], ADV["seed"], v_clip=ADV["v_clip"])
+    t0 = time.perf_counter()
+    OA.steps(pos, vel, mdir, p2c, m.c2c, m.c_pos_ll, ADV["dt"], m.extents, m.cell_width, 5)
+    t = time.perf_counter() - t0
+    return {"value": len(p2c) * 5 / t, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"one 128x128 instance, {len(p2c)} particles, 5 steps; C oracle single thread"}
+
+
 # ------------------------------------------------------------------------ reference arm
 
 def _reference_line(args, value: float, ms_per_step: float, particles_per_step: float, kind: str, cores: int,
@@ -597,6 +718,9 @@ def main():
     ap.add_argument("--cabana-only", action="store_true",
                     help="run only the CabanaPIC measurement and print its object")
     ap.add_argument("--cabana-dims", default=None, help="nx,ny,nz of the CabanaPIC mesh (default 32,32,256)")
+    ap.add_argument("--no-advec", dest="advec", action="store_false",
+                    help="skip the NESO-advection ensemble measurement")
+    ap.add_argument("--advec-only", action="store_true", help="run only the NESO-advection ensemble measurement")
     ap.add_argument("--deposit", choices=["warp", "table"], default="warp",
                     help="deposit strategy: warp-run FP64 atomics or per-CTA shared node table")
     args = ap.parse_args()
@@ -610,6 +734,11 @@ def main():
     if args.cabana_dims:
         nx, ny, nz = (int(v) for v in args.cabana_dims.split(","))
         CAB.update(nx=nx, ny=ny, nz=nz, lx=nx / 32, ly=ny / 32, lz=nz / 32)
+    if args.advec_only and args.impl != "reference":
+        import torch
+
+        print(json.dumps(run_advec(torch.device("cuda:0"), args.steps, args.warmup, args.cpu_baseline)), flush=True)
+        return
     if args.cabana_only and args.impl != "reference":
         import torch
 

@@ -36,7 +36,9 @@ typedef struct oppb_advec_instance {
 
 /* A batch.  instances: device array [n_instances].  tile_prefix: device array
  * [n_instances + 1], the first 256-particle work item of each instance (prefix sum of
- * ceil(n_parts / 256)).  cells: packed records [total cells][4] f64 = c_pos_ll x, y, then
+ * ceil(n_parts / 256)).  Blocks take items in order, a chunk at a time, from work_counter,
+ * so the items in flight stay within one or two instances (their cell records stay in L2)
+ * whatever the speed of each block.  cells: packed records [total cells][4] f64 = c_pos_ll x, y, then
  * c2c (CellMap order xd_y, xu_y, x_yd, x_yu) as four int32; 32-byte aligned. */
 typedef struct oppb_advec_batch {
     int32_t n_instances;
@@ -49,6 +51,8 @@ typedef struct oppb_advec_batch {
     const double* vel;         /* p_vel  [2][stride] */
     int32_t* mdir;             /* p_move_dir [2][stride] */
     int32_t* p2c;              /* p2c [stride] */
+    int32_t* work_counter;     /* device scratch, one int32: the launch hands out work items in
+                                  order from it (the launcher zeroes it on the launch's stream) */
 } oppb_advec_batch;
 
 /* Packs one instance's c_pos_ll (SoA [2][ld]) and c2c_map (SoA [4][ld]) into

@@ -3,8 +3,9 @@
 // persistent launch.
 //
 // Work is cut into 256-particle items that never straddle two instances (tile_prefix); a
-// grid sized to the resident capacity of the GPU loops over the items, so instances of
-// uneven size share the SMs without a launch per instance.  One thread per particle of an
+// grid sized to the resident capacity of the GPU takes the items in order from a counter, so
+// instances of uneven size share the SMs without a launch per instance and the items in
+// flight stay within one or two instances.  One thread per particle of an
 // item: update_pos (apps_codegen/app_neso_advection_mdir_cg/kernels.h update_pos_kernel) in
 // registers, then the hops of move_kernel (the direction chosen on the first call, x first,
 // then y), reading one 32-byte cell record {c_pos_ll, c2c} per call.  This file is compiled
@@ -22,17 +23,12 @@ constexpr int kAdvBlock = 256;  // = particles per work item
 constexpr int kAdvWarps = kAdvBlock / 32;
 enum AdvMode { kStep = 0, kUpdateOnly = 1, kMoveOnly = 2 };
 
-// Work item w belongs to the instance i with prefix[i] <= w < prefix[i + 1].
-__device__ __forceinline__ int find_instance(const int32_t* __restrict__ prefix, int n, int w) {
-    int lo = 0, hi = n;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(prefix + mid) <= w)
-            lo = mid;
-        else
-            hi = mid;
-    }
-    return lo;
+// Work item w belongs to the instance i with prefix[i] <= w < prefix[i + 1].  A block's items
+// only increase, so the search moves a cursor forward from the previous answer: usually one
+// comparison per item instead of a dependent binary search.
+__device__ __forceinline__ int find_instance(const int32_t* __restrict__ prefix, int n, int w, int& cursor) {
+    while (cursor + 1 < n && __ldg(prefix + cursor + 1) <= w) cursor++;
+    return cursor;
 }
 
 // update_pos_kernel for one axis: x += v dt, then the periodic wrap.
@@ -91,42 +87,83 @@ __device__ __forceinline__ int move_particle(const double* __restrict__ cells, i
     }
 }
 
-template <int kMode>
+constexpr int kChunkItems = 8;  // work items a block takes from the counter at once
+
+// A block takes a chunk of work items from the batch's counter (so items are processed in
+// order across the whole GPU) and walks it kItems items per pass (one particle of each per
+// thread), so every thread has kItems independent particles' loads in flight.
+template <int kMode, int kItems>
 __global__ void __launch_bounds__(kAdvBlock) advec_kernel(oppb_advec_batch b, oppb_move_status* st,
                                                           int32_t max_hops) {
+    static_assert(kChunkItems % kItems == 0, "a chunk is a whole number of passes");
+    __shared__ int s_chunk;
     unsigned long long my_calls = 0;
     int my_max = 0;
+    int cursor = 0;
     const int64_t sd = b.stride;
-    for (int w = blockIdx.x; w < b.n_work; w += gridDim.x) {
-        const int inst = find_instance(b.tile_prefix, b.n_instances, w);
-        const oppb_advec_instance& I = b.instances[inst];
-        const int32_t local = (w - __ldg(b.tile_prefix + inst)) * kAdvBlock + threadIdx.x;
-        const int32_t n_parts = __ldg(&I.n_parts);
-        if (local >= n_parts) continue;
-        const int64_t i = __ldg(&I.part_offset) + local;
-        double x = ld_stream(b.pos + i), y = ld_stream(b.pos + sd + i);
-        const double ex = __ldg(&I.extents[0]), ey = __ldg(&I.extents[1]);
-        if (kMode != kMoveOnly) {
-            const double dt = __ldg(&I.dt);
-            x = update_axis(x, __ldg(b.vel + i), dt, ex);
-            y = update_axis(y, __ldg(b.vel + sd + i), dt, ey);
-            st_stream(b.pos + i, x);
-            st_stream(b.pos + sd + i, y);
-        }
-        if (kMode != kUpdateOnly) {
-            int32_t cell = ld_stream(b.p2c + i);
-            if (cell == kRemoved) continue;
-            const int32_t cell0 = cell;
-            int mx = ld_stream(b.mdir + i), my = ld_stream(b.mdir + sd + i);
-            int err = 0;
-            const int calls = move_particle(b.cells, __ldg(&I.cell_offset), __ldg(&I.n_cells), x, y, mx, my, cell,
-                                            __ldg(&I.cell_width), ex, ey, max_hops, err);
-            if (err) raise_error(st, err, (int32_t)i);
-            st_stream(b.mdir + i, mx);
-            st_stream(b.mdir + sd + i, my);
-            if (cell != cell0) st_stream(b.p2c + i, cell);
-            my_calls += (unsigned long long)calls;
-            my_max = max(my_max, calls);
+    for (;;) {
+        if (threadIdx.x == 0) s_chunk = atomicAdd(b.work_counter, kChunkItems);
+        __syncthreads();
+        const int chunk = s_chunk;
+        __syncthreads();
+        if (chunk >= b.n_work) break;
+        for (int w0 = chunk; w0 < chunk + kChunkItems && w0 < b.n_work; w0 += kItems) {
+            double x[kItems], y[kItems], vx[kItems], vy[kItems];
+            int32_t cell[kItems], mx[kItems], my[kItems];
+            int64_t idx[kItems];
+            int inst[kItems];
+            bool ok[kItems];
+    #pragma unroll
+            for (int k = 0; k < kItems; k++) {  // all loads first
+                const int w = w0 + k;
+                ok[k] = false;
+                if (w >= b.n_work) continue;
+                inst[k] = find_instance(b.tile_prefix, b.n_instances, w, cursor);
+                const oppb_advec_instance& I = b.instances[inst[k]];
+                const int32_t local = (w - __ldg(b.tile_prefix + inst[k])) * kAdvBlock + threadIdx.x;
+                if (local >= __ldg(&I.n_parts)) continue;
+                ok[k] = true;
+                const int64_t i = __ldg(&I.part_offset) + local;
+                idx[k] = i;
+                x[k] = ld_stream(b.pos + i);
+                y[k] = ld_stream(b.pos + sd + i);
+                if (kMode != kMoveOnly) {
+                    vx[k] = __ldg(b.vel + i);
+                    vy[k] = __ldg(b.vel + sd + i);
+                }
+                if (kMode != kUpdateOnly) {
+                    cell[k] = ld_stream(b.p2c + i);
+                    mx[k] = ld_stream(b.mdir + i);
+                    my[k] = ld_stream(b.mdir + sd + i);
+                }
+            }
+    #pragma unroll
+            for (int k = 0; k < kItems; k++) {
+                if (!ok[k]) continue;
+                const oppb_advec_instance& I = b.instances[inst[k]];
+                const int64_t i = idx[k];
+                const double ex = __ldg(&I.extents[0]), ey = __ldg(&I.extents[1]);
+                if (kMode != kMoveOnly) {
+                    const double dt = __ldg(&I.dt);
+                    x[k] = update_axis(x[k], vx[k], dt, ex);
+                    y[k] = update_axis(y[k], vy[k], dt, ey);
+                    st_stream(b.pos + i, x[k]);
+                    st_stream(b.pos + sd + i, y[k]);
+                }
+                if (kMode != kUpdateOnly) {
+                    if (cell[k] == kRemoved) continue;
+                    const int32_t cell0 = cell[k];
+                    int err = 0;
+                    const int calls = move_particle(b.cells, __ldg(&I.cell_offset), __ldg(&I.n_cells), x[k], y[k], mx[k],
+                                                    my[k], cell[k], __ldg(&I.cell_width), ex, ey, max_hops, err);
+                    if (err) raise_error(st, err, (int32_t)i);
+                    st_stream(b.mdir + i, mx[k]);
+                    st_stream(b.mdir + sd + i, my[k]);
+                    if (cell[k] != cell0) st_stream(b.p2c + i, cell[k]);
+                    my_calls += (unsigned long long)calls;
+                    my_max = max(my_max, calls);
+                }
+            }
         }
     }
     if (kMode == kUpdateOnly) return;
@@ -169,24 +206,31 @@ __global__ void __launch_bounds__(256) advec_pack_kernel(double* cells, int32_t 
     reinterpret_cast<double4*>(cells)[(int64_t)cell_offset + c] = r;
 }
 
-// Persistent grid: resident blocks of the kernel on every SM (cached per device and mode).
-template <int kMode>
-int persistent_grid(int n_work) {
+// Persistent grid: resident blocks of the kernel on every SM (cached per device and variant).
+template <int kMode, int kItems>
+int persistent_grid(int n_blocks_needed) {
     static int cached[64] = {0};
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return n_work;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return n_blocks_needed;
     if (!cached[dev]) {
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, advec_kernel<kMode>, kAdvBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, advec_kernel<kMode, kItems>, kAdvBlock, 0);
         cached[dev] = sms * (per_sm > 0 ? per_sm : 1);
     }
-    return n_work < cached[dev] ? n_work : cached[dev];
+    return n_blocks_needed < cached[dev] ? n_blocks_needed : cached[dev];
+}
+
+template <int kMode, int kItems>
+void launch_items(const oppb_advec_batch* b, oppb_move_status* status, int32_t max_hops, cudaStream_t s) {
+    const int grid = persistent_grid<kMode, kItems>(ceil_div(b->n_work, kChunkItems));
+    advec_kernel<kMode, kItems><<<grid, kAdvBlock, 0, s>>>(*b, status, max_hops);
 }
 
 int check_batch(const oppb_advec_batch* b) {
     if (!b || b->n_instances <= 0 || b->n_work < 0 || !b->instances || !b->tile_prefix) return OPPB_ERR_ARG;
-    if (!b->pos || !b->vel || !b->mdir || !b->p2c || !b->cells || !aligned(b->cells, 32) || b->stride <= 0)
+    if (!b->pos || !b->vel || !b->mdir || !b->p2c || !b->cells || !aligned(b->cells, 32) || b->stride <= 0 ||
+        !b->work_counter)
         return OPPB_ERR_ARG;
     return OPPB_OK;
 }
@@ -197,7 +241,15 @@ int launch_advec(const oppb_advec_batch* b, oppb_move_status* status, int32_t ma
     if (rc) return rc;
     if (kMode != kUpdateOnly && (!status || max_hops <= 0)) return OPPB_ERR_ARG;
     if (b->n_work == 0) return OPPB_OK;
-    advec_kernel<kMode><<<persistent_grid<kMode>(b->n_work), kAdvBlock, 0, as_stream(stream)>>>(*b, status, max_hops);
+    cudaStream_t s = as_stream(stream);
+    if (cudaMemsetAsync(b->work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
+    const int items = tuning().advec_items;
+    if (items == 4)
+        launch_items<kMode, 4>(b, status, max_hops, s);
+    else if (items == 1)
+        launch_items<kMode, 1>(b, status, max_hops, s);
+    else
+        launch_items<kMode, 2>(b, status, max_hops, s);
     count_launches(1);
     return launch_status();
 }

@@ -46,7 +46,7 @@ class Dat(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("reserved", c_i32 * 6)]
+    _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("advec_items", c_i32), ("reserved", c_i32 * 5)]
 
 
 DEPOSIT_WARP_ATOMIC = 0
@@ -77,7 +77,8 @@ class AdvecInstance(C.Structure):
 
 class AdvecBatch(C.Structure):
     _fields_ = [("n_instances", c_i32), ("n_work", c_i32), ("instances", c_vp), ("tile_prefix", c_vp),
-                ("cells", c_vp), ("stride", c_i64), ("pos", c_vp), ("vel", c_vp), ("mdir", c_vp), ("p2c", c_vp)]
+                ("cells", c_vp), ("stride", c_i64), ("pos", c_vp), ("vel", c_vp), ("mdir", c_vp), ("p2c", c_vp),
+                ("work_counter", c_vp)]
 
 
 class FemPICMesh(C.Structure):
@@ -163,13 +164,15 @@ def check(fn: str, status: int) -> None:
         raise OppbError(fn, status)
 
 
-def set_tuning(deposit: int | None = None, replicas: int | None = None) -> None:
+def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_items: int | None = None) -> None:
     t = Tuning()
     load().oppb_get_tuning(C.byref(t))
     if deposit is not None:
         t.deposit = deposit
     if replicas is not None:
         t.replicas = replicas
+    if advec_items is not None:
+        t.advec_items = advec_items
     check("oppb_set_tuning", load().oppb_set_tuning(C.byref(t)))
 
 

@@ -80,6 +80,7 @@ class AdvecBatchDevice:
         self.mdir = torch.ones((2, cap), dtype=torch.int32, device=self.device)
         self.p2c = torch.zeros(cap, dtype=torch.int32, device=self.device)
         self.status = torch.zeros(8, dtype=torch.int32, device=self.device)
+        self.counter = torch.zeros(8, dtype=torch.int32, device=self.device)
         total_cells = sum(m.n_cells for m in meshes)
         self.cells = torch.zeros(total_cells * 4, dtype=torch.float64, device=self.device)
         table = (L.AdvecInstance * len(meshes))()
@@ -102,7 +103,7 @@ class AdvecBatchDevice:
         self.tile_prefix = torch.tensor(prefix, dtype=torch.int32, device=self.device)
         self.batch = L.AdvecBatch(len(meshes), prefix[-1], _ptr(self.instances), _ptr(self.tile_prefix),
                                   _ptr(self.cells), cap, _ptr(self.pos), _ptr(self.vel), _ptr(self.mdir),
-                                  _ptr(self.p2c))
+                                  _ptr(self.p2c), _ptr(self.counter))
         self.n_total = n_total
 
     def set_instance(self, k: int, pos, vel, mdir, p2c) -> None:
@@ -165,3 +166,23 @@ class AdvecBatchDevice:
         return {"pos": self.pos[:, a:a + n].T.contiguous().cpu().numpy(),
                 "mdir": self.mdir[:, a:a + n].T.contiguous().cpu().numpy(),
                 "p2c": self.p2c[a:a + n].cpu().numpy()}
+
+    def instance_batches(self) -> list:
+        """One single-instance batch per instance over the same buffers (for launching the
+        instances one by one).  Returns (batch, keep-alive tensors) pairs."""
+        import ctypes as C_
+
+        out = []
+        raw = self.instances.cpu().numpy().tobytes()
+        size = C_.sizeof(L.AdvecInstance)
+        for k, n in enumerate(self.counts):
+            inst = torch.frombuffer(bytearray(raw[k * size:(k + 1) * size]), dtype=torch.uint8).to(self.device)
+            pre = torch.tensor([0, (n + WORK_ITEM - 1) // WORK_ITEM], dtype=torch.int32, device=self.device)
+            b = L.AdvecBatch(1, int(pre[1].item()), _ptr(inst), _ptr(pre), _ptr(self.cells), self.capacity,
+                             _ptr(self.pos), _ptr(self.vel), _ptr(self.mdir), _ptr(self.p2c), _ptr(self.counter))
+            out.append((b, (inst, pre)))
+        return out
+
+    def step_batch(self, batch, max_hops: int = 4096, stream=None) -> None:
+        L.check("oppb_advec_step", self.lib.oppb_advec_step(C.byref(batch), _ptr(self.status), max_hops,
+                                                            _stream(stream)))
