@@ -417,6 +417,8 @@ CAB_WORKLOAD = ("CabanaPIC two-stream move + current deposit: 32x32x256 periodic
 # the interp record 160 B + faces 32 B read and the 12 accumulators read + written (192 B).
 CAB_BYTES_PER_PARTICLE = 108
 CAB_BYTES_PER_CELL = 384
+# DRAM bytes per particle of one full-size launch (ncu, profiles/cabana_move_deposit_kernel_twostream_32x32x256.txt).
+CAB_MEASURED_DRAM_BYTES_PER_PARTICLE = 122.0
 
 
 def run_cabana(dev, steps: int, warmup: int, cpu: bool, cpu_seconds: float) -> dict:
@@ -441,6 +443,7 @@ def run_cabana(dev, steps: int, warmup: int, cpu: bool, cpu_seconds: float) -> d
     s = torch.cuda.current_stream()
     t_ms, visits = [], 0
     l0 = lib.oppb_kernel_launches()
+    torch.cuda.profiler.start()
     for _ in range(steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
@@ -452,6 +455,7 @@ def run_cabana(dev, steps: int, warmup: int, cpu: bool, cpu_seconds: float) -> d
             raise L.OppbError("cabana move_deposit", st.error)
         t_ms.append(e0.elapsed_time(e1))
         visits += int(st.total_visits)
+    torch.cuda.profiler.stop()
     launches = lib.oppb_kernel_launches() - l0
     t = sum(t_ms) / 1e3
     bytes_call = CAB_BYTES_PER_PARTICLE * n + CAB_BYTES_PER_CELL * mesh.n_cells
@@ -462,7 +466,8 @@ def run_cabana(dev, steps: int, warmup: int, cpu: bool, cpu_seconds: float) -> d
            "gpu_launches": int(launches),
            "roofline": {"bound": "hbm", "achieved": bytes_call / (t / steps) / 1e9, "peak": peaks["hbm_gbs"],
                         "unit": "GB/s", "frac": bytes_call / (t / steps) / 1e9 / peaks["hbm_gbs"],
-                        "bytes_per_launch": bytes_call, "traffic": None}}
+                        "bytes_per_launch": bytes_call, "traffic": CAB_MEASURED_DRAM_BYTES_PER_PARTICLE * n,
+                        "traffic_source": TRAFFIC_SOURCE}}
     del cd
     torch.cuda.empty_cache()
     if cpu:
@@ -515,6 +520,8 @@ ADV_WORKLOAD = ("NESO-advection ensemble: 64 independent periodic square meshes,
 # Per step: read pos 16 + vel 16 + mdir 8 + p2c 4, write pos 16 + mdir 8 B per particle; 32 B per cell record.
 ADV_BYTES_PER_PARTICLE = 68
 ADV_BYTES_PER_CELL = 32
+# DRAM bytes per particle of one full-size launch (ncu, profiles/advec_kernel_neso_ensemble_64.txt).
+ADV_MEASURED_DRAM_BYTES_PER_PARTICLE = 76.2
 
 
 def run_advec(dev, steps: int, warmup: int, cpu: bool) -> dict:
@@ -572,7 +579,9 @@ def run_advec(dev, steps: int, warmup: int, cpu: bool) -> dict:
     l0 = lib.oppb_kernel_launches()
     t_graph, visits = timed(graph.replay, replays)
     graph_steps = replays * G
+    torch.cuda.profiler.start()
     t_direct, _ = timed(bd.step, graph_steps)
+    torch.cuda.profiler.stop()
     launches = lib.oppb_kernel_launches() - l0
     singles = bd.instance_batches()
     t_single, _ = timed(lambda: [bd.step_batch(b) for b, _ in singles], graph_steps)
@@ -589,7 +598,8 @@ def run_advec(dev, steps: int, warmup: int, cpu: bool) -> dict:
            "roofline": {"bound": "hbm", "achieved": bytes_step / (t_graph / graph_steps) / 1e9,
                         "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": bytes_step / (t_graph / graph_steps) / 1e9 / peaks["hbm_gbs"],
-                        "bytes_per_launch": bytes_step, "traffic": None}}
+                        "bytes_per_launch": bytes_step, "traffic": ADV_MEASURED_DRAM_BYTES_PER_PARTICLE * n,
+                        "traffic_source": TRAFFIC_SOURCE}}
     del bd, singles
     torch.cuda.empty_cache()
     if cpu:
@@ -721,6 +731,8 @@ def main():
     ap.add_argument("--no-advec", dest="advec", action="store_false",
                     help="skip the NESO-advection ensemble measurement")
     ap.add_argument("--advec-only", action="store_true", help="run only the NESO-advection ensemble measurement")
+    ap.add_argument("--advec-instances", type=int, default=None, help="ensemble size (default 64)")
+    ap.add_argument("--advec-side-max", type=int, default=None, help="largest mesh side (default 512)")
     ap.add_argument("--deposit", choices=["warp", "table"], default="warp",
                     help="deposit strategy: warp-run FP64 atomics or per-CTA shared node table")
     args = ap.parse_args()
@@ -734,6 +746,10 @@ def main():
     if args.cabana_dims:
         nx, ny, nz = (int(v) for v in args.cabana_dims.split(","))
         CAB.update(nx=nx, ny=ny, nz=nz, lx=nx / 32, ly=ny / 32, lz=nz / 32)
+    if args.advec_instances:
+        ADV["instances"] = args.advec_instances
+    if args.advec_side_max:
+        ADV["side_hi"] = max(args.advec_side_max, ADV["side_lo"])
     if args.advec_only and args.impl != "reference":
         import torch
 
