@@ -293,6 +293,33 @@ def cpu_baseline_port(hm, sample: dict, budget_s: float = 8.0) -> dict:
                       f"C oracle single thread, {ps // n} repetitions"}
 
 
+def replica_sum(v: float, dev) -> float:
+    """Sum of v over the ranks of the default process group (v itself without one)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def replica_job_value(particle_steps: float, seconds: float, ms_per_step: float, dev) -> tuple[float, float]:
+    """Whole-job throughput of independent replicas, one per rank: the particle-steps of all
+    ranks over the slowest rank's time (the max over ranks), and that rank's ms per step."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return particle_steps / seconds, ms_per_step
+    ps = torch.tensor([particle_steps], dtype=torch.float64, device=dev)
+    tm = torch.tensor([seconds, ms_per_step], dtype=torch.float64, device=dev)
+    dist.all_reduce(ps, op=dist.ReduceOp.SUM)
+    dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+    return float(ps.item()) / float(tm[0].item()), float(tm[1].item())
+
+
 def arm_ours(args) -> dict:
     import torch
     import torch.distributed as dist
@@ -335,22 +362,13 @@ def arm_ours(args) -> dict:
             dist.destroy_process_group()
         return {}
 
-    def reduce(v, op):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=op)
-        return float(t.item())
-
-    SUM, MAX = (dist.ReduceOp.SUM, dist.ReduceOp.MAX) if world > 1 else (None, None)
     res = {}
     for r in (f64, mixed):
         t = (r["t_move_ms"] + r["t_compact_ms"]) / 1e3
-        r["job_value"] = reduce(r["particle_steps"], SUM) / reduce(t, MAX)
-        r["job_ms_per_step"] = reduce(r["ms_per_step"], MAX)
+        r["job_value"], r["job_ms_per_step"] = replica_job_value(r["particle_steps"], t, r["ms_per_step"], dev)
     if "e2e" in mixed:
         e = mixed["e2e"]
-        e["value"] = reduce(e["value"], SUM) if world > 1 else e["value"]
+        e["value"] = replica_sum(e["value"], dev)
     res["f64"], res["mixed"] = f64, mixed
     if world > 1:
         dist.barrier()
