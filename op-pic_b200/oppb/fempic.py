@@ -252,6 +252,8 @@ class FemPIC:
         self._dep_ws = torch.empty(0, dtype=torch.uint8, device=self.device)
         self.lib = L.load()
         self.last = {}
+        self._pipe = None  # run_steps' copy stream, events and double buffers, made once
+        self._pipeline(5, inject_per_step)
 
     # workspace shared by hole fill and sort (grown on demand)
     def _workspace(self, nbytes: int) -> torch.Tensor:
@@ -387,6 +389,79 @@ class FemPIC:
                "compaction": kind}
         self.last = out
         self.iter += 1
+        return out
+
+
+    def _pipeline(self, rows: int, cols: int) -> dict:
+        """run_steps' state, kept between calls so that no call allocates or creates a stream
+        once it exists: the copy stream, its events, two device tables of at least
+        [rows][cols] and the node-charge buffer that alternates with node_charge."""
+        p = self._pipe
+        if p is None:
+            ev = lambda: torch.cuda.Event()  # noqa: E731
+            p = self._pipe = {"copy": torch.cuda.Stream(device=self.device), "alt": torch.empty_like(self.node_charge),
+                              "tables": [], "table_ready": [ev(), ev()], "table_free": [ev(), ev()],
+                              "charge_ready": [ev(), ev()], "charge_free": [ev(), ev()]}
+        t = p["tables"]
+        if not t or t[0].shape[0] < rows or t[0].shape[1] < cols:
+            rows, cols = max(rows, t[0].shape[0] if t else 0), max(cols, t[0].shape[1] if t else 0)
+            p["tables"] = [torch.empty((rows, cols), dtype=torch.float64, device=self.device) for _ in range(2)]
+        return p
+
+    def run_steps(self, host_tables: list[torch.Tensor], charges_out: list[torch.Tensor] | None = None) -> list[dict]:
+        """len(host_tables) steps fed from host memory, with the node charges of every step
+        copied back to the host.  host_tables: pinned CPU float64 [5][count] tables (the
+        step's injection randoms; count may differ between steps); charges_out: pinned CPU
+        float64 [n_nodes] tensors, one per step (or None).  Copies run on a second stream and
+        overlap the steps: the next step's table goes up while the current step computes,
+        and a step's charges come down (from one of two alternating node-charge buffers)
+        while the next step computes.  Returns the per-step records of step(); every copy
+        has completed on return, and node_charge holds the last step's charges."""
+        n = len(host_tables)
+        if n == 0:
+            return []
+        if charges_out is not None and len(charges_out) != n:
+            raise ValueError("charges_out needs one tensor per step")
+        cur = torch.cuda.current_stream(self.device)
+        p = self._pipeline(max(t.shape[0] for t in host_tables), max(t.shape[1] for t in host_tables))
+        copy = p["copy"]
+        table_ready, table_free = p["table_ready"], p["table_free"]
+        charge_ready, charge_free = p["charge_ready"], p["charge_free"]
+        charges = [self.node_charge, p["alt"]]
+        tables = [None, None]
+
+        def upload(k: int, b: int) -> None:  # on the copy stream, into buffer b once step k-2 has read it
+            rows, cols = host_tables[k].shape
+            tables[b] = p["tables"][b][:rows, :cols]
+            with torch.cuda.stream(copy):
+                copy.wait_event(table_free[b])
+                tables[b].copy_(host_tables[k], non_blocking=True)
+                table_ready[b].record(copy)
+
+        for e in table_free + charge_free:
+            e.record(cur)
+        upload(0, 0)
+        out = []
+        for k in range(n):
+            b = k % 2
+            if k + 1 < n:  # prefetch the next table into the other buffer
+                upload(k + 1, 1 - b)
+            cur.wait_event(table_ready[b])
+            cur.wait_event(charge_free[b])  # the copy of this buffer's previous charges is done
+            self.node_charge = charges[b]
+            out.append(self.step(tables[b]))
+            table_free[b].record(cur)
+            charge_ready[b].record(cur)
+            if charges_out is not None:
+                with torch.cuda.stream(copy):
+                    copy.wait_event(charge_ready[b])
+                    charges_out[k].copy_(charges[b], non_blocking=True)
+                    charge_free[b].record(copy)
+            else:
+                charge_free[b].record(cur)
+        p["alt"] = charges[n % 2]  # the buffer that does not hold the last step's charges
+        copy.synchronize()
+        cur.wait_stream(copy)
         return out
 
 

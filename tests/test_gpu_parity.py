@@ -448,3 +448,26 @@ def test_push_move_fused_equals_push_then_move(precision):
     for name in ("pos", "vel", "lc", "p2c"):
         np.testing.assert_array_equal(a[name].view(np.uint8), b[name].view(np.uint8), err_msg=name)
     _charge_close(qb, qa, CHARGE_RTOL)
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_run_steps_pipelined_equals_steps(precision):
+    """FemPIC.run_steps (host tables in, node charges out, copies overlapped on a second
+    stream) against step() one at a time: identical particles, each step's charges."""
+    hm = mesh()
+    kw = dict(inject_per_step=2000, precision=precision, fill="Sort_Periodic", fill_period=3)
+    a, b = FemPIC(hm, DEV, **kw), FemPIC(hm, DEV, **kw)
+    tables = [injection_randoms(5, k, 2000, 0.1) for k in range(7)]
+    host = [torch.from_numpy(np.ascontiguousarray(t.T)).pin_memory() for t in tables]
+    outs = [torch.empty(hm.n_nodes, dtype=torch.float64).pin_memory() for _ in tables]
+    # two calls (3 then 4 steps): the kept buffers are reused and, after an odd count, the
+    # second call starts from the other node-charge buffer
+    recs = a.run_steps(host[:3], outs[:3]) + a.run_steps(host[3:], outs[3:])
+    for k, t in enumerate(tables):
+        r = b.step(randoms_to_device(t, DEV))
+        assert (recs[k]["size"], recs[k]["removed"], recs[k]["visits"]) == (r["size"], r["removed"], r["visits"])
+        _charge_close(outs[k].numpy(), b.node_charge.cpu().numpy(), CHARGE_RTOL)
+    _charge_close(a.node_charge.cpu().numpy(), b.node_charge.cpu().numpy(), CHARGE_RTOL)
+    ga, gb = a.parts.host_aos(), b.parts.host_aos()
+    for name in ("pos", "vel", "lc", "p2c"):
+        np.testing.assert_array_equal(ga[name].view(np.uint8), gb[name].view(np.uint8), err_msg=name)
