@@ -371,6 +371,11 @@ def arm_ours(args) -> dict:
         e = mixed["e2e"]
         e["value"] = replica_sum(e["value"], dev)
     res["f64"], res["mixed"] = f64, mixed
+    advec = None
+    if args.advec:  # the ensemble is split over the ranks (before the process group goes)
+        if world > 1:
+            dist.barrier()
+        advec = run_advec(dev, min(args.steps, 20), args.warmup, args.cpu_baseline, rank, world)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -421,8 +426,8 @@ def arm_ours(args) -> dict:
     if args.cabana and world == 1:
         line["cabanapic"] = run_cabana(dev, min(args.steps, 20), args.warmup, args.cpu_baseline, args.cpu_seconds)
         line["gpu_launches_cabanapic"] = line["cabanapic"]["gpu_launches"]
-    if args.advec and world == 1:
-        line["advec_ensemble"] = run_advec(dev, min(args.steps, 20), args.warmup, args.cpu_baseline)
+    if advec is not None:
+        line["advec_ensemble"] = advec
     return line
 
 
@@ -543,85 +548,101 @@ ADV_BYTES_PER_CELL = 32
 ADV_MEASURED_DRAM_BYTES_PER_PARTICLE = 76.2
 
 
-def run_advec(dev, steps: int, warmup: int, cpu: bool) -> dict:
+def run_advec(dev, steps: int, warmup: int, cpu: bool, rank: int = 0, world: int = 1) -> dict:
     """The ensemble three ways on the same state: CUDA-graph replay of the batched step, the
-    batched step launched directly, and one launch per instance."""
+    batched step launched directly, and one launch per instance.  With world > 1 the
+    instances are split over the ranks by shard_instances (longest processing time first by
+    particle count); each rank advances its shard in its own persistent launch and the
+    figures are all particle-steps over the slowest rank's time (strong scaling: the ensemble
+    is the same at every N).  Every rank takes the same collective steps."""
     import numpy as np
     import torch
 
     from oppb import _lib as L
-    from oppb.advec import AdvecBatchDevice, AdvecMesh
+    from oppb.advec import AdvecBatchDevice, AdvecMesh, shard_instances
 
     rng = np.random.default_rng(ADV["seed"])
     sides = rng.integers(ADV["side_lo"], ADV["side_hi"] + 1, ADV["instances"])
     ppcs = rng.integers(ADV["ppc_lo"], ADV["ppc_hi"] + 1, ADV["instances"])
-    meshes = [AdvecMesh(int(s), int(s), ADV["cell_width"]) for s in sides]
-    counts = [m.n_cells * int(p) for m, p in zip(meshes, ppcs)]
-    bd = AdvecBatchDevice(meshes, counts, [ADV["dt"]] * len(meshes), dev)
-    for k, p in enumerate(ppcs):
-        bd.fill_instance(k, int(p), ADV["v_sd"], ADV["v_clip"], ADV["seed"] * 1000 + k)
-    n = bd.n_total
+    weights = [int(sd) * int(sd) * int(pc) for sd, pc in zip(sides, ppcs)]
+    shards = shard_instances(weights, world)
+    mine = shards[rank]
+    meshes = [AdvecMesh(int(sides[k]), int(sides[k]), ADV["cell_width"]) for k in mine]
+    counts = [m.n_cells * int(ppcs[k]) for m, k in zip(meshes, mine)]
+    n = sum(counts)
     lib = L.load()
-    for _ in range(warmup):
-        bd.step()
-    torch.cuda.synchronize()
-    s = torch.cuda.current_stream()
-    E = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-
-    def timed(fn, reps):
-        bd.zero_status()
-        torch.cuda.synchronize()
-        e0, e1 = E(), E()
-        e0.record(s)
-        for _ in range(reps):
-            fn()
-        e1.record(s)
-        e1.synchronize()
-        st = bd.status_host()
-        if st.error:
-            raise L.OppbError("advec step", st.error)
-        return e0.elapsed_time(e1) / 1e3, int(st.total_visits)
-
-    # Autotune the particles in flight per thread (the kernel's work items per block pass) on
-    # this state, then capture the graph with the fastest choice.
-    sweep = {}
-    for items in (1, 2, 4):
-        L.set_tuning(advec_items=items)
-        bd.step()
-        t_k, _ = timed(bd.step, 3)
-        sweep[items] = n * 3 / t_k
-    best = max(sweep, key=sweep.get)
-    L.set_tuning(advec_items=best)
     G = ADV["graph_steps"]
-    graph = bd.capture(G)
-    replays = max(1, steps // G)
-    l0 = lib.oppb_kernel_launches()
-    t_graph, visits = timed(graph.replay, replays)
-    graph_steps = replays * G
-    torch.cuda.profiler.start()
-    t_direct, _ = timed(bd.step, graph_steps)
-    torch.cuda.profiler.stop()
-    launches = lib.oppb_kernel_launches() - l0
-    singles = bd.instance_batches()
-    t_single, _ = timed(lambda: [bd.step_batch(b) for b, _ in singles], graph_steps)
-    del graph
-    bytes_step = ADV_BYTES_PER_PARTICLE * n + ADV_BYTES_PER_CELL * sum(m.n_cells for m in meshes)
+    graph_steps = max(1, steps // G) * G
+    t_graph = t_direct = t_single = 0.0
+    visits, launches, sweep, best = 0, 0, {}, None
+    if mine:
+        bd = AdvecBatchDevice(meshes, counts, [ADV["dt"]] * len(meshes), dev)
+        for j, k in enumerate(mine):  # seeded by the global instance index: same state at any N
+            bd.fill_instance(j, int(ppcs[k]), ADV["v_sd"], ADV["v_clip"], ADV["seed"] * 1000 + k)
+        for _ in range(warmup):
+            bd.step()
+        torch.cuda.synchronize()
+        s = torch.cuda.current_stream()
+        E = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+        def timed(fn, reps):
+            bd.zero_status()
+            torch.cuda.synchronize()
+            e0, e1 = E(), E()
+            e0.record(s)
+            for _ in range(reps):
+                fn()
+            e1.record(s)
+            e1.synchronize()
+            st = bd.status_host()
+            if st.error:
+                raise L.OppbError("advec step", st.error)
+            return e0.elapsed_time(e1) / 1e3, int(st.total_visits)
+
+        # Autotune the particles in flight per thread (the kernel's work items per block pass)
+        # on this state, then capture the graph with the fastest choice.
+        for items in (1, 2, 4):
+            L.set_tuning(advec_items=items)
+            bd.step()
+            t_k, _ = timed(bd.step, 3)
+            sweep[items] = n * 3 / t_k
+        best = max(sweep, key=sweep.get)
+        L.set_tuning(advec_items=best)
+        graph = bd.capture(G)
+        l0 = lib.oppb_kernel_launches()
+        t_graph, visits = timed(graph.replay, graph_steps // G)
+        torch.cuda.profiler.start()
+        t_direct, _ = timed(bd.step, graph_steps)
+        torch.cuda.profiler.stop()
+        launches = lib.oppb_kernel_launches() - l0
+        singles = bd.instance_batches()
+        t_single, _ = timed(lambda: [bd.step_batch(b) for b, _ in singles], graph_steps)
+        del graph, bd, singles
+        torch.cuda.empty_cache()
+    ps = n * graph_steps
+    value, ms_step = replica_job_value(ps, t_graph, 1e3 * t_graph / graph_steps, dev)
+    direct, _ = replica_job_value(ps, t_direct, 0.0, dev)
+    single, _ = replica_job_value(ps, t_single, 0.0, dev)
+    n_all = int(round(replica_sum(float(n), dev)))
+    cells = sum(m.n_cells for m in meshes)
+    bytes_step = ADV_BYTES_PER_PARTICLE * n + ADV_BYTES_PER_CELL * cells
     peaks = measured_peaks()
+    achieved = bytes_step / (t_graph / graph_steps) / 1e9 if t_graph > 0 else 0.0
     out = {"workload": ADV_WORKLOAD, "metric": "particle-steps/s (update_pos + move, all instances)", "unit": UNIT,
-           "value": n * graph_steps / t_graph, "particles": n, "instances": len(meshes),
-           "cells": int(sum(m.n_cells for m in meshes)), "steps": graph_steps, "warmup": warmup,
-           "ms_per_step": 1e3 * t_graph / graph_steps, "calls_per_particle": visits / (n * graph_steps),
-           "direct_launch_value": n * graph_steps / t_direct, "per_instance_launch_value": n * graph_steps / t_single,
-           "dtype": "f64", "gpu_launches": int(launches),
+           "value": value, "particles": n_all, "instances": len(sides),
+           "cells": int(sum(int(sd) * int(sd) for sd in sides)), "steps": graph_steps, "warmup": warmup,
+           "ms_per_step": ms_step, "calls_per_particle": visits / max(1, ps),
+           "direct_launch_value": direct, "per_instance_launch_value": single,
+           "dtype": "f64", "gpu_launches": int(launches), "scaling": "strong" if world > 1 else "weak",
+           "sharding": {"rule": "longest processing time first by particle count, no data-path collective",
+                        "ranks": world, "instances_per_rank": [len(x) for x in shards],
+                        "particles_per_rank": [sum(int(sides[k]) ** 2 * int(ppcs[k]) for k in x) for x in shards]},
            "autotune": {"advec_items": {str(k): v for k, v in sweep.items()}, "chosen": best},
-           "roofline": {"bound": "hbm", "achieved": bytes_step / (t_graph / graph_steps) / 1e9,
-                        "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                        "frac": bytes_step / (t_graph / graph_steps) / 1e9 / peaks["hbm_gbs"],
-                        "bytes_per_launch": bytes_step, "traffic": ADV_MEASURED_DRAM_BYTES_PER_PARTICLE * n,
-                        "traffic_source": TRAFFIC_SOURCE}}
-    del bd, singles
-    torch.cuda.empty_cache()
-    if cpu:
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": achieved / peaks["hbm_gbs"], "bytes_per_launch": bytes_step,
+                        "traffic": ADV_MEASURED_DRAM_BYTES_PER_PARTICLE * n, "traffic_source": TRAFFIC_SOURCE,
+                        "what": "rank 0's persistent launch over its shard"}}
+    if cpu and rank == 0:
         out["cpu_baseline"] = advec_cpu_baseline()
     return out
 

@@ -9,6 +9,9 @@ Host-side set-up mirrors the reference app where the particle path needs it:
               normal velocities, move direction (1, 1); seeded numpy generator
   AdvecBatch  device buffers of many instances concatenated, the instance table, the step
               launch and its CUDA-graph capture
+  shard_instances  the split of an ensemble over GPUs: instances are independent, so each
+              rank advances its own subset in its own persistent launch, with no collective
+              on the data path
 """
 from __future__ import annotations
 
@@ -51,6 +54,24 @@ def particles(mesh: AdvecMesh, ppc: int, v_sd: float, seed: int, v_clip: float |
 
 
 WORK_ITEM = 256  # particles per work item of the persistent launch
+
+
+def shard_instances(weights, n_ranks: int) -> list[list[int]]:
+    """Longest-processing-time-first split of independent instances over n_ranks GPUs:
+    instances in decreasing weight (ties: lower index first) each go to the rank with the
+    least weight so far (ties: lower rank).  The weight is the instance's particle count, the
+    work of a step.  Deterministic, so every rank computes the same split from the same
+    list.  Returns the instance indices of every rank in increasing order; the largest load
+    is within the largest weight of the mean."""
+    if n_ranks < 1:
+        raise ValueError("n_ranks must be at least 1")
+    loads = [0] * n_ranks
+    out: list[list[int]] = [[] for _ in range(n_ranks)]
+    for i in sorted(range(len(weights)), key=lambda i: (-weights[i], i)):
+        r = min(range(n_ranks), key=lambda r: (loads[r], r))
+        out[r].append(i)
+        loads[r] += weights[i]
+    return [sorted(o) for o in out]
 
 
 def _ptr(t) -> int:

@@ -51,3 +51,25 @@ def test_mesh_neighbours_periodic():
         np.testing.assert_array_equal(m.c2c[m.c2c[:, a], b], np.arange(12))
     np.testing.assert_allclose(m.c_pos_ll[5], [0.5, 0.5])
     assert m.extents == (2.0, 1.5)
+
+
+def test_shard_instances_lpt():
+    from oppb.advec import shard_instances
+
+    rng = np.random.default_rng(4)
+    w = [int(x) for x in rng.integers(1, 10**6, 64)]
+    for ranks in (1, 2, 3, 4, 8, 64, 70):
+        sh = shard_instances(w, ranks)
+        assert len(sh) == ranks
+        flat = sorted(i for s in sh for i in s)
+        assert flat == list(range(len(w)))  # a partition of the instances
+        assert all(s == sorted(s) for s in sh)
+        loads = [sum(w[i] for i in s) for s in sh]
+        assert max(loads) <= sum(w) / ranks + max(w)  # the LPT bound
+    assert shard_instances(w, 1) == [list(range(64))]
+    # by hand: 7 (#1) -> r0, 5 (#3) -> r1, 4 (#2) -> r1 (5 < 7), 3 (#0) -> r0 (7 < 9),
+    # 3 (#4) -> r1 (9 < 10); loads 10 and 12
+    assert shard_instances([3, 7, 4, 5, 3], 2) == [[0, 1], [2, 3, 4]]
+    assert shard_instances([5, 5], 2) == [[0], [1]]  # ties: lower index to lower rank
+    with pytest.raises(ValueError):
+        shard_instances(w, 0)
