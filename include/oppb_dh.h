@@ -1,0 +1,91 @@
+/* C ABI of the direct-hop (DH) seed of the FemPIC move: OP-PIC's structured cell mapper
+ * (opp_lib/include/opp_direct_hop_core.h CellMapper, seq build
+ * opp_lib/src/seq/opp_direct_hop_seq.cpp) and the global-move pre-pass of the move loop
+ * (apps_codegen/app_fempic_cg/seq/move_kernel_loop.hpp:112-131, CUDA
+ * opp_dev_checkForGlobalMove3D_kernel in opp_lib/include/device_kernels/cuda_inline_kernels.h).
+ *
+ * A uniform grid of spacing h covers the mesh's bounding box.  Every grid box holds one mesh
+ * cell (or none); with the seed on, every particle's walk starts from the cell of the box its
+ * position falls in instead of from its previous cell.
+ *
+ * Conventions are those of oppb.h (plain pointers, int status, explicit stream).  The map is
+ * built on the GPU: cells are binned into the grid boxes their bounding boxes overlap, and
+ * each query takes the lowest-index cell that contains the point among its box's candidates.
+ * That is the reference's answer, which is the first cell, in index order, that contains the
+ * point, found there by a search over all cells per point.
+ */
+#ifndef OPPB_DH_H
+#define OPPB_DH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "oppb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The structured grid (CellMapper fields).  min/max: the global bounding box of the nodes
+ * widened by `expansion` (BoundingBox(n_pos, 3, expansion), opp_direct_hop_core.h:70-120);
+ * dims: boxes per axis (CellMapper::init_host, :317-380); map: device [size] mesh cell of
+ * each box, x fastest (index = x + X*y + X*Y*z), OPPB_REMOVED_CELL where no cell. */
+typedef struct oppb_dh_grid {
+    double   min[3];
+    double   max[3];
+    double   spacing;       /* grid_spacing                                    */
+    double   inv_spacing;   /* 1.0 / spacing (CellMapper::oneOverGridSpacing)  */
+    int64_t  dims[3];
+    int64_t  size;          /* dims[0] * dims[1] * dims[2]                     */
+    int32_t* map;           /* device [size], filled by oppb_dh_build          */
+} oppb_dh_grid;
+
+/* Host: bounding box and grid dims from the node positions (host AoS [n_nodes][3]), as the
+ * reference computes them (including its floating-point loop counts).  Leaves map untouched.
+ * Returns OPPB_ERR_ARG for spacing <= 0, n_nodes <= 0 or a grid of more than 2^31 boxes. */
+int oppb_dh_grid_init(const double* n_pos, int32_t n_nodes, double spacing, const double expansion[3],
+                      oppb_dh_grid* grid);
+
+/* Device: fills grid->map (generateStructuredMesh, opp_direct_hop_seq.cpp:134-302, steps 1 and
+ * 3: box centroid, then the centroid nudged by h/100 along x, y and z in turn, then the
+ * lowest-index cell holding one of the box's 8 corners).  The cells' global ids are their
+ * indices (one unpartitioned mesh).  n_pos: device SoA [3][n_nodes].  Uses the mesh's FP64
+ * records (det, nav) and c2n.  Workspace: when ws_bytes is too small (or workspace is NULL)
+ * the call returns OPPB_ERR_WORKSPACE with *ws_needed set, after synchronising the stream
+ * once to read the number of (cell, box) pairs; call again with that much. */
+int oppb_dh_build(const oppb_tet_mesh* mesh, const double* n_pos, oppb_dh_grid* grid, void* workspace,
+                  size_t ws_bytes, size_t* ws_needed, void* stream);
+
+/* ------------------------------------------------------------- general move entry point */
+
+#define OPPB_PRECISION_F64   0
+#define OPPB_PRECISION_MIXED 1
+
+/* One call for every variant of the move launch.  deposit: 0 = move only (FP64 only),
+ * 1 = node-charge deposit fused.  push: 1 = calculate_new_pos_vel as the kernel's prologue
+ * (needs deposit).  dh: the direct-hop seed (NULL = walk from the previous cell), applied
+ * after the push, as the reference's global-move pre-pass runs after the push loop: a
+ * position outside the grid, or in a box with no cell, removes the particle (the CUDA
+ * backend's rule), else the walk starts from the box's cell. */
+typedef struct oppb_move_options {
+    int32_t precision;            /* OPPB_PRECISION_*                                  */
+    int32_t deposit;
+    int32_t push;
+    int32_t reserved;
+    double  qm, dt;               /* push constants (CONST_charge/CONST_mass, CONST_dt) */
+    double  band;                 /* mixed path: FP64 re-check band (e.g. 1e-5)        */
+    const oppb_dh_grid* dh;       /* host struct; map on the device; may be NULL        */
+} oppb_move_options;
+
+/* The move of oppb.h (oppb_move_f64 / oppb_move_deposit_* / oppb_push_move_deposit_*) with
+ * options; identical results for the same options without dh.  node_charge, workspace as
+ * oppb_move_deposit_f64. */
+int oppb_move_ex(const oppb_tet_mesh* mesh, const oppb_particles* parts, const oppb_move_options* opt,
+                 double* node_charge, oppb_move_status* status, int32_t max_hops, void* workspace,
+                 size_t ws_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPPB_DH_H */

@@ -27,7 +27,9 @@ NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", f"
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", f"-I{INC}", "-Wall"]
 # Sources whose FP64 expressions must keep the reference's written order with one rounding
 # per operation: no FMA contraction anywhere in the file.
-PER_FILE_NVCC_FLAGS = {"cabana.cu": ["-fmad=false"], "advec.cu": ["-fmad=false"]}
+PER_FILE_NVCC_FLAGS = {"cabana.cu": ["-fmad=false"], "advec.cu": ["-fmad=false"],
+                       # the grid set-up loops of the direct-hop mapper run on the host
+                       "dh.cu": ["-Xcompiler", "-ffp-contract=off"]}
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:

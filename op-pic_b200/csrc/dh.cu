@@ -1,0 +1,263 @@
+// Direct-hop (DH) structured grid of the FemPIC move (include/oppb_dh.h): the host set-up of
+// the grid (OP-PIC's BoundingBox and CellMapper::init_host) and its build on the GPU.
+//
+// The reference fills the map on the host by testing, for each grid box, every mesh cell in
+// index order until one contains the query point (opp_lib/src/seq/opp_direct_hop_seq.cpp:
+// 134-302 with the checker of apps_codegen/app_fempic_cg/seq/move_kernel_loop.hpp:170-198):
+// O(boxes x cells), hours at millions of cells.  Here the answer is the same, the lowest
+// index among the cells whose FP64 barycentric test accepts the point, but the candidates
+// come from a binning of the cells into the grid boxes:
+//   1. every cell is binned into each box that its node bounding box, widened by 1/1000 of
+//      its extent, overlaps (count, exclusive scan, fill);
+//   2. one thread per box runs the reference's query sequence, testing only the cells
+//      binned into the box that holds each query point.
+// A cell accepts a point only within the 1e-10 tolerance of its barycentric weights, far
+// inside the widening, and the bin of a coordinate is monotone in it, so every accepting
+// cell is among the candidates of the point's box: the lowest accepting index is found.
+
+#include <cfloat>
+#include <cmath>
+
+#include "oppb_common.cuh"
+#include "oppb_dh.h"
+#include "scan.cuh"
+#include "tet_f64.cuh"
+
+namespace oppb {
+namespace {
+
+constexpr int kDhBlock = 256;
+constexpr double kBoundOffset = 1e-12;  // BOUND_OFFSET, opp_lib/include/opp_direct_hop_core.h:37
+constexpr double kBinWiden = 1e-3;      // cells are binned with their box widened by this share of its extent
+constexpr int64_t kMaxLoop = int64_t(1) << 31;
+
+struct GridArgs {
+    double min[3], max[3];
+    double h;
+    int64_t dims[3];
+};
+
+inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Bin of coordinate v on axis d: (v - min) / h truncated and clamped to [0, dims - 1].
+// Non-decreasing in v.
+__device__ __forceinline__ int64_t bin_of(const GridArgs& g, int d, double v) {
+    const double t = __ddiv_rn(__dsub_rn(v, g.min[d]), g.h);
+    if (!(t > 0.0)) return 0;
+    if (t >= (double)(g.dims[d] - 1)) return g.dims[d] - 1;
+    return (int64_t)t;
+}
+
+// Node bounding box of cell c, widened; false for a cell with a node index out of range.
+__device__ __forceinline__ bool cell_bins(const oppb_tet_mesh& m, const double* npos, int32_t c, const GridArgs& g,
+                                          int64_t b0[3], int64_t b1[3]) {
+    const int4 nd = ldg_i4(m.c2n + (int64_t)c * 4);
+    const int n[4] = {nd.x, nd.y, nd.z, nd.w};
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if ((uint32_t)n[k] >= (uint32_t)m.n_nodes) return false;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double v = __ldg(npos + (int64_t)d * m.n_nodes + n[k]);
+            lo[d] = fmin(lo[d], v);
+            hi[d] = fmax(hi[d], v);
+        }
+    }
+    const double ext = fmax(fmax(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]);
+    const double w = kBinWiden * ext;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        b0[d] = bin_of(g, d, lo[d] - w);
+        b1[d] = bin_of(g, d, hi[d] + w);
+    }
+    return true;
+}
+
+// kMode 0: add the number of (cell, box) pairs to *pairs; 1: count the cells of every box;
+// 2: write each cell into its boxes' lists.
+template <int kMode>
+__global__ void __launch_bounds__(kDhBlock) dh_bin_kernel(oppb_tet_mesh m, const double* npos, GridArgs g,
+                                                          unsigned long long* pairs, int* counts, int* cursor,
+                                                          int* list) {
+    const int32_t c = (int32_t)(blockIdx.x * kDhBlock + threadIdx.x);
+    int64_t b0[3], b1[3];
+    const bool ok = c < m.n_cells && cell_bins(m, npos, c, g, b0, b1);
+    if (kMode == 0) {
+        unsigned long long s =
+            ok ? (unsigned long long)((b1[0] - b0[0] + 1) * (b1[1] - b0[1] + 1) * (b1[2] - b0[2] + 1)) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFullMask, s, o);
+        if ((threadIdx.x & 31) == 0 && s) atomicAdd(pairs, s);
+        return;
+    }
+    if (!ok) return;
+    for (int64_t z = b0[2]; z <= b1[2]; z++)
+        for (int64_t y = b0[1]; y <= b1[1]; y++)
+            for (int64_t x = b0[0]; x <= b1[0]; x++) {
+                const int64_t b = x + g.dims[0] * (y + g.dims[1] * z);
+                if (kMode == 1)
+                    atomicAdd(counts + b, 1);
+                else
+                    list[atomicAdd(cursor + b, 1)] = c;
+            }
+}
+
+// Lowest-index cell whose FP64 barycentric test (the move kernel's) accepts p, or kRemoved.
+__device__ int32_t first_cell(const oppb_tet_mesh& m, const GridArgs& g, const int* offsets, const int* list,
+                              const double p[3]) {
+    const int64_t b = bin_of(g, 0, p[0]) + g.dims[0] * (bin_of(g, 1, p[1]) + g.dims[1] * bin_of(g, 2, p[2]));
+    int32_t best = kRemoved;
+    for (int k = offsets[b]; k < offsets[b + 1]; k++) {
+        const int32_t c = list[k];
+        if (c >= best) continue;
+        double l[4];
+        int nb[4];
+        visit_f64(m, c, p[0], p[1], p[2], l, nb);
+        if (inside_f64(l)) best = c;
+    }
+    return best;
+}
+
+// One thread per grid box: generateStructuredMesh steps 1 and 3 for the box.
+__global__ void __launch_bounds__(kDhBlock) dh_query_kernel(oppb_tet_mesh m, GridArgs g, const int* offsets,
+                                                            const int* list, int32_t* map, int64_t size) {
+    const int64_t idx = (int64_t)blockIdx.x * kDhBlock + threadIdx.x;
+    if (idx >= size) return;
+    const int64_t ix = idx % g.dims[0], iy = (idx / g.dims[0]) % g.dims[1], iz = idx / (g.dims[0] * g.dims[1]);
+    const int64_t ii[3] = {ix, iy, iz};
+    // Box corner min + i*h (opp_direct_hop_seq.cpp:156-162) and centroid, clamped to the box's
+    // upper bound (getCentroidOfBox, ASSIGN_CENTROID_TO_DIM of opp_lib/include/opp_defs.h:121-127).
+    double corner[3], q[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        corner[d] = __dadd_rn(g.min[d], __dmul_rn((double)ii[d], g.h));
+        q[d] = (__dadd_rn(corner[d], g.h) <= g.max[d]) ? __dadd_rn(corner[d], __dmul_rn(g.h, 0.5))
+                                                       : __dmul_rn(__dadd_rn(corner[d], g.max[d]), 0.5);
+    }
+    int32_t cid = first_cell(m, g, offsets, list, q);
+    // Not found: nudge the centroid by h/100 along x, then y, then z (cumulative, :172-183).
+    const double nudge = __ddiv_rn(g.h, 100.0);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        if (cid != kRemoved) break;
+        q[d] = __dadd_rn(q[d], nudge);
+        cid = first_cell(m, g, offsets, list, q);
+    }
+    if (cid == kRemoved) {
+        // Step 3 (:214-246): the lowest cell holding one of the box's 8 corners, each corner
+        // clamped to the upper bound (GET_VERT, opp_defs.h:115).
+        for (int k = 0; k < 8; k++) {
+            double v[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const double t = ((k >> d) & 1) ? __dadd_rn(corner[d], g.h) : corner[d];
+                v[d] = (t > g.max[d]) ? g.max[d] : t;
+            }
+            const int32_t c = first_cell(m, g, offsets, list, v);
+            if (c < cid) cid = c;
+        }
+    }
+    map[idx] = cid;
+}
+
+// The (cell, box) pair counter of a build: fixed device scratch, so that sizing the
+// workspace needs no caller memory.  Calls on one device must not overlap.
+__device__ unsigned long long g_dh_pairs;
+
+}  // namespace
+}  // namespace oppb
+
+extern "C" int oppb_dh_grid_init(const double* n_pos, int32_t n_nodes, double spacing, const double expansion[3],
+                                 oppb_dh_grid* g) {
+    if (!n_pos || !expansion || !g || n_nodes <= 0 || !(spacing > 0.0) || !std::isfinite(spacing))
+        return OPPB_ERR_ARG;
+    // BoundingBox(n_pos, 3, expansion) (opp_lib/include/opp_direct_hop_core.h:70-120): the
+    // running max starts at MIN_REAL = DBL_MIN, and the x/y widening reads the expansion's
+    // x for both minima and its y for both maxima, as written there.
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {DBL_MIN, DBL_MIN, DBL_MIN};
+    for (int32_t i = 0; i < n_nodes; i++)
+        for (int d = 0; d < 3; d++) {
+            const double v = n_pos[3 * (int64_t)i + d];
+            mn[d] = (mn[d] < v) ? mn[d] : v;  // std::min(v, mn)
+            mx[d] = (v < mx[d]) ? mx[d] : v;  // std::max(v, mx)
+        }
+    mn[0] -= (expansion[0] + oppb::kBoundOffset);
+    mn[1] -= (expansion[0] + oppb::kBoundOffset);
+    mx[0] += (expansion[1] - oppb::kBoundOffset);
+    mx[1] += (expansion[1] - oppb::kBoundOffset);
+    mn[2] -= (expansion[2] + oppb::kBoundOffset);
+    mx[2] += (expansion[2] - oppb::kBoundOffset);
+    // CellMapper::init_host (:317-380): boxes per axis = 1 + the count of the loop
+    // `for (v = min; v < max; v += h)`, in floating point as there.
+    int64_t dims[3];
+    for (int d = 0; d < 3; d++) {
+        int64_t a = 0;
+        for (double v = mn[d]; v < mx[d]; v += spacing)
+            if (++a > oppb::kMaxLoop) return OPPB_ERR_ARG;
+        dims[d] = a + 1;
+    }
+    const double size = (double)dims[0] * (double)dims[1] * (double)dims[2];
+    if (size > 2147483646.0) return OPPB_ERR_ARG;
+    for (int d = 0; d < 3; d++) {
+        g->min[d] = mn[d];
+        g->max[d] = mx[d];
+        g->dims[d] = dims[d];
+    }
+    g->spacing = spacing;
+    g->inv_spacing = 1.0 / spacing;
+    g->size = dims[0] * dims[1] * dims[2];
+    return OPPB_OK;
+}
+
+extern "C" int oppb_dh_build(const oppb_tet_mesh* mesh, const double* n_pos, oppb_dh_grid* grid, void* workspace,
+                             size_t ws_bytes, size_t* ws_needed, void* stream) {
+    using namespace oppb;
+    if (!mesh || !n_pos || !grid || !grid->map || mesh->n_cells <= 0 || mesh->n_nodes <= 0) return OPPB_ERR_ARG;
+    if (!mesh->det || !mesh->nav || !mesh->c2n || !aligned(mesh->det, 32) || !aligned(mesh->nav, 32) ||
+        !aligned(mesh->c2n, 16))
+        return OPPB_ERR_ARG;
+    if (grid->size <= 0 || grid->size > 2147483646 || !(grid->spacing > 0.0) ||
+        grid->size != grid->dims[0] * grid->dims[1] * grid->dims[2])
+        return OPPB_ERR_ARG;
+    const GridArgs g{{grid->min[0], grid->min[1], grid->min[2]},
+                     {grid->max[0], grid->max[1], grid->max[2]},
+                     grid->spacing,
+                     {grid->dims[0], grid->dims[1], grid->dims[2]}};
+    cudaStream_t s = as_stream(stream);
+    unsigned long long* d_pairs = nullptr;
+    if (cudaGetSymbolAddress(reinterpret_cast<void**>(&d_pairs), g_dh_pairs) != cudaSuccess) return OPPB_ERR_LAUNCH;
+    const int cell_grid = ceil_div(mesh->n_cells, kDhBlock);
+    if (cudaMemsetAsync(d_pairs, 0, sizeof(unsigned long long), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
+    dh_bin_kernel<0><<<cell_grid, kDhBlock, 0, s>>>(*mesh, n_pos, g, d_pairs, nullptr, nullptr, nullptr);
+    count_launches(1);
+    unsigned long long pairs = 0;
+    if (cudaMemcpyAsync(&pairs, d_pairs, sizeof pairs, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return OPPB_ERR_LAUNCH;
+    if (pairs > 2147483647ull) return OPPB_ERR_ARG;  // grid far finer than the cells
+    const int64_t n = grid->size;
+    const size_t need = align256(sizeof(int) * (size_t)(n + 1)) + align256(sizeof(int) * (size_t)n) +
+                        align256(sizeof(int) * (size_t)(pairs ? pairs : 1)) +
+                        align256(sizeof(int) * scan_scratch_ints(n + 1));
+    if (ws_needed) *ws_needed = need;
+    if (!workspace || ws_bytes < need || !aligned(workspace, 256)) return OPPB_ERR_WORKSPACE;
+    char* w = static_cast<char*>(workspace);
+    int* offsets = reinterpret_cast<int*>(w);
+    w += align256(sizeof(int) * (size_t)(n + 1));
+    int* cursor = reinterpret_cast<int*>(w);
+    w += align256(sizeof(int) * (size_t)n);
+    int* list = reinterpret_cast<int*>(w);
+    w += align256(sizeof(int) * (size_t)(pairs ? pairs : 1));
+    int* scratch = reinterpret_cast<int*>(w);
+    if (cudaMemsetAsync(offsets, 0, sizeof(int) * (size_t)(n + 1), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
+    dh_bin_kernel<1><<<cell_grid, kDhBlock, 0, s>>>(*mesh, n_pos, g, nullptr, offsets, nullptr, nullptr);
+    count_launches(1);
+    device_exclusive_scan(offsets, offsets, n + 1, scratch, s);  // offsets[n] = pairs
+    if (cudaMemcpyAsync(cursor, offsets, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return OPPB_ERR_LAUNCH;
+    dh_bin_kernel<2><<<cell_grid, kDhBlock, 0, s>>>(*mesh, n_pos, g, nullptr, nullptr, cursor, list);
+    dh_query_kernel<<<ceil_div(n, kDhBlock), kDhBlock, 0, s>>>(*mesh, g, offsets, list, grid->map, n);
+    count_launches(2);
+    return launch_status();
+}

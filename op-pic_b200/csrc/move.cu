@@ -23,6 +23,8 @@
 // same nodes, do not serialise on one address; the copies are added afterwards.
 
 #include "oppb_common.cuh"
+#include "oppb_dh.h"
+#include "tet_f64.cuh"
 
 namespace oppb {
 namespace {
@@ -31,7 +33,6 @@ constexpr int kMoveBlock = 256;
 constexpr int kMinBlocks = 8;          // 8 x 256 threads per SM: 32 registers per thread
 constexpr int kSlots = 256;            // shared node-sum table (power of two, one slot per thread)
 constexpr int kMaxProbe = 16;          // linear-probe bound; beyond it the sum goes straight to global
-constexpr double kTol = 1e-10;         // KERNEL_TOLERENCE, apps/app_fempic/kernels.h:44
 constexpr int kDepNone = 0, kDepWarp = 1, kDepTable = 2;
 static_assert(kSlots == kMoveBlock, "table init/flush assume one slot per thread");
 
@@ -67,36 +68,29 @@ struct NodeTable {
     double vals[kSlots];
 };
 
+// Direct-hop seed (include/oppb_dh.h): the structured grid, passed by value.
+struct DhArgs {
+    const int32_t* map;
+    double min[3];
+    double inv;
+    unsigned long long dims[3];
+};
+
+// Cell of the grid box holding (x, y, z), or kRemoved: opp_dev_findStructuredCellIndex3D and
+// opp_dev_checkForGlobalMove (opp_lib/include/device_kernels/cuda_inline_kernels.h).  Each
+// index is (pos - min) * (1/h) truncated by a round-toward-zero conversion that saturates
+// (negative and NaN give 0), the conversion the reference's (size_t) cast compiles to.
+__device__ __forceinline__ int32_t dh_seed(const DhArgs& g, double x, double y, double z) {
+    const unsigned long long ix = __double2ull_rz(__dmul_rn(__dsub_rn(x, g.min[0]), g.inv));
+    const unsigned long long iy = __double2ull_rz(__dmul_rn(__dsub_rn(y, g.min[1]), g.inv));
+    const unsigned long long iz = __double2ull_rz(__dmul_rn(__dsub_rn(z, g.min[2]), g.inv));
+    if (ix >= g.dims[0] || iy >= g.dims[1] || iz >= g.dims[2]) return kRemoved;
+    return __ldg(g.map + (int64_t)(ix + g.dims[0] * (iy + g.dims[1] * iz)));
+}
+
 __device__ __forceinline__ double* deposit_target(const DepositArgs& d, int32_t n_nodes) {
     const int r = d.replicas > 1 ? (int)(blockIdx.x % (unsigned)d.replicas) : 0;
     return r == 0 ? d.node_charge : d.copies + (int64_t)(r - 1) * n_nodes;
-}
-
-// lambda_0..3 of point (x,y,z) in cell c, evaluated exactly as the FP64 reference.
-// Also returns the cell's neighbours (nav record).
-__device__ __forceinline__ void visit_f64(const oppb_tet_mesh& m, int32_t c, double x, double y, double z,
-                                          double l[4], int nb[4]) {
-    const double* d = m.det + (int64_t)c * 16;
-    double r[16];
-    ldg256(d, r[0], r[1], r[2], r[3]);
-    ldg256(d + 4, r[4], r[5], r[6], r[7]);
-    ldg256(d + 8, r[8], r[9], r[10], r[11]);
-    ldg256(d + 12, r[12], r[13], r[14], r[15]);
-    double coef, n01, n23, unused;
-    ldg256(m.nav + (int64_t)c * 4, coef, n01, n23, unused);
-    (void)unused;
-    const long long a = __double_as_longlong(n01), b = __double_as_longlong(n23);
-    nb[0] = (int)(a & 0xffffffffll);
-    nb[1] = (int)(a >> 32);
-    nb[2] = (int)(b & 0xffffffffll);
-    nb[3] = (int)(b >> 32);
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        double t = __dsub_rn(r[4 * i], __dmul_rn(r[4 * i + 1], x));
-        t = __dadd_rn(t, __dmul_rn(r[4 * i + 2], y));
-        t = __dsub_rn(t, __dmul_rn(r[4 * i + 3], z));
-        l[i] = __dmul_rn(coef, t);
-    }
 }
 
 // The FP64 re-evaluation of the mixed path, kept out of line: it is rare, and inlined it
@@ -105,29 +99,6 @@ __device__ __noinline__ void recheck_f64(const oppb_tet_mesh& m, int32_t c, doub
                                          double* l) {
     int nb[4];
     visit_f64(m, c, x, y, z, l, nb);
-}
-
-// Inside test of kernels.h:121-124 and first-index argmin of kernels.h:139-146.
-__device__ __forceinline__ bool inside_f64(const double l[4]) {
-    bool in = true;
-#pragma unroll
-    for (int i = 0; i < 4; i++) in = in && (l[i] > -kTol) && (__dsub_rn(l[i], 1.0) < kTol);
-    return in;
-}
-__device__ __forceinline__ int argmin4(const double l[4]) {
-    int mi = 0;
-    double mv = l[0];
-#pragma unroll
-    for (int i = 1; i < 4; i++)
-        if (l[i] < mv) {
-            mv = l[i];
-            mi = i;
-        }
-    return mi;
-}
-
-__device__ __forceinline__ int pick(const int nb[4], int i) {
-    return i == 0 ? nb[0] : i == 1 ? nb[1] : i == 2 ? nb[2] : nb[3];
 }
 
 // Bookkeeping shared by all move variants: the warp's removal bitmap word, then the CTA's
@@ -307,10 +278,10 @@ __device__ __forceinline__ void push_prologue(const oppb_tet_mesh& m, const Part
 
 // ------------------------------------------------------------------ FP64 move
 
-template <int kDep, bool kPush>
+template <int kDep, bool kPush, bool kSeed>
 __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     move_f64_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
-                    PushArgs push) {
+                    PushArgs push, DhArgs dh) {
     __shared__ NodeTable table;
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
@@ -326,7 +297,11 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
         double y = ld_stream(p.pos + p.stride + i);
         double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
         if (kPush && (uint32_t)cell < (uint32_t)m.n_cells) push_prologue<false>(m, p, push, i, cell, x, y, z);
-        for (;;) {
+        if (kSeed) {  // the walk starts from the grid box's cell (after the push, as the reference)
+            cell = dh_seed(dh, x, y, z);
+            if (cell == kRemoved) status = kNeedRemove;
+        }
+        while (!kSeed || cell != kRemoved) {
             if ((uint32_t)cell >= (uint32_t)m.n_cells) {
                 err = OPPB_ERR_CELL_RANGE;
                 break;
@@ -382,10 +357,10 @@ struct Band {
     float tie;     // 2 * band
 };
 
-template <int kDep, bool kPush>
+template <int kDep, bool kPush, bool kSeed>
 __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     move_mixed_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
-                      Band band, PushArgs push) {
+                      Band band, PushArgs push, DhArgs dh) {
     __shared__ NodeTable table;
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
@@ -408,7 +383,12 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
         double y = ld_stream(p.pos + p.stride + i);
         double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
         if (kPush) push_prologue<true>(m, p, push, i, cell, x, y, z);
-        for (;;) {
+        if (kSeed) {
+            cell = dh_seed(dh, x, y, z);
+            if (cell == kRemoved) status = kNeedRemove;
+            else if ((uint32_t)cell >= (uint32_t)m.n_cells) err = OPPB_ERR_CELL_RANGE;
+        }
+        while (!kSeed || (cell != kRemoved && !err)) {
             visits++;
             float g0[8], g1[8];  // rows 0..2, then the origin
             ldg256(m.geo32 + (int64_t)cell * 16, g0);
@@ -573,10 +553,10 @@ Replicas make_replicas(double* node_charge, void* workspace, size_t workspace_by
 
 enum MoveKind { kMoveOnly, kMoveDepositF64, kMoveDepositMixed };
 
-template <int kKind, bool kPush>
+template <int kKind, bool kPush, bool kSeed = false>
 int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
                 oppb_move_status* status, int32_t max_hops, double band, const PushArgs& push, void* workspace,
-                size_t ws_bytes, void* stream) {
+                size_t ws_bytes, void* stream, const DhArgs& dh = DhArgs{}) {
     constexpr bool kMixed = kKind == kMoveDepositMixed;
     int rc = check_mesh(mesh, kMixed, kKind != kMoveOnly);
     if (rc) return rc;
@@ -586,6 +566,7 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     if (kKind != kMoveOnly && !node_charge) return OPPB_ERR_ARG;
     if (kMixed && !(band > 0.0 && band < 0.25)) return OPPB_ERR_ARG;
     if (kPush && (!parts->vel || !mesh->ef || !aligned(mesh->ef, 16))) return OPPB_ERR_ARG;
+    if (kSeed && !dh.map) return OPPB_ERR_ARG;
     cudaStream_t s = as_stream(stream);
     if (cudaMemsetAsync(status, 0, sizeof(oppb_move_status), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
     if (parts->size == 0) return launch_status();
@@ -597,21 +578,50 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     const float bf = (float)band;
     const Band bd{bf, -bf, 1.0f - bf, 1.0f + bf, 2.0f * bf};
     if constexpr (kKind == kMoveOnly)
-        move_f64_kernel<kDepNone, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, push);
+        move_f64_kernel<kDepNone, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops,
+                                                                           push, dh);
     else if constexpr (kKind == kMoveDepositF64) {
         if (table)
-            move_f64_kernel<kDepTable, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, push);
+            move_f64_kernel<kDepTable, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+                                                                                max_hops, push, dh);
         else
-            move_f64_kernel<kDepWarp, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, push);
+            move_f64_kernel<kDepWarp, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+                                                                               max_hops, push, dh);
     } else if (table)
-        move_mixed_kernel<kDepTable, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, bd,
-                                                                        push);
+        move_mixed_kernel<kDepTable, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+                                                                              max_hops, bd, push, dh);
     else
-        move_mixed_kernel<kDepWarp, kPush><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops, bd,
-                                                                       push);
+        move_mixed_kernel<kDepWarp, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+                                                                             max_hops, bd, push, dh);
     count_launches(1);
     rep.end(s);
     return launch_status();
+}
+
+// oppb_move_ex: the options select one instantiation of launch_move.
+template <bool kSeed>
+int move_ex(const oppb_tet_mesh* mesh, const oppb_particles* parts, const oppb_move_options& o,
+            double* node_charge, oppb_move_status* status, int32_t max_hops, void* ws, size_t ws_bytes,
+            void* stream, const DhArgs& dh) {
+    const bool mixed = o.precision == OPPB_PRECISION_MIXED;
+    if (o.precision != OPPB_PRECISION_F64 && !mixed) return OPPB_ERR_ARG;
+    if ((o.deposit != 0 && o.deposit != 1) || (o.push != 0 && o.push != 1)) return OPPB_ERR_ARG;
+    if (o.push && !o.deposit) return OPPB_ERR_ARG;   // the push prologue exists on the deposit kernels
+    if (mixed && !o.deposit) return OPPB_ERR_ARG;    // the mixed move always deposits
+    // The coefficients of oppb_push_f64 / oppb_push_mixed: q/m and dt, f32(q/m * dt) and f32(dt).
+    const PushArgs push{o.qm, o.dt, (float)(o.qm * o.dt), (float)o.dt};
+    if (!o.deposit)
+        return launch_move<kMoveOnly, false, kSeed>(mesh, parts, nullptr, status, max_hops, 0.0, push, nullptr, 0,
+                                                    stream, dh);
+    if (mixed)
+        return o.push ? launch_move<kMoveDepositMixed, true, kSeed>(mesh, parts, node_charge, status, max_hops,
+                                                                    o.band, push, ws, ws_bytes, stream, dh)
+                      : launch_move<kMoveDepositMixed, false, kSeed>(mesh, parts, node_charge, status, max_hops,
+                                                                     o.band, push, ws, ws_bytes, stream, dh);
+    return o.push ? launch_move<kMoveDepositF64, true, kSeed>(mesh, parts, node_charge, status, max_hops, 0.0,
+                                                              push, ws, ws_bytes, stream, dh)
+                  : launch_move<kMoveDepositF64, false, kSeed>(mesh, parts, node_charge, status, max_hops, 0.0,
+                                                               push, ws, ws_bytes, stream, dh);
 }
 
 }  // namespace
@@ -682,4 +692,20 @@ extern "C" int oppb_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles*
     count_launches(1);
     rep.end(s);
     return launch_status();
+}
+
+extern "C" int oppb_move_ex(const oppb_tet_mesh* mesh, const oppb_particles* parts, const oppb_move_options* opt,
+                            double* node_charge, oppb_move_status* status, int32_t max_hops, void* workspace,
+                            size_t ws_bytes, void* stream) {
+    if (!opt) return OPPB_ERR_ARG;
+    if (!opt->dh)
+        return oppb::move_ex<false>(mesh, parts, *opt, node_charge, status, max_hops, workspace, ws_bytes, stream,
+                                    oppb::DhArgs{});
+    const oppb_dh_grid& g = *opt->dh;
+    if (!g.map || !(g.inv_spacing > 0.0) || g.dims[0] <= 0 || g.dims[1] <= 0 || g.dims[2] <= 0) return OPPB_ERR_ARG;
+    const oppb::DhArgs dh{g.map,
+                          {g.min[0], g.min[1], g.min[2]},
+                          g.inv_spacing,
+                          {(unsigned long long)g.dims[0], (unsigned long long)g.dims[1], (unsigned long long)g.dims[2]}};
+    return oppb::move_ex<true>(mesh, parts, *opt, node_charge, status, max_hops, workspace, ws_bytes, stream, dh);
 }

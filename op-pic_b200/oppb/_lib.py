@@ -1,4 +1,4 @@
-"""ctypes binding of the C ABI in include/oppb.h and include/oppb_fempic.h.
+"""ctypes binding of the C ABI in include/oppb*.h.
 
 The shared library is built in-tree (op-pic_b200/lib/liboppb.so).  Loading fails loudly
 when it is missing: there is no fallback implementation.
@@ -81,6 +81,20 @@ class AdvecBatch(C.Structure):
                 ("work_counter", c_vp)]
 
 
+class DhGrid(C.Structure):
+    _fields_ = [("min", C.c_double * 3), ("max", C.c_double * 3), ("spacing", C.c_double),
+                ("inv_spacing", C.c_double), ("dims", c_i64 * 3), ("size", c_i64), ("map", c_vp)]
+
+
+PRECISION_F64 = 0
+PRECISION_MIXED = 1
+
+
+class MoveOptions(C.Structure):
+    _fields_ = [("precision", c_i32), ("deposit", c_i32), ("push", c_i32), ("reserved", c_i32),
+                ("qm", C.c_double), ("dt", C.c_double), ("band", C.c_double), ("dh", C.POINTER(DhGrid))]
+
+
 class FemPICMesh(C.Structure):
     _fields_ = [("n_nodes", c_i32), ("n_cells", c_i32), ("n_ifaces", c_i32),
                 ("n_pos", c_dp), ("n_vol", c_dp), ("n_type", c_ip), ("n_bnd_pot", c_dp),
@@ -127,6 +141,10 @@ _SIGS = {
     "oppb_advec_step": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
     "oppb_advec_update_pos": (C.c_int, [P(AdvecBatch), c_vp]),
     "oppb_advec_move": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
+    "oppb_dh_grid_init": (C.c_int, [c_vp, c_i32, C.c_double, c_vp, P(DhGrid)]),
+    "oppb_dh_build": (C.c_int, [P(TetMesh), c_vp, P(DhGrid), c_vp, C.c_size_t, P(C.c_size_t), c_vp]),
+    "oppb_move_ex": (C.c_int, [P(TetMesh), P(Particles), P(MoveOptions), c_vp, c_vp, c_i32, c_vp, C.c_size_t,
+                               c_vp]),
     "oppb_fempic_box_mesh": (C.c_int, [c_i32, c_i32, c_i32, C.c_double, C.c_double, C.c_double, P(FemPICMesh)]),
     "oppb_fempic_solve_field": (C.c_int, [P(FemPICMesh), C.c_double, C.c_double, C.c_double, c_i32, c_dp,
                                           P(c_i32), P(C.c_double)]),

@@ -147,6 +147,39 @@ class DeviceMesh:
         self.dist.copy_(torch.from_numpy(np.ascontiguousarray(dist, np.int32)))
 
 
+class DirectHopGrid:
+    """The direct-hop seed's structured grid (include/oppb_dh.h), built on the device once:
+    grid spacing h, bounding box of the nodes widened by `expansion` per axis (default 4h,
+    the FemPIC app's choice, apps_codegen/app_fempic_cg/fempic_opp.cpp:69-76), map of every
+    box to its mesh cell (OPPB_REMOVED_CELL where none).  Role of opp_init_direct_hop_cg."""
+
+    def __init__(self, hm: HostMesh, mesh: DeviceMesh, spacing: float, expansion=None):
+        lib = L.load()
+        exp = np.full(3, 4.0 * spacing) if expansion is None else \
+            np.ascontiguousarray(np.broadcast_to(np.asarray(expansion, np.float64), (3,)))
+        n_pos = np.ascontiguousarray(hm.n_pos, np.float64)
+        self.g = L.DhGrid()
+        L.check("oppb_dh_grid_init", lib.oppb_dh_grid_init(n_pos.ctypes.data, hm.n_nodes, float(spacing),
+                                                           exp.ctypes.data, C.byref(self.g)))
+        self.map = torch.empty(int(self.g.size), dtype=torch.int32, device=mesh.device)
+        self.g.map = self.map.data_ptr()
+        npos_soa = torch.from_numpy(np.ascontiguousarray(hm.n_pos.T)).to(mesh.device)
+        need = C.c_size_t(0)
+        sp = _stream_ptr(None)
+        rc = lib.oppb_dh_build(C.byref(mesh.s), npos_soa.data_ptr(), C.byref(self.g), None, 0, C.byref(need), sp)
+        if rc != L.OPPB_ERR_WORKSPACE:
+            L.check("oppb_dh_build", rc)
+        ws = torch.empty(int(need.value), dtype=torch.uint8, device=mesh.device)
+        L.check("oppb_dh_build", lib.oppb_dh_build(C.byref(mesh.s), npos_soa.data_ptr(), C.byref(self.g),
+                                                   ws.data_ptr(), ws.numel(), C.byref(need), sp))
+        torch.cuda.current_stream(mesh.device).synchronize()  # the workspace is freed on return
+        self.spacing = float(spacing)
+        self.expansion = exp
+        self.dims = tuple(int(d) for d in self.g.dims)
+        self.size = int(self.g.size)
+        self.box = np.array(list(self.g.min) + list(self.g.max))
+
+
 class ParticleSet:
     """Particle dats p_position, p_velocity, p_lc, p2c in SoA [dim][capacity] with swap
     buffers for the sort, the removal bitmap and the move status word."""
@@ -228,7 +261,7 @@ class FemPIC:
                  ion_velocity: float = 1.0, qm: float = 1.0, dt: float = 0.01, precision: str = "f64",
                  fill: str = "HoleFill_All", fill_period: int = 10, alloc_mult: float = 2.0,
                  capacity: int = 0, max_hops: int = 4096, band: float = 1e-5, fused_deposit: bool = True,
-                 fused_push: bool = True):
+                 fused_push: bool = True, direct_hop: float | None = None, dh_expansion=None):
         if not torch.cuda.is_available():
             raise RuntimeError("FemPIC needs a CUDA device (there is no CPU fallback)")
         self.device = torch.device(device)
@@ -253,6 +286,9 @@ class FemPIC:
         self.lib = L.load()
         self.last = {}
         self._pipe = None  # run_steps' copy stream, events and double buffers, made once
+        # Global move: every walk starts from the cell of the structured grid's box that the
+        # particle is in (opp_global_move with grid_spacing = direct_hop).
+        self.dh = DirectHopGrid(hm, self.mesh, direct_hop, dh_expansion) if direct_hop else None
         self._pipeline(5, inject_per_step)
 
     # workspace shared by hole fill and sort (grown on demand)
@@ -284,8 +320,22 @@ class FemPIC:
             self._dep_ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
         return self._dep_ws
 
+    def _move_ex(self, push: bool, stream=None) -> None:
+        """The move through oppb_move_ex (the direct-hop seed is only reached there)."""
+        v = self.parts.view()
+        ws = self._deposit_ws()
+        mixed = self.precision == "mixed"
+        o = L.MoveOptions(precision=L.PRECISION_MIXED if mixed else L.PRECISION_F64,
+                          deposit=int(mixed or self.fused_deposit), push=int(push), qm=self.qm, dt=self.dt,
+                          band=self.band, dh=C.pointer(self.dh.g) if self.dh is not None else None)
+        L.check("oppb_move_ex", self.lib.oppb_move_ex(C.byref(self.mesh.s), C.byref(v), C.byref(o),
+                                                      _ptr(self.node_charge), _ptr(self.parts.status),
+                                                      self.max_hops, _ptr(ws), ws.numel(), _stream_ptr(stream)))
+
     def move(self, stream=None) -> None:
         """Move (+ fused deposit into node_charge, which the caller zeroes)."""
+        if self.dh is not None:
+            return self._move_ex(False, stream)
         v = self.parts.view()
         st = _ptr(self.parts.status)
         sp = _stream_ptr(stream)
@@ -303,6 +353,8 @@ class FemPIC:
     def push_move(self, stream=None) -> None:
         """Push + move + deposit in one launch (the push is the move kernel's prologue);
         bit-identical to push() followed by move()."""
+        if self.dh is not None:
+            return self._move_ex(True, stream)
         v = self.parts.view()
         st = _ptr(self.parts.status)
         sp = _stream_ptr(stream)

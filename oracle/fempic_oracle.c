@@ -265,3 +265,139 @@ int oracle_sort(int32_t size, int32_t n_cells, int32_t n_dats, char** dats, cons
     free(order);
     return 0;
 }
+
+/* ------------------------------------------------------------------ direct hop
+ *
+ * The structured cell mapper of the global move (opp_lib/include/opp_direct_hop_core.h,
+ * seq build opp_lib/src/seq/opp_direct_hop_seq.cpp) and the global-move pre-pass of the
+ * move loop (apps_codegen/app_fempic_cg/seq/move_kernel_loop.hpp:112-131).  box[6] =
+ * {min x, y, z, max x, y, z}; the map is x fastest (index = x + X*y + X*Y*z).
+ */
+
+#define ORACLE_DBL_MAX 1.7976931348623157e308
+#define ORACLE_DBL_MIN 2.2250738585072014e-308 /* MIN_REAL = numeric_limits<double>::min() */
+
+/* BoundingBox(n_pos, 3, expansion) (opp_direct_hop_core.h:70-120; the x/y widening
+ * reads expansion x for both minima and expansion y for both maxima, as written there)
+ * and CellMapper::init_host's box counts (:317-380): 1 + the number of iterations of
+ * `for (v = min; v < max; v += h)`.  Returns 0, or 1 for a grid above 2^31 boxes. */
+int oracle_dh_grid_init(int32_t n_nodes, const double* n_pos, double spacing, const double* expansion,
+                        double* box, int64_t* dims) {
+    double mn[3] = {ORACLE_DBL_MAX, ORACLE_DBL_MAX, ORACLE_DBL_MAX};
+    double mx[3] = {ORACLE_DBL_MIN, ORACLE_DBL_MIN, ORACLE_DBL_MIN};
+    for (int32_t i = 0; i < n_nodes; i++)
+        for (int d = 0; d < 3; d++) {
+            const double v = n_pos[(int64_t)i * 3 + d];
+            if (v < mn[d]) mn[d] = v;
+            if (mx[d] < v) mx[d] = v;
+        }
+    mn[0] -= (expansion[0] + 1e-12); /* BOUND_OFFSET, opp_direct_hop_core.h:37 */
+    mn[1] -= (expansion[0] + 1e-12);
+    mx[0] += (expansion[1] - 1e-12);
+    mx[1] += (expansion[1] - 1e-12);
+    mn[2] -= (expansion[2] + 1e-12);
+    mx[2] += (expansion[2] - 1e-12);
+    for (int d = 0; d < 3; d++) {
+        int64_t a = 0;
+        for (double v = mn[d]; v < mx[d]; v += spacing)
+            if (++a > ((int64_t)1 << 31)) return 1;
+        dims[d] = a + 1;
+        box[d] = mn[d];
+        box[3 + d] = mx[d];
+    }
+    return ((double)dims[0] * (double)dims[1] * (double)dims[2] > 2147483646.0) ? 1 : 0;
+}
+
+/* The checker of opp_init_direct_hop_cg (seq move_kernel_loop.hpp:170-198): the first cell,
+ * in index order, for which move_kernel ends with MOVE_DONE at point x. */
+static int32_t dh_first_cell(const double* x, int32_t n_cells, const double* c_volume, const double* c_det) {
+    static const int32_t dummy_c2c[4] = {0, 0, 0, 0};
+    double lc[4];
+    for (int32_t c = 0; c < n_cells; c++) {
+        int32_t next = c;
+        if (move_visit(x, lc, c_volume[c], c_det + (int64_t)c * 16, dummy_c2c, &next) == MOVE_DONE) return c;
+    }
+    return ORACLE_REMOVED;
+}
+
+/* CellMapper::generateStructuredMesh (opp_direct_hop_seq.cpp:134-302) on one unpartitioned
+ * mesh (global cell id = index): step 1 the box centroid (getCentroidOfBox, with the box's
+ * upper bound as in ASSIGN_CENTROID_TO_DIM, opp_defs.h:121-127), nudged by h/100 along x,
+ * then y, then z while no cell holds it; step 3 the lowest cell holding one of the box's
+ * corners, each clamped to the upper bound (GET_VERT, opp_defs.h:115).  Search over all
+ * cells per query, as the reference does. */
+static int32_t dh_box(int32_t n_cells, const double* c_volume, const double* c_det, const double* box,
+                      double spacing, const int64_t* dims, int64_t index) {
+    const double* mn = box;
+    const double* mx = box + 3;
+    const int64_t dx = index % dims[0], dy = (index / dims[0]) % dims[1], dz = index / (dims[0] * dims[1]);
+    const double corner[3] = {mn[0] + (double)dx * spacing, mn[1] + (double)dy * spacing,
+                              mn[2] + (double)dz * spacing};
+    double c[3];
+    for (int d = 0; d < 3; d++)
+        c[d] = (corner[d] + spacing <= mx[d]) ? corner[d] + spacing * 0.5 : (corner[d] + mx[d]) * 0.5;
+    int32_t cid = dh_first_cell(c, n_cells, c_volume, c_det);
+    for (int d = 0; d < 3 && cid == ORACLE_REMOVED; d++) {
+        c[d] += spacing / 100.0;
+        cid = dh_first_cell(c, n_cells, c_volume, c_det);
+    }
+    if (cid == ORACLE_REMOVED) {
+        for (int k = 0; k < 8; k++) {
+            double v[3];
+            for (int d = 0; d < 3; d++) {
+                const double t = ((k >> d) & 1) ? corner[d] + spacing : corner[d];
+                v[d] = (t > mx[d]) ? mx[d] : t;
+            }
+            const int32_t f = dh_first_cell(v, n_cells, c_volume, c_det);
+            if (f < cid) cid = f;
+        }
+    }
+    return cid;
+}
+
+void oracle_dh_build(int32_t n_cells, const double* c_volume, const double* c_det, const double* box,
+                     double spacing, const int64_t* dims, int32_t* map) {
+    const int64_t size = dims[0] * dims[1] * dims[2];
+    for (int64_t index = 0; index < size; index++)
+        map[index] = dh_box(n_cells, c_volume, c_det, box, spacing, dims, index);
+}
+
+/* The map entries of the boxes idx[0..n) only (spot checks of large grids). */
+void oracle_dh_boxes(int32_t n_cells, const double* c_volume, const double* c_det, const double* box,
+                     double spacing, const int64_t* dims, int32_t n, const int64_t* idx, int32_t* out) {
+    for (int32_t k = 0; k < n; k++) out[k] = dh_box(n_cells, c_volume, c_det, box, spacing, dims, idx[k]);
+}
+
+/* Truncation of the box index as the CUDA backend's (size_t) cast of a double runs on the
+ * device (round toward zero, saturating: negative and NaN give 0). */
+static uint64_t dh_index(double t) {
+    if (!(t > 0.0)) return 0;
+    if (t >= 18446744073709551616.0) return UINT64_MAX;
+    return (uint64_t)t;
+}
+
+/* Global-move pre-pass over [0,n) (seq move_kernel_loop.hpp:112-131 with
+ * findStructuredCellIndex3D, opp_direct_hop_core.h:410-429, and the CUDA rule for a
+ * position outside the grid, opp_dev_findStructuredCellIndex3D / opp_dev_checkForGlobalMove
+ * in opp_lib/include/device_kernels/cuda_inline_kernels.h): p2c = the box's cell, or
+ * REMOVED outside the grid or in a box without a cell.  Particles at REMOVED stay there.
+ * Returns the number of particles it removed. */
+int32_t oracle_dh_seed(int32_t n, const double* pos, int32_t* p2c, const double* box_min, double inv,
+                       const int64_t* dims, const int32_t* map) {
+    int32_t removed = 0;
+    for (int32_t i = 0; i < n; i++) {
+        if (p2c[i] == ORACLE_REMOVED) continue;
+        const double* x = pos + (int64_t)i * 3;
+        uint64_t ix[3];
+        int out = 0;
+        for (int d = 0; d < 3; d++) {
+            ix[d] = dh_index((x[d] - box_min[d]) * inv);
+            if (ix[d] >= (uint64_t)dims[d]) out = 1;
+        }
+        const int32_t cell = out ? ORACLE_REMOVED
+                                 : map[ix[0] + (uint64_t)dims[0] * (ix[1] + (uint64_t)dims[1] * ix[2])];
+        p2c[i] = cell;
+        if (cell == ORACLE_REMOVED) removed++;
+    }
+    return removed;
+}

@@ -41,6 +41,14 @@ def load() -> C.CDLL:
         lib.oracle_hole_fill.argtypes = [i32, i32, vp, i32, vp, vp, vp, vp]
         lib.oracle_sort.restype = C.c_int
         lib.oracle_sort.argtypes = [i32, i32, i32, vp, vp, i32, vp]
+        lib.oracle_dh_grid_init.restype = C.c_int
+        lib.oracle_dh_grid_init.argtypes = [i32, vp, C.c_double, vp, vp, vp]
+        lib.oracle_dh_build.restype = None
+        lib.oracle_dh_build.argtypes = [i32, vp, vp, vp, C.c_double, vp, vp]
+        lib.oracle_dh_boxes.restype = None
+        lib.oracle_dh_boxes.argtypes = [i32, vp, vp, vp, C.c_double, vp, i32, vp, vp]
+        lib.oracle_dh_seed.restype = i32
+        lib.oracle_dh_seed.argtypes = [i32, vp, vp, vp, C.c_double, vp, vp]
         _lib = lib
     return _lib
 
@@ -95,6 +103,50 @@ def sort(size, n_cells, dats, key_dat):
     return perm[:size].copy()
 
 
+class DirectHop:
+    """The structured cell mapper of the global move (oracle_dh_*): grid from the node
+    positions (AoS [n][3]), spacing h and expansion (3,), map built by searching all cells
+    per query as the reference does (slow: small meshes only)."""
+
+    def __init__(self, n_pos, spacing: float, expansion, mesh=None):
+        lib = load()
+        n_pos = np.ascontiguousarray(n_pos, np.float64)
+        self.spacing = float(spacing)
+        self.expansion = np.ascontiguousarray(expansion, np.float64)
+        self.box = np.zeros(6)
+        self.dims = np.zeros(3, np.int64)
+        if lib.oracle_dh_grid_init(len(n_pos), _p(n_pos), self.spacing, _p(self.expansion), _p(self.box),
+                                   _p(self.dims)) != 0:
+            raise ValueError("grid too large")
+        self.inv = 1.0 / self.spacing
+        self.size = int(np.prod(self.dims))
+        self.map = None
+        if mesh is not None:
+            self.build(mesh)
+
+    def build(self, mesh) -> np.ndarray:
+        self.map = np.zeros(self.size, np.int32)
+        load().oracle_dh_build(mesh.n_cells, _p(np.ascontiguousarray(mesh.c_vol)),
+                               _p(np.ascontiguousarray(mesh.c_det)), _p(self.box), self.spacing, _p(self.dims),
+                               _p(self.map))
+        return self.map
+
+    def boxes(self, mesh, idx) -> np.ndarray:
+        """Map entries of the boxes idx only (the same search, for spot checks)."""
+        idx = np.ascontiguousarray(idx, np.int64)
+        out = np.zeros(len(idx), np.int32)
+        load().oracle_dh_boxes(mesh.n_cells, _p(np.ascontiguousarray(mesh.c_vol)),
+                               _p(np.ascontiguousarray(mesh.c_det)), _p(self.box), self.spacing, _p(self.dims),
+                               len(idx), _p(idx), _p(out))
+        return out
+
+    def seed(self, pos, p2c, n=None) -> int:
+        """Global-move pre-pass over [0,n): p2c from the grid; returns the removals."""
+        n = len(p2c) if n is None else n
+        return int(load().oracle_dh_seed(n, _p(pos), _p(p2c), _p(self.box[:3].copy()), self.inv, _p(self.dims),
+                                         _p(self.map)))
+
+
 class OracleFemPIC:
     """The FemPIC particle step on AoS host arrays, seq-backend order.
 
@@ -104,8 +156,9 @@ class OracleFemPIC:
     """
 
     def __init__(self, mesh, dist, ion_velocity=1.0, qm=1.0, dt=0.01, fill="HoleFill_All", fill_period=10,
-                 alloc_mult=2.0, mixed=False, max_hops=1 << 20):
+                 alloc_mult=2.0, mixed=False, max_hops=1 << 20, dh: DirectHop | None = None):
         self.m = mesh
+        self.dh = dh  # global move: every walk starts from the grid's cell
         self.dist = np.ascontiguousarray(dist, np.int32)
         self.ion_velocity, self.qm, self.dt = ion_velocity, qm, dt
         self.fill, self.fill_period, self.alloc_mult = fill, fill_period, alloc_mult
@@ -153,10 +206,12 @@ class OracleFemPIC:
         self.node_charge[:] = 0.0
         push(self.p2c, m.c_ef, self.pos, self.vel, self.qm, self.dt, n=self.size, mixed=self.mixed)
         n_before = self.size
+        seeded_out = self.dh.seed(self.pos, self.p2c, n=self.size) if self.dh is not None else 0
         rc, visits, _ = move(self.pos, self.lc, self.p2c, m.c2c, m.c_vol, m.c_det, n=self.size,
                              max_hops=self.max_hops)
         if visits < 0:
             raise RuntimeError("oracle: hop limit")
+        rc += seeded_out
         self.finalize(rc)
         deposit(self.lc, self.p2c, m.c2n, self.node_charge, n=self.size)
         self.last_remove, self.last_visits = rc, visits

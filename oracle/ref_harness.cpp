@@ -5,7 +5,9 @@
 // particle part of the generated main loop (apps_codegen/app_fempic_cg/fempic_opp.cpp:160-215):
 //   opp_inc_part_count_with_distribution -> inject_ions (+ thermal velocity from the case)
 //   -> reset n_charge_den -> calculate_new_pos_vel -> move (with its finalize) -> deposit.
-// The field is the static cell field of the case (no field solve).  Per step it records
+// The field is the static cell field of the case (no field solve).  A direct-hop case
+// turns on the global move (opp_init_direct_hop_cg builds the structured map by the
+// reference's own search) and the output ends with the reference's grid and map.  Per step it records
 // sizes and wall times and, unless the case is a timing case (record_state 0), FNV-1a
 // hashes of the particle dats and of the node charges.
 //
@@ -30,12 +32,14 @@ void opp_par_loop_injected__inject_ions_kernel(opp_set, opp_arg, opp_arg, opp_ar
 void opp_par_loop_all__calculate_new_pos_vel_kernel(opp_set, opp_arg, opp_arg, opp_arg);
 void opp_particle_move__move_kernel(opp_set, opp_map, opp_map, opp_arg, opp_arg, opp_arg, opp_arg);
 void opp_par_loop_all__deposit_charge_on_nodes_kernel(opp_set, opp_arg, opp_arg, opp_arg, opp_arg, opp_arg);
+void opp_init_direct_hop_cg(double, const opp_dat, const opp::BoundingBox&, opp_map, opp_map, opp_arg, opp_arg,
+                            opp_arg, opp_arg);
 
 namespace {
 
 struct Header {
     char magic[8];
-    int32_t n_nodes, n_cells, n_ifaces, inject, steps, n_tables, record_state, pad;
+    int32_t n_nodes, n_cells, n_ifaces, inject, steps, n_tables, record_state, direct_hop;
     double dt, qm, ion_velocity, sigma;
 };
 
@@ -103,6 +107,12 @@ int main(int argc, char** argv) {
     auto if_n_pos = read_vec<double>(f, nf * 9);
     auto if_dist = read_vec<int>(f, nf);
     auto tables = read_vec<double>(f, (size_t)h.n_tables * h.inject * 5);
+    // Direct-hop cases: grid spacing, expansion[3] and the node positions follow the tables.
+    std::vector<double> dh_par(4, 0.0), n_pos;
+    if (h.direct_hop) {
+        dh_par = read_vec<double>(f, 4);
+        n_pos = read_vec<double>(f, nn * 3);
+    }
     fclose(f);
     std::vector<double> n_charge(nn, 0.0);
 
@@ -134,6 +144,20 @@ int main(int argc, char** argv) {
         opp_dat p_lc = opp_decl_dat(particle_set, 4, DT_REAL, nullptr, "p_lc");
         opp_map p2c_map = opp_decl_map(particle_set, cell_set, 1, nullptr, "p2c_map");
         opp_dat dp_rand = opp_decl_dat(dummy_part_set, 2, DT_REAL, nullptr, "dummy_part_rand");
+
+        // Global move (the params file sets opp_global_move and opp_dh_data_generate): the
+        // app's set-up of fempic_opp.cpp:69-76,95,147-153 with the case's spacing/expansion.
+        if (h.direct_hop) {
+            std::vector<int> c_id(nc);
+            for (size_t c = 0; c < nc; c++) c_id[c] = (int)c;
+            opp_dat n_pos_d = opp_decl_dat(node_set, 3, DT_REAL, n_pos.data(), "n_pos");
+            opp_dat c_gbl_id = opp_decl_dat(cell_set, 1, DT_INT, c_id.data(), "c_gbl_id");
+            opp::BoundingBox bounding_box(n_pos_d, 3, opp_point(dh_par[1], dh_par[2], dh_par[3]));
+            opp_init_direct_hop_cg(dh_par[0], c_gbl_id, bounding_box, c2c_map, p2c_map,
+                                   opp_arg_dat(p_pos, OPP_READ), opp_arg_dat(p_lc, OPP_WRITE),
+                                   opp_arg_dat(c_volume, p2c_map, OPP_READ),
+                                   opp_arg_dat(c_det_d, p2c_map, OPP_READ));
+        }
 
         double one = 1.0, dt = h.dt, vion = h.ion_velocity, zero = 0.0;
         opp_decl_const<OPP_REAL>(1, &zero, "CONST_spwt");
@@ -233,6 +257,16 @@ int main(int argc, char** argv) {
             fwrite(p_vel->data, sizeof(double), (size_t)fin * 3, o);
             fwrite(p_lc->data, sizeof(double), (size_t)fin * 4, o);
             fwrite(n_charge_den->data, sizeof(double), nn, o);
+        }
+        if (h.direct_hop) {  // the reference's grid: box counts, bounds and the map
+            const int64_t dims[3] = {(int64_t)cellMapper->globalGridDimsX, (int64_t)cellMapper->globalGridDimsY,
+                                     (int64_t)cellMapper->globalGridDimsZ};
+            const opp_point& mn = boundingBox->getGlobalMin();
+            const opp_point& mx = boundingBox->getGlobalMax();
+            const double box[6] = {mn.x, mn.y, mn.z, mx.x, mx.y, mx.z};
+            fwrite(dims, sizeof(int64_t), 3, o);
+            fwrite(box, sizeof(double), 6, o);
+            fwrite(cellMapper->structMeshToCellMapping, sizeof(int), cellMapper->globalGridSize, o);
         }
         fclose(o);
     }

@@ -34,11 +34,14 @@ def fnv1a(a: np.ndarray) -> int:
 
 
 def write_case(path: Path, mesh, dist: np.ndarray, steps: int, tables: list[np.ndarray], dt: float = 0.01,
-               qm: float = 1.0, ion_velocity: float = 1.0, sigma: float = 0.1, record_state: bool = True) -> None:
+               qm: float = 1.0, ion_velocity: float = 1.0, sigma: float = 0.1, record_state: bool = True,
+               dh: tuple | None = None) -> None:
+    """dh = (grid_spacing, expansion[3]): a global-move case; the node positions follow."""
     inject = int(dist[-1])
     hdr = np.zeros(1, dtype=[("magic", "S8"), ("ints", "<i4", 8), ("dbl", "<f8", 4)])
     hdr["magic"] = b"OPPBCAS1"
-    hdr["ints"] = [mesh.n_nodes, mesh.n_cells, mesh.n_ifaces, inject, steps, len(tables), int(record_state), 0]
+    hdr["ints"] = [mesh.n_nodes, mesh.n_cells, mesh.n_ifaces, inject, steps, len(tables), int(record_state),
+                   int(dh is not None)]
     hdr["dbl"] = [dt, qm, ion_velocity, sigma]
     with open(path, "wb") as f:
         f.write(hdr.tobytes())
@@ -49,12 +52,18 @@ def write_case(path: Path, mesh, dist: np.ndarray, steps: int, tables: list[np.n
         for t in tables:
             assert t.shape == (inject, 5)
             f.write(np.ascontiguousarray(t, dtype="<f8").tobytes())
+        if dh is not None:
+            spacing, expansion = dh
+            f.write(np.array([spacing, *expansion], "<f8").tobytes())
+            f.write(np.ascontiguousarray(mesh.n_pos, dtype="<f8").tobytes())
 
 
-def params_text(fill: str, period: int, alloc_mult: float) -> str:
+def params_text(fill: str, period: int, alloc_mult: float, global_move: bool = False) -> str:
+    gm = "true" if global_move else "false"
     return (f"STRING opp_fill = {fill}\nINT opp_fill_period = {period}\n"
             f"REAL opp_allocation_multiple = {alloc_mult}\nBOOL opp_profile_all = false\n"
-            f"BOOL opp_global_move = false\nINT opp_threads_per_block = 256\nBOOL print_final = false\n")
+            f"BOOL opp_global_move = {gm}\nBOOL opp_dh_data_generate = {gm}\n"
+            f"INT opp_threads_per_block = 256\nBOOL print_final = false\n")
 
 
 def run(kind: str, mesh, dist, steps: int, tables, fill: str = "HoleFill_All", period: int = 10,
@@ -65,7 +74,7 @@ def run(kind: str, mesh, dist, steps: int, tables, fill: str = "HoleFill_All", p
     with tempfile.TemporaryDirectory() as d:
         d = Path(d)
         write_case(d / "case.bin", mesh, dist, steps, tables, record_state=record_state, **kw)
-        (d / "params.txt").write_text(params_text(fill, period, alloc_mult))
+        (d / "params.txt").write_text(params_text(fill, period, alloc_mult, global_move=kw.get("dh") is not None))
         env = dict(os.environ)
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
@@ -73,10 +82,10 @@ def run(kind: str, mesh, dist, steps: int, tables, fill: str = "HoleFill_All", p
                            capture_output=True, text=True, env=env)
         if r.returncode != 0:
             raise RuntimeError(f"{exe.name} failed ({r.returncode}): {r.stderr[-2000:]}")
-        return read_output(d / "out.bin", mesh.n_nodes, record_state)
+        return read_output(d / "out.bin", mesh.n_nodes, record_state, direct_hop=kw.get("dh") is not None)
 
 
-def read_output(path: Path, n_nodes: int, record_state: bool = True) -> dict:
+def read_output(path: Path, n_nodes: int, record_state: bool = True, direct_hop: bool = False) -> dict:
     """Per-step records and final state written by the harness (and by the library's
     FemPIC app, which uses the same layout)."""
     raw = Path(path).read_bytes()
@@ -98,4 +107,11 @@ def read_output(path: Path, n_nodes: int, record_state: bool = True) -> dict:
         out["vel"] = take("<f8", fin * 3).reshape(fin, 3)
         out["lc"] = take("<f8", fin * 4).reshape(fin, 4)
         out["node_charge"] = take("<f8", n_nodes)
+    if direct_hop:  # the reference's structured grid: box counts, bounds, map
+        out["dh_dims"] = np.frombuffer(raw[off:off + 24], "<i8").copy()
+        off += 24
+        out["dh_box"] = np.frombuffer(raw[off:off + 48], "<f8").copy()
+        off += 48
+        n = int(np.prod(out["dh_dims"]))
+        out["dh_map"] = np.frombuffer(raw[off:off + 4 * n], "<i4").copy()
     return out

@@ -15,8 +15,8 @@ INCLUDE = Path(__file__).resolve().parent.parent / "include"
 
 def declared_functions():
     names = set()
-    for h in ("oppb.h", "oppb_fempic.h"):
-        text = (INCLUDE / h).read_text()
+    for h in sorted(INCLUDE.glob("oppb*.h")):  # every header of the C ABI library
+        text = h.read_text()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"^\s*(?:const\s+)?[\w\s\*]+?\b(oppb_\w+)\s*\(", text, flags=re.M):
             names.add(m.group(1))
@@ -69,3 +69,46 @@ def test_mesh_bytes(n):
     out = (C.c_size_t * 6)()
     L.load().oppb_tet_mesh_bytes(n, out)
     assert list(out) == [128 * n, 32 * n, 16 * n, 32 * n, 64 * n, 32 * n]
+
+
+def test_declared_functions_cover_every_header():
+    names = declared_functions()
+    for n in ("oppb_move_ex", "oppb_dh_build", "oppb_cabana_move_deposit", "oppb_advec_step"):
+        assert n in names
+
+
+@pytest.mark.parametrize("dims,spacing,expansion", [
+    ((4, 4, 8, 1.0, 1.0, 2.0), 0.1, (0.4, 0.4, 0.4)),
+    ((5, 3, 6, 1.0, 0.6, 1.2), 0.07, (0.3, 0.2, 0.25)),
+    ((48, 48, 192, 1.0, 1.0, 4.0), 1.0 / 48, (4.0 / 48,) * 3),
+])
+def test_dh_grid_init_matches_oracle(dims, spacing, expansion):
+    """The host half of the direct-hop set-up (bounding box and box counts) equals the
+    oracle's restatement of the reference, bit for bit, without a GPU."""
+    import numpy as np
+
+    from oppb.fempic import HostMesh
+    from oracle import oracle as O
+
+    hm = HostMesh(*dims, solve_field=False)
+    g = L.DhGrid()
+    exp = np.array(expansion)
+    assert L.load().oppb_dh_grid_init(np.ascontiguousarray(hm.n_pos).ctypes.data, hm.n_nodes, spacing,
+                                      exp.ctypes.data, C.byref(g)) == L.OPPB_OK
+    o = O.DirectHop(hm.n_pos, spacing, expansion)
+    assert list(g.dims) == list(o.dims) and g.size == o.size
+    box = np.array(list(g.min) + list(g.max))
+    np.testing.assert_array_equal(box.view(np.uint64), o.box.view(np.uint64))
+    assert g.inv_spacing == 1.0 / spacing
+
+
+def test_dh_and_move_ex_argument_validation():
+    lib = L.load()
+    g = L.DhGrid()
+    one = (C.c_double * 3)(0.0, 0.0, 0.0)
+    pts = (C.c_double * 3)(0.0, 0.0, 0.0)
+    assert lib.oppb_dh_grid_init(pts, 1, 0.0, one, C.byref(g)) == L.OPPB_ERR_ARG      # spacing 0
+    assert lib.oppb_dh_grid_init(pts, 0, 0.1, one, C.byref(g)) == L.OPPB_ERR_ARG      # no nodes
+    assert lib.oppb_dh_grid_init(pts, 1, 1e-12, (C.c_double * 3)(1.0, 1.0, 1.0), C.byref(g)) == L.OPPB_ERR_ARG
+    assert lib.oppb_dh_build(None, None, C.byref(g), None, 0, None, None) == L.OPPB_ERR_ARG
+    assert lib.oppb_move_ex(None, None, None, None, None, 16, None, 0, None) == L.OPPB_ERR_ARG

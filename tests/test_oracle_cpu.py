@@ -20,6 +20,8 @@ def _golden(name):
     mesh = SimpleNamespace(**{k: z[k] for k in ("c2n", "c2c", "c_det", "c_vol", "c_ef", "if2c", "if_u", "if_v",
                                                 "if_norm", "if_n_pos")})
     mesh.n_nodes, mesh.n_cells, mesh.n_ifaces = int(z["n_nodes"]), int(z["n_cells"]), int(z["n_ifaces"])
+    if "n_pos" in z:
+        mesh.n_pos = z["n_pos"]
     return z, mesh
 
 
@@ -128,3 +130,73 @@ def test_oracle_sort_is_stable():
     ref = np.argsort(np.where(p2c == O.REMOVED, 50, p2c), kind="stable")
     np.testing.assert_array_equal(perm, ref)
     np.testing.assert_array_equal(idx[:, 0], ref.astype(np.float64))
+
+
+def test_dh_oracle_matches_golden():
+    """Direct hop: the structured grid (box counts, bounds, every map entry) and 30 global-move
+    steps of the reference seq backend (fixture made by tests/golden/make_golden.py)."""
+    z, mesh = _golden("fempic_4x4x8_dh")
+    sp = float(z["spacing"])
+    dh = O.DirectHop(z["n_pos"], sp, (4 * sp,) * 3, mesh=mesh)
+    np.testing.assert_array_equal(dh.dims, z["dh_dims"])
+    np.testing.assert_array_equal(dh.box.view(np.uint64), z["dh_box"].view(np.uint64))
+    np.testing.assert_array_equal(dh.map, z["dh_map"])
+    assert 0 < (dh.map != O.REMOVED).sum() < dh.size  # boxes inside and outside the mesh
+    o = O.OracleFemPIC(mesh, z["dist"], dt=float(z["dt"]), fill=str(z["fill"]), fill_period=int(z["period"]), dh=dh)
+    for s in range(int(z["steps"])):
+        r = o.step(z["tables"][s])
+        rec = z["records"][s]
+        n = o.size
+        assert (r["size"], r["removed"]) == (int(rec["size"]), int(rec["removed"])), s
+        assert R.fnv1a(o.p2c[:n]) == int(rec["h_p2c"]), s
+        assert R.fnv1a(o.pos[:n]) == int(rec["h_pos"]), s
+        assert R.fnv1a(o.lc[:n]) == int(rec["h_lc"]), s
+        assert R.fnv1a(o.node_charge) == int(rec["h_charge"]), s
+    np.testing.assert_array_equal(o.p2c[:o.size], z["p2c"])
+
+
+def test_dh_seed_removes_outside_grid():
+    """Positions outside the grid, or in a box without a cell, are removed (the CUDA
+    backend's rule); inside, p2c becomes the box's cell."""
+    z, mesh = _golden("fempic_4x4x8_dh")
+    sp = float(z["spacing"])
+    dh = O.DirectHop(z["n_pos"], sp, (4 * sp,) * 3)
+    dh.map = z["dh_map"].copy()
+    lo, hi = dh.box[:3], dh.box[3:]
+    pos = np.array([[0.5, 0.5, 1.0],            # inside the mesh
+                    [lo[0] - 1.0, 0.5, 1.0],    # below the grid in x
+                    [0.5, hi[1] + 1.0, 1.0],    # above the grid in y
+                    [-0.3, -0.3, -0.3],         # in the grid, outside the mesh (no cell)
+                    [np.nan, 0.5, 1.0]])        # NaN truncates to box 0: no cell there
+    p2c = np.zeros(len(pos), np.int32)
+    assert dh.seed(pos, p2c) == 4
+    assert p2c[0] != O.REMOVED and (p2c[1:] == O.REMOVED).all()
+    ix = ((pos[0] - lo) * dh.inv).astype(np.int64)
+    assert p2c[0] == dh.map[ix[0] + dh.dims[0] * (ix[1] + dh.dims[1] * ix[2])]
+
+
+@pytest.mark.skipif(not R.available("seq_stable"), reason="compiled reference not built (needs its sources)")
+def test_dh_oracle_matches_live_reference():
+    """A spacing that does not divide the box and unequal expansions (the reference widens
+    both x and y minima by the x expansion and both maxima by the y expansion)."""
+    from oppb.fempic import HostMesh, injection_randoms
+
+    hm = HostMesh(5, 3, 6, 1.0, 0.6, 1.2)
+    dist = hm.inject_distribution(150)
+    steps = 20
+    tables = [injection_randoms(9, s, 150, 0.1) for s in range(steps)]
+    sp, ex = 0.07, (0.3, 0.2, 0.25)
+    ref = R.run("seq_stable", hm, dist, steps, tables, fill="HoleFill_All", period=10, dt=0.2, dh=(sp, ex))
+    dh = O.DirectHop(hm.n_pos, sp, ex, mesh=hm)
+    np.testing.assert_array_equal(dh.dims, ref["dh_dims"])
+    np.testing.assert_array_equal(dh.box.view(np.uint64), ref["dh_box"].view(np.uint64))
+    np.testing.assert_array_equal(dh.map, ref["dh_map"])
+    o = O.OracleFemPIC(hm, dist, dt=0.2, fill="HoleFill_All", fill_period=10, dh=dh)
+    for s in range(steps):
+        o.step(tables[s])
+        rec = ref["records"][s]
+        n = o.size
+        assert o.size == rec["size"], s
+        assert R.fnv1a(o.p2c[:n]) == int(rec["h_p2c"]), s
+        assert R.fnv1a(o.lc[:n]) == int(rec["h_lc"]), s
+        assert R.fnv1a(o.node_charge) == int(rec["h_charge"]), s
