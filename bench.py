@@ -423,12 +423,111 @@ def arm_ours(args) -> dict:
         line["e2e"] = mixed["e2e"]
     if args.cpu_baseline and "cpu_sample_state" in f64:
         line["cpu_baseline"] = cpu_baseline_port(hm, f64["cpu_sample_state"], args.cpu_seconds)
+    if args.dh and world == 1:
+        line["direct_hop"] = run_direct_hop(hm, dev, min(args.steps, 20), args.warmup, seed, args.cpu_baseline)
     if args.cabana and world == 1:
         line["cabanapic"] = run_cabana(dev, min(args.steps, 20), args.warmup, args.cpu_baseline, args.cpu_seconds)
         line["gpu_launches_cabanapic"] = line["cabanapic"]["gpu_launches"]
     if advec is not None:
         line["advec_ensemble"] = advec
     return line
+
+
+# ------------------------------------------------------------ direct-hop (global move)
+
+DH_SPACING = 1.0 / 48  # one grid box per hexahedron of the 48x48x192 mesh
+
+
+def run_direct_hop(hm, dev, steps: int, warmup: int, seed: int, cpu: bool) -> dict:
+    """The global move (direct-hop seed, include/oppb_dh.h) on the bench workload: the GPU
+    build of the structured map over the 2,654,208 cells, then the mixed step with every walk
+    started from the grid's cell: push + move + deposit + compaction per step, device time,
+    after the same 300-step fill.  cpu: the reference's map search (all cells per query)
+    timed by the oracle on sampled boxes and scaled to the grid."""
+    import numpy as np
+    import torch
+
+    from oppb import _lib as L
+    from oppb.fempic import DirectHopGrid, FemPIC
+
+    sim = FemPIC(hm, dev, inject_per_step=CFG["inject"], ion_velocity=CFG["v_ion"], qm=CFG["qm"], dt=CFG["dt"],
+                 precision="mixed", fill=CFG["fill"], fill_period=CFG["period"], capacity=CFG["capacity"])
+    builds = []
+    for _ in range(3):  # the first build pays the module's first launches
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        grid = DirectHopGrid(hm, sim.mesh, DH_SPACING)
+        builds.append(time.perf_counter() - t0)
+    sim.dh = grid
+    gmap = grid.map.cpu().numpy()
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    rnd = torch.empty((5, CFG["inject"]), dtype=torch.float64, device=dev)
+
+    def device_randoms(out):
+        out[0:2].uniform_(0.0, 1.0, generator=gen)
+        out[2:5].normal_(0.0, CFG["sigma"], generator=gen)
+        return out
+
+    for _ in range(CFG["fill_steps"] + warmup):
+        sim.step(device_randoms(rnd))
+    tables = [device_randoms(torch.empty_like(rnd)) for _ in range(min(steps, 16))]
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    E = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    ps, t_ms, visits = 0, 0.0, 0
+    l0 = L.load().oppb_kernel_launches()
+    for k in range(steps):
+        ev = [E() for _ in range(4)]
+        sim.inject(tables[k % len(tables)])
+        sim.node_charge.zero_()
+        n_alive = sim.parts.size
+        ev[0].record(s)
+        sim.push_move()
+        ev[1].record(s)
+        st = sim.parts.status_host()
+        if st.error:
+            raise L.OppbError("push_move (direct hop)", st.error)
+        ev[2].record(s)
+        sim.finalize(st.remove_count)
+        ev[3].record(s)
+        sim.iter += 1
+        torch.cuda.synchronize()
+        ps += n_alive
+        visits += int(st.total_visits)
+        t_ms += ev[0].elapsed_time(ev[1]) + ev[2].elapsed_time(ev[3])
+    launches = L.load().oppb_kernel_launches() - l0
+    out = {"what": "mixed push + move + deposit + compaction with the global move on (every walk starts from "
+                   "the structured grid's cell), device time; grid spacing = hex size",
+           "unit": UNIT, "value": ps / (t_ms / 1e3), "steps": steps, "mean_particles": ps / steps,
+           "visits_per_particle": visits / ps, "gpu_launches": int(launches),
+           "grid": {"spacing": DH_SPACING, "dims": list(grid.dims), "boxes": grid.size,
+                    "boxes_with_cell": int((gmap != L.REMOVED_CELL).sum()),
+                    "build_s": min(builds[1:]), "first_build_s": builds[0],
+                    "build_what": "host bounding box + box counts, node upload, GPU binning and query "
+                                  "(one stream sync to size the workspace)"}}
+    del sim, grid
+    torch.cuda.empty_cache()
+    if cpu:
+        from oracle import oracle as O
+
+        dh = O.DirectHop(hm.n_pos, DH_SPACING, (4 * DH_SPACING,) * 3)
+        rng = np.random.default_rng(seed)
+        inside = np.flatnonzero(gmap != L.REMOVED_CELL)
+        outside = np.flatnonzero(gmap == L.REMOVED_CELL)
+        k_in, k_out = 24, 4
+        t0 = time.perf_counter()
+        dh.boxes(hm, rng.choice(inside, k_in, replace=False))
+        t_in = (time.perf_counter() - t0) / k_in
+        t0 = time.perf_counter()
+        dh.boxes(hm, rng.choice(outside, k_out, replace=False))
+        t_out = (time.perf_counter() - t0) / k_out
+        est = t_in * len(inside) + t_out * len(outside)
+        out["grid"]["cpu_baseline"] = {
+            "value": est, "unit": "s (estimated map build)", "cores": 1, "kind": "port",
+            "sample": f"C oracle (the reference's search over all cells per query) on {k_in} boxes with a cell and "
+                      f"{k_out} without, scaled by the grid's {len(inside)} and {len(outside)} boxes"}
+    return out
 
 
 # ------------------------------------------------------------- CabanaPIC (second workload)
@@ -773,6 +872,9 @@ def main():
     ap.add_argument("--advec-only", action="store_true", help="run only the NESO-advection ensemble measurement")
     ap.add_argument("--advec-instances", type=int, default=None, help="ensemble size (default 64)")
     ap.add_argument("--advec-side-max", type=int, default=None, help="largest mesh side (default 512)")
+    ap.add_argument("--no-dh", dest="dh", action="store_false",
+                    help="skip the global-move (direct-hop) measurement")
+    ap.add_argument("--dh-only", action="store_true", help="run only the global-move (direct-hop) measurement")
     ap.add_argument("--deposit", choices=["warp", "table"], default="warp",
                     help="deposit strategy: warp-run FP64 atomics or per-CTA shared node table")
     args = ap.parse_args()
@@ -794,6 +896,15 @@ def main():
         import torch
 
         print(json.dumps(run_advec(torch.device("cuda:0"), args.steps, args.warmup, args.cpu_baseline)), flush=True)
+        return
+    if args.dh_only and args.impl != "reference":
+        import torch
+
+        from oppb.fempic import HostMesh
+
+        hm = HostMesh(CFG["nx"], CFG["ny"], CFG["nz"], CFG["lx"], CFG["ly"], CFG["lz"])
+        print(json.dumps(run_direct_hop(hm, torch.device("cuda:0"), args.steps, args.warmup, CFG["seed"],
+                                        args.cpu_baseline)), flush=True)
         return
     if args.cabana_only and args.impl != "reference":
         import torch

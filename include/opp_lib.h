@@ -171,6 +171,29 @@ class Profiler {
     std::map<std::string, Entry> entries_;
 };
 
+// Bounding box of the direct-hop grid (opp_lib/include/opp_direct_hop_core.h:41-177): the box of
+// the node positions widened by `expansion`, computed by oppb_dh_bounding_box exactly as the
+// reference does.  One unpartitioned mesh: the global box is the local one.  3-D only.
+class BoundingBox {
+   public:
+    BoundingBox(const opp_dat node_pos_dat, int dim, const opp_point expansion);
+    BoundingBox(int dim, opp_point min_coordinate, opp_point max_coordinate);
+    const opp_point& getLocalMin() const { return box_[0]; }
+    const opp_point& getLocalMax() const { return box_[1]; }
+    const opp_point& getGlobalMin() const { return box_[0]; }
+    const opp_point& getGlobalMax() const { return box_[1]; }
+    int getDim() const { return dim_; }
+    // The node positions the box was made from (nullptr for a box given by its corners); the
+    // grid build bins the cells with them.
+    opp_dat nodePositions() const { return node_pos_; }
+    opp_point domain_expansion;
+
+   private:
+    int dim_ = 0;
+    opp_point box_[2];
+    opp_dat node_pos_ = nullptr;
+};
+
 }  // namespace opp
 
 extern std::unique_ptr<opp::Params> opp_params;

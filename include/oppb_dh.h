@@ -40,9 +40,17 @@ typedef struct oppb_dh_grid {
     int32_t* map;           /* device [size], filled by oppb_dh_build          */
 } oppb_dh_grid;
 
-/* Host: bounding box and grid dims from the node positions (host AoS [n_nodes][3]), as the
- * reference computes them (including its floating-point loop counts).  Leaves map untouched.
- * Returns OPPB_ERR_ARG for spacing <= 0, n_nodes <= 0 or a grid of more than 2^31 boxes. */
+/* Host: the bounding box of the node positions (host AoS [n_nodes][3]) widened by expansion,
+ * as opp::BoundingBox(n_pos, 3, expansion) computes it (opp_direct_hop_core.h:70-120). */
+int oppb_dh_bounding_box(const double* n_pos, int32_t n_nodes, const double expansion[3],
+                         double min_out[3], double max_out[3]);
+
+/* Host: the grid over a box, as CellMapper::init_host counts its boxes (:317-380, floating-point
+ * loop counts included).  Leaves map untouched.  OPPB_ERR_ARG for spacing <= 0, a non-finite
+ * box or a grid of more than 2^31 boxes. */
+int oppb_dh_grid_from_box(const double min[3], const double max[3], double spacing, oppb_dh_grid* grid);
+
+/* Host: oppb_dh_bounding_box then oppb_dh_grid_from_box. */
 int oppb_dh_grid_init(const double* n_pos, int32_t n_nodes, double spacing, const double expansion[3],
                       oppb_dh_grid* grid);
 

@@ -26,12 +26,14 @@ void opp_par_loop_injected__inject_ions_kernel(opp_set, opp_arg, opp_arg, opp_ar
 void opp_par_loop_all__calculate_new_pos_vel_kernel(opp_set, opp_arg, opp_arg, opp_arg);
 void opp_particle_move__move_kernel(opp_set, opp_map, opp_map, opp_arg, opp_arg, opp_arg, opp_arg);
 void opp_par_loop_all__deposit_charge_on_nodes_kernel(opp_set, opp_arg, opp_arg, opp_arg, opp_arg, opp_arg);
+void opp_init_direct_hop_cg(double, const opp_dat, const opp::BoundingBox&, opp_map, opp_map, opp_arg, opp_arg,
+                            opp_arg, opp_arg);
 
 namespace {
 
 struct CaseHeader {
     char magic[8];
-    int32_t n_nodes, n_cells, n_ifaces, inject, steps, n_tables, record_state, pad;
+    int32_t n_nodes, n_cells, n_ifaces, inject, steps, n_tables, record_state, direct_hop;
     double dt, qm, ion_velocity, sigma;
 };
 
@@ -78,7 +80,7 @@ int main(int argc, char** argv) {
     {
         Mesh m;
         CaseHeader h{};
-        std::vector<double> tables;
+        std::vector<double> tables, dh_par, n_pos;
         if (argc >= 3) {
             std::FILE* f = std::fopen(argv[2], "rb");
             if (!f || std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, "OPPBCAS1", 8) != 0)
@@ -97,6 +99,10 @@ int main(int argc, char** argv) {
             read_into(f, m.if_n_pos, nf * 9);
             read_into(f, m.if_dist, nf);
             read_into(f, tables, (size_t)h.n_tables * h.inject * 5);
+            if (h.direct_hop) {  // grid spacing, expansion[3], node positions [n_nodes][3]
+                read_into(f, dh_par, 4);
+                read_into(f, n_pos, (size_t)m.n_nodes * 3);
+            }
             std::fclose(f);
         } else {
             // Box mesh and static field from the parameter file.
@@ -157,6 +163,19 @@ int main(int argc, char** argv) {
         opp_map p2c_map = opp_decl_map(particle_set, cell_set, 1, nullptr, "p2c_map");
         // Injection table: (a, b, thermal vx, vy, vz) per injected particle, refreshed each step.
         opp_dat dp_rand = opp_decl_dat(dummy_part_set, 5, DT_REAL, nullptr, "dummy_part_rand");
+
+        // Global move (opp_global_move in the parameter file): the app's direct-hop set-up
+        // (fempic_opp.cpp:69-76,95,147-153) with the case's grid spacing and expansion.
+        if (h.direct_hop) {
+            std::vector<int> c_id((size_t)m.n_cells);
+            for (int c = 0; c < m.n_cells; c++) c_id[(size_t)c] = c;
+            opp_dat n_pos_d = opp_decl_dat(node_set, 3, DT_REAL, n_pos.data(), "n_pos");
+            opp_dat c_gbl_id = opp_decl_dat(cell_set, 1, DT_INT, c_id.data(), "c_gbl_id");
+            opp::BoundingBox bounding_box(n_pos_d, 3, opp_point(dh_par[1], dh_par[2], dh_par[3]));
+            opp_init_direct_hop_cg(dh_par[0], c_gbl_id, bounding_box, c2c_map, p2c_map, opp_arg_dat(p_pos, OPP_READ),
+                                   opp_arg_dat(p_lc, OPP_WRITE), opp_arg_dat(c_volume, p2c_map, OPP_READ),
+                                   opp_arg_dat(c_det, p2c_map, OPP_READ));
+        }
 
         double one = 1.0, zero = 0.0;
         opp_decl_const<OPP_REAL>(1, &zero, "CONST_spwt");

@@ -168,10 +168,9 @@ __device__ unsigned long long g_dh_pairs;
 }  // namespace
 }  // namespace oppb
 
-extern "C" int oppb_dh_grid_init(const double* n_pos, int32_t n_nodes, double spacing, const double expansion[3],
-                                 oppb_dh_grid* g) {
-    if (!n_pos || !expansion || !g || n_nodes <= 0 || !(spacing > 0.0) || !std::isfinite(spacing))
-        return OPPB_ERR_ARG;
+extern "C" int oppb_dh_bounding_box(const double* n_pos, int32_t n_nodes, const double expansion[3],
+                                    double min_out[3], double max_out[3]) {
+    if (!n_pos || !expansion || !min_out || !max_out || n_nodes <= 0) return OPPB_ERR_ARG;
     // BoundingBox(n_pos, 3, expansion) (opp_lib/include/opp_direct_hop_core.h:70-120): the
     // running max starts at MIN_REAL = DBL_MIN, and the x/y widening reads the expansion's
     // x for both minima and its y for both maxima, as written there.
@@ -188,26 +187,43 @@ extern "C" int oppb_dh_grid_init(const double* n_pos, int32_t n_nodes, double sp
     mx[1] += (expansion[1] - oppb::kBoundOffset);
     mn[2] -= (expansion[2] + oppb::kBoundOffset);
     mx[2] += (expansion[2] - oppb::kBoundOffset);
+    for (int d = 0; d < 3; d++) {
+        min_out[d] = mn[d];
+        max_out[d] = mx[d];
+    }
+    return OPPB_OK;
+}
+
+extern "C" int oppb_dh_grid_from_box(const double min[3], const double max[3], double spacing, oppb_dh_grid* g) {
+    if (!min || !max || !g || !(spacing > 0.0) || !std::isfinite(spacing)) return OPPB_ERR_ARG;
     // CellMapper::init_host (:317-380): boxes per axis = 1 + the count of the loop
     // `for (v = min; v < max; v += h)`, in floating point as there.
     int64_t dims[3];
     for (int d = 0; d < 3; d++) {
+        if (!std::isfinite(min[d]) || !std::isfinite(max[d])) return OPPB_ERR_ARG;
         int64_t a = 0;
-        for (double v = mn[d]; v < mx[d]; v += spacing)
+        for (double v = min[d]; v < max[d]; v += spacing)
             if (++a > oppb::kMaxLoop) return OPPB_ERR_ARG;
         dims[d] = a + 1;
     }
     const double size = (double)dims[0] * (double)dims[1] * (double)dims[2];
     if (size > 2147483646.0) return OPPB_ERR_ARG;
     for (int d = 0; d < 3; d++) {
-        g->min[d] = mn[d];
-        g->max[d] = mx[d];
+        g->min[d] = min[d];
+        g->max[d] = max[d];
         g->dims[d] = dims[d];
     }
     g->spacing = spacing;
     g->inv_spacing = 1.0 / spacing;
     g->size = dims[0] * dims[1] * dims[2];
     return OPPB_OK;
+}
+
+extern "C" int oppb_dh_grid_init(const double* n_pos, int32_t n_nodes, double spacing, const double expansion[3],
+                                 oppb_dh_grid* g) {
+    double mn[3], mx[3];
+    const int rc = oppb_dh_bounding_box(n_pos, n_nodes, expansion, mn, mx);
+    return rc ? rc : oppb_dh_grid_from_box(mn, mx, spacing, g);
 }
 
 extern "C" int oppb_dh_build(const oppb_tet_mesh* mesh, const double* n_pos, oppb_dh_grid* grid, void* workspace,

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "opp_lib.h"
+#include "oppb_dh.h"
 
 namespace {
 
@@ -26,6 +27,12 @@ oppb_particles particles(opp_set set, opp_dat pos, opp_dat vel, opp_dat lc) {
 }
 
 double charge_over_mass() { return opp_get_const("CONST_charge") / opp_get_const("CONST_mass"); }
+
+// The global move's structured grid, set up by opp_init_direct_hop_cg when opp_global_move is on.
+struct DirectHop {
+    bool on = false;
+    oppb_dh_grid grid{};
+} g_dh;
 
 // Inlet geometry record [n_faces][12] = u, v, normal, node0, packed from the iface dats.
 struct InletCache {
@@ -113,7 +120,17 @@ void opp_particle_move__move_kernel(opp_set set, opp_map c2c_map, opp_map p2c_ma
     const oppb_tet_mesh& mesh = oppb_rt::tet_mesh(arg3.dat, arg2.dat, c2c_map, nullptr, nullptr);
     oppb_particles p = particles(set, arg0.dat, nullptr, arg1.dat);
     opp_profiler->start("move_kernel_only");
-    check(oppb_move_f64(&mesh, &p, oppb_rt::move_status(), OPP_move_max_hops, oppb_rt::stream()), "oppb_move_f64");
+    if (g_dh.on) {  // global move: the walks start from the structured grid's cells
+        oppb_move_options o{};
+        o.precision = OPPB_PRECISION_F64;
+        o.dh = &g_dh.grid;
+        check(oppb_move_ex(&mesh, &p, &o, nullptr, oppb_rt::move_status(), OPP_move_max_hops, nullptr, 0,
+                           oppb_rt::stream()),
+              "oppb_move_ex");
+    } else {
+        check(oppb_move_f64(&mesh, &p, oppb_rt::move_status(), OPP_move_max_hops, oppb_rt::stream()),
+              "oppb_move_f64");
+    }
     oppb_rt::mark_device_written(arg1.dat);
     oppb_rt::mark_device_written(set->mesh_relation_dat);
     opp_profiler->end("move_kernel_only");
@@ -137,4 +154,49 @@ void opp_par_loop_all__deposit_charge_on_nodes_kernel(opp_set set, opp_arg arg0,
     oppb_rt::mark_device_written(arg1.dat);
     if (cudaStreamSynchronize(oppb_rt::stream()) != cudaSuccess) opp_abort("deposit");
     opp_profiler->end("deposit_charge_on_nodes_kernel");
+}
+
+// opp_init_direct_hop_cg (apps_codegen/app_fempic_cg/cuda/move_kernel_loop.hpp:403-475): with
+// opp_global_move set, builds the structured grid of spacing grid_spacing over b_box on the
+// GPU (the reference searches all cells per grid box on the host, or reads a file made that
+// way); every later move starts each walk from its grid box's cell.  One unpartitioned mesh:
+// the cells' global ids must be their indices.
+void opp_init_direct_hop_cg(double grid_spacing, const opp_dat c_gbl_id, const opp::BoundingBox& b_box,
+                            opp_map c2c_map, opp_map p2c_map, opp_arg arg0, opp_arg arg1, opp_arg arg2,
+                            opp_arg arg3) {
+    (void)p2c_map, (void)arg0, (void)arg1;
+    if (!opp_params->get<OPP_BOOL>("opp_global_move")) return;
+    opp_profiler->start("Setup_Mover");
+    opp_set cells = c2c_map->from;
+    if (c_gbl_id) {
+        opp_download_dat(c_gbl_id);
+        const int* id = reinterpret_cast<const int*>(c_gbl_id->data);
+        for (int c = 0; c < cells->size; c++)
+            if (id[c] != c) opp_abort("opp_init_direct_hop_cg: c_gbl_id must be the cell index on one GPU");
+    }
+    opp_dat npos = b_box.nodePositions();
+    if (!npos) opp_abort("opp_init_direct_hop_cg: the bounding box must come from the node positions");
+    opp_map c2n = nullptr;  // the cell -> node map the binning reads
+    for (opp_map m : opp_maps)
+        if (m && m->from == cells && m->to == npos->set && m->dim == 4) c2n = m;
+    if (!c2n) opp_abort("opp_init_direct_hop_cg: no cell -> node map of dimension 4 is declared");
+    const opp_point& mn = b_box.getGlobalMin();
+    const opp_point& mx = b_box.getGlobalMax();
+    const double lo[3] = {mn.x, mn.y, mn.z}, hi[3] = {mx.x, mx.y, mx.z};
+    if (g_dh.grid.map) cudaFree(g_dh.grid.map);
+    g_dh = DirectHop{};
+    check(oppb_dh_grid_from_box(lo, hi, grid_spacing, &g_dh.grid), "oppb_dh_grid_from_box");
+    if (cudaMalloc(&g_dh.grid.map, sizeof(int32_t) * (size_t)g_dh.grid.size) != cudaSuccess)
+        opp_abort("cudaMalloc direct-hop map");
+    oppb_rt::sync_host_to_device(npos);
+    const oppb_tet_mesh& mesh = oppb_rt::tet_mesh(arg3.dat, arg2.dat, c2c_map, c2n, nullptr);
+    const double* npos_d = reinterpret_cast<const double*>(npos->data_d);
+    size_t need = 0;
+    int rc = oppb_dh_build(&mesh, npos_d, &g_dh.grid, nullptr, 0, &need, oppb_rt::stream());
+    if (rc == OPPB_ERR_WORKSPACE)
+        rc = oppb_dh_build(&mesh, npos_d, &g_dh.grid, oppb_rt::workspace(need), need, &need, oppb_rt::stream());
+    check(rc, "oppb_dh_build");
+    if (cudaStreamSynchronize(oppb_rt::stream()) != cudaSuccess) opp_abort("direct-hop grid build");
+    g_dh.on = true;
+    opp_profiler->end("Setup_Mover");
 }

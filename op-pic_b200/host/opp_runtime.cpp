@@ -14,6 +14,7 @@
 #include <sstream>
 
 #include "opp_lib.h"
+#include "oppb_dh.h"
 
 std::unique_ptr<opp::Params> opp_params;
 std::unique_ptr<opp::Profiler> opp_profiler;
@@ -797,3 +798,29 @@ const oppb_tet_mesh& tet_mesh(opp_dat c_det, opp_dat c_volume, opp_map c2c, opp_
 }
 
 }  // namespace oppb_rt
+
+// ------------------------------------------------------------- direct-hop box
+
+namespace opp {
+
+BoundingBox::BoundingBox(const opp_dat node_pos_dat, int dim, const opp_point expansion)
+    : domain_expansion(expansion), dim_(dim), node_pos_(node_pos_dat) {
+    if (dim != 3) opp_abort("BoundingBox: the direct-hop grid of this backend is 3-D");
+    if (!node_pos_dat || node_pos_dat->dim != 3) opp_abort("BoundingBox: node positions must be a 3-component dat");
+    opp_download_dat(node_pos_dat);
+    const double e[3] = {expansion.x, expansion.y, expansion.z};
+    double mn[3], mx[3];
+    if (oppb_dh_bounding_box(reinterpret_cast<const double*>(node_pos_dat->data), node_pos_dat->set->size, e, mn,
+                             mx) != OPPB_OK)
+        opp_abort("BoundingBox: no node positions");
+    box_[0] = opp_point(mn[0], mn[1], mn[2]);
+    box_[1] = opp_point(mx[0], mx[1], mx[2]);
+}
+
+BoundingBox::BoundingBox(int dim, opp_point min_coordinate, opp_point max_coordinate) : dim_(dim) {
+    if (dim != 3) opp_abort("BoundingBox: the direct-hop grid of this backend is 3-D");
+    box_[0] = min_coordinate;
+    box_[1] = max_coordinate;
+}
+
+}  // namespace opp

@@ -48,3 +48,31 @@ def test_fempic_app_matches_oracle(tmp_path, fill, period, steps):
     np.testing.assert_array_equal(got["lc"].view(np.uint64), o.lc[:n].view(np.uint64))
     err = np.abs(got["node_charge"] - o.node_charge) / np.maximum(np.abs(o.node_charge), 1.0)
     assert err.max() <= 1e-12
+
+
+def test_fempic_app_global_move_matches_reference_golden(tmp_path):
+    """The app with opp_global_move on (opp::BoundingBox + opp_init_direct_hop_cg, the
+    reference app's set-up) against the reference seq backend's own global-move run
+    (tests/golden/fempic_4x4x8_dh.npz): per-step sizes, removals and digests, final state."""
+    from oppb.fempic import HostMesh
+
+    z = np.load(Path(__file__).resolve().parent / "golden" / "fempic_4x4x8_dh.npz")
+    hm = HostMesh(*[float(v) if i >= 3 else int(v) for i, v in enumerate(z["dims"])])
+    steps, sp = int(z["steps"]), float(z["spacing"])
+    R.write_case(tmp_path / "case.bin", hm, z["dist"], steps, list(z["tables"]), dt=float(z["dt"]),
+                 dh=(sp, (4 * sp,) * 3))
+    (tmp_path / "params.txt").write_text(R.params_text(str(z["fill"]), int(z["period"]), 2.0, global_move=True))
+    r = subprocess.run([str(APP), str(tmp_path / "params.txt"), str(tmp_path / "case.bin"), str(tmp_path / "out.bin")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = R.read_output(tmp_path / "out.bin", hm.n_nodes)
+    for s in range(steps):
+        g, ref = got["records"][s], z["records"][s]
+        assert (int(g["size"]), int(g["removed"])) == (int(ref["size"]), int(ref["removed"])), s
+        assert int(g["h_p2c"]) == int(ref["h_p2c"]), s
+        assert int(g["h_pos"]) == int(ref["h_pos"]), s
+        assert int(g["h_lc"]) == int(ref["h_lc"]), s
+    np.testing.assert_array_equal(got["p2c"], z["p2c"])
+    np.testing.assert_array_equal(got["lc"].view(np.uint64), z["lc"].view(np.uint64))
+    err = np.abs(got["node_charge"] - z["node_charge"]) / np.maximum(np.abs(z["node_charge"]), 1.0)
+    assert err.max() <= 1e-12
