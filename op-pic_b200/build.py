@@ -27,7 +27,7 @@ NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", f"
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", f"-I{INC}", "-Wall"]
 # Sources whose FP64 expressions must keep the reference's written order with one rounding
 # per operation: no FMA contraction anywhere in the file.
-PER_FILE_NVCC_FLAGS = {"cabana.cu": ["-fmad=false"], "advec.cu": ["-fmad=false"],
+PER_FILE_NVCC_FLAGS = {"cabana.cu": ["-fmad=false"], "advec.cu": ["-fmad=false"], "field.cu": ["-fmad=false"],
                        # the grid set-up loops of the direct-hop mapper run on the host
                        "dh.cu": ["-Xcompiler", "-ffp-contract=off"]}
 
@@ -48,8 +48,8 @@ def _run(cmd: list[str]) -> None:
 
 CUDA_INC = "/usr/local/cuda/include"
 # Host sources of the C ABI library (set-up utilities) and of the C++ drop-in runtime.
-ABI_HOST = ("fempic_mesh.cpp",)
-RUNTIME_HOST = ("fempic_mesh.cpp", "opp_runtime.cpp", "fempic_loops.cpp")
+ABI_HOST = ("fempic_mesh.cpp", "fempic_field.cpp")
+RUNTIME_HOST = ("fempic_mesh.cpp", "fempic_field.cpp", "opp_runtime.cpp", "fempic_loops.cpp")
 
 
 def _objects(force: bool, names) -> list[Path]:
@@ -93,7 +93,8 @@ def build_oppb(force: bool = False) -> Path:
 
 def build_oracle(force: bool = False) -> Path:
     """Compile the C oracle (test infrastructure) into oracle/lib/liboppb_oracle.so."""
-    srcs = [ROOT / "oracle" / "fempic_oracle.c", ROOT / "oracle" / "cabana_oracle.c", ROOT / "oracle" / "advec_oracle.c"]
+    srcs = [ROOT / "oracle" / "fempic_oracle.c", ROOT / "oracle" / "cabana_oracle.c", ROOT / "oracle" / "advec_oracle.c",
+            ROOT / "oracle" / "field_oracle.c"]
     out_dir = ROOT / "oracle" / "lib"
     out_dir.mkdir(exist_ok=True)
     so = out_dir / "liboppb_oracle.so"

@@ -95,6 +95,28 @@ class MoveOptions(C.Structure):
                 ("qm", C.c_double), ("dt", C.c_double), ("band", C.c_double), ("dh", C.POINTER(DhGrid))]
 
 
+class FieldSystem(C.Structure):
+    _fields_ = [("n_nodes", c_i32), ("n_cells", c_i32), ("neq", c_i32), ("node_to_eq", c_ip), ("c2n", c_ip),
+                ("det_j", c_dp), ("c_sd", c_dp), ("n_bnd_pot", c_dp), ("k_rowptr", C.POINTER(c_i64)),
+                ("k_col", c_ip), ("k_val", c_dp), ("f0", c_dp), ("nnz", c_i64)]
+
+
+class FieldConsts(C.Structure):
+    _fields_ = [("n0", C.c_double), ("phi0", C.c_double), ("kte", C.c_double), ("qe", C.c_double),
+                ("eps0", C.c_double), ("rtol", C.c_double), ("atol", C.c_double), ("max_iter", c_i32),
+                ("reserved", c_i32)]
+
+
+class FieldDevice(C.Structure):
+    _fields_ = [("n_nodes", c_i32), ("n_cells", c_i32), ("neq", c_i32), ("reserved", c_i32),
+                ("node_to_eq", c_vp), ("c2n", c_vp), ("det_j", c_vp), ("n_bnd_pot", c_vp), ("k_rowptr", c_vp),
+                ("k_col", c_vp), ("k_val", c_vp), ("f0", c_vp), ("d", c_vp), ("f1", c_vp), ("work", c_vp)]
+
+
+class FieldStatus(C.Structure):
+    _fields_ = [("iterations", c_i32), ("converged", c_i32), ("resid", C.c_double), ("b_norm", C.c_double)]
+
+
 class FemPICMesh(C.Structure):
     _fields_ = [("n_nodes", c_i32), ("n_cells", c_i32), ("n_ifaces", c_i32),
                 ("n_pos", c_dp), ("n_vol", c_dp), ("n_type", c_ip), ("n_bnd_pot", c_dp),
@@ -145,6 +167,12 @@ _SIGS = {
     "oppb_dh_build": (C.c_int, [P(TetMesh), c_vp, P(DhGrid), c_vp, C.c_size_t, P(C.c_size_t), c_vp]),
     "oppb_move_ex": (C.c_int, [P(TetMesh), P(Particles), P(MoveOptions), c_vp, c_vp, c_i32, c_vp, C.c_size_t,
                                c_vp]),
+    "oppb_field_setup": (C.c_int, [P(FemPICMesh), P(FieldSystem)]),
+    "oppb_field_system_free": (None, [P(FieldSystem)]),
+    "oppb_field_work_doubles": (C.c_size_t, [c_i32]),
+    "oppb_node_charge_density": (C.c_int, [c_vp, c_vp, C.c_double, c_i32, c_vp]),
+    "oppb_field_solve": (C.c_int, [P(FieldDevice), P(FieldConsts), c_vp, c_vp, c_vp, c_vp]),
+    "oppb_electric_field": (C.c_int, [c_vp, c_vp, c_vp, c_vp, c_i32, c_i32, c_vp]),
     "oppb_fempic_box_mesh": (C.c_int, [c_i32, c_i32, c_i32, C.c_double, C.c_double, C.c_double, P(FemPICMesh)]),
     "oppb_fempic_solve_field": (C.c_int, [P(FemPICMesh), C.c_double, C.c_double, C.c_double, c_i32, c_dp,
                                           P(c_i32), P(C.c_double)]),
