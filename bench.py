@@ -423,6 +423,8 @@ def arm_ours(args) -> dict:
         line["e2e"] = mixed["e2e"]
     if args.cpu_baseline and "cpu_sample_state" in f64:
         line["cpu_baseline"] = cpu_baseline_port(hm, f64["cpu_sample_state"], args.cpu_seconds)
+    if args.field and world == 1:
+        line["field_phase"] = run_field_phase(hm, dev, min(args.steps, 20), args.warmup, seed, args.cpu_baseline)
     if args.dh and world == 1:
         line["direct_hop"] = run_direct_hop(hm, dev, min(args.steps, 20), args.warmup, seed, args.cpu_baseline)
     if args.cabana and world == 1:
@@ -527,6 +529,115 @@ def run_direct_hop(hm, dev, steps: int, warmup: int, seed: int, cpu: bool) -> di
             "value": est, "unit": "s (estimated map build)", "cores": 1, "kind": "port",
             "sample": f"C oracle (the reference's search over all cells per query) on {k_in} boxes with a cell and "
                       f"{k_out} without, scaled by the grid's {len(inside)} and {len(outside)} boxes"}
+    return out
+
+
+# ------------------------------------------------------------------ field phase
+
+# Electron model of the field-phase leg in the workload's units: unit charge and permittivity,
+# n0 = 1 and spwt so that the steady state's ion density (~5.7e7 particles in a volume of 4)
+# is about n0, kTe = 100 so that exp((D - phi0) / kTe) stays O(1) while F1 accumulates over
+# the timed steps (the reference never resets F1; over hundreds of steps D grows until the
+# exponential overflows, so the leg fills with the set-up field and turns the phase on after).
+FIELD = dict(n0=1.0, phi0=0.0, kte=100.0, qe=1.0, eps0=1.0, spwt=4.0 / 5.7e7)
+
+
+def run_field_phase(hm, dev, steps: int, warmup: int, seed: int, cpu: bool) -> dict:
+    """The mixed step with the field phase on (compute_node_charge_density, compute_phi's
+    Newton step with the cooperative CG, compute_electric_field into the move's field, one
+    CUDA graph per step), after the same 300-step fill with the set-up field: time of the
+    field phase alone and of the whole step.  cpu: the oracle's compute_phi (C, one core) on
+    the same state."""
+    import numpy as np
+    import torch
+
+    from oppb import _lib as L
+    from oppb.fempic import FemPIC
+    from oppb.field import FieldConstants
+
+    consts = FieldConstants(**{k: v for k, v in FIELD.items() if k != "spwt"})
+    t0 = time.perf_counter()
+    sim = FemPIC(hm, dev, inject_per_step=CFG["inject"], ion_velocity=CFG["v_ion"], qm=CFG["qm"], dt=CFG["dt"],
+                 precision="mixed", fill=CFG["fill"], fill_period=CFG["period"], capacity=CFG["capacity"],
+                 field=consts, spwt=FIELD["spwt"])
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    rnd = torch.empty((5, CFG["inject"]), dtype=torch.float64, device=dev)
+
+    def device_randoms(out):
+        out[0:2].uniform_(0.0, 1.0, generator=gen)
+        out[2:5].normal_(0.0, CFG["sigma"], generator=gen)
+        return out
+
+    sim.field_enabled = False
+    for _ in range(CFG["fill_steps"]):
+        sim.step(device_randoms(rnd))
+    sim.field_enabled = True
+    for _ in range(warmup):
+        sim.step(device_randoms(rnd))
+    tables = [device_randoms(torch.empty_like(rnd)) for _ in range(min(steps, 16))]
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    E = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    ps, t_step, t_field, iters, pmax = 0, 0.0, 0.0, [], 0.0
+    l0 = L.load().oppb_kernel_launches()
+    for k in range(steps):
+        e0, e1 = E(), E()
+        n_before = sim.parts.size
+        e0.record(s)
+        sim.step(tables[k % len(tables)])  # includes the field phase at its end
+        e1.record(s)
+        torch.cuda.synchronize()
+        ps += n_before + CFG["inject"]
+        t_step += e0.elapsed_time(e1)
+        st = sim.field.status_host()
+        if not st.converged:
+            raise RuntimeError(f"field solve did not converge ({st.iterations} iterations)")
+        iters.append(st.iterations)
+        pmax = max(pmax, float(sim.field.potential.abs().max()))
+    # The field phase alone, replayed on the last step's node charge (recovered from the
+    # density the step left: charge = density * n_vol / spwt, to rounding); the Newton state
+    # advances with each replay, as it would step to step.
+    reps = 10
+    charge = sim.node_charge * sim.n_vol / FIELD["spwt"]
+    saved = (sim.field.d.clone(), sim.field.f1.clone(), charge)
+    f0, f1 = E(), E()
+    torch.cuda.synchronize()
+    f0.record(s)
+    for _ in range(reps):
+        sim.node_charge.copy_(saved[2])
+        sim.field_phase()
+    f1.record(s)
+    f1.synchronize()
+    t_field = f0.elapsed_time(f1) / reps
+    launches = L.load().oppb_kernel_launches() - l0
+    out = {"what": "mixed step with the field phase (node charge density, Newton step of the Poisson-Boltzmann "
+                   "potential with cooperative CG, cell field), device time; the field phase is one CUDA graph",
+           "unit": UNIT, "whole_step_value": ps / (t_step / 1e3), "steps": steps,
+           "field_ms": t_field, "field_what": "graph replay of the field phase on the last step's charge "
+                                              "(node copy of 3.7 MB included)",
+           "cg_iterations": {"mean": float(np.mean(iters)), "min": int(min(iters)), "max": int(max(iters))},
+           "max_abs_potential": pmax, "visits_per_particle_last": sim.last["visits"] / max(1, sim.last["size_before_move"]),
+           "nodes": hm.n_nodes, "unknowns": sim.field.neq, "nnz": sim.field.nnz, "setup_s": setup_s,
+           "constants": FIELD, "gpu_launches": int(launches)}
+    if cpu:
+        from oracle import field as F
+
+        fs = F.FieldSystem(hm.n_pos, hm.n_type, sim.field.d_bnd.cpu().numpy(), hm.c2n)
+        fs.d[:fs.neq] = saved[0][:fs.neq].cpu().numpy()
+        fs.f1[:fs.neq] = saved[1][:fs.neq].cpu().numpy()
+        den = saved[2].cpu().numpy()
+        t0 = time.perf_counter()  # density scaling + compute_phi, as one field phase minus the cell field
+        _, it, _ = fs.solve(F.node_charge_density(den, hm.n_vol, FIELD["spwt"]),
+                            F.FieldConsts(**{k: v for k, v in FIELD.items() if k != "spwt"}))
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": t * 1e3, "unit": "ms per compute_phi", "cores": 1, "kind": "port",
+                               "sample": f"C oracle (Jacobi CG, {it} iterations) on the same state; the reference "
+                                         f"solves with PETSc KSPCG, absent here"}
+    del sim
+    torch.cuda.empty_cache()
     return out
 
 
@@ -872,6 +983,9 @@ def main():
     ap.add_argument("--advec-only", action="store_true", help="run only the NESO-advection ensemble measurement")
     ap.add_argument("--advec-instances", type=int, default=None, help="ensemble size (default 64)")
     ap.add_argument("--advec-side-max", type=int, default=None, help="largest mesh side (default 512)")
+    ap.add_argument("--no-field", dest="field", action="store_false",
+                    help="skip the field-phase measurement")
+    ap.add_argument("--field-only", action="store_true", help="run only the field-phase measurement")
     ap.add_argument("--no-dh", dest="dh", action="store_false",
                     help="skip the global-move (direct-hop) measurement")
     ap.add_argument("--dh-only", action="store_true", help="run only the global-move (direct-hop) measurement")
@@ -896,6 +1010,15 @@ def main():
         import torch
 
         print(json.dumps(run_advec(torch.device("cuda:0"), args.steps, args.warmup, args.cpu_baseline)), flush=True)
+        return
+    if args.field_only and args.impl != "reference":
+        import torch
+
+        from oppb.fempic import HostMesh
+
+        hm = HostMesh(CFG["nx"], CFG["ny"], CFG["nz"], CFG["lx"], CFG["ly"], CFG["lz"])
+        print(json.dumps(run_field_phase(hm, torch.device("cuda:0"), args.steps, args.warmup, CFG["seed"],
+                                         args.cpu_baseline)), flush=True)
         return
     if args.dh_only and args.impl != "reference":
         import torch

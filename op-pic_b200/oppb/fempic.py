@@ -261,7 +261,8 @@ class FemPIC:
                  ion_velocity: float = 1.0, qm: float = 1.0, dt: float = 0.01, precision: str = "f64",
                  fill: str = "HoleFill_All", fill_period: int = 10, alloc_mult: float = 2.0,
                  capacity: int = 0, max_hops: int = 4096, band: float = 1e-5, fused_deposit: bool = True,
-                 fused_push: bool = True, direct_hop: float | None = None, dh_expansion=None):
+                 fused_push: bool = True, direct_hop: float | None = None, dh_expansion=None,
+                 field=None, spwt: float = 1.0, phi_inlet: float = 1.0, phi_fixed: float = 0.0):
         if not torch.cuda.is_available():
             raise RuntimeError("FemPIC needs a CUDA device (there is no CPU fallback)")
         self.device = torch.device(device)
@@ -289,6 +290,21 @@ class FemPIC:
         # Global move: every walk starts from the cell of the structured grid's box that the
         # particle is in (opp_global_move with grid_spacing = direct_hop).
         self.dh = DirectHopGrid(hm, self.mesh, direct_hop, dh_expansion) if direct_hop else None
+        # Field phase (field: oppb.field.FieldConstants): after the compaction, as the generated
+        # main loop (fempic_opp.cpp:195-215): compute_node_charge_density, compute_phi (the
+        # Newton step with phi_inlet / phi_fixed on the Dirichlet nodes), opp_reset_dat(c_ef)
+        # and compute_electric_field into the move's packed field, which the next step's push
+        # and injection read.  Replayed as one CUDA graph per node-charge buffer.
+        self.field_consts = field
+        self.field = None
+        self.field_enabled = True  # the field phase can be paused (e.g. to fill with the set-up field)
+        if field is not None:
+            from .field import FieldDevice, boundary_potential
+
+            self.field = FieldDevice(hm, self.device, boundary_potential(hm.n_type, phi_inlet, phi_fixed))
+            self.n_vol = torch.from_numpy(np.ascontiguousarray(hm.n_vol)).to(self.device)
+            self.spwt = float(spwt)
+            self._field_graphs = {}
         self._pipeline(5, inject_per_step)
 
     # workspace shared by hole fill and sort (grown on demand)
@@ -319,6 +335,24 @@ class FemPIC:
         if self._dep_ws.numel() < nbytes:
             self._dep_ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
         return self._dep_ws
+
+    def field_phase(self, stream=None) -> None:
+        """Node charge density, potential and cell field from node_charge (in place, as the
+        reference scales n_charge_den), replayed from a CUDA graph."""
+        key = self.node_charge.data_ptr()
+        g = self._field_graphs.get(key)
+        if g is None:
+            state = (self.field.d.clone(), self.field.f1.clone(), self.node_charge.clone())
+            g = self.field.capture(self.node_charge, self.n_vol, self.spwt, self.field_consts, self.mesh.ef, 4)
+            self.field.d.copy_(state[0])  # capture and its warm-up leave the state as it was
+            self.field.f1.copy_(state[1])
+            self.node_charge.copy_(state[2])
+            self._field_graphs[key] = g
+        if stream is not None:
+            with torch.cuda.stream(stream):
+                g.replay()
+        else:
+            g.replay()
 
     def _move_ex(self, push: bool, stream=None) -> None:
         """The move through oppb_move_ex (the direct-hop seed is only reached there)."""
@@ -429,6 +463,8 @@ class FemPIC:
         kind = self.finalize(st.remove_count, stream)
         if not self.fused_deposit and self.precision == "f64":
             self.deposit(stream)
+        if self.field is not None and self.field_enabled:
+            self.field_phase(stream)
         if ev:
             ev[4].record(s)
             ev[4].synchronize()

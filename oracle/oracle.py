@@ -156,9 +156,13 @@ class OracleFemPIC:
     """
 
     def __init__(self, mesh, dist, ion_velocity=1.0, qm=1.0, dt=0.01, fill="HoleFill_All", fill_period=10,
-                 alloc_mult=2.0, mixed=False, max_hops=1 << 20, dh: DirectHop | None = None):
+                 alloc_mult=2.0, mixed=False, max_hops=1 << 20, dh: DirectHop | None = None, field=None):
         self.m = mesh
         self.dh = dh  # global move: every walk starts from the grid's cell
+        # field phase after the deposit: (oracle.field.FieldSystem, FieldConsts, spwt, n_vol);
+        # the new cell field replaces mesh.c_ef, which the next push and injection read
+        self.field = field
+        self.potential = None
         self.dist = np.ascontiguousarray(dist, np.int32)
         self.ion_velocity, self.qm, self.dt = ion_velocity, qm, dt
         self.fill, self.fill_period, self.alloc_mult = fill, fill_period, alloc_mult
@@ -214,6 +218,13 @@ class OracleFemPIC:
         rc += seeded_out
         self.finalize(rc)
         deposit(self.lc, self.p2c, m.c2n, self.node_charge, n=self.size)
+        if self.field is not None:
+            from oracle import field as F
+
+            fs, consts, spwt, n_vol = self.field
+            self.node_charge[:] = F.node_charge_density(self.node_charge, n_vol, spwt)
+            self.potential, _, _ = fs.solve(self.node_charge, consts)
+            m.c_ef[:] = F.electric_field(m.c2n, fs.c_sd, self.potential)
         self.last_remove, self.last_visits = rc, visits
         out = {"iter": self.iter, "size_before_move": n_before, "removed": rc, "size": self.size, "visits": visits}
         self.iter += 1

@@ -123,3 +123,35 @@ def test_full_size_solve_matches_oracle():
     pot_o, it_o, _ = fs.solve(ion, F.FieldConsts(**c))
     assert st.converged == 1 and abs(st.iterations - it_o) <= 2
     _close(pot, pot_o, 1e-8)
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_fempic_steps_with_field_phase_match_oracle(precision):
+    """Whole steps with the field phase (the generated main loop's order): cells and counts
+    equal to the oracle's, positions and fields within the CG tolerance's reach."""
+    from oppb.fempic import FemPIC, injection_randoms, randoms_to_device
+    from oracle import oracle as O
+
+    hm = HostMesh(10, 10, 40, 1.0, 1.0, 4.0)
+    hm_o = HostMesh(10, 10, 40, 1.0, 1.0, 4.0)  # the oracle rewrites its mesh's c_ef
+    c = dict(n0=100.0, phi0=0.0, kte=1.0, qe=1.0, eps0=1.0)
+    spwt = 100.0 * 4.0 / 20_000  # ion density ~ n0 once ~20k particles are in the box
+    sim = FemPIC(hm, DEV, inject_per_step=2000, dt=0.05, precision=precision, field=FieldConstants(**c), spwt=spwt)
+    fs = F.FieldSystem(hm_o.n_pos, hm_o.n_type, boundary_potential(hm_o.n_type, 1.0, 0.0), hm_o.c2n)
+    orc = O.OracleFemPIC(hm_o, sim.dist_host, dt=0.05, mixed=(precision == "mixed"),
+                         field=(fs, F.FieldConsts(**c), spwt, hm_o.n_vol))
+    for s in range(12):
+        rnd = injection_randoms(13, s, 2000, 0.1)
+        g = sim.step(randoms_to_device(rnd, DEV))
+        o = orc.step(rnd)
+        assert (g["size"], g["removed"]) == (o["size"], o["removed"]), s
+        assert sim.field.status_host().converged == 1
+    got = sim.parts.host_aos()
+    np.testing.assert_array_equal(got["p2c"], orc.p2c[:orc.size])
+    # The mixed push rounds E to FP32: a field difference at the CG tolerance can move f32(E)
+    # by one FP32 unit (6e-8 relative), so its positions agree to FP32 increments only.
+    _close(got["pos"], orc.pos[:orc.size], 1e-9 if precision == "f64" else 1e-6)
+    _close(sim.field.potential.cpu().numpy(), orc.potential, 1e-8)
+    ef = sim.mesh.ef.view(-1, 4)[:, :3].cpu().numpy()
+    _close(ef, hm_o.c_ef, 1e-7)
+    assert np.abs(hm_o.c_ef - hm.c_ef).max() > 1e-3  # the field did change from the static one
