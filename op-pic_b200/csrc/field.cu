@@ -83,6 +83,41 @@ __device__ __forceinline__ double shape_na(int a, int i, int j, int k) {
     return a == 0 ? ni : a == 1 ? nj : a == 2 ? nk : ((1 - ni) - nj) - nk;
 }
 
+// Row u of J v (K with its diagonal replaced by du) or, with kDiag false, of K v: four column
+// indices and values are loaded before their four vector gathers, so each thread keeps several
+// independent loads in flight; the terms are still added one by one in column order.  K is
+// read-only for the whole launch (non-coherent loads); v is not (plain loads: the vectors are
+// rewritten between grid barriers).
+template <bool kDiag>
+__device__ __forceinline__ double row_dot(const FieldArgs& a, int64_t u, double du, const double* v) {
+    int64_t k = __ldg(a.k_rowptr + u);
+    const int64_t end = __ldg(a.k_rowptr + u + 1);
+    double s = 0.0;
+    for (; k + 4 <= end; k += 4) {
+        const int32_t c0 = __ldg(a.k_col + k), c1 = __ldg(a.k_col + k + 1);
+        const int32_t c2 = __ldg(a.k_col + k + 2), c3 = __ldg(a.k_col + k + 3);
+        double v0 = __ldg(a.k_val + k), v1 = __ldg(a.k_val + k + 1);
+        double v2 = __ldg(a.k_val + k + 2), v3 = __ldg(a.k_val + k + 3);
+        const double p0 = v[c0], p1 = v[c1], p2 = v[c2], p3 = v[c3];
+        if (kDiag) {
+            v0 = c0 == u ? du : v0;
+            v1 = c1 == u ? du : v1;
+            v2 = c2 == u ? du : v2;
+            v3 = c3 == u ? du : v3;
+        }
+        s += v0 * p0;
+        s += v1 * p1;
+        s += v2 * p2;
+        s += v3 * p3;
+    }
+    for (; k < end; k++) {
+        const int32_t c = __ldg(a.k_col + k);
+        const double vk = (kDiag && c == u) ? du : __ldg(a.k_val + k);
+        s += vk * v[c];
+    }
+    return s;
+}
+
 __global__ void __launch_bounds__(kFieldBlock) field_newton_kernel(FieldArgs a) {
     cg::grid_group grid = cg::this_grid();
     __shared__ double sm[kWarps];
@@ -158,12 +193,7 @@ __global__ void __launch_bounds__(kFieldBlock) field_newton_kernel(FieldArgs a) 
     while (it < a.max_iter && sqrt(rr) > stop) {
         double pq = 0.0;
         for (int64_t u = tid; u < a.neq; u += nth) {  // q = J p
-            const double du = a.diag[u];
-            double s = 0.0;
-            for (int64_t k = a.k_rowptr[u]; k < a.k_rowptr[u + 1]; k++) {
-                const int32_t col = a.k_col[k];
-                s += (col == u ? du : a.k_val[k]) * a.p[col];
-            }
+            const double s = row_dot<true>(a, u, a.diag[u], a.p);
             a.q[u] = s;
             pq += a.p[u] * s;
         }
