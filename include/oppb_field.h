@@ -103,6 +103,27 @@ int oppb_field_solve(const oppb_field_device* f, const oppb_field_consts* c, con
 int oppb_electric_field(const int32_t* c2n, const double* c_sd, const double* node_potential, double* c_ef,
                         int32_t ef_stride, int32_t n_cells, void* stream);
 
+/* Element (c, k) of a per-cell array at base[c * cell_stride + k * comp_stride]: AoS arrays
+ * have (dim, 1), the opp_* runtime's device dats and maps (SoA) have (1, n_cells). */
+typedef struct oppb_cell_layout {
+    int64_t cell_stride;
+    int64_t comp_stride;
+} oppb_cell_layout;
+
+/* compute_electric_field_kernel with explicit layouts: c2n components = the 4 vertices,
+ * c_sd components = vertex * 3 + dimension, c_ef components = dimension.  accumulate = 1
+ * subtracts from c_ef as the generated loop's OPP_INC does (the caller resets c_ef first,
+ * as the generated main does); accumulate = 0 writes 0 - sum. */
+int oppb_electric_field_ex(const int32_t* c2n, oppb_cell_layout c2n_layout, const double* c_sd,
+                           oppb_cell_layout sd_layout, const double* node_potential, double* c_ef,
+                           oppb_cell_layout ef_layout, int32_t n_cells, int32_t accumulate, void* stream);
+
+/* Largest of init and the n values x[i] (|x[i]| when absolute = 1): the OPP_MAX global
+ * reduction of get_max_cef_kernel and get_final_max_values_kernel (apps/app_fempic/kernels.h:
+ * 205-223).  Synchronous: *result (host) holds the value on return.  The reduction word is
+ * fixed device scratch, so calls on one device must not overlap. */
+int oppb_reduce_max(const double* x, int64_t n, int32_t absolute, double init, double* result, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,8 +16,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <vector>
 
+#include "opp_fempic_solver.h"
 #include "opp_lib.h"
 #include "oppb_fempic.h"
 
@@ -28,6 +30,11 @@ void opp_particle_move__move_kernel(opp_set, opp_map, opp_map, opp_arg, opp_arg,
 void opp_par_loop_all__deposit_charge_on_nodes_kernel(opp_set, opp_arg, opp_arg, opp_arg, opp_arg, opp_arg);
 void opp_init_direct_hop_cg(double, const opp_dat, const opp::BoundingBox&, opp_map, opp_map, opp_arg, opp_arg,
                             opp_arg, opp_arg);
+void opp_par_loop_all__init_boundary_pot_kernel(opp_set, opp_arg, opp_arg);
+void opp_par_loop_all__compute_node_charge_density_kernel(opp_set, opp_arg, opp_arg);
+void opp_par_loop_all__compute_electric_field_kernel(opp_set, opp_arg, opp_arg, opp_arg, opp_arg, opp_arg, opp_arg);
+void opp_par_loop_all__get_max_cef_kernel(opp_set, opp_arg, opp_arg);
+void opp_par_loop_all__get_final_max_values_kernel(opp_set, opp_arg, opp_arg, opp_arg, opp_arg);
 
 namespace {
 
@@ -81,6 +88,12 @@ int main(int argc, char** argv) {
         Mesh m;
         CaseHeader h{};
         std::vector<double> tables, dh_par, n_pos;
+        // Field phase (an optional block tagged OPPBFLD1 at the end of the case file): node types,
+        // positions and volumes, CONST_wall_potential and CONST_spwt; plasma_den and
+        // electron_temperature come from the parameter file, as the reference's FESolver takes them.
+        bool field = false;
+        std::vector<int> f_type;
+        std::vector<double> f_pos, f_vol, f_par;
         if (argc >= 3) {
             std::FILE* f = std::fopen(argv[2], "rb");
             if (!f || std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, "OPPBCAS1", 8) != 0)
@@ -102,6 +115,14 @@ int main(int argc, char** argv) {
             if (h.direct_hop) {  // grid spacing, expansion[3], node positions [n_nodes][3]
                 read_into(f, dh_par, 4);
                 read_into(f, n_pos, (size_t)m.n_nodes * 3);
+            }
+            char tag[8];
+            if (std::fread(tag, 1, 8, f) == 8 && std::memcmp(tag, "OPPBFLD1", 8) == 0) {
+                field = true;
+                read_into(f, f_type, (size_t)m.n_nodes);
+                read_into(f, f_pos, (size_t)m.n_nodes * 3);
+                read_into(f, f_vol, (size_t)m.n_nodes);
+                read_into(f, f_par, 2);  // wall_potential, spwt
             }
             std::fclose(f);
         } else {
@@ -177,12 +198,33 @@ int main(int argc, char** argv) {
                                    opp_arg_dat(c_det, p2c_map, OPP_READ));
         }
 
+
         double one = 1.0, zero = 0.0;
-        opp_decl_const<OPP_REAL>(1, &zero, "CONST_spwt");
+        double spwt = field ? f_par[1] : 0.0, wall = field ? f_par[0] : 0.0;
+        opp_decl_const<OPP_REAL>(1, &spwt, "CONST_spwt");
+        opp_decl_const<OPP_REAL>(1, &wall, "CONST_wall_potential");
         opp_decl_const<OPP_REAL>(1, &h.ion_velocity, "CONST_ion_velocity");
         opp_decl_const<OPP_REAL>(1, &h.dt, "CONST_dt");
         opp_decl_const<OPP_REAL>(1, &one, "CONST_mass");
         opp_decl_const<OPP_REAL>(1, &h.qm, "CONST_charge");
+
+        // The reference main's field set-up (fempic_opp.cpp:101-110,139-141,155-156).
+        opp_dat n_type_d = nullptr, n_pos_f = nullptr, n_volume = nullptr, n_bnd_pot = nullptr, n_potential = nullptr;
+        opp_dat c_sd = nullptr;
+        std::unique_ptr<FESolver> field_solver;
+        std::vector<double> zeros_n((size_t)m.n_nodes, 0.0), zeros_sd((size_t)m.n_cells * 12, 0.0);
+        if (field) {
+            n_type_d = opp_decl_dat(node_set, 1, DT_INT, f_type.data(), "n_type");
+            n_pos_f = opp_decl_dat(node_set, 3, DT_REAL, f_pos.data(), "n_pos_field");
+            n_volume = opp_decl_dat(node_set, 1, DT_REAL, f_vol.data(), "n_vol");
+            n_bnd_pot = opp_decl_dat(node_set, 1, DT_REAL, zeros_n.data(), "n_bnd_pot");
+            n_potential = opp_decl_dat(node_set, 1, DT_REAL, zeros_n.data(), "n_potential");
+            c_sd = opp_decl_dat(cell_set, 12, DT_REAL, zeros_sd.data(), "c_shape_deri");
+            opp_par_loop_all__init_boundary_pot_kernel(node_set, opp_arg_dat(n_type_d, OPP_READ),
+                                                       opp_arg_dat(n_bnd_pot, OPP_WRITE));
+            field_solver = std::make_unique<FESolver>(c2n_map, n_type_d, n_pos_f, n_bnd_pot);
+            field_solver->enrich_cell_shape_deriv(c_sd);
+        }
 
         opp_increase_particle_count(dummy_part_set, h.inject);
         std::vector<StepRecord> recs;
@@ -232,6 +274,27 @@ int main(int argc, char** argv) {
                 opp_arg_dat(n_charge_den, 1, c2n_map, p2c_map, OPP_INC),
                 opp_arg_dat(n_charge_den, 2, c2n_map, p2c_map, OPP_INC),
                 opp_arg_dat(n_charge_den, 3, c2n_map, p2c_map, OPP_INC));
+            if (field) {  // fempic_opp.cpp:195-231
+                opp_par_loop_all__compute_node_charge_density_kernel(node_set, opp_arg_dat(n_charge_den, OPP_RW),
+                                                                     opp_arg_dat(n_volume, OPP_READ));
+                field_solver->compute_phi(opp_arg_dat(n_potential, OPP_WRITE), opp_arg_dat(n_charge_den, OPP_READ),
+                                          opp_arg_dat(n_bnd_pot, OPP_READ));
+                opp_reset_dat(c_ef, opp_zero_double16);
+                opp_par_loop_all__compute_electric_field_kernel(
+                    cell_set, opp_arg_dat(c_ef, OPP_INC), opp_arg_dat(c_sd, OPP_READ),
+                    opp_arg_dat(n_potential, 0, c2n_map, OPP_READ), opp_arg_dat(n_potential, 1, c2n_map, OPP_READ),
+                    opp_arg_dat(n_potential, 2, c2n_map, OPP_READ), opp_arg_dat(n_potential, 3, c2n_map, OPP_READ));
+                if (opp_params->get<OPP_BOOL>("print_final")) {
+                    double max_cef = 0.0, max_den = 0.0, max_pot = 0.0;
+                    opp_par_loop_all__get_max_cef_kernel(cell_set, opp_arg_dat(c_ef, OPP_READ),
+                                                         opp_arg_gbl(&max_cef, 1, "double", OPP_MAX));
+                    opp_par_loop_all__get_final_max_values_kernel(
+                        node_set, opp_arg_dat(n_charge_den, OPP_READ), opp_arg_gbl(&max_den, 1, "double", OPP_MAX),
+                        opp_arg_dat(n_potential, OPP_READ), opp_arg_gbl(&max_pot, 1, "double", OPP_MAX));
+                    opp_printf("Main", "ts: %d max_c_ef %2.15lE max_n_pot %2.15lE max_n_chg_den %2.15lE cg %d", s,
+                               max_cef, max_pot, max_den, field_solver->last_iterations());
+                }
+            }
             auto t4 = clk::now();
             r.size = particle_set->size;
             r.removed = r.size_before_move - r.size;

@@ -17,6 +17,8 @@
 
 #include <cooperative_groups.h>
 
+#include <cstring>
+
 #include "oppb_common.cuh"
 #include "oppb_field.h"
 
@@ -248,21 +250,53 @@ __global__ void __launch_bounds__(256) node_charge_density_kernel(double* den, c
     if (i < n) den[i] *= (spwt / vol[i]);
 }
 
-__global__ void __launch_bounds__(256) electric_field_kernel(const int32_t* c2n, const double* sd,
-                                                             const double* phi, double* ef, int32_t stride,
-                                                             int32_t n) {
+__global__ void __launch_bounds__(256) electric_field_kernel(const int32_t* c2n, oppb_cell_layout nl,
+                                                             const double* sd, oppb_cell_layout sl,
+                                                             const double* phi, double* ef, oppb_cell_layout el,
+                                                             int32_t n, int32_t accumulate) {
     const int64_t c = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (c >= n) return;
-    const int4 nd = ldg_i4(c2n + c * 4);
-    const double p0 = __ldg(phi + nd.x), p1 = __ldg(phi + nd.y), p2 = __ldg(phi + nd.z), p3 = __ldg(phi + nd.w);
-    const double* s = sd + c * 12;
+    double p[4];
+#pragma unroll
+    for (int v = 0; v < 4; v++) p[v] = __ldg(phi + __ldg(c2n + c * nl.cell_stride + v * nl.comp_stride));
+    const double* s = sd + c * sl.cell_stride;
 #pragma unroll
     for (int dim = 0; dim < 3; dim++) {
-        const double c1 = s[0 * 3 + dim] * p0;
-        const double c2 = s[1 * 3 + dim] * p1;
-        const double c3 = s[2 * 3 + dim] * p2;
-        const double c4 = s[3 * 3 + dim] * p3;
-        ef[c * stride + dim] = 0.0 - (c1 + c2 + c3 + c4);
+        const double c1 = __ldg(s + (0 * 3 + dim) * sl.comp_stride) * p[0];
+        const double c2 = __ldg(s + (1 * 3 + dim) * sl.comp_stride) * p[1];
+        const double c3 = __ldg(s + (2 * 3 + dim) * sl.comp_stride) * p[2];
+        const double c4 = __ldg(s + (3 * 3 + dim) * sl.comp_stride) * p[3];
+        double* e = ef + c * el.cell_stride + dim * el.comp_stride;
+        *e = (accumulate ? *e : 0.0) - (c1 + c2 + c3 + c4);
+    }
+}
+
+// Doubles mapped to 64-bit words whose unsigned order is the doubles' order (negative values
+// complemented, positive ones with the sign bit set), so atomicMax on the words is a max.
+__device__ __forceinline__ unsigned long long order_key(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ unsigned long long g_max_key;
+
+__global__ void __launch_bounds__(256) reduce_max_kernel(const double* x, int64_t n, int32_t absolute) {
+    __shared__ unsigned long long sm[8];
+    unsigned long long k = 0ull;  // below every key of a non-NaN double
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        const double v = absolute ? fabs(x[i]) : x[i];
+        const unsigned long long kv = order_key(v);
+        k = kv > k ? kv : k;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(kFullMask, k, o);
+        k = other > k ? other : k;
+    }
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = k;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; w++) k = sm[w] > k ? sm[w] : k;
+        atomicMax(&g_max_key, k);
     }
 }
 
@@ -297,14 +331,49 @@ extern "C" int oppb_node_charge_density(double* n_charge_den, const double* n_vo
     return oppb::launch_status();
 }
 
+extern "C" int oppb_electric_field_ex(const int32_t* c2n, oppb_cell_layout c2n_layout, const double* c_sd,
+                                      oppb_cell_layout sd_layout, const double* node_potential, double* c_ef,
+                                      oppb_cell_layout ef_layout, int32_t n_cells, int32_t accumulate,
+                                      void* stream) {
+    if (n_cells < 0 || (accumulate != 0 && accumulate != 1)) return OPPB_ERR_ARG;
+    if (n_cells == 0) return OPPB_OK;
+    if (!c2n || !c_sd || !node_potential || !c_ef) return OPPB_ERR_ARG;
+    oppb::electric_field_kernel<<<oppb::ceil_div(n_cells, 256), 256, 0, oppb::as_stream(stream)>>>(
+        c2n, c2n_layout, c_sd, sd_layout, node_potential, c_ef, ef_layout, n_cells, accumulate);
+    oppb::count_launches(1);
+    return oppb::launch_status();
+}
+
 extern "C" int oppb_electric_field(const int32_t* c2n, const double* c_sd, const double* node_potential,
                                    double* c_ef, int32_t ef_stride, int32_t n_cells, void* stream) {
-    if (n_cells < 0 || ef_stride < 3) return OPPB_ERR_ARG;
-    if (n_cells == 0) return OPPB_OK;
-    if (!c2n || !c_sd || !node_potential || !c_ef || !oppb::aligned(c2n, 16)) return OPPB_ERR_ARG;
-    oppb::electric_field_kernel<<<oppb::ceil_div(n_cells, 256), 256, 0, oppb::as_stream(stream)>>>(
-        c2n, c_sd, node_potential, c_ef, ef_stride, n_cells);
+    if (ef_stride < 3) return OPPB_ERR_ARG;
+    return oppb_electric_field_ex(c2n, oppb_cell_layout{4, 1}, c_sd, oppb_cell_layout{12, 1}, node_potential, c_ef,
+                                  oppb_cell_layout{ef_stride, 1}, n_cells, 0, stream);
+}
+
+extern "C" int oppb_reduce_max(const double* x, int64_t n, int32_t absolute, double init, double* result,
+                               void* stream) {
+    if (!result || n < 0 || (n > 0 && !x) || (absolute != 0 && absolute != 1)) return OPPB_ERR_ARG;
+    *result = init;
+    if (n == 0) return OPPB_OK;
+    cudaStream_t s = oppb::as_stream(stream);
+    unsigned long long* key = nullptr;
+    if (cudaGetSymbolAddress(reinterpret_cast<void**>(&key), oppb::g_max_key) != cudaSuccess ||
+        cudaMemsetAsync(key, 0, sizeof(unsigned long long), s) != cudaSuccess)
+        return OPPB_ERR_LAUNCH;
+    const int blocks = oppb::ceil_div(n, 256) < 148 * 8 ? oppb::ceil_div(n, 256) : 148 * 8;
+    oppb::reduce_max_kernel<<<blocks, 256, 0, s>>>(x, n, absolute);
     oppb::count_launches(1);
+    unsigned long long k = 0;
+    if (cudaMemcpyAsync(&k, key, sizeof k, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return OPPB_ERR_LAUNCH;
+    if (k != 0ull) {  // decode the largest key (0 = no value, n > 0 makes that impossible)
+        const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+        double v;
+        memcpy(&v, &b, sizeof v);
+        if (v > *result) *result = v;  // MAX(value, init) of the reference's kernels
+    }
     return oppb::launch_status();
 }
 

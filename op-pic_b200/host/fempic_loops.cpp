@@ -5,8 +5,12 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "opp_lib.h"
 #include "oppb_dh.h"
+#include "oppb_fempic.h"
+#include "oppb_field.h"
 
 namespace {
 
@@ -199,4 +203,82 @@ void opp_init_direct_hop_cg(double grid_spacing, const opp_dat c_gbl_id, const o
     if (cudaStreamSynchronize(oppb_rt::stream()) != cudaSuccess) opp_abort("direct-hop grid build");
     g_dh.on = true;
     opp_profiler->end("Setup_Mover");
+}
+
+// ------------------------------------------------------------ node and cell loops
+// The generated node- and cell-set loops of the FemPIC main (fempic_opp.cpp:40-48) around the
+// field solve.  Mesh dats and maps live on the device as SoA with stride = the set size.
+
+namespace {
+oppb_cell_layout soa(opp_set set) { return oppb_cell_layout{1, (int64_t)std::max(set->size, 1)}; }
+}  // namespace
+
+// init_boundary_pot_kernel (apps/app_fempic/kernels.h:48-60): FIXED nodes get
+// -CONST_wall_potential, every other node 0.  Runs on the host at set-up.
+void opp_par_loop_all__init_boundary_pot_kernel(opp_set set, opp_arg arg0, opp_arg arg1) {
+    opp_profiler->start("init_boundary_pot_kernel");
+    opp_download_dat(arg0.dat);
+    const int* type = reinterpret_cast<const int*>(arg0.dat->data);
+    double* pot = reinterpret_cast<double*>(arg1.dat->data);
+    const double wall = opp_get_const("CONST_wall_potential");
+    for (int n = 0; n < set->size; n++) pot[n] = (type[n] == OPPB_NODE_FIXED) ? -1 * wall : 0;
+    arg1.dat->dirty_hd = Device;  // the host copy is the newer one
+    arg1.dat->version++;
+    opp_profiler->end("init_boundary_pot_kernel");
+}
+
+// compute_node_charge_density_kernel: n_charge_den *= CONST_spwt / n_volume.
+void opp_par_loop_all__compute_node_charge_density_kernel(opp_set set, opp_arg arg0, opp_arg arg1) {
+    opp_profiler->start("compute_node_charge_density_kernel");
+    oppb_rt::sync_host_to_device(arg0.dat);
+    oppb_rt::sync_host_to_device(arg1.dat);
+    check(oppb_node_charge_density(reinterpret_cast<double*>(arg0.dat->data_d),
+                                   reinterpret_cast<const double*>(arg1.dat->data_d), opp_get_const("CONST_spwt"),
+                                   set->size, oppb_rt::stream()),
+          "oppb_node_charge_density");
+    oppb_rt::mark_device_written(arg0.dat);
+    opp_profiler->end("compute_node_charge_density_kernel");
+}
+
+// compute_electric_field_kernel: c_ef (OPP_INC) -= sum_i c_sd[i] * n_potential[c2n[i]].
+void opp_par_loop_all__compute_electric_field_kernel(opp_set set, opp_arg arg0, opp_arg arg1, opp_arg arg2,
+                                                     opp_arg arg3, opp_arg arg4, opp_arg arg5) {
+    opp_profiler->start("compute_electric_field_kernel");
+    (void)arg3, (void)arg4, (void)arg5;
+    opp_dat c_ef = arg0.dat, c_sd = arg1.dat, pot = arg2.dat;
+    if (!arg2.map || !arg2.map->map_d) opp_abort("compute_electric_field_kernel: c2n map has no device copy");
+    oppb_rt::sync_host_to_device(c_ef);
+    oppb_rt::sync_host_to_device(c_sd);
+    oppb_rt::sync_host_to_device(pot);
+    check(oppb_electric_field_ex(arg2.map->map_d, soa(set), reinterpret_cast<const double*>(c_sd->data_d), soa(set),
+                                 reinterpret_cast<const double*>(pot->data_d), reinterpret_cast<double*>(c_ef->data_d),
+                                 soa(set), set->size, 1, oppb_rt::stream()),
+          "oppb_electric_field_ex");
+    oppb_rt::mark_device_written(c_ef);
+    opp_profiler->end("compute_electric_field_kernel");
+}
+
+// get_max_cef_kernel: the OPP_MAX global of every component of c_ef.
+void opp_par_loop_all__get_max_cef_kernel(opp_set set, opp_arg arg0, opp_arg arg1) {
+    opp_dat c_ef = arg0.dat;
+    oppb_rt::sync_host_to_device(c_ef);
+    double* out = reinterpret_cast<double*>(arg1.data);
+    const int64_t stride = std::max(set->size, 1);
+    for (int d = 0; d < c_ef->dim; d++)
+        check(oppb_reduce_max(reinterpret_cast<const double*>(c_ef->data_d) + d * stride, set->size, 0, *out, out,
+                              oppb_rt::stream()),
+              "oppb_reduce_max");
+}
+
+// get_final_max_values_kernel: OPP_MAX of |n_charge_den| and of |n_potential|.
+void opp_par_loop_all__get_final_max_values_kernel(opp_set set, opp_arg arg0, opp_arg arg1, opp_arg arg2,
+                                                   opp_arg arg3) {
+    oppb_rt::sync_host_to_device(arg0.dat);
+    oppb_rt::sync_host_to_device(arg2.dat);
+    double* m0 = reinterpret_cast<double*>(arg1.data);
+    double* m1 = reinterpret_cast<double*>(arg3.data);
+    check(oppb_reduce_max(reinterpret_cast<const double*>(arg0.dat->data_d), set->size, 1, *m0, m0, oppb_rt::stream()),
+          "oppb_reduce_max");
+    check(oppb_reduce_max(reinterpret_cast<const double*>(arg2.dat->data_d), set->size, 1, *m1, m1, oppb_rt::stream()),
+          "oppb_reduce_max");
 }

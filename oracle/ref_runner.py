@@ -35,8 +35,11 @@ def fnv1a(a: np.ndarray) -> int:
 
 def write_case(path: Path, mesh, dist: np.ndarray, steps: int, tables: list[np.ndarray], dt: float = 0.01,
                qm: float = 1.0, ion_velocity: float = 1.0, sigma: float = 0.1, record_state: bool = True,
-               dh: tuple | None = None) -> None:
-    """dh = (grid_spacing, expansion[3]): a global-move case; the node positions follow."""
+               dh: tuple | None = None, field: tuple | None = None) -> None:
+    """dh = (grid_spacing, expansion[3]): a global-move case; the node positions follow.
+    field = (wall_potential, spwt): a block tagged OPPBFLD1 at the end with the node types,
+    positions and volumes, for the library's FemPIC app with its field phase (the reference
+    harness does not read it)."""
     inject = int(dist[-1])
     hdr = np.zeros(1, dtype=[("magic", "S8"), ("ints", "<i4", 8), ("dbl", "<f8", 4)])
     hdr["magic"] = b"OPPBCAS1"
@@ -56,14 +59,23 @@ def write_case(path: Path, mesh, dist: np.ndarray, steps: int, tables: list[np.n
             spacing, expansion = dh
             f.write(np.array([spacing, *expansion], "<f8").tobytes())
             f.write(np.ascontiguousarray(mesh.n_pos, dtype="<f8").tobytes())
+        if field is not None:
+            f.write(b"OPPBFLD1")
+            f.write(np.ascontiguousarray(mesh.n_type, dtype="<i4").tobytes())
+            f.write(np.ascontiguousarray(mesh.n_pos, dtype="<f8").tobytes())
+            f.write(np.ascontiguousarray(mesh.n_vol, dtype="<f8").tobytes())
+            f.write(np.array(field, "<f8").tobytes())
 
 
-def params_text(fill: str, period: int, alloc_mult: float, global_move: bool = False) -> str:
+def params_text(fill: str, period: int, alloc_mult: float, global_move: bool = False, print_final: bool = False,
+                extra: str = "") -> str:
+    """The opp_* parameter file of a run; extra: more `TYPE key = value` lines."""
     gm = "true" if global_move else "false"
+    pf = "true" if print_final else "false"
     return (f"STRING opp_fill = {fill}\nINT opp_fill_period = {period}\n"
             f"REAL opp_allocation_multiple = {alloc_mult}\nBOOL opp_profile_all = false\n"
             f"BOOL opp_global_move = {gm}\nBOOL opp_dh_data_generate = {gm}\n"
-            f"INT opp_threads_per_block = 256\nBOOL print_final = false\n")
+            f"INT opp_threads_per_block = 256\nBOOL print_final = {pf}\n" + extra)
 
 
 def run(kind: str, mesh, dist, steps: int, tables, fill: str = "HoleFill_All", period: int = 10,

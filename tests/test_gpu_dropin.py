@@ -76,3 +76,45 @@ def test_fempic_app_global_move_matches_reference_golden(tmp_path):
     np.testing.assert_array_equal(got["lc"].view(np.uint64), z["lc"].view(np.uint64))
     err = np.abs(got["node_charge"] - z["node_charge"]) / np.maximum(np.abs(z["node_charge"]), 1.0)
     assert err.max() <= 1e-12
+
+
+def test_fempic_app_field_phase_matches_oracle(tmp_path):
+    """The app with the reference main's field phase, through the opp_* API only:
+    init_boundary_pot, FESolver (set-up, enrich_cell_shape_deriv, compute_phi),
+    compute_node_charge_density, opp_reset_dat + compute_electric_field and the two OPP_MAX
+    logging loops, with the reference's physical constants, against the oracle running the
+    same phase (FemPIC's QE, EPS0, Kb; plasma_den 1e9, electron_temperature 1e6 K)."""
+    from oppb.fempic import HostMesh
+    from oracle import field as F
+
+    hm = HostMesh(10, 10, 40, 1.0, 1.0, 4.0)
+    hm_o = HostMesh(10, 10, 40, 1.0, 1.0, 4.0)  # the oracle rewrites its mesh's c_ef
+    inject, steps, dt, wall, spwt = 2000, 10, 0.05, 1.0, 2e5
+    n0, temp = 1e9, 1e6
+    dist = hm.inject_distribution(inject)
+    tables = [injection_randoms(31, s, inject, 0.1) for s in range(steps)]
+    R.write_case(tmp_path / "case.bin", hm, dist, steps, tables, dt=dt, field=(wall, spwt))
+    (tmp_path / "params.txt").write_text(R.params_text(
+        "HoleFill_All", 10, 2.0, print_final=True,
+        extra=f"REAL plasma_den = {n0}\nREAL electron_temperature = {temp}\n"))
+    r = subprocess.run([str(APP), str(tmp_path / "params.txt"), str(tmp_path / "case.bin"), str(tmp_path / "out.bin")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "max_c_ef" in r.stdout + r.stderr and "did not converge" not in r.stdout + r.stderr
+    got = R.read_output(tmp_path / "out.bin", hm.n_nodes)
+
+    bnd = np.where(hm_o.n_type == 3, -1.0 * wall, 0.0)  # init_boundary_pot_kernel
+    fs = F.FieldSystem(hm_o.n_pos, hm_o.n_type, bnd, hm_o.c2n)
+    consts = F.FieldConsts(n0=n0, phi0=0.0, kte=8.617333262e-5 * temp, qe=1.602e-19, eps0=8.8541878e-12,
+                           max_iter=10000)
+    o = O.OracleFemPIC(hm_o, dist, dt=dt, field=(fs, consts, spwt, hm_o.n_vol))
+    for s in range(steps):
+        out = o.step(tables[s])
+        rec = got["records"][s]
+        assert (int(rec["size"]), int(rec["removed"])) == (out["size"], out["removed"]), s
+    n = o.size
+    np.testing.assert_array_equal(got["p2c"], o.p2c[:n])
+    assert np.abs(got["pos"] - o.pos[:n]).max() <= 1e-9 * np.abs(o.pos[:n]).max()
+    den = got["node_charge"]  # n_charge_den after compute_node_charge_density
+    assert np.abs(den - o.node_charge).max() <= 1e-9 * np.abs(o.node_charge).max()
+    assert np.abs(hm_o.c_ef - hm.c_ef).max() > 1e-6 * np.abs(hm.c_ef).max()  # the field phase changed the field
