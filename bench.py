@@ -655,19 +655,14 @@ CAB_BYTES_PER_CELL = 384
 CAB_MEASURED_DRAM_BYTES_PER_PARTICLE = 122.0
 
 
-def run_cabana(dev, steps: int, warmup: int, cpu: bool, cpu_seconds: float) -> dict:
-    """move_deposit on the config-sized two-stream state: `warmup` untimed then `steps` timed
-    calls (c_acc zeroed + kernel each, as the reference main loop between field updates)."""
+def _cabana_leg(dev, mesh, deck, n, precision: str, steps: int, warmup: int):
+    """warmup untimed then steps timed move_deposit calls of one form; the device state is kept."""
     import torch
 
     from oppb import _lib as L
-    from oppb.cabana import CabanaDevice, Deck, HexMesh, synthetic_interp
+    from oppb.cabana import CabanaDevice, synthetic_interp
 
-    mesh = HexMesh(CAB["nx"], CAB["ny"], CAB["nz"])
-    deck = Deck(CAB["nx"], CAB["ny"], CAB["nz"], CAB["lx"], CAB["ly"], CAB["lz"], nppc=CAB["nppc"],
-                courant_frac=CAB["courant"])
-    n = len(mesh.interior) * CAB["nppc"]
-    cd = CabanaDevice(mesh, dev, n)
+    cd = CabanaDevice(mesh, dev, n, precision=precision)
     cd.set_interp(synthetic_interp(mesh, CAB["seed"]))
     cd.fill_two_stream(mesh, deck, CAB["v0"], CAB["sigma"], CAB["seed"])
     lib = L.load()
@@ -690,8 +685,23 @@ def run_cabana(dev, steps: int, warmup: int, cpu: bool, cpu_seconds: float) -> d
         t_ms.append(e0.elapsed_time(e1))
         visits += int(st.total_visits)
     torch.cuda.profiler.stop()
-    launches = lib.oppb_kernel_launches() - l0
-    t = sum(t_ms) / 1e3
+    return cd, sum(t_ms) / 1e3, visits, lib.oppb_kernel_launches() - l0
+
+
+def run_cabana(dev, steps: int, warmup: int, cpu: bool, cpu_seconds: float) -> dict:
+    """move_deposit on the config-sized two-stream state: `warmup` untimed then `steps` timed
+    calls (c_acc zeroed + kernel each, as the reference main loop between field updates), for
+    the FP64 form (bit-identical to the reference) and the FP32-momentum form (FP64 position,
+    FP32 momentum) from the same construction, with the second's departure from the first."""
+    import torch
+
+    from oppb.cabana import Deck, HexMesh
+
+    mesh = HexMesh(CAB["nx"], CAB["ny"], CAB["nz"])
+    deck = Deck(CAB["nx"], CAB["ny"], CAB["nz"], CAB["lx"], CAB["ly"], CAB["lz"], nppc=CAB["nppc"],
+                courant_frac=CAB["courant"])
+    n = len(mesh.interior) * CAB["nppc"]
+    cd, t, visits, launches = _cabana_leg(dev, mesh, deck, n, "f64", steps, warmup)
     bytes_call = CAB_BYTES_PER_PARTICLE * n + CAB_BYTES_PER_CELL * mesh.n_cells
     peaks = measured_peaks()
     out = {"workload": CAB_WORKLOAD, "metric": "particle-steps/s (move + current deposit)", "unit": UNIT,
@@ -702,7 +712,23 @@ def run_cabana(dev, steps: int, warmup: int, cpu: bool, cpu_seconds: float) -> d
                         "unit": "GB/s", "frac": bytes_call / (t / steps) / 1e9 / peaks["hbm_gbs"],
                         "bytes_per_launch": bytes_call, "traffic": CAB_MEASURED_DRAM_BYTES_PER_PARTICLE * n,
                         "traffic_source": TRAFFIC_SOURCE}}
-    del cd
+    cm, tm, _, _ = _cabana_leg(dev, mesh, deck, n, "mixed", steps, warmup)
+    # Departure of the FP32-momentum form from the FP64 form after the same calls.
+    u64, u32 = cd.vel[:, :n], cm.vel32[:, :n].double()
+    du = float((u32 - u64).abs().max() / u64.abs().max())
+    du_mean = float((u32 - u64).abs().mean() / u64.abs().mean())
+    dacc = float((cm.acc - cd.acc).abs().max() / cd.acc.abs().max())
+    cells = float((cm.p2c[:n] != cd.p2c[:n]).double().mean())
+    bytes_mixed = bytes_call - 24 * n + 80 * mesh.n_cells  # momentum 12 B read + 12 B written, f32 record read
+    out["fp32_momentum"] = {"what": "FP64 position, FP32 momentum (FP32 push from an FP32 field record); positions, "
+                                    "cells and current deposit in FP64",
+                            "value": n * steps / tm, "ms_per_step": 1e3 * tm / steps,
+                            "speedup_over_f64": t / tm,
+                            "vs_f64_after_steps": {"momentum_max_rel": du, "momentum_mean_rel": du_mean,
+                                                   "current_max_rel": dacc,
+                                                   "cells_differing": cells, "calls": warmup + steps},
+                            "roofline_frac": bytes_mixed / (tm / steps) / 1e9 / peaks["hbm_gbs"]}
+    del cd, cm
     torch.cuda.empty_cache()
     if cpu:
         out["cpu_baseline"] = cabana_cpu_baseline(cpu_seconds)

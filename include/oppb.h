@@ -126,7 +126,8 @@ typedef struct oppb_tuning {
     int32_t replicas;    /* node-sum copies the deposit spreads its atomics over (1..64, default 8) */
     int32_t advec_items; /* NESO-advection step: 256-particle work items per block pass, i.e.
                             particles per thread in flight (1, 2 or 4; default 2) */
-    int32_t reserved[5];
+    int32_t sort_gather_cols; /* cell sort: particle-dat columns gathered per launch (1..16, default 16) */
+    int32_t reserved[4];
 } oppb_tuning;
 
 /* Set / read the tuning used by subsequent launches (OPPB_ERR_ARG on unknown values). */

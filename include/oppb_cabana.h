@@ -25,11 +25,14 @@ extern "C" {
  *                              apps/app_cabanapic/cabana_defs.h:134-141), then 2 unused words
  *   interp [n_cells][20] f64 : c_interp, the 18 CellInterp values (cabana_defs.h:95-114),
  *                              then 2 unused doubles (160-B records)
+ *   interp32 [n_cells][20] f32 : the same values rounded to FP32, for the FP32-momentum form
+ *                              (may be NULL; 16-byte aligned)
  * Buffers are owned by the caller, 32-byte aligned. */
 typedef struct oppb_hex_mesh {
     int32_t  n_cells;
     int32_t* c2f;
     double*  interp;
+    float*   interp32;
 } oppb_hex_mesh;
 
 /* Particles, SoA [dim][stride]: p_pos (cell-local coordinates in [-1,1]^3), p_vel (momentum
@@ -71,6 +74,16 @@ int oppb_hex_mesh_pack(const oppb_hex_mesh* mesh, int32_t stride, const int32_t*
 int oppb_cabana_move_deposit(const oppb_hex_mesh* mesh, const oppb_cabana_particles* parts,
                              const oppb_cabana_consts* consts, double* acc, int32_t acc_stride,
                              oppb_move_status* status, int32_t max_hops, void* stream);
+
+/* The FP32-momentum form of the two-stream workload (FP64 position, FP32 momentum): as
+ * oppb_cabana_move_deposit, with p_vel held in FP32 in vel32 (SoA [3][stride], parts->vel
+ * unused) and the OPP_DO_ONCE Boris push computed in FP32 from mesh->interp32, in the FP64
+ * expression's order with correctly rounded divides and square roots.  The push's
+ * displacement returns to FP64: positions, the streak walk, cells and the 12-accumulator
+ * current deposit are FP64 as in the FP64 form. */
+int oppb_cabana_move_deposit_mixed(const oppb_hex_mesh* mesh, const oppb_cabana_particles* parts, float* vel32,
+                                   const oppb_cabana_consts* consts, double* acc, int32_t acc_stride,
+                                   oppb_move_status* status, int32_t max_hops, void* stream);
 
 #ifdef __cplusplus
 }

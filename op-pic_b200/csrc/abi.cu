@@ -7,7 +7,7 @@
 namespace oppb {
 namespace {
 std::atomic<uint64_t> g_launches{0};
-oppb_tuning g_tuning = {OPPB_DEPOSIT_WARP_ATOMIC, 8, 2, {0, 0, 0, 0, 0}};
+oppb_tuning g_tuning = {OPPB_DEPOSIT_WARP_ATOMIC, 8, 2, 16, {0, 0, 0, 0}};
 }  // namespace
 void count_launches(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 const oppb_tuning& tuning() { return g_tuning; }
@@ -19,6 +19,7 @@ extern "C" int oppb_set_tuning(const oppb_tuning* t) {
     if (!t || (t->deposit != OPPB_DEPOSIT_WARP_ATOMIC && t->deposit != OPPB_DEPOSIT_CTA_TABLE)) return OPPB_ERR_ARG;
     if (t->replicas < 1 || t->replicas > 64) return OPPB_ERR_ARG;
     if (t->advec_items != 1 && t->advec_items != 2 && t->advec_items != 4) return OPPB_ERR_ARG;
+    if (t->sort_gather_cols < 1 || t->sort_gather_cols > 16) return OPPB_ERR_ARG;
     oppb::g_tuning = *t;
     return OPPB_OK;
 }

@@ -27,6 +27,7 @@ struct HexArgs {
     int32_t n_cells;
     const int32_t* c2f;
     const double* interp;
+    const float* interp32;  // FP32-momentum form
 };
 
 struct CabParts {
@@ -34,6 +35,7 @@ struct CabParts {
     int32_t stride;
     double* pos;
     double* vel;
+    float* vel32;  // FP32-momentum form: p_vel in FP32
     double* streak;
     const double* weight;
     int32_t* p2c;
@@ -145,6 +147,84 @@ __device__ __forceinline__ bool push_once(const double* __restrict__ rec, double
     return false;
 }
 
+// The same OPP_DO_ONCE push with FP32 momentum (the FP32-momentum form of the two-stream
+// workload): u is stored and updated in FP32 from the cell's FP32 field record at the FP32
+// rounding of the position, in the FP64 expression's order with correctly rounded divides and
+// square roots; the displacement it produces returns to FP64 for the position, the face test
+// and the current deposit, as in push_once.
+__device__ __forceinline__ bool push_once_f32(const float* __restrict__ rec, float qdt_2mc, float cdx, float cdy,
+                                              float cdz, double q, double pos[3], float u[3], double s[3],
+                                              double* j) {
+    float r[20];
+    const float4* r4 = reinterpret_cast<const float4*>(rec);
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const float4 v = __ldg(r4 + k);
+        r[4 * k] = v.x;
+        r[4 * k + 1] = v.y;
+        r[4 * k + 2] = v.z;
+        r[4 * k + 3] = v.w;
+    }
+    const float ex = r[0], dexdy = r[1], dexdz = r[2], d2exdydz = r[3];
+    const float ey = r[4], deydz = r[5], deydx = r[6], d2eydzdx = r[7];
+    const float ez = r[8], dezdx = r[9], dezdy = r[10], d2ezdxdy = r[11];
+    float cbx = r[12], cby = r[14], cbz = r[16];
+    const float dcbxdx = r[13], dcbydy = r[15], dcbzdz = r[17];
+    const float dx = __double2float_rn(pos[0]), dy = __double2float_rn(pos[1]), dz = __double2float_rn(pos[2]);
+
+    const float hax = qdt_2mc * ((ex + dy * dexdy) + dz * (dexdz + dy * d2exdydz));
+    const float hay = qdt_2mc * ((ey + dz * deydz) + dx * (deydx + dz * d2eydzdx));
+    const float haz = qdt_2mc * ((ez + dx * dezdx) + dy * (dezdy + dx * d2ezdxdy));
+    cbx = cbx + dx * dcbxdx;
+    cby = cby + dy * dcbydy;
+    cbz = cbz + dz * dcbzdz;
+
+    float ux = u[0], uy = u[1], uz = u[2];
+    ux += hax;
+    uy += hay;
+    uz += haz;
+    float v0 = __fdiv_rn(qdt_2mc, __fsqrt_rn(1.0f + (ux * ux + (uy * uy + uz * uz))));
+    float v1 = cbx * cbx + (cby * cby + cbz * cbz);
+    float v2 = (v0 * v0) * v1;
+    const float v3 = v0 * (1.0f + v2 * ((1.0f / 3.0f) + v2 * (2.0f / 15.0f)));
+    float v4 = __fdiv_rn(v3, 1.0f + v1 * (v3 * v3));
+    v4 += v4;
+    v0 = ux + v3 * (uy * cbz - uz * cby);
+    v1 = uy + v3 * (uz * cbx - ux * cbz);
+    v2 = uz + v3 * (ux * cby - uy * cbx);
+    ux += v4 * (v1 * cbz - v2 * cby);
+    uy += v4 * (v2 * cbx - v0 * cbz);
+    uz += v4 * (v0 * cby - v1 * cbx);
+    ux += hax;
+    uy += hay;
+    uz += haz;
+    u[0] = ux;
+    u[1] = uy;
+    u[2] = uz;
+
+    v0 = __fdiv_rn(1.0f, __fsqrt_rn(1.0f + (ux * ux + (uy * uy + uz * uz))));
+    ux *= cdx;
+    uy *= cdy;
+    uz *= cdz;
+    ux *= v0;
+    uy *= v0;
+    uz *= v0;
+    const double sx = ux, sy = uy, sz = uz;  // the displacement, back in FP64
+    const double w0 = pos[0] + sx, w1 = pos[1] + sy, w2 = pos[2] + sz;
+    const double w3 = w0 + sx, w4 = w1 + sy, w5 = w2 + sz;
+    if (w3 <= 1.0 && w4 <= 1.0 && w5 <= 1.0 && -w3 <= 1.0 && -w4 <= 1.0 && -w5 <= 1.0) {
+        pos[0] = w3;
+        pos[1] = w4;
+        pos[2] = w5;
+        weight_current(j, q, sx, sy, sz, w0, w1, w2);
+        return true;
+    }
+    s[0] = sx;
+    s[1] = sy;
+    s[2] = sz;
+    return false;
+}
+
 // One streak segment (kernels.h:256-354): deposits into j, advances pos and s; returns the
 // crossed face (0..5, Face order) or -1 when the streak ends in this cell.
 __device__ __forceinline__ int streak_step(double q, double pos[3], double s[3], double* j) {
@@ -235,10 +315,16 @@ __device__ __forceinline__ void warp_deposit(WarpStage& ws, double* acc, int32_t
     }
 }
 
+// FP32 copies of the constants the FP32 push reads.
+struct ConstsF32 {
+    float qdt_2mc, cdx, cdy, cdz;
+};
+
+template <bool kF32Mom>
 __global__ void __launch_bounds__(kCabBlock) cabana_move_deposit_kernel(HexArgs m, CabParts p,
-                                                                        oppb_cabana_consts k, double* acc,
-                                                                        int32_t acc_stride, oppb_move_status* st,
-                                                                        int32_t max_hops) {
+                                                                        oppb_cabana_consts k, ConstsF32 kf,
+                                                                        double* acc, int32_t acc_stride,
+                                                                        oppb_move_status* st, int32_t max_hops) {
     __shared__ __align__(16) WarpStage stage[kCabWarps];
     const int64_t i = (int64_t)blockIdx.x * kCabBlock + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -252,13 +338,17 @@ __global__ void __launch_bounds__(kCabBlock) cabana_move_deposit_kernel(HexArgs 
         going = false;
     }
     double pos[3] = {0.0, 0.0, 0.0}, u[3] = {0.0, 0.0, 0.0}, s[3] = {0.0, 0.0, 0.0};
+    float uf[3] = {0.0f, 0.0f, 0.0f};
     double q = 0.0;
     const int64_t sd = p.stride;
     if (going) {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             pos[d] = ld_stream(p.pos + d * sd + i);
-            u[d] = ld_stream(p.vel + d * sd + i);
+            if (kF32Mom)
+                uf[d] = __ldcs(p.vel32 + d * sd + i);
+            else
+                u[d] = ld_stream(p.vel + d * sd + i);
         }
         q = __ldg(p.weight + i) * k.qsp;
     }
@@ -275,8 +365,12 @@ __global__ void __launch_bounds__(kCabBlock) cabana_move_deposit_kernel(HexArgs 
             // goes on, in the same call, with the first streak segment.
             bool stay = false;
             if (calls == 1) {
-                stay = push_once(m.interp + (int64_t)cell * 20, k.qdt_2mc, k.cdt_d[0], k.cdt_d[1], k.cdt_d[2], q,
-                                 pos, u, s, j);
+                if (kF32Mom)
+                    stay = push_once_f32(m.interp32 + (int64_t)cell * 20, kf.qdt_2mc, kf.cdx, kf.cdy, kf.cdz, q, pos,
+                                         uf, s, j);
+                else
+                    stay = push_once(m.interp + (int64_t)cell * 20, k.qdt_2mc, k.cdt_d[0], k.cdt_d[1], k.cdt_d[2],
+                                     q, pos, u, s, j);
                 streaking = !stay;
             }
             if (stay) {
@@ -314,7 +408,10 @@ __global__ void __launch_bounds__(kCabBlock) cabana_move_deposit_kernel(HexArgs 
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             st_stream(p.pos + d * sd + i, pos[d]);
-            st_stream(p.vel + d * sd + i, u[d]);
+            if (kF32Mom)
+                __stcs(p.vel32 + d * sd + i, uf[d]);
+            else
+                st_stream(p.vel + d * sd + i, u[d]);
             if (streaking) st_stream(p.streak + d * sd + i, s[d]);
         }
         if (cell != cell0) st_stream(p.p2c + i, cell);
@@ -330,7 +427,8 @@ __global__ void __launch_bounds__(kCabBlock) cabana_move_deposit_kernel(HexArgs 
 
 // c2ngc SoA [6][stride] -> c2f [n][8]; c_interp SoA [18][stride] -> interp [n][20].
 __global__ void __launch_bounds__(256) hex_pack_kernel(int32_t n_cells, int32_t stride, const int32_t* c2ngc,
-                                                       const double* c_interp, int32_t* c2f, double* interp) {
+                                                       const double* c_interp, int32_t* c2f, double* interp,
+                                                       float* interp32) {
     const int64_t c = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (c >= n_cells) return;
     if (c2ngc) {
@@ -350,6 +448,13 @@ __global__ void __launch_bounds__(256) hex_pack_kernel(int32_t n_cells, int32_t 
         double2* o = reinterpret_cast<double2*>(interp + c * 20);
 #pragma unroll
         for (int k = 0; k < 10; k++) o[k] = make_double2(r[2 * k], r[2 * k + 1]);
+        if (interp32) {  // the FP32-momentum form's record: the same 20 values rounded to FP32
+            float4* o32 = reinterpret_cast<float4*>(interp32 + c * 20);
+#pragma unroll
+            for (int k = 0; k < 5; k++)
+                o32[k] = make_float4(__double2float_rn(r[4 * k]), __double2float_rn(r[4 * k + 1]),
+                                     __double2float_rn(r[4 * k + 2]), __double2float_rn(r[4 * k + 3]));
+        }
     }
 }
 
@@ -362,31 +467,54 @@ extern "C" int oppb_hex_mesh_pack(const oppb_hex_mesh* mesh, int32_t stride, con
     if (!mesh || mesh->n_cells <= 0 || stride < mesh->n_cells) return OPPB_ERR_ARG;
     if (c2ngc && (!mesh->c2f || !aligned(mesh->c2f, 32))) return OPPB_ERR_ARG;
     if (c_interp && (!mesh->interp || !aligned(mesh->interp, 32))) return OPPB_ERR_ARG;
+    if (mesh->interp32 && !aligned(mesh->interp32, 16)) return OPPB_ERR_ARG;
     if (!c2ngc && !c_interp) return OPPB_OK;
-    hex_pack_kernel<<<ceil_div(mesh->n_cells, 256), 256, 0, as_stream(stream)>>>(mesh->n_cells, stride, c2ngc,
-                                                                                 c_interp, mesh->c2f, mesh->interp);
+    hex_pack_kernel<<<ceil_div(mesh->n_cells, 256), 256, 0, as_stream(stream)>>>(
+        mesh->n_cells, stride, c2ngc, c_interp, mesh->c2f, mesh->interp, mesh->interp32);
     count_launches(1);
     return launch_status();
 }
 
-extern "C" int oppb_cabana_move_deposit(const oppb_hex_mesh* mesh, const oppb_cabana_particles* parts,
-                                        const oppb_cabana_consts* consts, double* acc, int32_t acc_stride,
-                                        oppb_move_status* status, int32_t max_hops, void* stream) {
-    using namespace oppb;
+namespace oppb {
+namespace {
+template <bool kF32Mom>
+int launch_cabana(const oppb_hex_mesh* mesh, const oppb_cabana_particles* parts, float* vel32,
+                  const oppb_cabana_consts* consts, double* acc, int32_t acc_stride, oppb_move_status* status,
+                  int32_t max_hops, void* stream) {
     if (!mesh || mesh->n_cells <= 0 || !mesh->c2f || !mesh->interp || !aligned(mesh->c2f, 32) ||
         !aligned(mesh->interp, 32))
         return OPPB_ERR_ARG;
+    if (kF32Mom && (!mesh->interp32 || !aligned(mesh->interp32, 16) || !vel32)) return OPPB_ERR_ARG;
     if (!parts || parts->size < 0 || parts->stride < parts->size) return OPPB_ERR_ARG;
-    if (!parts->pos || !parts->vel || !parts->streak_mid || !parts->weight || !parts->p2c) return OPPB_ERR_ARG;
+    if (!parts->pos || (!kF32Mom && !parts->vel) || !parts->streak_mid || !parts->weight || !parts->p2c)
+        return OPPB_ERR_ARG;
     if (!consts || !acc || acc_stride < mesh->n_cells || !status || max_hops <= 0) return OPPB_ERR_ARG;
     cudaStream_t s = as_stream(stream);
     if (cudaMemsetAsync(status, 0, sizeof(oppb_move_status), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
     if (parts->size == 0) return launch_status();
-    const HexArgs m{mesh->n_cells, mesh->c2f, mesh->interp};
-    const CabParts p{parts->size, parts->stride, parts->pos, parts->vel, parts->streak_mid, parts->weight,
+    const HexArgs m{mesh->n_cells, mesh->c2f, mesh->interp, mesh->interp32};
+    const CabParts p{parts->size, parts->stride, parts->pos, parts->vel, vel32, parts->streak_mid, parts->weight,
                      parts->p2c};
-    cabana_move_deposit_kernel<<<ceil_div(parts->size, kCabBlock), kCabBlock, 0, s>>>(m, p, *consts, acc,
-                                                                                      acc_stride, status, max_hops);
+    // FP32 constants: the round-to-nearest FP32 values of the FP64 ones.
+    const ConstsF32 kf{(float)consts->qdt_2mc, (float)consts->cdt_d[0], (float)consts->cdt_d[1],
+                       (float)consts->cdt_d[2]};
+    cabana_move_deposit_kernel<kF32Mom><<<ceil_div(parts->size, kCabBlock), kCabBlock, 0, s>>>(
+        m, p, *consts, kf, acc, acc_stride, status, max_hops);
     count_launches(1);
     return launch_status();
+}
+}  // namespace
+}  // namespace oppb
+
+extern "C" int oppb_cabana_move_deposit(const oppb_hex_mesh* mesh, const oppb_cabana_particles* parts,
+                                        const oppb_cabana_consts* consts, double* acc, int32_t acc_stride,
+                                        oppb_move_status* status, int32_t max_hops, void* stream) {
+    return oppb::launch_cabana<false>(mesh, parts, nullptr, consts, acc, acc_stride, status, max_hops, stream);
+}
+
+extern "C" int oppb_cabana_move_deposit_mixed(const oppb_hex_mesh* mesh, const oppb_cabana_particles* parts,
+                                              float* vel32, const oppb_cabana_consts* consts, double* acc,
+                                              int32_t acc_stride, oppb_move_status* status, int32_t max_hops,
+                                              void* stream) {
+    return oppb::launch_cabana<true>(mesh, parts, vel32, consts, acc, acc_stride, status, max_hops, stream);
 }

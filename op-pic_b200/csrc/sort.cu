@@ -249,6 +249,7 @@ extern "C" int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride, 
         in = PassIn{nullptr, keys[p & 1], vals[p & 1]};
     }
     GatherCols g{};
+    const int group = tuning().sort_gather_cols < kMaxCols ? tuning().sort_gather_cols : kMaxCols;
     for (int d = 0; d < n_dats; d++) {
         if (d == key_dat) continue;
         for (int c = 0; c < dats[d].dim; c++) {
@@ -256,7 +257,7 @@ extern "C" int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride, 
             g.src[g.n] = static_cast<const char*>(dats[d].data) + off;
             g.dst[g.n] = static_cast<char*>(dats[d].swap) + off;
             g.bytes[g.n] = dats[d].elem_bytes;
-            if (++g.n == kMaxCols) {
+            if (++g.n == group) {
                 gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(size, perm, g);
                 count_launches(1);
                 g.n = 0;

@@ -46,7 +46,8 @@ class Dat(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("advec_items", c_i32), ("reserved", c_i32 * 5)]
+    _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("advec_items", c_i32), ("sort_gather_cols", c_i32),
+                ("reserved", c_i32 * 4)]
 
 
 DEPOSIT_WARP_ATOMIC = 0
@@ -58,7 +59,7 @@ class Inlet(C.Structure):
 
 
 class HexMesh(C.Structure):
-    _fields_ = [("n_cells", c_i32), ("c2f", c_vp), ("interp", c_vp)]
+    _fields_ = [("n_cells", c_i32), ("c2f", c_vp), ("interp", c_vp), ("interp32", c_vp)]
 
 
 class CabanaParticles(C.Structure):
@@ -159,6 +160,8 @@ _SIGS = {
     "oppb_hex_mesh_pack": (C.c_int, [P(HexMesh), c_i32, c_vp, c_vp, c_vp]),
     "oppb_cabana_move_deposit": (C.c_int, [P(HexMesh), P(CabanaParticles), P(CabanaConsts), c_vp, c_i32, c_vp,
                                            c_i32, c_vp]),
+    "oppb_cabana_move_deposit_mixed": (C.c_int, [P(HexMesh), P(CabanaParticles), c_vp, P(CabanaConsts), c_vp, c_i32,
+                                                 c_vp, c_i32, c_vp]),
     "oppb_advec_pack_cells": (C.c_int, [c_vp, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp]),
     "oppb_advec_step": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
     "oppb_advec_update_pos": (C.c_int, [P(AdvecBatch), c_vp]),
@@ -210,7 +213,8 @@ def check(fn: str, status: int) -> None:
         raise OppbError(fn, status)
 
 
-def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_items: int | None = None) -> None:
+def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_items: int | None = None,
+               sort_gather_cols: int | None = None) -> None:
     t = Tuning()
     load().oppb_get_tuning(C.byref(t))
     if deposit is not None:
@@ -219,6 +223,8 @@ def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_it
         t.replicas = replicas
     if advec_items is not None:
         t.advec_items = advec_items
+    if sort_gather_cols is not None:
+        t.sort_gather_cols = sort_gather_cols
     check("oppb_set_tuning", load().oppb_set_tuning(C.byref(t)))
 
 

@@ -121,9 +121,16 @@ def _ptr(t) -> int:
 
 class CabanaDevice:
     """Device state of the particle path: packed mesh, particle dats SoA [dim][capacity],
-    c_acc SoA [12][n_cells], move status.  There is no CPU fallback."""
+    c_acc SoA [12][n_cells], move status.  There is no CPU fallback.
 
-    def __init__(self, mesh: HexMesh, device, capacity: int):
+    precision 'f64' is the reference's form (bit-identical to the seq backend); 'mixed' holds
+    the momentum in FP32 (vel32) and pushes it in FP32 (oppb_cabana_move_deposit_mixed), with
+    FP64 positions, cells and current deposit."""
+
+    def __init__(self, mesh: HexMesh, device, capacity: int, precision: str = "f64"):
+        if precision not in ("f64", "mixed"):
+            raise ValueError(precision)
+        self.precision = precision
         if not torch.cuda.is_available():
             raise RuntimeError("CabanaDevice needs a CUDA device (there is no CPU fallback)")
         self.device = torch.device(device)
@@ -132,12 +139,15 @@ class CabanaDevice:
         self.n_cells = nc
         self.c2f = torch.zeros(nc * 8, dtype=torch.int32, device=self.device)
         self.interp = torch.zeros(nc * 20, dtype=torch.float64, device=self.device)
-        self.mesh = L.HexMesh(nc, _ptr(self.c2f), _ptr(self.interp))
+        self.interp32 = torch.zeros(nc * 20, dtype=torch.float32, device=self.device) if precision == "mixed" else None
+        self.mesh = L.HexMesh(nc, _ptr(self.c2f), _ptr(self.interp), _ptr(self.interp32))
         self.acc = torch.zeros((12, nc), dtype=torch.float64, device=self.device)
         self.capacity = max(capacity, 1)
         cap = self.capacity
         self.pos = torch.zeros((3, cap), dtype=torch.float64, device=self.device)
-        self.vel = torch.zeros((3, cap), dtype=torch.float64, device=self.device)
+        # p_vel: FP64 in the reference's form; FP32 in the mixed form (vel32; vel unused there)
+        self.vel = torch.zeros((3, cap if precision == "f64" else 1), dtype=torch.float64, device=self.device)
+        self.vel32 = torch.zeros((3, cap), dtype=torch.float32, device=self.device) if precision == "mixed" else None
         self.streak = torch.zeros((3, cap), dtype=torch.float64, device=self.device)
         self.weight = torch.zeros(cap, dtype=torch.float64, device=self.device)
         self.p2c = torch.zeros(cap, dtype=torch.int32, device=self.device)
@@ -157,8 +167,10 @@ class CabanaDevice:
         if n > self.capacity:
             raise ValueError("capacity exceeded")
         self.size = n
-        for name, a in (("pos", pos), ("vel", vel), ("streak", streak)):
-            getattr(self, name)[:, :n] = torch.from_numpy(np.ascontiguousarray(a.T)).to(self.device)
+        vel_name = "vel" if self.precision == "f64" else "vel32"
+        for name, a in (("pos", pos), (vel_name, vel), ("streak", streak)):
+            t = getattr(self, name)
+            t[:, :n] = torch.from_numpy(np.ascontiguousarray(a.T)).to(device=self.device, dtype=t.dtype)
         self.weight[:n] = torch.from_numpy(np.ascontiguousarray(weight)).to(self.device)
         self.p2c[:n] = torch.from_numpy(np.ascontiguousarray(p2c, dtype=np.int32)).to(self.device)
 
@@ -173,11 +185,16 @@ class CabanaDevice:
         g = torch.Generator(device=self.device)
         g.manual_seed(seed)
         self.pos[:, :n].uniform_(-1.0, 1.0, generator=g)
-        self.vel[:, :n].normal_(0.0, sigma, generator=g)
+        u = torch.empty((3, n), dtype=torch.float64, device=self.device)
+        u.normal_(0.0, sigma, generator=g)
         drift = v0 / math.sqrt(1.0 - v0 * v0)
-        pairs = self.vel[2, :n].view(-1, 2)
+        pairs = u[2].view(-1, 2)
         pairs[:, 0] += drift
         pairs[:, 1] -= drift
+        if self.precision == "f64":
+            self.vel[:, :n] = u
+        else:
+            self.vel32[:, :n] = u.to(torch.float32)  # the same draw, rounded to FP32
         self.streak[:, :n].zero_()
         self.weight[:n] = deck.we
         cells = torch.from_numpy(mesh.interior).to(self.device)
@@ -194,6 +211,12 @@ class CabanaDevice:
         v = self.view()
         k = deck.consts()
         sp = None if stream is None else stream.cuda_stream
+        if self.precision == "mixed":
+            L.check("oppb_cabana_move_deposit_mixed",
+                    self.lib.oppb_cabana_move_deposit_mixed(C.byref(self.mesh), C.byref(v), _ptr(self.vel32),
+                                                            C.byref(k), _ptr(self.acc), self.n_cells,
+                                                            _ptr(self.status), max_hops, sp))
+            return
         L.check("oppb_cabana_move_deposit",
                 self.lib.oppb_cabana_move_deposit(C.byref(self.mesh), C.byref(v), C.byref(k), _ptr(self.acc),
                                                   self.n_cells, _ptr(self.status), max_hops, sp))
@@ -203,6 +226,7 @@ class CabanaDevice:
 
     def host(self) -> dict:
         n = self.size
-        return {"pos": self.pos[:, :n].T.contiguous().cpu().numpy(), "vel": self.vel[:, :n].T.contiguous().cpu().numpy(),
+        vel = self.vel if self.precision == "f64" else self.vel32
+        return {"pos": self.pos[:, :n].T.contiguous().cpu().numpy(), "vel": vel[:, :n].T.contiguous().cpu().numpy(),
                 "streak": self.streak[:, :n].T.contiguous().cpu().numpy(), "p2c": self.p2c[:n].cpu().numpy(),
                 "acc": self.acc.T.contiguous().cpu().numpy()}

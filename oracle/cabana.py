@@ -18,6 +18,8 @@ def _lib() -> C.CDLL:
         lib.oracle_cabana_move_deposit.restype = C.c_int
         lib.oracle_cabana_move_deposit.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp,
                                                    C.c_double, i32, C.POINTER(C.c_int64)]
+        lib.oracle_cabana_move_deposit_mixed.restype = C.c_int
+        lib.oracle_cabana_move_deposit_mixed.argtypes = lib.oracle_cabana_move_deposit.argtypes
         lib._cabana_bound = True
     return lib
 
@@ -36,6 +38,19 @@ def move_deposit(pos, vel, streak, weight, p2c, c2ngc, interp, acc, qdt_2mc, cdt
     visits = C.c_int64(0)
     rc = _lib().oracle_cabana_move_deposit(n, _p(pos), _p(vel), _p(streak), _p(weight), _p(p2c), _p(c2ngc),
                                            _p(interp), _p(acc), qdt_2mc, _p(cd), qsp, max_hops, C.byref(visits))
+    if rc != 0:
+        raise RuntimeError("oracle: a particle exceeded max_hops")
+    return int(visits.value)
+
+
+def move_deposit_mixed(pos, vel32, streak, weight, p2c, c2ngc, interp, acc, qdt_2mc, cdt_d, qsp, max_hops=1 << 20):
+    """The FP32-momentum form (oracle_cabana_move_deposit_mixed): as move_deposit with vel32
+    [n,3] FP32.  Returns the number of kernel calls."""
+    n = len(p2c)
+    cd = np.ascontiguousarray(cdt_d, dtype=np.float64)
+    visits = C.c_int64(0)
+    rc = _lib().oracle_cabana_move_deposit_mixed(n, _p(pos), _p(vel32), _p(streak), _p(weight), _p(p2c), _p(c2ngc),
+                                                 _p(interp), _p(acc), qdt_2mc, _p(cd), qsp, max_hops, C.byref(visits))
     if rc != 0:
         raise RuntimeError("oracle: a particle exceeded max_hops")
     return int(visits.value)

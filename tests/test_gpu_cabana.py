@@ -41,8 +41,8 @@ def _acc_close(got, ref):
     assert err <= CUR_RTOL, f"accumulator max err {err:.2e} of max |acc|"
 
 
-def _run_gpu(mesh, interp, pos, vel, streak, w, p2c, k, calls=1, max_hops=4096):
-    dev = CabanaDevice(mesh, DEV, len(p2c))
+def _run_gpu(mesh, interp, pos, vel, streak, w, p2c, k, calls=1, max_hops=4096, precision="f64"):
+    dev = CabanaDevice(mesh, DEV, len(p2c), precision=precision)
     dev.set_interp(interp)
     dev.set_particles(pos, vel, streak, w, p2c)
     for _ in range(calls):
@@ -51,13 +51,15 @@ def _run_gpu(mesh, interp, pos, vel, streak, w, p2c, k, calls=1, max_hops=4096):
     return dev.host(), dev.status_host()
 
 
-def _run_oracle(mesh, interp, pos, vel, streak, w, p2c, k, calls=1):
-    a = {"pos": pos.copy(), "vel": vel.copy(), "streak": streak.copy(), "p2c": p2c.copy()}
+def _run_oracle(mesh, interp, pos, vel, streak, w, p2c, k, calls=1, precision="f64"):
+    a = {"pos": pos.copy(), "vel": vel.astype(np.float32 if precision == "mixed" else np.float64),
+         "streak": streak.copy(), "p2c": p2c.copy()}
+    fn = OC.move_deposit_mixed if precision == "mixed" else OC.move_deposit
     visits = 0
     for _ in range(calls):
         acc = np.zeros((mesh.n_cells, 12))
-        visits = OC.move_deposit(a["pos"], a["vel"], a["streak"], w, a["p2c"], mesh.c2ngc, interp, acc, k.qdt_2mc,
-                                 np.array(k.cdt_d), k.qsp)
+        visits = fn(a["pos"], a["vel"], a["streak"], w, a["p2c"], mesh.c2ngc, interp, acc, k.qdt_2mc,
+                    np.array(k.cdt_d), k.qsp)
     a["acc"] = acc
     return a, visits
 
@@ -127,3 +129,52 @@ def test_errors_reported():
     _, st = _run_gpu(mesh, interp, np.zeros((1, 3)), vel2, np.zeros((1, 3)), np.ones(1),
                      np.array([mesh.interior[0]], np.int32), _K(-0.2, (3.0, 3.0, 3.0), -1.0), max_hops=2)
     assert st.error == L.OPPB_ERR_HOP_LIMIT and st.error_index == 0
+
+
+# ---------------------------------------------------------------- FP32-momentum form
+
+@pytest.mark.parametrize("n,seed,scale", [(1, 0, 2.0), (5000, 2, 0.5), (200_003, 3, 2.5)])
+def test_mixed_matches_oracle_random(n, seed, scale):
+    """FP32 momentum: bit-exact against the oracle running the same FP32 push (positions,
+    FP32 momenta, streaks, cells, call counts); accumulators within CUR_RTOL."""
+    mesh = HexMesh(6, 5, 7)
+    rng = np.random.default_rng(seed)
+    interp = synthetic_interp(mesh, seed + 100, e_scale=0.3, b_scale=0.4)
+    p2c = np.sort(rng.choice(mesh.interior, n)).astype(np.int32)
+    pos = rng.uniform(-1, 1, (n, 3))
+    vel = rng.normal(0, scale, (n, 3)).astype(np.float32)
+    if n > 200:
+        pos[:60, 1] = 1.0
+        vel[60:120, 0] = 0.0
+    w = rng.uniform(0.1, 2.0, n)
+    k = _K(-0.27, (1.4, 0.8, 2.2), -1.0)
+    streak = np.zeros((n, 3))
+    got, st = _run_gpu(mesh, interp, pos, vel, streak, w, p2c, k, precision="mixed")
+    ref, visits = _run_oracle(mesh, interp, pos, vel, streak, w, p2c, k, precision="mixed")
+    assert st.error == 0 and int(st.total_visits) == visits
+    assert got["vel"].dtype == np.float32
+    for name in ("pos", "vel", "streak", "p2c"):
+        _bits_equal(got[name], ref[name], name)
+    _acc_close(got["acc"], ref["acc"])
+
+
+def test_mixed_two_stream_steps_match_oracle_and_track_fp64():
+    """The workload's construction, five calls: the FP32-momentum form equals its oracle bit for
+    bit and stays close to the FP64 reference form started from the same (FP32-rounded)
+    momenta: momenta within 1e-5 of the largest, currents within 1e-4 of the largest, and all
+    but a few cells the same."""
+    mesh = HexMesh(4, 4, 16)
+    deck = Deck(4, 4, 16, 1.0, 1.0, 4.0, nppc=64, courant_frac=0.5)
+    pos, vel, streak, w, p2c = two_stream(mesh, deck, 0.2, 0.01, seed=5)
+    vel32 = vel.astype(np.float32)
+    interp = synthetic_interp(mesh, 6)
+    got, st = _run_gpu(mesh, interp, pos, vel32, streak, w, p2c, deck, calls=5, precision="mixed")
+    ref, visits = _run_oracle(mesh, interp, pos, vel32, streak, w, p2c, deck, calls=5, precision="mixed")
+    assert st.error == 0 and int(st.total_visits) == visits
+    for name in ("pos", "vel", "streak", "p2c"):
+        _bits_equal(got[name], ref[name], name)
+    _acc_close(got["acc"], ref["acc"])
+    f64, _ = _run_oracle(mesh, interp, pos, vel32.astype(np.float64), streak, w, p2c, deck, calls=5)
+    assert np.abs(got["vel"] - f64["vel"]).max() <= 1e-5 * np.abs(f64["vel"]).max()
+    assert np.abs(got["acc"] - f64["acc"]).max() <= 1e-4 * np.abs(f64["acc"]).max()
+    assert (got["p2c"] != f64["p2c"]).mean() <= 1e-3
