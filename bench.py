@@ -133,6 +133,11 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     log(f"[{precision}] fill {CFG['fill_steps']} steps in {time.time() - t0:.1f}s, size {sim.parts.size}")
     for _ in range(warmup):
         sim.step(device_randoms(rnd_buf))
+    # Launch choices (deposit strategy, node-sum copies, sort gather columns) timed on this
+    # state before the timed steps; the state is restored after each trial.
+    from oppb.autotune import tune_move, tune_sort
+    tuned = {"move": tune_move(sim, with_push=False).report(), "sort": tune_sort(sim).report()}
+    log(f"[{precision}] autotune move {tuned['move']['choice']} sort cols {tuned['sort']['choice']}")
     # Inputs of the timed steps generated before timing (device-resident).
     tables = [device_randoms(torch.empty_like(rnd_buf)) for _ in range(min(steps, 16))]
     torch.cuda.synchronize()
@@ -194,6 +199,7 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
         "sorts": sum(1 for r in rec if r[2] == "sort"),
         "launches": int(launches),
         "clocks": clocks,
+        "autotune": tuned,
     }
     # Roofline of the move(+deposit) kernel: algorithmic bytes / mean launch time.
     bytes_per_launch = [BYTES_PER_PARTICLE * r[0] + BYTES_PER_CELL[precision] * hm.n_cells
@@ -410,6 +416,9 @@ def arm_ours(args) -> dict:
                            "f64_unfused": f64["push_inclusive"], "f64_fused": f64["push_inclusive_fused"],
                            "fused_steps": mixed["fused_steps"]},
         "mixed_over_plain": mixed["job_value"] / f64["job_value"],
+        "autotune": {"what": "move launch (deposit strategy, node-sum copies) and sort gather columns, "
+                             "median of 3 timed trials on the warmed-up state",
+                     "f64": f64["autotune"], "mixed": mixed["autotune"]},
         "roofline": {"bound": "hbm", "kernel": "move_mixed_kernel (move + fused deposit)",
                      "achieved": mixed["move_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": mixed["move_gbs"] / peaks["hbm_gbs"], "peak_source": peaks["source"],

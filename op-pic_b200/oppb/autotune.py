@@ -1,0 +1,120 @@
+"""The launch choices of the FemPIC path, picked by timing them on the live state.
+
+The move + deposit launch has two choices (oppb_tuning): the deposit strategy (warp-matched
+FP64 atomics, or a per-CTA shared-memory node table) and how many node-sum copies the atomics
+are spread over; the cell sort has one (particle-dat columns gathered per launch).  tune_move
+and tune_sort time every candidate on the simulation's current particle state, restoring a
+snapshot of the particle dats before each trial so that every candidate sees the same input,
+then keep the fastest as the process-wide tuning.  The choice of a trial is the median of
+its repetitions.  The sort interval is not tuned: it is the reference's Sort_Periodic period,
+which fixes the particle order the results are compared in.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import statistics
+from dataclasses import dataclass, field
+from typing import Callable
+
+import torch
+
+from oppb import _lib as L
+
+MOVE_CANDIDATES = [(dep, rep) for dep in (L.DEPOSIT_WARP_ATOMIC, L.DEPOSIT_CTA_TABLE) for rep in (1, 4, 8, 16)]
+SORT_CANDIDATES = [16, 10, 5]
+
+
+@dataclass
+class TuneResult:
+    choice: object
+    times_ms: dict = field(default_factory=dict)
+
+    def report(self) -> dict:
+        return {"choice": str(self.choice), "ms": {str(k): v for k, v in self.times_ms.items()}}
+
+
+def pick(candidates, run: Callable[[object], float], reps: int = 3) -> TuneResult:
+    """Times run(candidate) reps times per candidate (each call returns milliseconds) and returns
+    the candidate with the smallest median; ties go to the earlier candidate."""
+    if not candidates:
+        raise ValueError("no candidates")
+    res = TuneResult(choice=None)
+    for c in candidates:
+        res.times_ms[c] = statistics.median(run(c) for _ in range(reps))
+    res.choice = min(candidates, key=lambda c: (res.times_ms[c], candidates.index(c)))
+    return res
+
+
+class _Snapshot:
+    """Copies of the particle dats [0, size) and the move's outputs, restored before each trial."""
+
+    def __init__(self, sim):
+        self.sim = sim
+        p = sim.parts
+        n = p.size
+        self.saved = {name: getattr(p, name)[:, :n].clone() for name, _, _ in p.DATS}
+
+    def restore(self) -> None:
+        p = self.sim.parts
+        for name, t in self.saved.items():
+            getattr(p, name)[:, :t.shape[1]].copy_(t)
+        self.sim.node_charge.zero_()
+
+
+def _timed(fn) -> float:
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    fn()
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None) -> TuneResult:
+    """Deposit strategy x node-sum copies for sim's move + deposit launch, on sim's current
+    state, pushed as a step pushes it (so the walks have a step's hops): timed with the push as
+    its prologue when with_push (default: when sim fuses the push), else the move launch alone
+    after an untimed push.  Sets the fastest; sim's state is left as found."""
+    snap = _Snapshot(sim)
+    before = L.Tuning()
+    L.load().oppb_get_tuning(C.byref(before))
+    fused = sim.fused_push if with_push is None else with_push
+
+    def run(c) -> float:
+        L.set_tuning(deposit=c[0], replicas=c[1])
+        snap.restore()
+        if fused:
+            return _timed(sim.push_move)
+        sim.push()
+        return _timed(sim.move)
+
+    try:
+        res = pick(candidates or MOVE_CANDIDATES, run, reps)
+    except Exception:
+        L.load().oppb_set_tuning(C.byref(before))
+        raise
+    finally:
+        snap.restore()
+    L.set_tuning(deposit=res.choice[0], replicas=res.choice[1])
+    return res
+
+
+def tune_sort(sim, candidates=None, reps: int = 3) -> TuneResult:
+    """Columns per gather launch of the cell sort, timed on sim's current (unsorted) state; the
+    sort writes into the swap buffers only, so the state is not changed."""
+    p = sim.parts
+    lib = sim.lib
+    nbytes = lib.oppb_sort_workspace_bytes(p.size, sim.mesh.n_cells)
+    ws = sim._workspace(nbytes)
+    dats = p.dat_list()
+
+    def run(cols) -> float:
+        L.set_tuning(sort_gather_cols=cols)
+        return _timed(lambda: L.check("oppb_sort_by_cell", lib.oppb_sort_by_cell(
+            p.size, sim.mesh.n_cells, p.capacity, len(p.DATS), dats, 3, None, ws.data_ptr(), ws.numel(), None)))
+
+    res = pick(candidates or SORT_CANDIDATES, run, reps)
+    L.set_tuning(sort_gather_cols=res.choice)
+    return res

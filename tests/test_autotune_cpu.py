@@ -1,0 +1,33 @@
+"""The autotuner's choice rule without a GPU: the candidate with the smallest median time wins,
+ties go to the earlier candidate, and every candidate is timed the requested number of times."""
+from __future__ import annotations
+
+import pytest
+
+from oppb.autotune import MOVE_CANDIDATES, SORT_CANDIDATES, pick
+
+
+def test_pick_smallest_median():
+    times = {"a": [5.0, 1.0, 5.0], "b": [3.0, 3.0, 3.0], "c": [4.0, 2.0, 9.0]}
+    calls = {k: 0 for k in times}
+
+    def run(c):
+        calls[c] += 1
+        return times[c][calls[c] - 1]
+
+    res = pick(["a", "b", "c"], run, reps=3)
+    assert res.choice == "b"  # medians 5, 3, 4
+    assert res.times_ms == {"a": 5.0, "b": 3.0, "c": 4.0}
+    assert all(v == 3 for v in calls.values())
+    assert res.report()["choice"] == "b"
+
+
+def test_pick_ties_and_errors():
+    assert pick([(1, 8), (0, 4)], lambda c: 1.0, reps=1).choice == (1, 8)
+    with pytest.raises(ValueError):
+        pick([], lambda c: 0.0)
+
+
+def test_candidate_sets():
+    assert len(set(MOVE_CANDIDATES)) == len(MOVE_CANDIDATES) == 8
+    assert all(1 <= c <= 16 for c in SORT_CANDIDATES) and SORT_CANDIDATES[0] == 16

@@ -471,3 +471,33 @@ def test_run_steps_pipelined_equals_steps(precision):
     ga, gb = a.parts.host_aos(), b.parts.host_aos()
     for name in ("pos", "vel", "lc", "p2c"):
         np.testing.assert_array_equal(ga[name].view(np.uint8), gb[name].view(np.uint8), err_msg=name)
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_autotune_leaves_state_and_picks_valid(precision):
+    """tune_move / tune_sort time their candidates on the live state and leave it bit for bit;
+    the run continues with the chosen tuning and matches a run without tuning (particles
+    bit-exact, node charges within the FP64 atomics' reordering)."""
+    from oppb.autotune import tune_move, tune_sort
+
+    hm = mesh()
+    kw = dict(inject_per_step=2000, precision=precision, fill="Sort_Periodic", fill_period=4)
+    a, b = FemPIC(hm, DEV, **kw), FemPIC(hm, DEV, **kw)
+    tables = [injection_randoms(8, k, 2000, 0.1) for k in range(10)]
+    for t in tables[:6]:
+        a.step(randoms_to_device(t, DEV))
+        b.step(randoms_to_device(t, DEV))
+    before = a.parts.host_aos()
+    rm, rs = tune_move(a, reps=1), tune_sort(a, reps=1)
+    after = a.parts.host_aos()
+    for name in before:
+        np.testing.assert_array_equal(before[name].view(np.uint8), after[name].view(np.uint8), err_msg=name)
+    assert rm.choice in rm.times_ms and rs.choice in rs.times_ms
+    for t in tables[6:]:
+        ra, rb = a.step(randoms_to_device(t, DEV)), b.step(randoms_to_device(t, DEV))
+        assert (ra["size"], ra["removed"], ra["visits"]) == (rb["size"], rb["removed"], rb["visits"])
+    ga, gb = a.parts.host_aos(), b.parts.host_aos()
+    for name in ("pos", "vel", "lc", "p2c"):
+        np.testing.assert_array_equal(ga[name].view(np.uint8), gb[name].view(np.uint8), err_msg=name)
+    _charge_close(a.node_charge.cpu().numpy(), b.node_charge.cpu().numpy(), CHARGE_RTOL)
+    L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC, replicas=8, sort_gather_cols=16)  # defaults for later tests
