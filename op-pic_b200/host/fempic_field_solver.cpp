@@ -80,11 +80,11 @@ FESolver::FESolver(const opp_map c2n_map, const opp_dat n_type, const opp_dat n_
     d.k_col = I.keep(upload(s.k_col, nnz));
     d.k_val = I.keep(upload(s.k_val, nnz));
     d.f0 = I.keep(upload(s.f0, neq));
-    oppb_field_system_free(&s);
+    oppb_field_system_free(&s);  // s is zeroed: sizes below come from the copies taken above
     const std::vector<double> zeros(neq ? neq : 1, 0.0);
     d.d = I.keep(upload(zeros.data(), zeros.size()));   // D (dLocal) starts at 0
     d.f1 = I.keep(upload(zeros.data(), zeros.size()));  // f1Local starts at 0
-    const std::vector<double> work(oppb_field_work_doubles(s.neq), 0.0);
+    const std::vector<double> work(oppb_field_work_doubles((int32_t)neq), 0.0);
     d.work = I.keep(upload(work.data(), work.size()));
     const oppb_field_status st0{};
     I.status = I.keep(upload(&st0, 1));
