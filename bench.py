@@ -107,6 +107,9 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- our arm
 
+HBM_SPEC_GBS = 8000.0  # B200 HBM3e data-sheet bandwidth (DGX figure), for context beside the measured copy peak
+
+
 def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, sampler=None,
                   e2e_steps: int = 0, cpu_sample: bool = False) -> dict:
     import numpy as np
@@ -422,6 +425,7 @@ def arm_ours(args) -> dict:
         "roofline": {"bound": "hbm", "kernel": "move_mixed_kernel (move + fused deposit)",
                      "achieved": mixed["move_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": mixed["move_gbs"] / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                     "frac_of_spec": mixed["move_gbs"] / HBM_SPEC_GBS, "spec_gbs": HBM_SPEC_GBS,
                      "bytes_per_launch": mixed["move_bytes_per_launch"],
                      "traffic": MEASURED_DRAM_BYTES_PER_PARTICLE["mixed"] * mixed["mean_particles"],
                      "traffic_source": TRAFFIC_SOURCE},
