@@ -367,7 +367,7 @@ def arm_ours(args) -> dict:
             print(json.dumps({"precision": r["precision"], "value": r["value"], "move_only": r["move_only"],
                               "move_ms_per_launch": r["move_ms_per_launch"], "move_gbs": r["move_gbs"],
                               "mean_particles": r["mean_particles"], "visits_per_particle": r["visits_per_particle"],
-                              "clocks": r["clocks"]}), flush=True)
+                              "clocks": r["clocks"], "autotune": r["autotune"]}), flush=True)
         if world > 1:
             dist.destroy_process_group()
         return {}
