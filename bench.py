@@ -210,6 +210,17 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     out["move_gbs"] = sum(bytes_per_launch) / (sum(t_move) / 1e3) / 1e9
     out["move_bytes_per_launch"] = sum(bytes_per_launch) / steps
     out["move_ms_per_launch"] = sum(t_move) / steps
+    # Move time against the steps since the last cell sort (0 = the first move after a sort):
+    # particles leave their sorted neighbours as they hop, so a warp's lanes spread over more
+    # cells until the next sort.
+    by_phase, phase = {}, None
+    for r, t in zip(rec, t_move):
+        if phase is not None:
+            by_phase.setdefault(phase, []).append(t)
+            phase += 1
+        if r[2] == "sort":
+            phase = 0
+    out["move_ms_since_sort"] = {str(k): sum(v) / len(v) for k, v in sorted(by_phase.items())}
     out["push_ms_per_launch"] = sum(t_push) / steps
     out["push_inclusive"] = ps / ((sum(t_push) + sum(t_move) + sum(t_comp)) / 1e3)
 
@@ -367,7 +378,8 @@ def arm_ours(args) -> dict:
             print(json.dumps({"precision": r["precision"], "value": r["value"], "move_only": r["move_only"],
                               "move_ms_per_launch": r["move_ms_per_launch"], "move_gbs": r["move_gbs"],
                               "mean_particles": r["mean_particles"], "visits_per_particle": r["visits_per_particle"],
-                              "clocks": r["clocks"], "autotune": r["autotune"]}), flush=True)
+                              "clocks": r["clocks"], "autotune": r["autotune"],
+                              "move_ms_since_sort": r["move_ms_since_sort"]}), flush=True)
         if world > 1:
             dist.destroy_process_group()
         return {}
@@ -410,10 +422,12 @@ def arm_ours(args) -> dict:
         "plain_fp64": {"value": f64["job_value"], "move_only": f64["move_only"], "whole_step": f64["whole_step"],
                        "ms_per_step": f64["ms_per_step"], "move_ms_per_launch": f64["move_ms_per_launch"],
                        "move_gbs": f64["move_gbs"], "frac_of_hbm": f64["move_gbs"] / peaks["hbm_gbs"],
-                       "visits_per_particle": f64["visits_per_particle"], "mean_particles": f64["mean_particles"]},
+                       "visits_per_particle": f64["visits_per_particle"], "mean_particles": f64["mean_particles"],
+                       "move_ms_since_sort": f64["move_ms_since_sort"]},
         "mixed": {"value": mixed["job_value"], "move_only": mixed["move_only"], "whole_step": mixed["whole_step"],
                   "move_ms_per_launch": mixed["move_ms_per_launch"], "recheck_frac": mixed["recheck_frac"],
-                  "visits_per_particle": mixed["visits_per_particle"]},
+                  "visits_per_particle": mixed["visits_per_particle"],
+                  "move_ms_since_sort": mixed["move_ms_since_sort"]},
         "push_inclusive": {"unit": UNIT, "what": "push + move + deposit + compaction, device time",
                            "mixed_unfused": mixed["push_inclusive"], "mixed_fused": mixed["push_inclusive_fused"],
                            "f64_unfused": f64["push_inclusive"], "f64_fused": f64["push_inclusive_fused"],
