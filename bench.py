@@ -107,6 +107,51 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- our arm
 
+def mixed_vs_f64(sim) -> dict:
+    """One move + deposit of the mixed kernel and one of the FP64 kernel from the same pushed
+    particle state (the steady state after the timed steps, pushed once and restored between
+    the two): cells, lambdas and node charges of the mixed form against the FP64 form.  The
+    state the timed steps left is put back afterwards."""
+    import ctypes as C
+
+    import torch
+
+    from oppb import _lib as L
+    from oppb.autotune import ParticleSnapshot
+
+    before = ParticleSnapshot(sim)
+    sim.push()  # the walks of a step: both moves start from the same pushed state
+    snap = ParticleSnapshot(sim)
+    p, n = sim.parts, sim.parts.size
+    out = {}
+    for name in ("mixed", "f64"):
+        snap.restore()
+        if name == "mixed":
+            sim.move()
+        else:
+            v, ws = p.view(), sim._deposit_ws()
+            L.check("oppb_move_deposit_f64", sim.lib.oppb_move_deposit_f64(
+                C.byref(sim.mesh.s), C.byref(v), sim.node_charge.data_ptr(), p.status.data_ptr(), sim.max_hops,
+                ws.data_ptr(), ws.numel(), None))
+        torch.cuda.synchronize()
+        st = p.status_host()
+        if st.error:
+            raise L.OppbError(f"{name} move", st.error)
+        out[name] = (p.p2c[0, :n].clone(), p.lc[:, :n].clone(), sim.node_charge.clone(), st.remove_count)
+    before.restore()  # the state the timed steps left, for the steps that follow
+    (c_m, l_m, q_m, r_m), (c_f, l_f, q_f, r_f) = out["mixed"], out["f64"]
+    kept = c_f != L.REMOVED_CELL
+    dq = (q_m - q_f).abs()
+    big = q_f.abs() >= 1.0
+    return {"what": "one mixed and one FP64 move + deposit from the same steady state (57M particles)",
+            "particles": n, "cells_differing": int((c_m != c_f).sum()), "removed": [int(r_m), int(r_f)],
+            "lambda_max_abs_diff": float((l_m - l_f)[:, kept].abs().max()),
+            "node_charge_normwise_rel": float(dq.max() / q_f.abs().max()),
+            "node_charge_max_err_over_max_q_or_1": float((dq / q_f.abs().clamp(min=1.0)).max()),
+            "node_charge_mean_rel_where_q_ge_1": float((dq[big] / q_f.abs()[big]).mean()),
+            "node_charge_max_abs": float(q_f.abs().max())}
+
+
 HBM_SPEC_GBS = 8000.0  # B200 HBM3e data-sheet bandwidth (DGX figure), for context beside the measured copy peak
 
 
@@ -204,6 +249,8 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
         "clocks": clocks,
         "autotune": tuned,
     }
+    if precision == "mixed":
+        out["vs_f64"] = mixed_vs_f64(sim)
     # Roofline of the move(+deposit) kernel: algorithmic bytes / mean launch time.
     bytes_per_launch = [BYTES_PER_PARTICLE * r[0] + BYTES_PER_CELL[precision] * hm.n_cells
                         + BYTES_PER_NODE * hm.n_nodes for r in rec]
@@ -379,7 +426,8 @@ def arm_ours(args) -> dict:
                               "move_ms_per_launch": r["move_ms_per_launch"], "move_gbs": r["move_gbs"],
                               "mean_particles": r["mean_particles"], "visits_per_particle": r["visits_per_particle"],
                               "clocks": r["clocks"], "autotune": r["autotune"],
-                              "move_ms_since_sort": r["move_ms_since_sort"]}), flush=True)
+                              "move_ms_since_sort": r["move_ms_since_sort"], "vs_f64": r.get("vs_f64")}),
+                  flush=True)
         if world > 1:
             dist.destroy_process_group()
         return {}
@@ -427,7 +475,7 @@ def arm_ours(args) -> dict:
         "mixed": {"value": mixed["job_value"], "move_only": mixed["move_only"], "whole_step": mixed["whole_step"],
                   "move_ms_per_launch": mixed["move_ms_per_launch"], "recheck_frac": mixed["recheck_frac"],
                   "visits_per_particle": mixed["visits_per_particle"],
-                  "move_ms_since_sort": mixed["move_ms_since_sort"]},
+                  "move_ms_since_sort": mixed["move_ms_since_sort"], "vs_f64": mixed["vs_f64"]},
         "push_inclusive": {"unit": UNIT, "what": "push + move + deposit + compaction, device time",
                            "mixed_unfused": mixed["push_inclusive"], "mixed_fused": mixed["push_inclusive_fused"],
                            "f64_unfused": f64["push_inclusive"], "f64_fused": f64["push_inclusive_fused"],

@@ -45,7 +45,7 @@ def pick(candidates, run: Callable[[object], float], reps: int = 3) -> TuneResul
     return res
 
 
-class _Snapshot:
+class ParticleSnapshot:
     """Copies of the particle dats [0, size) and the move's outputs, restored before each trial."""
 
     def __init__(self, sim):
@@ -77,7 +77,7 @@ def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None
     state, pushed as a step pushes it (so the walks have a step's hops): timed with the push as
     its prologue when with_push (default: when sim fuses the push), else the move launch alone
     after an untimed push.  Sets the fastest; sim's state is left as found."""
-    snap = _Snapshot(sim)
+    snap = ParticleSnapshot(sim)
     before = L.Tuning()
     L.load().oppb_get_tuning(C.byref(before))
     fused = sim.fused_push if with_push is None else with_push
