@@ -107,11 +107,12 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- our arm
 
-def mixed_vs_f64(sim) -> dict:
+def mixed_vs_f64(sim, charges: bool = False):
     """One move + deposit of the mixed kernel and one of the FP64 kernel from the same pushed
     particle state (the steady state after the timed steps, pushed once and restored between
     the two): cells, lambdas and node charges of the mixed form against the FP64 form.  The
-    state the timed steps left is put back afterwards."""
+    state the timed steps left is put back afterwards.  charges: also return the two node-charge
+    vectors."""
     import ctypes as C
 
     import torch
@@ -143,13 +144,14 @@ def mixed_vs_f64(sim) -> dict:
     kept = c_f != L.REMOVED_CELL
     dq = (q_m - q_f).abs()
     big = q_f.abs() >= 1.0
-    return {"what": "one mixed and one FP64 move + deposit from the same steady state (57M particles)",
+    rep = {"what": "one mixed and one FP64 move + deposit from the same pushed steady state",
             "particles": n, "cells_differing": int((c_m != c_f).sum()), "removed": [int(r_m), int(r_f)],
             "lambda_max_abs_diff": float((l_m - l_f)[:, kept].abs().max()),
             "node_charge_normwise_rel": float(dq.max() / q_f.abs().max()),
             "node_charge_max_err_over_max_q_or_1": float((dq / q_f.abs().clamp(min=1.0)).max()),
             "node_charge_mean_rel_where_q_ge_1": float((dq[big] / q_f.abs()[big]).mean()),
             "node_charge_max_abs": float(q_f.abs().max())}
+    return (rep, q_m, q_f) if charges else rep
 
 
 HBM_SPEC_GBS = 8000.0  # B200 HBM3e data-sheet bandwidth (DGX figure), for context beside the measured copy peak
@@ -697,6 +699,28 @@ def run_field_phase(hm, dev, steps: int, warmup: int, seed: int, cpu: bool) -> d
            "max_abs_potential": pmax, "visits_per_particle_last": sim.last["visits"] / max(1, sim.last["size_before_move"]),
            "nodes": hm.n_nodes, "unknowns": sim.field.neq, "nnz": sim.field.nnz, "setup_s": setup_s,
            "constants": FIELD, "gpu_launches": int(launches)}
+    # The field from mixed node charges against the field from FP64 ones: both charge vectors
+    # come from one move + deposit of each kernel on the same pushed state, and each field
+    # phase starts from the same Newton state.
+    rep, q_m, q_f = mixed_vs_f64(sim, charges=True)
+    d0, f10 = sim.field.d.clone(), sim.field.f1.clone()
+    res = {}
+    for name, q in (("mixed", q_m), ("f64", q_f)):
+        sim.field.d.copy_(d0)
+        sim.field.f1.copy_(f10)
+        sim.node_charge.copy_(q)
+        sim.field_phase()
+        torch.cuda.synchronize()
+        res[name] = (sim.field.potential.clone(), sim.mesh.ef.view(-1, 4)[:, :3].clone())
+    sim.field.d.copy_(d0)
+    sim.field.f1.copy_(f10)
+    (pm, em), (pf, ef_) = res["mixed"], res["f64"]
+    out["mixed_vs_f64"] = {
+        "what": "field phase on the node charges of one mixed and one FP64 move + deposit from the same pushed "
+                "state, both from the same Newton state (CG stops at 1e-10 relative residual)",
+        "node_charge_normwise_rel": rep["node_charge_normwise_rel"], "cells_differing": rep["cells_differing"],
+        "potential_normwise_rel": float((pm - pf).abs().max() / pf.abs().max()),
+        "field_normwise_rel": float((em - ef_).abs().max() / ef_.abs().max())}
     if cpu:
         from oracle import field as F
 
