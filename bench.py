@@ -161,6 +161,7 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
                   e2e_steps: int = 0, cpu_sample: bool = False) -> dict:
     import numpy as np
     import torch
+    import torch.distributed as dist
 
     from oppb import _lib as L
     from oppb.fempic import FemPIC, injection_randoms
@@ -200,6 +201,9 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     if sampler:
         sampler.start()
     torch.cuda.synchronize()
+    if dist.is_initialized():  # every rank enters the timed steps together
+        dist.barrier()
+        torch.cuda.synchronize()
     # Profiler range = the timed steps (for `ncu --profile-from-start off`); no effect otherwise.
     torch.cuda.profiler.start()
     ev_all0, ev_all1 = E(), E()
@@ -224,6 +228,8 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
         rec.append((n_alive, ev, kind, st.total_visits, st.recheck_count, st.remove_count))
     ev_all1.record(s)
     torch.cuda.synchronize()
+    if dist.is_initialized():
+        dist.barrier()
     torch.cuda.profiler.stop()
     clocks = sampler.stop() if sampler else None
     launches = lib.oppb_kernel_launches() - launches0
