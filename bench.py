@@ -188,6 +188,9 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     # state before the timed steps; the state is restored after each trial.
     from oppb.autotune import tune_move, tune_sort
     tuned = {"move": tune_move(sim, with_push=False).report(), "sort": tune_sort(sim).report()}
+    # The deterministic deposit (integer fixed-point node sums) on the same state, for the record.
+    from oppb.autotune import time_move
+    tuned["deterministic_deposit_ms"] = time_move(sim, L.DEPOSIT_EXACT, with_push=False)
     log(f"[{precision}] autotune move {tuned['move']['choice']} sort cols {tuned['sort']['choice']}")
     # Inputs of the timed steps generated before timing (device-resident).
     tables = [device_randoms(torch.empty_like(rnd_buf)) for _ in range(min(steps, 16))]

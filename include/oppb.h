@@ -121,6 +121,13 @@ uint64_t oppb_kernel_launches(void);
 /* Launch choices of the move kernels (process-wide; the autotuner's output). */
 #define OPPB_DEPOSIT_WARP_ATOMIC 0  /* lanes grouped by final cell (warp match), FP64 atomics per group */
 #define OPPB_DEPOSIT_CTA_TABLE   1  /* per-CTA shared-memory node-sum table, one global atomic per node */
+/* Deterministic mode: every weight w is cut to the fixed-point value floor(w 2^52) 2^-52 (held
+ * as an int32 multiple of 2^-20 plus a uint32 multiple of 2^-52) and the node sums are integer sums,
+ * so node_charge gains exactly sum_i trunc(w_i) whatever the particle order, warp grouping or
+ * launch shape, bit for bit from run to run (one rounding when the integer sum is turned into
+ * FP64).  Each term is within 2^-52 of its weight.  Needs 16 B per node of workspace
+ * (oppb_deposit_workspace_bytes) and weights in (-2^11, 2^11). */
+#define OPPB_DEPOSIT_EXACT       2
 typedef struct oppb_tuning {
     int32_t deposit;     /* OPPB_DEPOSIT_* */
     int32_t replicas;    /* node-sum copies the deposit spreads its atomics over (1..64, default 8) */
@@ -169,8 +176,9 @@ int oppb_move_f64(const oppb_tet_mesh* mesh, const oppb_particles* parts,
                   oppb_move_status* status, int32_t max_hops, void* stream);
 
 /* Scratch bytes a deposit (fused or standalone) can use for n_nodes nodes: the node-sum
- * copies beyond the first for the tuned replica count.  With less (or NULL) the deposit
- * adds straight into node_charge. */
+ * copies beyond the first for the tuned replica count (with less, or NULL, the deposit adds
+ * straight into node_charge); with OPPB_DEPOSIT_EXACT the two integer sums per node, which
+ * the deposit requires (OPPB_ERR_WORKSPACE when they do not fit). */
 size_t oppb_deposit_workspace_bytes(int32_t n_nodes);
 
 /* FP64 move with the node-charge deposit of the final cell fused in:

@@ -16,7 +16,9 @@ const oppb_tuning& tuning() { return g_tuning; }
 extern "C" uint64_t oppb_kernel_launches(void) { return oppb::g_launches.load(std::memory_order_relaxed); }
 
 extern "C" int oppb_set_tuning(const oppb_tuning* t) {
-    if (!t || (t->deposit != OPPB_DEPOSIT_WARP_ATOMIC && t->deposit != OPPB_DEPOSIT_CTA_TABLE)) return OPPB_ERR_ARG;
+    if (!t || (t->deposit != OPPB_DEPOSIT_WARP_ATOMIC && t->deposit != OPPB_DEPOSIT_CTA_TABLE &&
+               t->deposit != OPPB_DEPOSIT_EXACT))
+        return OPPB_ERR_ARG;
     if (t->replicas < 1 || t->replicas > 64) return OPPB_ERR_ARG;
     if (t->advec_items != 1 && t->advec_items != 2 && t->advec_items != 4) return OPPB_ERR_ARG;
     if (t->sort_gather_cols < 1 || t->sort_gather_cols > 16) return OPPB_ERR_ARG;

@@ -33,7 +33,7 @@ constexpr int kMoveBlock = 256;
 constexpr int kMinBlocks = 8;          // 8 x 256 threads per SM: 32 registers per thread
 constexpr int kSlots = 256;            // shared node-sum table (power of two, one slot per thread)
 constexpr int kMaxProbe = 16;          // linear-probe bound; beyond it the sum goes straight to global
-constexpr int kDepNone = 0, kDepWarp = 1, kDepTable = 2;
+constexpr int kDepNone = 0, kDepWarp = 1, kDepTable = 2, kDepExact = 3;
 static_assert(kSlots == kMoveBlock, "table init/flush assume one slot per thread");
 
 enum : int { kDone = 0, kNeedMove = 1, kNeedRemove = 2, kFailed = 3 };
@@ -61,6 +61,7 @@ struct DepositArgs {
     double* node_charge;
     double* copies;     // replicas - 1 arrays of n_nodes, or nullptr
     int32_t replicas;
+    unsigned long long* exact;  // OPPB_DEPOSIT_EXACT: [2][n_nodes] sums of multiples of 2^-20, of 2^-52
 };
 
 struct NodeTable {
@@ -216,11 +217,68 @@ __device__ __forceinline__ void warp_deposit(const oppb_tet_mesh& m, NodeTable& 
     }
 }
 
+// Fixed-point parts of a weight for OPPB_DEPOSIT_EXACT: u = floor(w 2^52) (w 2^52 is exact,
+// a power-of-two scaling, and so is its floor; |u| < 2^63 for |w| < 2^11) split as
+// u = a 2^32 + b with a = u >> 32 (the floor of u / 2^32) and b = u mod 2^32, so that
+// w = a 2^-20 + b 2^-52 + r with 0 <= r < 2^-52 for weights of either sign.
+__device__ __forceinline__ void exact_parts(double w, int32_t& a, uint32_t& b) {
+    const long long u = __double2ll_rz(floor(__dmul_rn(w, 4503599627370496.0)));
+    a = (int32_t)(u >> 32);
+    b = (uint32_t)(u & 0xffffffffll);
+}
+
+// The warp-grouped deposit of OPPB_DEPOSIT_EXACT: each lane cuts its four weights to fixed
+// point, the lowest lane of a cell group adds the group's integers, and the sums go to the
+// integer node sums with 64-bit atomics.  Integer sums do not depend on their order.
+template <typename T>
+__device__ __forceinline__ void warp_deposit_exact(const oppb_tet_mesh& m, unsigned long long* acc, int32_t key,
+                                                   T l0, T l1, T l2, T l3) {
+    const int lane = threadIdx.x & 31;
+    int32_t a0, a1, a2, a3;
+    uint32_t b0, b1, b2, b3;
+    exact_parts((double)l0, a0, b0);
+    exact_parts((double)l1, a1, b1);
+    exact_parts((double)l2, a2, b2);
+    exact_parts((double)l3, a3, b3);
+    const unsigned peers = __match_any_sync(kFullMask, key);
+    const bool leader = (lane == __ffs(peers) - 1) && key >= 0;
+    unsigned rest = leader ? (peers & ~(1u << lane)) : 0u;
+    long long h0 = a0, h1 = a1, h2 = a2, h3 = a3;
+    unsigned long long g0 = b0, g1 = b1, g2 = b2, g3 = b3;
+    while (__any_sync(kFullMask, rest != 0)) {
+        const int src = rest ? __ffs(rest) - 1 : lane;
+        const int32_t x0 = __shfl_sync(kFullMask, a0, src), x1 = __shfl_sync(kFullMask, a1, src);
+        const int32_t x2 = __shfl_sync(kFullMask, a2, src), x3 = __shfl_sync(kFullMask, a3, src);
+        const uint32_t y0 = __shfl_sync(kFullMask, b0, src), y1 = __shfl_sync(kFullMask, b1, src);
+        const uint32_t y2 = __shfl_sync(kFullMask, b2, src), y3 = __shfl_sync(kFullMask, b3, src);
+        if (rest) {
+            h0 += x0, h1 += x1, h2 += x2, h3 += x3;
+            g0 += y0, g1 += y1, g2 += y2, g3 += y3;
+            rest &= rest - 1;
+        }
+    }
+    if (leader) {
+        const int4 nodes = ldg_i4(m.c2n + (int64_t)key * 4);
+        const uint32_t nn = (uint32_t)m.n_nodes;
+        unsigned long long* lo = acc + nn;
+        if ((uint32_t)nodes.x < nn) atomicAdd(acc + nodes.x, (unsigned long long)h0), atomicAdd(lo + nodes.x, g0);
+        if ((uint32_t)nodes.y < nn) atomicAdd(acc + nodes.y, (unsigned long long)h1), atomicAdd(lo + nodes.y, g1);
+        if ((uint32_t)nodes.z < nn) atomicAdd(acc + nodes.z, (unsigned long long)h2), atomicAdd(lo + nodes.z, g2);
+        if ((uint32_t)nodes.w < nn) atomicAdd(acc + nodes.w, (unsigned long long)h3), atomicAdd(lo + nodes.w, g3);
+    }
+}
+
 // Deposit epilogue shared by the move kernels.  Every thread of the CTA must call it.
 template <int kDep, typename T>
 __device__ __forceinline__ void deposit_epilogue(const oppb_tet_mesh& m, NodeTable& table, const DepositArgs& d,
                                                  bool dep, int32_t cell, const T l[4]) {
     if (kDep == kDepNone) return;
+    if (kDep == kDepExact) {
+        const T zero = 0;
+        warp_deposit_exact<T>(m, d.exact, dep ? cell : -1, dep ? l[0] : zero, dep ? l[1] : zero, dep ? l[2] : zero,
+                              dep ? l[3] : zero);
+        return;
+    }
     double* target = deposit_target(d, m.n_nodes);
     if (kDep == kDepTable) __syncthreads();  // table initialised by every thread
     const T zero = 0;
@@ -501,6 +559,20 @@ __global__ void __launch_bounds__(256) reduce_copies_kernel(double* node_charge,
     }
 }
 
+// OPPB_DEPOSIT_EXACT: node_charge[n] += hi[n] 2^-20 + lo[n] 2^-52.  The carry of lo above
+// 2^32 moves into hi first, so both terms are exact in FP64 (|hi| < 2^53) and their sum is
+// rounded once.
+__global__ void __launch_bounds__(256) exact_finish_kernel(double* node_charge, const unsigned long long* acc,
+                                                           int32_t n) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long lo = acc[n + k];
+        const long long hi = (long long)(acc[k] + (lo >> 32));
+        const double v = __dadd_rn(__dmul_rn(__ll2double_rn(hi), 0x1p-20),
+                                   __dmul_rn(__ull2double_rn(lo & 0xffffffffull), 0x1p-52));
+        node_charge[k] = __dadd_rn(node_charge[k], v);
+    }
+}
+
 int check_mesh(const oppb_tet_mesh* mesh, bool mixed, bool need_c2n) {
     if (!mesh || mesh->n_cells <= 0 || mesh->n_nodes <= 0) return OPPB_ERR_ARG;
     if (!mesh->det || !mesh->nav || !aligned(mesh->det, 32) || !aligned(mesh->nav, 32)) return OPPB_ERR_ARG;
@@ -528,27 +600,46 @@ int replicas_for(size_t workspace_bytes, const void* workspace, int32_t n_nodes)
     return (int)(fit < (size_t)want ? fit : (size_t)want);
 }
 
-// Zeroes the copies before, and folds them into node_charge after, the deposit launch.
+// Zeroes the copies (or the exact mode's integer sums) before, and folds them into
+// node_charge after, the deposit launch.
 struct Replicas {
     DepositArgs args;
     int n_nodes;
     int begin(cudaStream_t s) {
+        if (args.exact)
+            return cudaMemsetAsync(args.exact, 0, 2 * (size_t)n_nodes * sizeof(unsigned long long), s) == cudaSuccess
+                       ? OPPB_OK
+                       : OPPB_ERR_LAUNCH;
         if (args.replicas > 1 &&
             cudaMemsetAsync(args.copies, 0, (size_t)(args.replicas - 1) * n_nodes * sizeof(double), s) != cudaSuccess)
             return OPPB_ERR_LAUNCH;
         return OPPB_OK;
     }
     void end(cudaStream_t s) {
-        if (args.replicas <= 1) return;
         const int grid = ceil_div(n_nodes, 256) < 148 * 8 ? ceil_div(n_nodes, 256) : 148 * 8;
+        if (args.exact) {
+            exact_finish_kernel<<<grid, 256, 0, s>>>(args.node_charge, args.exact, n_nodes);
+            count_launches(1);
+            return;
+        }
+        if (args.replicas <= 1) return;
         reduce_copies_kernel<<<grid, 256, 0, s>>>(args.node_charge, args.copies, n_nodes, args.replicas - 1);
         count_launches(1);
     }
 };
 
-Replicas make_replicas(double* node_charge, void* workspace, size_t workspace_bytes, int32_t n_nodes) {
+bool exact_mode() { return tuning().deposit == OPPB_DEPOSIT_EXACT; }
+
+// The deposit's targets; *rc = OPPB_ERR_WORKSPACE when the exact mode's sums do not fit.
+Replicas make_replicas(double* node_charge, void* workspace, size_t workspace_bytes, int32_t n_nodes, int* rc) {
+    *rc = OPPB_OK;
+    if (exact_mode()) {
+        if (!workspace || !aligned(workspace, 8) || workspace_bytes < 2 * (size_t)n_nodes * sizeof(unsigned long long))
+            *rc = OPPB_ERR_WORKSPACE;
+        return Replicas{DepositArgs{node_charge, nullptr, 1, static_cast<unsigned long long*>(workspace)}, n_nodes};
+    }
     const int r = replicas_for(workspace_bytes, workspace, n_nodes);
-    return Replicas{DepositArgs{node_charge, r > 1 ? static_cast<double*>(workspace) : nullptr, r}, n_nodes};
+    return Replicas{DepositArgs{node_charge, r > 1 ? static_cast<double*>(workspace) : nullptr, r, nullptr}, n_nodes};
 }
 
 enum MoveKind { kMoveOnly, kMoveDepositF64, kMoveDepositMixed };
@@ -572,9 +663,14 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     if (parts->size == 0) return launch_status();
     const PartArgs p = part_args(parts);
     const int grid = ceil_div(parts->size, kMoveBlock);
-    Replicas rep = make_replicas(node_charge, kKind == kMoveOnly ? nullptr : workspace, ws_bytes, mesh->n_nodes);
+    Replicas rep{};
+    if (kKind != kMoveOnly) {
+        rep = make_replicas(node_charge, workspace, ws_bytes, mesh->n_nodes, &rc);
+        if (rc) return rc;
+    }
     if ((rc = rep.begin(s))) return rc;
     const bool table = tuning().deposit == OPPB_DEPOSIT_CTA_TABLE;
+    const bool exact = exact_mode();
     const float bf = (float)band;
     const Band bd{bf, -bf, 1.0f - bf, 1.0f + bf, 2.0f * bf};
     if constexpr (kKind == kMoveOnly)
@@ -584,10 +680,16 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
         if (table)
             move_f64_kernel<kDepTable, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                                 max_hops, push, dh);
+        else if (exact)
+            move_f64_kernel<kDepExact, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+                                                                                max_hops, push, dh);
         else
             move_f64_kernel<kDepWarp, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                                max_hops, push, dh);
-    } else if (table)
+    } else if (exact)
+        move_mixed_kernel<kDepExact, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+                                                                              max_hops, bd, push, dh);
+    else if (table)
         move_mixed_kernel<kDepTable, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                               max_hops, bd, push, dh);
     else
@@ -629,6 +731,7 @@ int move_ex(const oppb_tet_mesh* mesh, const oppb_particles* parts, const oppb_m
 
 extern "C" size_t oppb_deposit_workspace_bytes(int32_t n_nodes) {
     const int r = oppb::tuning().replicas;
+    if (n_nodes > 0 && oppb::exact_mode()) return 2 * (size_t)n_nodes * sizeof(unsigned long long);
     if (n_nodes <= 0 || r <= 1) return 0;
     return (size_t)(r - 1) * (size_t)n_nodes * sizeof(double);
 }
@@ -681,12 +784,14 @@ extern "C" int oppb_deposit_f64(const oppb_tet_mesh* mesh, const oppb_particles*
         return OPPB_ERR_ARG;
     if (parts->size == 0) return OPPB_OK;
     cudaStream_t s = as_stream(stream);
-    Replicas rep = make_replicas(node_charge, workspace, workspace_bytes, mesh->n_nodes);
-    int rc = rep.begin(s);
-    if (rc) return rc;
+    int rc = OPPB_OK;
+    Replicas rep = make_replicas(node_charge, workspace, workspace_bytes, mesh->n_nodes, &rc);
+    if (rc || (rc = rep.begin(s))) return rc;
     const int grid = ceil_div(parts->size, kMoveBlock);
     if (tuning().deposit == OPPB_DEPOSIT_CTA_TABLE)
         deposit_f64_kernel<kDepTable><<<grid, kMoveBlock, 0, s>>>(*mesh, part_args(parts), rep.args);
+    else if (exact_mode())
+        deposit_f64_kernel<kDepExact><<<grid, kMoveBlock, 0, s>>>(*mesh, part_args(parts), rep.args);
     else
         deposit_f64_kernel<kDepWarp><<<grid, kMoveBlock, 0, s>>>(*mesh, part_args(parts), rep.args);
     count_launches(1);

@@ -52,6 +52,7 @@ class Tuning(C.Structure):
 
 DEPOSIT_WARP_ATOMIC = 0
 DEPOSIT_CTA_TABLE = 1
+DEPOSIT_EXACT = 2  # OPPB_DEPOSIT_EXACT: integer fixed-point node sums, order-independent
 
 
 class Inlet(C.Structure):

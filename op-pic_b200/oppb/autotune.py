@@ -101,6 +101,17 @@ def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None
     return res
 
 
+def time_move(sim, deposit: int, replicas: int = 1, reps: int = 3, with_push: bool | None = None) -> float:
+    """Median milliseconds of sim's move + deposit launch with the given deposit strategy, timed as
+    tune_move times its candidates; the tuning and sim's state are left as found."""
+    before = L.Tuning()
+    L.load().oppb_get_tuning(C.byref(before))
+    try:
+        return tune_move(sim, [(deposit, replicas)], reps, with_push).times_ms[(deposit, replicas)]
+    finally:
+        L.load().oppb_set_tuning(C.byref(before))
+
+
 def tune_sort(sim, candidates=None, reps: int = 3) -> TuneResult:
     """Columns per gather launch of the cell sort, timed on sim's current (unsorted) state; the
     sort writes into the swap buffers only, so the state is not changed."""

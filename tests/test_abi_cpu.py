@@ -6,6 +6,7 @@ import ctypes as C
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 from oppb import _lib as L
@@ -112,3 +113,44 @@ def test_dh_and_move_ex_argument_validation():
     assert lib.oppb_dh_grid_init(pts, 1, 1e-12, (C.c_double * 3)(1.0, 1.0, 1.0), C.byref(g)) == L.OPPB_ERR_ARG
     assert lib.oppb_dh_build(None, None, C.byref(g), None, 0, None, None) == L.OPPB_ERR_ARG
     assert lib.oppb_move_ex(None, None, None, None, None, 16, None, 0, None) == L.OPPB_ERR_ARG
+
+
+def test_tuning_exact_deposit_mode_and_workspace():
+    """OPPB_DEPOSIT_EXACT is a valid deposit choice (unknown ones are refused) and asks for
+    two 8-B integer sums per node of workspace; the other modes keep the copy sizing."""
+    lib = L.load()
+    before = L.Tuning()
+    lib.oppb_get_tuning(C.byref(before))
+    try:
+        L.set_tuning(deposit=L.DEPOSIT_EXACT)
+        assert lib.oppb_deposit_workspace_bytes(1000) == 16 * 1000
+        assert lib.oppb_deposit_workspace_bytes(0) == 0
+        L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC, replicas=4)
+        assert lib.oppb_deposit_workspace_bytes(1000) == 3 * 8 * 1000
+        bad = L.Tuning()
+        lib.oppb_get_tuning(C.byref(bad))
+        bad.deposit = 3
+        assert lib.oppb_set_tuning(C.byref(bad)) == L.OPPB_ERR_ARG
+    finally:
+        lib.oppb_set_tuning(C.byref(before))
+
+
+def test_exact_deposit_split_bounds():
+    """The fixed-point split of the exact deposit, restated in numpy: u = floor(w 2^52) (exact
+    in FP64 for |w| < 2^11), a = u >> 32, b = u mod 2^32, so w = a 2^-20 + b 2^-52 + r with
+    0 <= r < 2^-52, for weights of either sign, tiny negative ones (where 1 + w 2^20 is not
+    exact in FP64) and the mixed path's FP32 weights widened to FP64 included."""
+    rng = np.random.default_rng(3)
+    tiny = -(2.0 ** -52) * (1 + rng.uniform(0, 1, 1000))
+    w = np.concatenate([rng.uniform(-1e-9, 1.0 + 1e-9, 100_000), rng.uniform(-1000, 1000, 1000), tiny,
+                        rng.uniform(0, 1, 1000).astype(np.float32).astype(np.float64),
+                        [0.0, 1.0, -1e-10, 2 ** -52, -(2 ** -52), -(2 ** -52 + 2 ** -105)]])
+    u = np.floor(w * 2.0 ** 52).astype(np.int64)
+    a, b = u >> 32, u & 0xFFFFFFFF
+    assert (b >= 0).all() and (b < 2 ** 32).all() and (np.abs(a) < 2 ** 31).all()
+    np.testing.assert_array_equal(a * 2 ** 32 + b, u)
+    # r = w - u 2^-52 in [0, 2^-52): checked in exact rational arithmetic on a sample
+    from fractions import Fraction
+    for x, k in zip(w[::97], u[::97]):
+        r = Fraction(float(x)) - Fraction(int(k), 2 ** 52)
+        assert 0 <= r < Fraction(1, 2 ** 52)
