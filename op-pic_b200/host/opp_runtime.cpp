@@ -242,6 +242,14 @@ void opp_init(int argc, char** argv) {
     if (OPP_fill_type == OPP_Sort_Periodic && period != INT_MAX && period >= 0) OPP_fill_period = period;
     const int hops = opp_params->get<OPP_INT>("opp_move_max_hops");
     if (hops != INT_MAX && hops > 0) OPP_move_max_hops = hops;
+    // B200 extension (absent from the reference's parameter files, default false): node-charge
+    // deposits with order-independent integer sums, bit-identical from run to run.
+    if (opp_params->get<OPP_BOOL>("oppb_deterministic_deposit")) {
+        oppb_tuning t{};
+        oppb_get_tuning(&t);
+        t.deposit = OPPB_DEPOSIT_EXACT;
+        if (oppb_set_tuning(&t) != OPPB_OK) opp_abort("oppb_set_tuning");
+    }
     for (int n = 1; n < argc; n++) {
         const char* p = std::strstr(argv[n], "OPP_ALLOC_MULT=");
         if (p) OPP_part_alloc_mult = std::atof(p + 15);

@@ -50,6 +50,35 @@ def test_fempic_app_matches_oracle(tmp_path, fill, period, steps):
     assert err.max() <= 1e-12
 
 
+def test_fempic_app_deterministic_deposit_repeats(tmp_path):
+    """BOOL oppb_deterministic_deposit = true in the parameter file selects the integer
+    fixed-point deposit: two runs give node charges identical bit for bit, particles equal to
+    the oracle's and charges within 1e-12 of its sequential sums."""
+    hm = mesh()
+    inject, steps = 2000, 25
+    dist = hm.inject_distribution(inject)
+    tables = [injection_randoms(17, s, inject, 0.1) for s in range(steps)]
+    R.write_case(tmp_path / "case.bin", hm, dist, steps, tables)
+    (tmp_path / "params.txt").write_text(R.params_text("Sort_Periodic", 5, 2.0,
+                                                       extra="BOOL oppb_deterministic_deposit = true\n"))
+    outs = []
+    for k in range(2):
+        out = tmp_path / f"out{k}.bin"
+        r = subprocess.run([str(APP), str(tmp_path / "params.txt"), str(tmp_path / "case.bin"), str(out)],
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append(R.read_output(out, hm.n_nodes))
+    np.testing.assert_array_equal(outs[0]["node_charge"].view(np.uint64), outs[1]["node_charge"].view(np.uint64))
+    o = O.OracleFemPIC(hm, dist, fill="Sort_Periodic", fill_period=5)
+    for s in range(steps):
+        o.step(tables[s])
+    n = o.size
+    np.testing.assert_array_equal(outs[0]["p2c"], o.p2c[:n])
+    np.testing.assert_array_equal(outs[0]["lc"].view(np.uint64), o.lc[:n].view(np.uint64))
+    err = np.abs(outs[0]["node_charge"] - o.node_charge) / np.maximum(np.abs(o.node_charge), 1.0)
+    assert err.max() <= 1e-12
+
+
 def test_fempic_app_global_move_matches_reference_golden(tmp_path):
     """The app with opp_global_move on (opp::BoundingBox + opp_init_direct_hop_cg, the
     reference app's set-up) against the reference seq backend's own global-move run
