@@ -133,3 +133,26 @@ def test_errors_reported():
     dev2.step(max_hops=64)
     st = dev2.status_host()
     assert st.error == L.OPPB_ERR_HOP_LIMIT and st.error_index == 0
+
+
+def test_verify_kernel_invariant_on_a_large_batch():
+    """The reference's verify_kernel (apps/app_neso_advection/kernels.h:115-151) after many steps
+    of a batch of larger instances: every particle's position lies in the closed box
+    [ix w, ix w + w] x [iy w, iy w + w] of its cell (ix, iy) = (cell mod nx, cell div nx), so the
+    incorrect count is 0."""
+    specs = [(128, 96, 1.0, 0.5, 60, 0.5), (200, 64, 0.25, 0.1, 25, 1.0), (33, 257, 0.7, 0.3, 40, 0.8),
+             (256, 256, 1.0, 0.5, 20, 0.5)]
+    meshes, _, dev = _build(specs, seed0=40)
+    dev.zero_status()
+    for _ in range(40):
+        dev.step()
+    torch.cuda.synchronize()
+    assert dev.status_host().error == 0
+    for k, m in enumerate(meshes):
+        got = dev.host_instance(k)
+        ix, iy = got["p2c"] % m.nx, got["p2c"] // m.nx
+        w = m.cell_width
+        llx, lly = ix * w, iy * w  # the reference's boundary_ll, in FP64
+        x, y = got["pos"][:, 0], got["pos"][:, 1]
+        incorrect = (ix < 0) | (iy < 0) | (x < llx) | (x > llx + w) | (y < lly) | (y > lly + w)
+        assert int(incorrect.sum()) == 0, (k, int(incorrect.sum()))
