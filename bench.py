@@ -190,7 +190,8 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     tuned = {"move": tune_move(sim, with_push=False).report(), "sort": tune_sort(sim).report()}
     # The deterministic deposit (integer fixed-point node sums) on the same state, for the record.
     from oppb.autotune import time_move
-    tuned["deterministic_deposit_ms"] = time_move(sim, L.DEPOSIT_EXACT, with_push=False)
+    t_exact = time_move(sim, L.DEPOSIT_EXACT, with_push=False)
+    tuned["deterministic_deposit_ms"] = t_exact if t_exact == t_exact else None  # NaN: not measured
     log(f"[{precision}] autotune move {tuned['move']['choice']} sort cols {tuned['sort']['choice']}")
     # Inputs of the timed steps generated before timing (device-resident).
     tables = [device_randoms(torch.empty_like(rnd_buf)) for _ in range(min(steps, 16))]

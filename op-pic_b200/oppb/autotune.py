@@ -61,6 +61,15 @@ class ParticleSnapshot:
         self.sim.node_charge.zero_()
 
 
+def snapshot_fits(sim, headroom: float = 1.25) -> bool:
+    """Whether a ParticleSnapshot of sim (a copy of every particle dat over [0, size)) fits in
+    the device's free memory with some headroom."""
+    p = sim.parts
+    nbytes = sum(getattr(p, name)[:, :p.size].numel() * getattr(p, name).element_size() for name, _, _ in p.DATS)
+    free, _ = torch.cuda.mem_get_info(sim.device)
+    return nbytes * headroom <= free
+
+
 def _timed(fn) -> float:
     s = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -77,9 +86,13 @@ def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None
     state, pushed as a step pushes it (so the walks have a step's hops): timed with the push as
     its prologue when with_push (default: when sim fuses the push), else the move launch alone
     after an untimed push.  Sets the fastest; sim's state is left as found."""
-    snap = ParticleSnapshot(sim)
     before = L.Tuning()
     L.load().oppb_get_tuning(C.byref(before))
+    cands = candidates or MOVE_CANDIDATES
+    if not snapshot_fits(sim):  # keep the current choice rather than run out of device memory
+        cur = (before.deposit, before.replicas)
+        return TuneResult(choice=cur if cur in cands else cands[0])
+    snap = ParticleSnapshot(sim)
     fused = sim.fused_push if with_push is None else with_push
 
     def run(c) -> float:
@@ -91,7 +104,7 @@ def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None
         return _timed(sim.move)
 
     try:
-        res = pick(candidates or MOVE_CANDIDATES, run, reps)
+        res = pick(cands, run, reps)
     except Exception:
         L.load().oppb_set_tuning(C.byref(before))
         raise
@@ -103,11 +116,12 @@ def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None
 
 def time_move(sim, deposit: int, replicas: int = 1, reps: int = 3, with_push: bool | None = None) -> float:
     """Median milliseconds of sim's move + deposit launch with the given deposit strategy, timed as
-    tune_move times its candidates; the tuning and sim's state are left as found."""
+    tune_move times its candidates (NaN when the state's snapshot does not fit in device memory);
+    the tuning and sim's state are left as found."""
     before = L.Tuning()
     L.load().oppb_get_tuning(C.byref(before))
     try:
-        return tune_move(sim, [(deposit, replicas)], reps, with_push).times_ms[(deposit, replicas)]
+        return tune_move(sim, [(deposit, replicas)], reps, with_push).times_ms.get((deposit, replicas), float("nan"))
     finally:
         L.load().oppb_set_tuning(C.byref(before))
 

@@ -31,3 +31,26 @@ def test_pick_ties_and_errors():
 def test_candidate_sets():
     assert len(set(MOVE_CANDIDATES)) == len(MOVE_CANDIDATES) == 8
     assert all(1 <= c <= 16 for c in SORT_CANDIDATES) and SORT_CANDIDATES[0] == 16
+
+
+def test_snapshot_fits_counts_live_columns(monkeypatch):
+    """snapshot_fits compares the bytes of every particle dat over [0, size) (with headroom)
+    against the free device memory the driver reports."""
+    import types
+
+    import torch
+
+    from oppb import autotune as A
+
+    class Parts:
+        DATS = (("pos", 3, torch.float64), ("p2c", 1, torch.int32))
+        size = 1000
+        pos = torch.zeros(3, 4000, dtype=torch.float64)
+        p2c = torch.zeros(1, 4000, dtype=torch.int32)
+
+    sim = types.SimpleNamespace(parts=Parts(), device="cpu")
+    need = 1000 * (3 * 8 + 4)
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (int(need * 1.25), 1 << 40))
+    assert A.snapshot_fits(sim)
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (need, 1 << 40))
+    assert not A.snapshot_fits(sim)
