@@ -20,7 +20,10 @@
 // (kDepWarp), or adds into a per-CTA shared-memory node table flushed once per node
 // (kDepTable).  The atomics of CTA b go to node-sum copy b % R (copy 0 = node_charge,
 // copies 1..R-1 in the caller's workspace) so that neighbouring CTAs, which deposit on the
-// same nodes, do not serialise on one address; the copies are added afterwards.
+// same nodes, do not serialise on one address; the copies are added afterwards.  The
+// deterministic mode (kDepExact) groups lanes the same way but sums weights cut to
+// multiples of 2^-52 as integers, with 64-bit integer atomics into two sums per node that a
+// finishing kernel turns into FP64: the result does not depend on the order of the additions.
 
 #include "oppb_common.cuh"
 #include "oppb_dh.h"
