@@ -143,9 +143,6 @@ class DeviceMesh:
         self.dist = t(dist if dist is not None else np.zeros(hm.n_ifaces, np.int32), torch.int32)
         self.inlet = L.Inlet(hm.n_ifaces, _ptr(self.dist), _ptr(self.if2c), _ptr(self.if_geom))
 
-    def set_distribution(self, dist: np.ndarray) -> None:
-        self.dist.copy_(torch.from_numpy(np.ascontiguousarray(dist, np.int32)))
-
 
 class DirectHopGrid:
     """The direct-hop seed's structured grid (include/oppb_dh.h), built on the device once:
