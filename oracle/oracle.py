@@ -74,6 +74,24 @@ def deposit(lc, p2c, c2n, node_charge, n=None):
     load().oracle_deposit(n, _p(lc), _p(p2c), _p(c2n), _p(node_charge))
 
 
+def deposit_exact(lc, p2c, c2n, n_nodes):
+    """The node charges of the deterministic deposit mode (OPPB_DEPOSIT_EXACT), from its
+    definition: each weight w cut to floor(w 2^52) 2^-52 and the cut weights of a node added
+    exactly (integers), the total rounded once to FP64.  lc [n][4], p2c [n] (REMOVED
+    particles skipped), c2n [cells][4]; weights |w| < 2^11.  The reference sums the uncut
+    weights sequentially in FP64 (deposit above); the two differ by the cut and that
+    rounding."""
+    keep = p2c != REMOVED
+    units = np.floor(np.asarray(lc)[keep] * 2.0 ** 52).astype(np.int64)  # exact: |w| 2^52 < 2^63
+    nodes = np.asarray(c2n)[p2c[keep]]
+    total = np.zeros(n_nodes, dtype=object)
+    for k in range(4):  # one column at a time keeps each int64 partial sum small
+        part = np.zeros(n_nodes, dtype=np.int64)
+        np.add.at(part, nodes[:, k], units[:, k])
+        total += part.astype(object)
+    return np.array([float(int(v)) * 2.0 ** -52 for v in total])
+
+
 def push(p2c, c_ef, pos, vel, qm, dt, n=None, mixed=False):
     n = len(p2c) if n is None else n
     fn = load().oracle_push_mixed if mixed else load().oracle_push

@@ -1,6 +1,6 @@
 """The deterministic deposit (OPPB_DEPOSIT_EXACT): node charges equal, bit for bit, the
-correctly rounded sum of the weights cut to multiples of 2^-52, computed here in integers from
-the oracle's FP64 weights; they do not change when the particles are permuted, and whole FemPIC
+correctly rounded sum of the weights cut to multiples of 2^-52 (the oracle's deposit_exact,
+integer sums of the stored weights); they do not change when the particles are permuted, and whole FemPIC
 steps repeat bit for bit.  Against the oracle's sequential FP64 sums they agree within 1e-12
 of max(|q|, 1)."""
 from __future__ import annotations
@@ -25,19 +25,6 @@ def exact_mode():
     L.set_tuning(deposit=L.DEPOSIT_EXACT)
     yield
     L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC, replicas=8)
-
-
-def exact_sums(lc: np.ndarray, p2c: np.ndarray, c2n: np.ndarray, n_nodes: int) -> np.ndarray:
-    """sum_i floor(w_i 2^52) per node in integers, rounded once to FP64 and scaled by 2^-52."""
-    keep = p2c != REMOVED
-    units = np.floor(lc[keep] * 2.0 ** 52).astype(np.int64)  # exact: |w| < 2^11
-    acc = np.zeros(n_nodes, dtype=object)
-    nodes = c2n[p2c[keep]]
-    for k in range(4):
-        part = np.zeros(n_nodes, dtype=np.int64)
-        np.add.at(part, nodes[:, k], units[:, k])  # per column below 2^63 for these sizes
-        acc += part.astype(object)
-    return np.array([float(int(v)) * 2.0 ** -52 for v in acc])
 
 
 def _load(ps, pos, p2c):
@@ -74,7 +61,7 @@ def test_exact_deposit_bit_exact_and_order_free(kind, n, seed):
     q = _move_deposit(dm, ps, kind)
     got = ps.host_aos()
     # the integer sums of the weights the kernel stored (FP64 lambdas, or FP32 ones widened)
-    ref = exact_sums(got["lc"], got["p2c"], hm.c2n, hm.n_nodes)
+    ref = O.deposit_exact(got["lc"], got["p2c"], hm.c2n, hm.n_nodes)
     np.testing.assert_array_equal(q.view(np.uint64), ref.view(np.uint64))
     # any particle order gives the same charges
     perm = np.random.default_rng(seed + 7).permutation(n)

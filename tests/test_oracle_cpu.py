@@ -200,3 +200,30 @@ def test_dh_oracle_matches_live_reference():
         assert R.fnv1a(o.p2c[:n]) == int(rec["h_p2c"]), s
         assert R.fnv1a(o.lc[:n]) == int(rec["h_lc"]), s
         assert R.fnv1a(o.node_charge) == int(rec["h_charge"]), s
+
+
+def test_oracle_deposit_exact_definition():
+    """deposit_exact against exact rational arithmetic on a small case: per node, the sum of
+    floor(w 2^52) 2^-52 over its particles' weights, rounded once to FP64; removed particles
+    skipped; and within a few FP64 rounding units of the oracle's sequential deposit."""
+    from fractions import Fraction
+
+    rng = np.random.default_rng(4)
+    n_cells, n_nodes, n = 40, 30, 500
+    c2n = np.stack([rng.choice(n_nodes, 4, replace=False) for _ in range(n_cells)]).astype(np.int32)
+    p2c = rng.integers(0, n_cells, n).astype(np.int32)
+    p2c[::17] = O.REMOVED
+    lc = rng.uniform(-1e-10, 1.0, (n, 4))
+    lc[3] = [-2.0 ** -52 * 1.5, 2.0 ** -60, 0.3, 1.0]
+    got = O.deposit_exact(lc, p2c, c2n, n_nodes)
+    ref = [Fraction(0)] * n_nodes
+    for i in range(n):
+        if p2c[i] == O.REMOVED:
+            continue
+        for k in range(4):
+            ref[c2n[p2c[i], k]] += Fraction(int(np.floor(lc[i, k] * 2.0 ** 52)), 2 ** 52)
+    np.testing.assert_array_equal(got, np.array([float(r) for r in ref]))  # float(Fraction) rounds once
+    keep = p2c != O.REMOVED
+    seq = np.zeros(n_nodes)
+    O.deposit(np.ascontiguousarray(lc[keep]), np.ascontiguousarray(p2c[keep]), c2n, seq)
+    assert np.abs(got - seq).max() <= 1e-13
