@@ -215,7 +215,7 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     for k in range(steps):
         ev = [E() for _ in range(5)]
         sim.inject(tables[k % len(tables)])
-        sim.node_charge.zero_()
+        sim.zero_node_charge()
         ev[4].record(s)
         sim.push()
         n_alive = sim.parts.size
@@ -290,7 +290,7 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     for k in range(n_fused):
         ev = [E() for _ in range(4)]
         sim.inject(tables[k % len(tables)])
-        sim.node_charge.zero_()
+        sim.zero_node_charge()
         n_alive = sim.parts.size
         ev[0].record(s)
         sim.push_move()
@@ -335,7 +335,7 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
         # One more step up to the push, then a contiguous slice of the particles as the
         # CPU sample (positions after the push, cells before the move).
         sim.inject(tables[0])
-        sim.node_charge.zero_()
+        sim.zero_node_charge()
         sim.push()
         m = sim.parts.size
         k = min(m, 1_000_000)
@@ -476,9 +476,9 @@ def arm_ours(args) -> dict:
         "vs_baseline": None,
         "dtype": "f32+f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cells": hm.n_cells, "nodes": hm.n_nodes,
-                   "mean_particles": round(mixed["mean_particles"]), "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (particle dats ~4 GB), no flush"},
+        "config": workload_config(),
+        "parallelism": f"replicas x{world}",
+        "mean_particles": round(mixed["mean_particles"]),
         "plain_fp64": {"value": f64["job_value"], "move_only": f64["move_only"], "whole_step": f64["whole_step"],
                        "ms_per_step": f64["ms_per_step"], "move_ms_per_launch": f64["move_ms_per_launch"],
                        "move_gbs": f64["move_gbs"], "frac_of_hbm": f64["move_gbs"] / peaks["hbm_gbs"],
@@ -569,7 +569,7 @@ def run_direct_hop(hm, dev, steps: int, warmup: int, seed: int, cpu: bool) -> di
     for k in range(steps):
         ev = [E() for _ in range(4)]
         sim.inject(tables[k % len(tables)])
-        sim.node_charge.zero_()
+        sim.zero_node_charge()
         n_alive = sim.parts.size
         ev[0].record(s)
         sim.push_move()
@@ -1021,78 +1021,100 @@ def advec_cpu_baseline() -> dict:
 
 # ------------------------------------------------------------------------ reference arm
 
-def _reference_line(args, value: float, ms_per_step: float, particles_per_step: float, kind: str, cores: int,
-                    sample: str) -> dict:
+def workload_config() -> dict:
+    """The bench line's config: the workload alone, the same object in both arms."""
+    return {"workload": WORKLOAD, "cells": 6 * CFG["nx"] * CFG["ny"] * CFG["nz"],
+            "nodes": (CFG["nx"] + 1) * (CFG["ny"] + 1) * (CFG["nz"] + 1), "inject_per_step": CFG["inject"],
+            "fill_steps": CFG["fill_steps"], "sort_period": CFG["period"],
+            "l2": "inputs larger than L2 (particle dats ~4 GB), no flush"}
+
+
+def arm_reference(args) -> dict:
+    """The reference's own CPU path on the same workload: the compiled OP-PIC omp backend with
+    the generated FemPIC loops (oracle/_ref/fempic_ref_omp) on every host thread.  The mesh is
+    the same box, written as the app's text mesh files and loaded by the app's own loader
+    (load_mesh, fempic_misc_mesh_loader.h); the injection distribution is the workload's; the
+    field is the exact static field of the workload's Laplace problem; the randoms come from
+    the harness's seeded generator.  Per step: inject -> push -> move (with its hole fill or
+    cell sort, Sort_Periodic every 10 steps) -> deposit, all the reference's code; the fill
+    steps reach the steady state, then W warm-up and K timed steps, timing move (+ compaction)
+    and deposit with the harness's clock.  Nothing of this library is loaded.  Without the
+    compiled reference it runs the C oracle port on the oracle's restatement of the loader."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return {}
+    from oracle import ref_runner as R
+
+    dims = (CFG["nx"], CFG["ny"], CFG["nz"], CFG["lx"], CFG["ly"], CFG["lz"])
+    fill, w, k = CFG["fill_steps"], args.warmup, args.steps
+    cores = len(os.sched_getaffinity(0))
+    if R.available("omp"):
+        out = R.run_box("omp", dims, CFG["inject"], fill + w + k, fill=CFG["fill"], period=CFG["period"],
+                        alloc_mult=REF_ALLOC_MULTIPLE, threads=cores, seed=CFG["seed"], dt=CFG["dt"], qm=CFG["qm"],
+                        ion_velocity=CFG["v_ion"], sigma=CFG["sigma"])
+        recs = out["records"][fill + w:]
+        t = float((recs["t_move"] + recs["t_deposit"]).sum())
+        ps = float(recs["size_before_move"].sum())
+        kind = "reference"
+        sample = (f"the whole workload: {fill} fill steps + {w} warm-up + {k} timed steps at "
+                  f"{CFG['inject']:,} ions per step; compiled OP-PIC omp backend + generated FemPIC loops, "
+                  f"OMP_NUM_THREADS={cores}; mesh from the app's loader")
+    else:
+        ps, t, cores = reference_port(fill, w, k)
+        kind = "port"
+        sample = f"{fill} fill + {w} warm-up + {k} timed steps; C oracle, one thread"
+    value = ps / t
     return {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"first {args.ref_fill_steps} steps of injection (inlet region "
-                                                  f"at steady-state density), {round(particles_per_step)} "
-                                                  f"particles per step"},
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": k,
+        "warmup": w, "ms_per_step": 1e3 * t / k, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "mean_particles": round(ps / k),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
-def arm_reference_compiled(args, hm, dist) -> dict:
-    """The compiled OP-PIC omp backend with the generated FemPIC loops (oracle/_ref), on
-    every host thread: per step inject -> push -> move with its finalize -> deposit, the
-    move (with hole fill / sort) and the deposit timed by the harness."""
-    from oracle import ref_runner as R
-
-    fill = args.ref_fill_steps
-    cores = len(os.sched_getaffinity(0))
-    out = R.run("omp", hm, dist, fill + args.warmup + args.steps, [], fill=CFG["fill"], period=CFG["period"],
-                alloc_mult=2.0, record_state=False, threads=cores, dt=CFG["dt"], qm=CFG["qm"],
-                ion_velocity=CFG["v_ion"], sigma=CFG["sigma"])
-    recs = out["records"][fill + args.warmup:]
-    t = float((recs["t_move"] + recs["t_deposit"]).sum())
-    ps = float(recs["size_before_move"].sum())
-    return _reference_line(args, ps / t, 1e3 * t / args.steps, ps / args.steps, "reference", cores,
-                           f"{fill}+{args.warmup} fill steps then {args.steps} timed steps; compiled OP-PIC omp "
-                           f"backend + generated FemPIC loops, OMP_NUM_THREADS={cores}")
+# opp_allocation_multiple of the reference's FemPIC configuration (apps_codegen/app_fempic_cg/configs/coarse.param).
+REF_ALLOC_MULTIPLE = 11.0
 
 
-def arm_reference(args) -> dict:
-    """The reference's CPU path on a bounded sample: config mesh, FILL steps of 250,000
-    injected ions (the inlet region then holds the steady-state density), then
-    W + K steps, timing move + compaction + deposit.  The compiled reference (oracle/_ref)
-    when it is present, else the C oracle."""
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return {}
-    import numpy as np
-
-    from oppb.fempic import HostMesh, injection_randoms
+def reference_port(fill: int, warmup: int, steps: int) -> tuple[float, float, int]:
+    """The C oracle (one thread) on the workload, its mesh from the oracle's restatement of the
+    app's loader: (particle-steps, seconds of move + compaction + deposit, cores)."""
+    from oracle import mesh as OM
     from oracle import oracle as O
-    from oracle import ref_runner as R
 
-    fill = args.ref_fill_steps
-    hm = HostMesh(CFG["nx"], CFG["ny"], CFG["nz"], CFG["lx"], CFG["ly"], CFG["lz"])
-    dist = hm.inject_distribution(CFG["inject"])
-    if R.available("omp"):
-        return arm_reference_compiled(args, hm, dist)
+    hm = OM.box_mesh(CFG["nx"], CFG["ny"], CFG["nz"], CFG["lx"], CFG["ly"], CFG["lz"])
+    hm.c_ef = OM.static_field(hm, 1.0, 0.0, CFG["lz"])
+    dist = OM.area_distribution(hm.if_area, CFG["inject"])
     orc = O.OracleFemPIC(hm, dist, ion_velocity=CFG["v_ion"], qm=CFG["qm"], dt=CFG["dt"], fill=CFG["fill"],
                          fill_period=CFG["period"], alloc_mult=2.0)
-    for s in range(fill + args.warmup):
-        orc.step(injection_randoms(CFG["seed"], s, CFG["inject"], CFG["sigma"]))
+    rng = __import__("numpy").random.default_rng(CFG["seed"])
+
+    def table():
+        import numpy as np
+
+        out = np.empty((CFG["inject"], 5))
+        out[:, 0:2] = rng.random((CFG["inject"], 2))
+        out[:, 2:5] = CFG["sigma"] * rng.standard_normal((CFG["inject"], 3))
+        return out
+
+    for _ in range(fill + warmup):
+        orc.step(table())
     ps, t = 0, 0.0
-    for k in range(args.steps):
-        rnd = injection_randoms(CFG["seed"], fill + args.warmup + k, CFG["inject"], CFG["sigma"])
-        orc.inject(rnd)
+    for _ in range(steps):
+        orc.inject(table())
         orc.node_charge[:] = 0
         O.push(orc.p2c, hm.c_ef, orc.pos, orc.vel, orc.qm, orc.dt, n=orc.size)
         n_alive = orc.size
         t0 = time.perf_counter()
-        rc, visits, _ = O.move(orc.pos, orc.lc, orc.p2c, hm.c2c, hm.c_vol, hm.c_det, n=orc.size)
+        rc, _, _ = O.move(orc.pos, orc.lc, orc.p2c, hm.c2c, hm.c_vol, hm.c_det, n=orc.size)
         orc.finalize(rc)
         O.deposit(orc.lc, orc.p2c, hm.c2n, orc.node_charge, n=orc.size)
         t += time.perf_counter() - t0
         orc.iter += 1
         ps += n_alive
-    return _reference_line(args, ps / t, 1e3 * t / args.steps, ps / args.steps, "port", 1,
-                           f"{fill}+{args.warmup} fill steps then {args.steps} timed steps; C oracle")
+    return ps, t, 1
 
 
 def main():
@@ -1104,7 +1126,6 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
-    ap.add_argument("--ref-fill-steps", type=int, default=20)
     ap.add_argument("--fill-steps", type=int, default=CFG["fill_steps"], help="steps to reach the steady state")
     ap.add_argument("--capacity", type=int, default=CFG["capacity"], help="particle set capacity")
     ap.add_argument("--precision", choices=["both", "f64", "mixed"], default="both")

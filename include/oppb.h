@@ -291,7 +291,9 @@ int oppb_hole_fill(int32_t size, int32_t remove_count, const uint32_t* remove_bi
  * the library, held until the process exits; remove_count above
  * OPPB_HOLE_FILL_STATIC_MAX_REMOVES returns OPPB_ERR_SCRATCH_LIMIT and changes nothing.
  * The first call on each device looks the array's device address up with that device
- * current; make that first call before any stream capture begins.  All calls on a device
+ * current; make that first call before any stream capture begins.  Calls outside a capture
+ * look the address up again, so the entry point stays valid after cudaDeviceReset once a
+ * call outside a capture has been made on the reset device.  All calls on a device
  * share the one array, so calls that may overlap on the GPU (other streams, other host
  * threads) race and must be ordered by the caller. */
 int oppb_hole_fill_static(int32_t size, int32_t remove_count, const uint32_t* remove_bits,

@@ -104,14 +104,22 @@ def build_oracle(force: bool = False) -> Path:
     return so
 
 
+def reference_dir() -> Path:
+    """Root of the OP-PIC source tree: the OPPB_REFERENCE_DIR environment variable, else a
+    `reference` directory beside this repository."""
+    env = os.environ.get("OPPB_REFERENCE_DIR")
+    return Path(env) if env else ROOT.parent / "reference"
+
+
 def build_reference(force: bool = False) -> bool:
     """Compile the reference seq/omp backends + harness into oracle/_ref (needs the
     reference sources; skipped when they are absent)."""
-    if not Path("/root/reference/opp_lib").is_dir() or shutil.which("make") is None:
+    ref = reference_dir()
+    if not (ref / "opp_lib").is_dir() or shutil.which("make") is None:
         return False
     if not (ROOT / "oracle" / "Makefile").exists():
         return False
-    args = ["make", "-s", "-C", str(ROOT / "oracle"), "-j8"]
+    args = ["make", "-s", "-C", str(ROOT / "oracle"), "-j8", f"REF={ref}"]
     if force:
         args.append("-B")
     _run(args)

@@ -237,18 +237,26 @@ constexpr int kStaticMaxDevices = 64;
 std::mutex g_static_mu;
 int32_t* g_static_addr[kStaticMaxDevices];  // device address of g_hole_fill_scratch, per device
 
-// Device address of the scratch array on the current device, looked up on the first call
-// for that device.  In host code the array's name only stands in for the symbol; a kernel
-// must be given this address instead.
-int static_scratch(int32_t** out) {
+// Device address of the scratch array on the current device.  In host code the array's name
+// only stands in for the symbol; a kernel must be given this address instead.  It is looked
+// up again on every call made outside a stream capture (cheap once the module is loaded), so
+// that a device reset, which unloads the module and may place the array elsewhere when it is
+// loaded again, never leaves a stale address behind; a call inside a capture uses the address
+// found by the last call outside one.
+int static_scratch(cudaStream_t stream, int32_t** out) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         return OPPB_ERR_NO_DEVICE;
     }
     if (dev < 0 || dev >= kStaticMaxDevices) return OPPB_ERR_NO_DEVICE;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        return OPPB_ERR_LAUNCH;
+    }
     std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_addr[dev]) {
+    if (!g_static_addr[dev] || cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_hole_fill_scratch);
         if (e != cudaSuccess || !p) {
@@ -282,8 +290,9 @@ extern "C" int oppb_hole_fill_static(int32_t size, int32_t remove_count, const u
         dl.bytes[d] = dats[d].elem_bytes;
         dl.total_cols += dats[d].dim;
     }
+    cudaStream_t s = as_stream(stream);
     int32_t* scratch = nullptr;
-    const int rc = static_scratch(&scratch);
+    const int rc = static_scratch(s, &scratch);
     if (rc != OPPB_OK) return rc;
     const int64_t n_words = ceil_div(size, 32);
     const int n_blocks = ceil_div(n_words, kHfWords);  // <= kStaticMaxBlocks for any int32 size
@@ -291,7 +300,6 @@ extern "C" int oppb_hole_fill_static(int32_t size, int32_t remove_count, const u
     int32_t* hole_list = scratch + kStaticBaseWords;
     int32_t* mover_list = hole_list + kStaticListWords;
 
-    cudaStream_t s = as_stream(stream);
     hf_count_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base);
     scan_single_block_kernel<<<1, kScanBlock, 0, s>>>(block_base, n_blocks);
     hf_emit_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base, n_blocks, remove_count,

@@ -58,7 +58,7 @@ class ParticleSnapshot:
         p = self.sim.parts
         for name, t in self.saved.items():
             getattr(p, name)[:, :t.shape[1]].copy_(t)
-        self.sim.node_charge.zero_()
+        self.sim.zero_node_charge()
 
 
 def snapshot_fits(sim, headroom: float = 1.25) -> bool:

@@ -206,8 +206,9 @@ class CabanaDevice:
 
     def move_deposit(self, deck: Deck, max_hops: int = 4096, stream=None, zero_acc: bool = True) -> None:
         """opp_reset_dat(c_acc) + opp_particle_move__move_deposit_kernel."""
-        if zero_acc:
-            self.acc.zero_()
+        if zero_acc:  # with the library's fill kernel, so that the call launches only library kernels
+            L.check("oppb_fill", L.load().oppb_fill(_ptr(self.acc), self.acc.numel(), 8, 0,
+                                                    None if stream is None else stream.cuda_stream))
         v = self.view()
         k = deck.consts()
         sp = None if stream is None else stream.cuda_stream

@@ -322,6 +322,11 @@ class FemPIC:
             C.byref(self.mesh.s), C.byref(self.mesh.inlet), C.byref(v), start, count, _ptr(rnd_soa),
             rnd_soa.stride(0), rnd_soa.shape[0], self.ion_velocity, self.qm, self.dt, _stream_ptr(stream)))
 
+    def zero_node_charge(self, stream=None) -> None:
+        """opp_reset_dat(n_charge_den) with the library's fill kernel (oppb_fill)."""
+        L.check("oppb_fill", self.lib.oppb_fill(_ptr(self.node_charge), self.node_charge.numel(), 8, 0,
+                                                _stream_ptr(stream)))
+
     def push(self, stream=None) -> None:
         v = self.parts.view()
         fn = self.lib.oppb_push_mixed if self.precision == "mixed" else self.lib.oppb_push_f64
@@ -443,7 +448,7 @@ class FemPIC:
         s = stream if stream is not None else torch.cuda.current_stream()
         if ev: ev[0].record(s)
         self.inject(rnd_soa, stream)
-        self.node_charge.zero_()
+        self.zero_node_charge(stream)
         if ev: ev[1].record(s)
         n_before = self.parts.size
         if self.fused_push:

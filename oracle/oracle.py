@@ -83,13 +83,15 @@ def deposit_exact(lc, p2c, c2n, n_nodes):
     rounding."""
     keep = p2c != REMOVED
     units = np.floor(np.asarray(lc)[keep] * 2.0 ** 52).astype(np.int64)  # exact: |w| 2^52 < 2^63
-    nodes = np.asarray(c2n)[p2c[keep]]
-    total = np.zeros(n_nodes, dtype=object)
-    for k in range(4):  # one column at a time keeps each int64 partial sum small
-        part = np.zeros(n_nodes, dtype=np.int64)
-        np.add.at(part, nodes[:, k], units[:, k])
-        total += part.astype(object)
-    return np.array([float(int(v)) * 2.0 ** -52 for v in total])
+    nodes = np.asarray(c2n)[p2c[keep]].ravel()
+    units = units.ravel()
+    # Each cut weight is hi 2^32 + lo with hi = units >> 32 (|hi| < 2^31) and lo in [0, 2^32):
+    # int64 sums of either part cannot wrap for fewer than 2^31 terms, whatever a node's total.
+    hi = np.zeros(n_nodes, dtype=np.int64)
+    lo = np.zeros(n_nodes, dtype=np.int64)
+    np.add.at(hi, nodes, units >> 32)
+    np.add.at(lo, nodes, units & 0xFFFFFFFF)
+    return np.array([float(int(h) * 2 ** 32 + int(l)) * 2.0 ** -52 for h, l in zip(hi, lo)])
 
 
 def push(p2c, c_ef, pos, vel, qm, dt, n=None, mixed=False):

@@ -5,11 +5,26 @@
 // particle part of the generated main loop (apps_codegen/app_fempic_cg/fempic_opp.cpp:160-215):
 //   opp_inc_part_count_with_distribution -> inject_ions (+ thermal velocity from the case)
 //   -> reset n_charge_den -> calculate_new_pos_vel -> move (with its finalize) -> deposit.
-// The field is the static cell field of the case (no field solve).  A direct-hop case
-// turns on the global move (opp_init_direct_hop_cg builds the structured map by the
-// reference's own search) and the output ends with the reference's grid and map.  Per step it records
-// sizes and wall times and, unless the case is a timing case (record_state 0), FNV-1a
-// hashes of the particle dats and of the node charges.
+// The field is a static cell field (no field solve).  A direct-hop case turns on the global
+// move (opp_init_direct_hop_cg builds the structured map by the reference's own search) and
+// the output ends with the reference's grid and map.  Per step it records sizes and wall
+// times and, unless the case is a timing case (record_state 0), FNV-1a hashes of the
+// particle dats and of the node charges.
+//
+// Two kinds of case file:
+//   OPPBCAS1  mesh arrays, injection distribution and random tables supplied by the caller;
+//   OPPBBOX1  a box of nx*ny*nz hexahedra cut into 6 tetrahedra each: the harness writes the
+//             box as the app's text mesh files (node list in mm, 304 tetrahedra, the 203
+//             inlet triangles at z=0 and the z=lz wall nodes) at the paths the params file
+//             names (global_mesh, inlet_mesh, wall_mesh), and the mesh then comes from the
+//             app's own loader, load_mesh() of apps_codegen/app_fempic_cg/fempic_misc_mesh_loader.h
+//             (LoadVolumeMesh / LoadSurfaceMesh of minifempic_funcs.h): connectivity flip,
+//             alpha..delta cofactors, volumes, face neighbours, node volumes and types, inlet
+//             cells and normals are all the reference's.  With mesh_only set the harness writes
+//             those arrays and stops; otherwise it runs the step loop on them with the
+//             workload's injection distribution, the exact field of its Laplace problem and
+//             randoms from its own seeded generator.  No code of the library under test is
+//             involved.
 //
 //   ref_harness <opp params file> <case file> <out file>
 //
@@ -26,6 +41,7 @@
 #include <vector>
 
 #include "opp_lib.h"
+#include "fempic_misc_mesh_loader.h"
 
 void opp_par_loop_injected__inject_ions_kernel(opp_set, opp_arg, opp_arg, opp_arg, opp_arg, opp_arg, opp_arg,
                                                opp_arg, opp_arg, opp_arg, opp_arg);
@@ -77,6 +93,102 @@ struct StepRecord {
     double t_inject, t_push, t_move, t_deposit;
 };
 
+// A box case: the workload's mesh dimensions, injection and constants.
+struct BoxHeader {
+    char magic[8];
+    int32_t nx, ny, nz, inject, steps, record_state, mesh_only, seed;
+    double lx, ly, lz, dt, qm, ion_velocity, sigma, phi_inlet, phi_fixed;
+};
+
+// Writes the box as the app's text mesh files, in the formats LoadVolumeMesh and
+// LoadSurfaceMesh read (apps/app_fempic/minifempic_funcs.h:230-270,477-520): the node count and
+// element count, then "index x y z" per node (1-based, mm), then "index 304 n1 n2 n3 n4" per
+// tetrahedron; a surface file lists its nodes the same way and, for the inlet, its triangles
+// as "index 203 n1 n2 n3".  The workload's construction: node i + (nx+1)(j + (ny+1)k) at
+// (i hx, j hy, k hz) (the last node of an axis at the box length), hexahedron (i,j,k) cut
+// into 6 tetrahedra along its main diagonal, tetrahedron t walking 000 -> e_a -> e_a + e_b ->
+// 111 for the t-th permutation (a,b,c) of the axes in lexicographic order; per z=0 hexahedron
+// face the triangles (000, 110, 100) and (000, 010, 110); the z=lz nodes as the wall.
+bool write_box_files(const BoxHeader& b, const std::string& vol, const std::string& inlet,
+                     const std::string& wall) {
+    const int64_t NX = b.nx + 1, NY = b.ny + 1, NZ = b.nz + 1;
+    const double hx = b.lx / b.nx, hy = b.ly / b.ny, hz = b.lz / b.nz;
+    auto nid = [&](int64_t i, int64_t j, int64_t k) { return i + NX * (j + NY * k) + 1; };
+    auto coord = [](int64_t i, int n, double h, double l) { return (i == n) ? l : double(i) * h; };
+    auto node_line = [&](FILE* f, int64_t i, int64_t j, int64_t k) {
+        fprintf(f, "%lld %.17g %.17g %.17g\n", (long long)nid(i, j, k), coord(i, b.nx, hx, b.lx) * 1000.0,
+                coord(j, b.ny, hy, b.ly) * 1000.0, coord(k, b.nz, hz, b.lz) * 1000.0);
+    };
+    FILE* f = fopen(vol.c_str(), "w");
+    if (!f) return false;
+    const int64_t n_tets = 6 * (int64_t)b.nx * b.ny * b.nz;
+    fprintf(f, "%lld %lld\n", (long long)(NX * NY * NZ), (long long)n_tets);
+    for (int64_t k = 0; k < NZ; k++)
+        for (int64_t j = 0; j < NY; j++)
+            for (int64_t i = 0; i < NX; i++) node_line(f, i, j, k);
+    static const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    int64_t e = 1;
+    for (int64_t k = 0; k < b.nz; k++)
+        for (int64_t j = 0; j < b.ny; j++)
+            for (int64_t i = 0; i < b.nx; i++)
+                for (int t = 0; t < 6; t++) {
+                    int o[3] = {0, 0, 0};
+                    const int64_t v0 = nid(i, j, k);
+                    o[perm[t][0]] = 1;
+                    const int64_t v1 = nid(i + o[0], j + o[1], k + o[2]);
+                    o[perm[t][1]] = 1;
+                    const int64_t v2 = nid(i + o[0], j + o[1], k + o[2]);
+                    const int64_t v3 = nid(i + 1, j + 1, k + 1);
+                    fprintf(f, "%lld 304 %lld %lld %lld %lld\n", (long long)e++, (long long)v0, (long long)v1,
+                            (long long)v2, (long long)v3);
+                }
+    fclose(f);
+    f = fopen(inlet.c_str(), "w");
+    if (!f) return false;
+    fprintf(f, "%lld %lld\n", (long long)(NX * NY), (long long)(2 * (int64_t)b.nx * b.ny));
+    for (int64_t j = 0; j < NY; j++)
+        for (int64_t i = 0; i < NX; i++) node_line(f, i, j, 0);
+    e = 1;
+    for (int64_t j = 0; j < b.ny; j++)
+        for (int64_t i = 0; i < b.nx; i++) {
+            const long long n000 = nid(i, j, 0), n100 = nid(i + 1, j, 0), n010 = nid(i, j + 1, 0),
+                            n110 = nid(i + 1, j + 1, 0);
+            fprintf(f, "%lld 203 %lld %lld %lld\n", (long long)e++, n000, n110, n100);
+            fprintf(f, "%lld 203 %lld %lld %lld\n", (long long)e++, n000, n010, n110);
+        }
+    fclose(f);
+    f = fopen(wall.c_str(), "w");
+    if (!f) return false;
+    fprintf(f, "%lld 0\n", (long long)(NX * NY));
+    for (int64_t j = 0; j < NY; j++)
+        for (int64_t i = 0; i < NX; i++) node_line(f, i, j, b.nz);
+    fclose(f);
+    return true;
+}
+
+// The workload's injection distribution: cumulative counts per inlet face from the rounded
+// cumulative area share, the last face closing at `total`.
+std::vector<int> area_distribution(const double* area, int n_faces, int total) {
+    std::vector<int> dist(n_faces > 0 ? n_faces : 1, 0);
+    double sum = 0;
+    for (int f = 0; f < n_faces; f++) sum += area[f];
+    double acc = 0;
+    for (int f = 0; f < n_faces; f++) {
+        acc += area[f];
+        long long cum = (f == n_faces - 1) ? total : std::llround(double(total) * (acc / sum));
+        if (cum > total) cum = total;
+        dist[f] = (int)cum;
+    }
+    for (int f = 1; f < n_faces; f++)
+        if (dist[f] < dist[f - 1]) dist[f] = dist[f - 1];
+    return dist;
+}
+
+template <typename T>
+void put(FILE* o, const T* p, size_t n) {
+    if (n) fwrite(p, sizeof(T), n, o);
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -89,35 +201,106 @@ int main(int argc, char** argv) {
         fprintf(stderr, "cannot open %s\n", argv[2]);
         return 2;
     }
-    Header h;
-    if (fread(&h, sizeof h, 1, f) != 1 || memcmp(h.magic, "OPPBCAS1", 8) != 0) {
+    char magic[8];
+    if (fread(magic, 8, 1, f) != 1) {
         fprintf(stderr, "bad case file\n");
         return 2;
     }
-    const size_t nc = h.n_cells, nf = h.n_ifaces, nn = h.n_nodes;
-    auto c2n = read_vec<int>(f, nc * 4);
-    auto c2c = read_vec<int>(f, nc * 4);
-    auto c_det = read_vec<double>(f, nc * 16);
-    auto c_vol = read_vec<double>(f, nc);
-    auto c_ef = read_vec<double>(f, nc * 3);
-    auto if2c = read_vec<int>(f, nf);
-    auto if_u = read_vec<double>(f, nf * 3);
-    auto if_v = read_vec<double>(f, nf * 3);
-    auto if_norm = read_vec<double>(f, nf * 3);
-    auto if_n_pos = read_vec<double>(f, nf * 9);
-    auto if_dist = read_vec<int>(f, nf);
-    auto tables = read_vec<double>(f, (size_t)h.n_tables * h.inject * 5);
-    // Direct-hop cases: grid spacing, expansion[3] and the node positions follow the tables.
+    rewind(f);
+    char* args[2] = {argv[0], argv[1]};
+    Header h{};
+    std::vector<int> c2n, c2c, if2c, if_dist;
+    std::vector<double> c_det, c_vol, c_ef, if_u, if_v, if_norm, if_n_pos, tables;
     std::vector<double> dh_par(4, 0.0), n_pos;
-    if (h.direct_hop) {
-        dh_par = read_vec<double>(f, 4);
-        n_pos = read_vec<double>(f, nn * 3);
+    uint64_t rng = 0x5eedull;
+    if (memcmp(magic, "OPPBBOX1", 8) == 0) {
+        BoxHeader b{};
+        if (fread(&b, sizeof b, 1, f) != 1 || b.nx <= 0 || b.ny <= 0 || b.nz <= 0) {
+            fprintf(stderr, "bad box case\n");
+            return 2;
+        }
+        fclose(f);
+        opp_init(2, args);
+        if (!write_box_files(b, opp_params->get<OPP_STRING>("global_mesh"), opp_params->get<OPP_STRING>("inlet_mesh"),
+                             opp_params->get<OPP_STRING>("wall_mesh"))) {
+            fprintf(stderr, "cannot write the mesh files\n");
+            return 2;
+        }
+        std::shared_ptr<DataPointers> m = load_mesh();  // the app's loader
+        const size_t nn = m->n_nodes, nc = m->n_cells, nf = m->n_ifaces;
+        if (b.mesh_only) {
+            FILE* o = fopen(argv[3], "wb");
+            if (!o) return 2;
+            const int32_t counts[3] = {m->n_nodes, m->n_cells, m->n_ifaces};
+            put(o, counts, 3);
+            put(o, m->n_pos, nn * 3);
+            put(o, m->n_vol, nn);
+            put(o, m->n_type, nn);
+            put(o, m->c_to_n, nc * 4);
+            put(o, m->c_to_c, nc * 4);
+            put(o, m->c_det, nc * 16);
+            put(o, m->c_vol, nc);
+            put(o, m->c_centroid, nc * 3);
+            put(o, m->if_to_c, nf);
+            put(o, m->if_to_n, nf * 3);
+            put(o, m->if_u_norm, nf * 3);
+            put(o, m->if_v_norm, nf * 3);
+            put(o, m->if_norm, nf * 3);
+            put(o, m->if_area, nf);
+            put(o, m->if_n_pos, nf * 9);
+            fclose(o);
+            opp_exit();
+            return 0;
+        }
+        memcpy(h.magic, "OPPBCAS1", 8);
+        h.n_nodes = m->n_nodes, h.n_cells = m->n_cells, h.n_ifaces = m->n_ifaces;
+        h.inject = b.inject, h.steps = b.steps, h.n_tables = 0, h.record_state = b.record_state, h.direct_hop = 0;
+        h.dt = b.dt, h.qm = b.qm, h.ion_velocity = b.ion_velocity, h.sigma = b.sigma;
+        c2n.assign(m->c_to_n, m->c_to_n + nc * 4);
+        c2c.assign(m->c_to_c, m->c_to_c + nc * 4);
+        c_det.assign(m->c_det, m->c_det + nc * 16);
+        c_vol.assign(m->c_vol, m->c_vol + nc);
+        if2c.assign(m->if_to_c, m->if_to_c + nf);
+        if_u.assign(m->if_u_norm, m->if_u_norm + nf * 3);
+        if_v.assign(m->if_v_norm, m->if_v_norm + nf * 3);
+        if_norm.assign(m->if_norm, m->if_norm + nf * 3);
+        if_n_pos.assign(m->if_n_pos, m->if_n_pos + nf * 9);
+        if_dist = area_distribution(m->if_area, m->n_ifaces, b.inject);
+        // Static field: the Laplace problem (phi_inlet on the z=0 nodes, phi_fixed on the z=lz
+        // wall, natural boundary elsewhere) has the linear potential in z as its exact discrete
+        // solution, so every cell's field is -grad(phi) = (0, 0, (phi_inlet - phi_fixed) / lz).
+        c_ef.assign(nc * 3, 0.0);
+        for (size_t c = 0; c < nc; c++) c_ef[3 * c + 2] = (b.phi_inlet - b.phi_fixed) / b.lz;
+        rng ^= (uint64_t)(uint32_t)b.seed * 0x9e3779b97f4a7c15ull;
+    } else {
+        if (fread(&h, sizeof h, 1, f) != 1 || memcmp(h.magic, "OPPBCAS1", 8) != 0) {
+            fprintf(stderr, "bad case file\n");
+            return 2;
+        }
+        const size_t nc = h.n_cells, nf = h.n_ifaces, nn = h.n_nodes;
+        c2n = read_vec<int>(f, nc * 4);
+        c2c = read_vec<int>(f, nc * 4);
+        c_det = read_vec<double>(f, nc * 16);
+        c_vol = read_vec<double>(f, nc);
+        c_ef = read_vec<double>(f, nc * 3);
+        if2c = read_vec<int>(f, nf);
+        if_u = read_vec<double>(f, nf * 3);
+        if_v = read_vec<double>(f, nf * 3);
+        if_norm = read_vec<double>(f, nf * 3);
+        if_n_pos = read_vec<double>(f, nf * 9);
+        if_dist = read_vec<int>(f, nf);
+        tables = read_vec<double>(f, (size_t)h.n_tables * h.inject * 5);
+        // Direct-hop cases: grid spacing, expansion[3] and the node positions follow the tables.
+        if (h.direct_hop) {
+            dh_par = read_vec<double>(f, 4);
+            n_pos = read_vec<double>(f, nn * 3);
+        }
+        fclose(f);
+        opp_init(2, args);
     }
-    fclose(f);
+    const size_t nc = h.n_cells, nn = h.n_nodes;
     std::vector<double> n_charge(nn, 0.0);
 
-    char* args[2] = {argv[0], argv[1]};
-    opp_init(2, args);
     {
         opp_set node_set = opp_decl_set(h.n_nodes, "mesh_nodes");
         opp_set cell_set = opp_decl_set(h.n_cells, "mesh_cells");
@@ -171,7 +354,6 @@ int main(int argc, char** argv) {
         opp_increase_particle_count(dummy_part_set, h.inject);
         std::vector<double> thermal((size_t)h.inject * 3);
         std::vector<StepRecord> recs;
-        uint64_t rng = 0x5eedull;
         using clk = std::chrono::steady_clock;
         auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
 

@@ -1,6 +1,11 @@
 """TEST INFRASTRUCTURE ONLY — runs the compiled OP-PIC reference (oracle/_ref, built by
 oracle/Makefile from the reference sources) on a FemPIC case and reads back its per-step
 records (sizes, FNV-1a digests of the particle dats and node charges, wall times).
+
+Box cases (run_box, box_mesh) take the mesh from the reference app's own loader: the harness
+writes the box as the app's text mesh files and loads them with load_mesh()
+(apps_codegen/app_fempic_cg/fempic_misc_mesh_loader.h), so nothing of the library under test
+is involved.
 """
 from __future__ import annotations
 
@@ -76,6 +81,81 @@ def params_text(fill: str, period: int, alloc_mult: float, global_move: bool = F
             f"REAL opp_allocation_multiple = {alloc_mult}\nBOOL opp_profile_all = false\n"
             f"BOOL opp_global_move = {gm}\nBOOL opp_dh_data_generate = {gm}\n"
             f"INT opp_threads_per_block = 256\nBOOL print_final = {pf}\n" + extra)
+
+
+BOX_DTYPE = np.dtype([("magic", "S8"), ("ints", "<i4", 8), ("dbl", "<f8", 9)])
+
+
+def write_box_case(path: Path, dims, inject: int = 0, steps: int = 0, dt: float = 0.01, qm: float = 1.0,
+                   ion_velocity: float = 1.0, sigma: float = 0.1, phi_inlet: float = 1.0, phi_fixed: float = 0.0,
+                   record_state: bool = False, mesh_only: bool = False, seed: int = 0) -> None:
+    """dims = (nx, ny, nz, lx, ly, lz): the box the harness writes and loads."""
+    nx, ny, nz, lx, ly, lz = dims
+    hdr = np.zeros(1, dtype=BOX_DTYPE)
+    hdr["magic"] = b"OPPBBOX1"
+    hdr["ints"] = [nx, ny, nz, inject, steps, int(record_state), int(mesh_only), seed]
+    hdr["dbl"] = [lx, ly, lz, dt, qm, ion_velocity, sigma, phi_inlet, phi_fixed]
+    Path(path).write_bytes(hdr.tobytes())
+
+
+def mesh_params(d: Path) -> str:
+    """The app's mesh-file parameters (apps_codegen/app_fempic_cg/configs/coarse.param) for files in d."""
+    return (f"STRING global_mesh = {d / 'mesh.dat'}\nSTRING inlet_mesh = {d / 'inlet.dat'}\n"
+            f"STRING wall_mesh = {d / 'wall.dat'}\n")
+
+
+def box_mesh(dims, kind: str = "seq") -> dict:
+    """The mesh arrays load_mesh() gives for the box dims = (nx, ny, nz, lx, ly, lz), in the
+    app's host layout: n_pos, n_vol, n_type, c2n, c2c, c_det, c_vol, c_centroid, if2c, if2n,
+    if_u, if_v, if_norm, if_area, if_n_pos."""
+    exe = REF_DIR / BINARIES[kind]
+    if not exe.exists():
+        raise FileNotFoundError(exe)
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        write_box_case(d / "case.bin", dims, mesh_only=True)
+        (d / "params.txt").write_text(params_text("HoleFill_All", 10, 2.0, extra=mesh_params(d)))
+        r = subprocess.run([str(exe), str(d / "params.txt"), str(d / "case.bin"), str(d / "out.bin")],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"{exe.name} failed ({r.returncode}): {r.stderr[-2000:]}")
+        raw = (d / "out.bin").read_bytes()
+    nn, nc, nf = (int(v) for v in np.frombuffer(raw[:12], "<i4"))
+    off = 12
+    out = {"n_nodes": nn, "n_cells": nc, "n_ifaces": nf}
+    for name, dt, shape in (("n_pos", "<f8", (nn, 3)), ("n_vol", "<f8", (nn,)), ("n_type", "<i4", (nn,)),
+                            ("c2n", "<i4", (nc, 4)), ("c2c", "<i4", (nc, 4)), ("c_det", "<f8", (nc, 16)),
+                            ("c_vol", "<f8", (nc,)), ("c_centroid", "<f8", (nc, 3)), ("if2c", "<i4", (nf,)),
+                            ("if2n", "<i4", (nf, 3)), ("if_u", "<f8", (nf, 3)), ("if_v", "<f8", (nf, 3)),
+                            ("if_norm", "<f8", (nf, 3)), ("if_area", "<f8", (nf,)), ("if_n_pos", "<f8", (nf, 9))):
+        n = int(np.prod(shape)) * np.dtype(dt).itemsize
+        out[name] = np.frombuffer(raw[off:off + n], dt).reshape(shape).copy()
+        off += n
+    return out
+
+
+def run_box(kind: str, dims, inject: int, steps: int, fill: str = "HoleFill_All", period: int = 10,
+            alloc_mult: float = 2.0, threads: int | None = None, record_state: bool = False, seed: int = 0,
+            **kw) -> dict:
+    """The step loop on the box mesh loaded by the app's loader (the workload's injection
+    distribution, the exact static field of its Laplace problem, the harness's own seeded
+    randoms).  kw: dt, qm, ion_velocity, sigma, phi_inlet, phi_fixed."""
+    exe = REF_DIR / BINARIES[kind]
+    if not exe.exists():
+        raise FileNotFoundError(exe)
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        write_box_case(d / "case.bin", dims, inject=inject, steps=steps, record_state=record_state, seed=seed, **kw)
+        (d / "params.txt").write_text(params_text(fill, period, alloc_mult, extra=mesh_params(d)))
+        env = dict(os.environ)
+        if threads:
+            env["OMP_NUM_THREADS"] = str(threads)
+        r = subprocess.run([str(exe), str(d / "params.txt"), str(d / "case.bin"), str(d / "out.bin")],
+                           stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True, env=env)
+        if r.returncode != 0:
+            raise RuntimeError(f"{exe.name} failed ({r.returncode}): {r.stderr[-2000:]}")
+        nn = int(np.prod([dims[0] + 1, dims[1] + 1, dims[2] + 1]))
+        return read_output(d / "out.bin", nn, record_state)
 
 
 def run(kind: str, mesh, dist, steps: int, tables, fill: str = "HoleFill_All", period: int = 10,

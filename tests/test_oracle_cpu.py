@@ -227,3 +227,24 @@ def test_oracle_deposit_exact_definition():
     seq = np.zeros(n_nodes)
     O.deposit(np.ascontiguousarray(lc[keep]), np.ascontiguousarray(p2c[keep]), c2n, seq)
     assert np.abs(got - seq).max() <= 1e-13
+
+
+def test_oracle_deposit_exact_large_node_sums():
+    """Node totals far beyond 2^63 units of 2^-52 (a node column summing to more than 2048):
+    the checker stays exact where one int64 accumulator would wrap."""
+    from fractions import Fraction
+
+    rng = np.random.default_rng(9)
+    n_cells, n_nodes, n = 3, 6, 12000
+    c2n = np.array([[0, 1, 2, 3], [0, 1, 4, 5], [0, 2, 3, 5]], np.int32)
+    p2c = rng.integers(0, n_cells, n).astype(np.int32)
+    lc = rng.uniform(0.5, 1.0, (n, 4))
+    lc[:50, 2] = -rng.uniform(0, 0.3, 50)
+    got = O.deposit_exact(lc, p2c, c2n, n_nodes)
+    units = np.floor(lc * 2.0 ** 52).astype(np.int64)
+    ref = [0] * n_nodes
+    for i in range(n):
+        for k in range(4):
+            ref[c2n[p2c[i], k]] += int(units[i, k])
+    assert max(abs(r) for r in ref) > 2 ** 63  # node 0 gathers ~9,000 weights of ~0.75
+    np.testing.assert_array_equal(got, np.array([float(Fraction(r, 2 ** 52)) for r in ref]))
