@@ -308,6 +308,39 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     out["push_inclusive_fused"] = ps_f / (t_f / 1e3)
     out["fused_steps"] = n_fused
 
+    # Whole steps replayed from CUDA graphs (include/oppb_graph.h): one graph = one sort cycle
+    # of steps (inject, push + move + deposit, hole fill / sort, step record), the particle
+    # count kept on the device; one readback of the count and the records per replay.  The
+    # tables are refilled between replays, outside the timed replay.
+    G = CFG["period"]
+    reps = max(2, min(steps, 40) // G)
+    g = sim.graph_for(G)
+    for t in g.tables:
+        device_randoms(t)
+    sim.replay(g)  # the first replay of each buffer parity (a sort swaps the buffers) is untimed
+    g = sim.graph_for(G)
+    for t in g.tables:
+        device_randoms(t)
+    sim.replay(g)
+    ps_g, t_g, l_g = 0, 0.0, 0
+    for _ in range(reps):
+        g = sim.graph_for(G)
+        for t in g.tables:
+            device_randoms(t)
+        e0, e1 = E(), E()
+        e0.record(s)
+        g.graph.replay()
+        e1.record(s)
+        recs = sim.replay_finish(g)
+        ps_g += sum(r["size_before_move"] for r in recs)
+        t_g += e0.elapsed_time(e1)
+        l_g += g.launches
+    out["graph_step"] = {"value": ps_g / (t_g / 1e3), "unit": UNIT, "ms_per_step": t_g / (reps * G),
+                         "steps_per_graph": G, "replays": reps, "launches_per_replay": g.launches,
+                         "gpu_launches": l_g, "captured_graphs": len(sim._graphs),
+                         "what": "whole steps (inject, push + move + deposit, hole fill / cell sort) replayed "
+                                 "from one CUDA graph per sort cycle, particle count on the device, device time"}
+
     if e2e_steps:
         # End to end through the public API (FemPIC.run_steps): every step's injection table
         # goes up from pinned host memory and its node charges (plus the move status) come
@@ -492,6 +525,7 @@ def arm_ours(args) -> dict:
                            "mixed_unfused": mixed["push_inclusive"], "mixed_fused": mixed["push_inclusive_fused"],
                            "f64_unfused": f64["push_inclusive"], "f64_fused": f64["push_inclusive_fused"],
                            "fused_steps": mixed["fused_steps"]},
+        "graph_step": {"mixed": mixed["graph_step"], "f64": f64["graph_step"]},
         "mixed_over_plain": mixed["job_value"] / f64["job_value"],
         "autotune": {"what": "move launch (deposit strategy, node-sum copies) and sort gather columns, "
                              "median of 3 timed trials on the warmed-up state",

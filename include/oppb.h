@@ -313,6 +313,20 @@ int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride,
                       int32_t* perm_out, void* workspace, size_t workspace_bytes,
                       void* stream);
 
+/* Shuffle of particles [0,size) for opp_fill = Shuffle_All / Shuffle_Periodic: the particles
+ * with a valid cell in a random order, removed particles (p2c outside [0,n_cells)) last, then
+ * every dat, the p2c dat included, gathered into its `swap` buffer (the CUDA backend's
+ * particle_sort_device with shuffle = true, opp_lib/src/cuda/opp_particle_sorter.cu:167-246,
+ * which sorts by random keys from a RandomFunctor seeded 123, :40-54).  Here the keys are 30
+ * bits of a splitmix64 hash of (seed, index), seed != 0, sorted stably by the same radix sort:
+ * deterministic for a seed, but not the reference's draws (its engine is Thrust's), so the
+ * order within the live particles is not the reference's.  The seq backend's shuffle sorts by
+ * cell (opp_particle_sort_core ignores the flag, opp_particle_organize_core.cpp:98-121).
+ * Workspace as oppb_sort_by_cell. */
+int oppb_shuffle(int32_t size, int32_t n_cells, int32_t stride, int32_t n_dats, const oppb_dat* dats,
+                 int32_t key_dat, uint64_t seed, int32_t* perm_out, void* workspace, size_t workspace_bytes,
+                 void* stream);
+
 #ifdef __cplusplus
 }
 #endif

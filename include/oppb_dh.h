@@ -74,7 +74,11 @@ int oppb_dh_build(const oppb_tet_mesh* mesh, const double* n_pos, oppb_dh_grid* 
  * (needs deposit).  dh: the direct-hop seed (NULL = walk from the previous cell), applied
  * after the push, as the reference's global-move pre-pass runs after the push loop: a
  * position outside the grid, or in a box with no cell, removes the particle (the CUDA
- * backend's rule), else the walk starts from the box's cell. */
+ * backend's rule), else the walk starts from the box's cell.  set_count: the particle count
+ * in device memory (include/oppb_graph.h; NULL = parts->size is the count): the move then
+ * processes [0, min(set_count->size + pending, parts->size)), parts->size being the upper
+ * bound that sizes the grid. */
+struct oppb_set_count;
 typedef struct oppb_move_options {
     int32_t precision;            /* OPPB_PRECISION_*                                  */
     int32_t deposit;
@@ -83,6 +87,9 @@ typedef struct oppb_move_options {
     double  qm, dt;               /* push constants (CONST_charge/CONST_mass, CONST_dt) */
     double  band;                 /* mixed path: FP64 re-check band (e.g. 1e-5)        */
     const oppb_dh_grid* dh;       /* host struct; map on the device; may be NULL        */
+    const struct oppb_set_count* set_count;  /* device; may be NULL                      */
+    int32_t pending;              /* particles injected since set_count->size was set   */
+    int32_t reserved2;
 } oppb_move_options;
 
 /* The move of oppb.h (oppb_move_f64 / oppb_move_deposit_* / oppb_push_move_deposit_*) with

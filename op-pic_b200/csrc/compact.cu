@@ -14,6 +14,7 @@
 #include <climits>
 #include <mutex>
 
+#include "oppb_graph.h"
 #include "scan.cuh"
 
 namespace oppb {
@@ -32,6 +33,20 @@ struct DatList {
     int32_t bytes[kMaxDats];
 };
 
+// A count of a launch: the host's value, or (dev != nullptr) the value in device memory plus
+// `add`, capped by the host's value, which is then its upper bound (include/oppb_graph.h).
+struct CountArg {
+    int32_t host;
+    const int32_t* dev;
+    int32_t add;
+};
+
+__device__ __forceinline__ int32_t resolve(const CountArg& c) {
+    if (!c.dev) return c.host;
+    const int32_t v = *c.dev + c.add;
+    return v < 0 ? 0 : (v < c.host ? v : c.host);
+}
+
 // Bitmap word w restricted to particles < size.
 __device__ __forceinline__ uint32_t hole_word(const uint32_t* bits, int64_t w, int32_t size) {
     const int64_t first = w * 32;
@@ -42,9 +57,10 @@ __device__ __forceinline__ uint32_t hole_word(const uint32_t* bits, int64_t w, i
     return v;
 }
 
-__global__ void __launch_bounds__(kHfBlock) hf_count_kernel(const uint32_t* __restrict__ bits, int32_t size,
+__global__ void __launch_bounds__(kHfBlock) hf_count_kernel(const uint32_t* __restrict__ bits, CountArg size_arg,
                                                             int64_t n_words, int* __restrict__ block_holes) {
     __shared__ int sm[kHfBlock / 32 + 1];
+    const int32_t size = resolve(size_arg);
     const int64_t w0 = (int64_t)blockIdx.x * kHfWords;
     int c = 0;
 #pragma unroll
@@ -58,12 +74,14 @@ __global__ void __launch_bounds__(kHfBlock) hf_count_kernel(const uint32_t* __re
 }
 
 // block_base: exclusive hole prefix per block, block_base[n_blocks] = total holes H.
-__global__ void __launch_bounds__(kHfBlock) hf_emit_kernel(const uint32_t* __restrict__ bits, int32_t size,
+__global__ void __launch_bounds__(kHfBlock) hf_emit_kernel(const uint32_t* __restrict__ bits, CountArg size_arg,
                                                            int64_t n_words, const int* __restrict__ block_base,
-                                                           int n_blocks, int32_t remove_count,
+                                                           int n_blocks, CountArg remove_arg,
                                                            int32_t* __restrict__ hole_list,
                                                            int32_t* __restrict__ mover_list) {
     __shared__ int sm[kHfBlock / 32 + 1];
+    const int32_t size = resolve(size_arg);
+    const int32_t remove_count = resolve(remove_arg);
     // Thread t owns words [w0 + t*8, w0 + t*8 + 8) (blocked, so ranks follow index order).
     const int64_t wt = (int64_t)blockIdx.x * kHfWords + (int64_t)threadIdx.x * kHfWordsPerThread;
     uint32_t w[kHfWordsPerThread];
@@ -114,32 +132,60 @@ __global__ void __launch_bounds__(kHfBlock) hf_emit_kernel(const uint32_t* __res
     }
 }
 
-// One thread per (pair, column): copies the element of column col of the mover to the hole.
-__global__ void hf_copy_kernel(int32_t n_pairs_max, const int32_t* __restrict__ hole_list,
+// One (pair, column) per thread and pass of a grid-stride loop: copies the element of column
+// col of the mover to the hole.
+__global__ void hf_copy_kernel(CountArg pairs_arg, const int32_t* __restrict__ hole_list,
                                const int32_t* __restrict__ mover_list, const int* __restrict__ totals,
-                               int32_t size, int32_t stride, DatList dats) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t k = t / dats.total_cols;
-    const int col = (int)(t - k * dats.total_cols);
-    if (k >= n_pairs_max) return;
+                               CountArg size_arg, int32_t stride, DatList dats) {
+    const int64_t n_pairs_max = resolve(pairs_arg);
+    const int64_t size = resolve(size_arg);
     const int64_t H = totals[0];
-    if (k >= H || k >= (int64_t)size - H) return;
-    const int32_t to = hole_list[k], from = mover_list[k];
-    if (from <= to) return;
-    int d = 0, c = col;
-    while (d < dats.n && c >= dats.dim[d]) {
-        c -= dats.dim[d];
-        d++;
+    const int64_t n_items = n_pairs_max * dats.total_cols;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_items;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = t / dats.total_cols;
+        const int col = (int)(t - k * dats.total_cols);
+        if (k >= H || k >= size - H) continue;
+        const int32_t to = hole_list[k], from = mover_list[k];
+        if (from <= to) continue;
+        int d = 0, c = col;
+        while (d < dats.n && c >= dats.dim[d]) {
+            c -= dats.dim[d];
+            d++;
+        }
+        if (d >= dats.n) continue;
+        const int64_t off = (int64_t)c * stride;
+        if (dats.bytes[d] == 8) {
+            int64_t* a = reinterpret_cast<int64_t*>(dats.data[d]) + off;
+            a[to] = a[from];
+        } else {
+            int32_t* a = reinterpret_cast<int32_t*>(dats.data[d]) + off;
+            a[to] = a[from];
+        }
     }
-    if (d >= dats.n) return;
-    const int64_t off = (int64_t)c * stride;
-    if (dats.bytes[d] == 8) {
-        int64_t* a = reinterpret_cast<int64_t*>(dats.data[d]) + off;
-        a[to] = a[from];
-    } else {
-        int32_t* a = reinterpret_cast<int32_t*>(dats.data[d]) + off;
-        a[to] = a[from];
+}
+
+// Closes a device-sized step (one thread): the step record, the first error, the new count.
+__global__ void step_end_kernel(oppb_set_count* cnt, int32_t pending, const oppb_move_status* st,
+                                oppb_step_record* records, int32_t n_records) {
+    const int32_t n = cnt->size + pending;
+    const int32_t removed = st->remove_count;
+    oppb_step_record r;
+    r.size_before_move = n;
+    r.removed = removed;
+    r.size = n - removed;
+    r.max_visits = st->max_visits;
+    r.total_visits = st->total_visits;
+    r.recheck_count = st->recheck_count;
+    r.error = st->error;
+    const int32_t step = cnt->steps;
+    if (records && n_records > 0) records[step % n_records] = r;
+    if (st->error && !cnt->error) {
+        cnt->error = st->error;
+        cnt->error_step = step;
     }
+    cnt->size = n - removed;
+    cnt->steps = step + 1;
 }
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -187,19 +233,82 @@ extern "C" int oppb_hole_fill(int32_t size, int32_t remove_count, const uint32_t
     ws += align256(sizeof(int32_t) * (size_t)remove_count);
     int32_t* mover_list = reinterpret_cast<int32_t*>(ws);
 
-    hf_count_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base);
+    const CountArg sz{size, nullptr, 0}, rc{remove_count, nullptr, 0};
+    hf_count_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, sz, n_words, block_base);
     // block_base[0..n_blocks) exclusive, block_base[n_blocks] = total holes.
     scan_single_block_kernel<<<1, kScanBlock, 0, s>>>(block_base, n_blocks);
     (void)scan_tmp;
-    hf_emit_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base, n_blocks, remove_count,
-                                                 hole_list, mover_list);
+    hf_emit_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, sz, n_words, block_base, n_blocks, rc, hole_list,
+                                                 mover_list);
     count_launches(3);
     if (dl.total_cols > 0) {
         const int64_t threads = (int64_t)remove_count * dl.total_cols;
-        hf_copy_kernel<<<ceil_div(threads, 256), 256, 0, s>>>(remove_count, hole_list, mover_list,
-                                                             block_base + n_blocks, size, stride, dl);
+        hf_copy_kernel<<<ceil_div(threads, 256), 256, 0, s>>>(rc, hole_list, mover_list, block_base + n_blocks, sz,
+                                                             stride, dl);
         count_launches(1);
     }
+    return launch_status();
+}
+
+extern "C" size_t oppb_hole_fill_dev_workspace_bytes(int32_t size_bound) {
+    return oppb_hole_fill_workspace_bytes(size_bound, size_bound);
+}
+
+extern "C" int oppb_hole_fill_dev(int32_t size_bound, const oppb_set_count* count, int32_t pending,
+                                  const oppb_move_status* status, const uint32_t* remove_bits, int32_t stride,
+                                  int32_t n_dats, const oppb_dat* dats, void* workspace, size_t workspace_bytes,
+                                  void* stream) {
+    using namespace oppb;
+    if (size_bound < 0 || pending < 0 || stride < size_bound || n_dats < 0 || n_dats > kMaxDats) return OPPB_ERR_ARG;
+    if (!count || !status) return OPPB_ERR_ARG;
+    if (size_bound == 0) return OPPB_OK;
+    if (!remove_bits || !dats || !workspace) return OPPB_ERR_ARG;
+    if (workspace_bytes < oppb_hole_fill_dev_workspace_bytes(size_bound)) return OPPB_ERR_WORKSPACE;
+    DatList dl{};
+    dl.n = n_dats;
+    dl.total_cols = 0;
+    for (int d = 0; d < n_dats; d++) {
+        if (!dats[d].data || dats[d].dim <= 0 || (dats[d].elem_bytes != 4 && dats[d].elem_bytes != 8))
+            return OPPB_ERR_ARG;
+        dl.data[d] = dats[d].data;
+        dl.dim[d] = dats[d].dim;
+        dl.bytes[d] = dats[d].elem_bytes;
+        dl.total_cols += dats[d].dim;
+    }
+    cudaStream_t s = as_stream(stream);
+    const int64_t n_words = ceil_div(size_bound, 32);
+    const int n_blocks = ceil_div(n_words, kHfWords);
+    char* ws = static_cast<char*>(workspace);
+    int* block_base = reinterpret_cast<int*>(ws);
+    ws += align256(sizeof(int) * (size_t)(n_blocks + 1));
+    ws += align256(sizeof(int) * scan_scratch_ints(n_blocks));
+    int32_t* hole_list = reinterpret_cast<int32_t*>(ws);
+    ws += align256(sizeof(int32_t) * (size_t)size_bound);
+    int32_t* mover_list = reinterpret_cast<int32_t*>(ws);
+    // The count and the move's remove count are read on the device; the lists hold up to
+    // size_bound pairs, and no more than the count can be removed.
+    const CountArg sz{size_bound, &count->size, pending};
+    const CountArg rc{size_bound, &status->remove_count, 0};
+    hf_count_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, sz, n_words, block_base);
+    scan_single_block_kernel<<<1, kScanBlock, 0, s>>>(block_base, n_blocks);
+    hf_emit_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, sz, n_words, block_base, n_blocks, rc, hole_list,
+                                                 mover_list);
+    count_launches(3);
+    if (dl.total_cols > 0) {
+        const int64_t items = (int64_t)size_bound * dl.total_cols;
+        const int grid = ceil_div(items, 256) < 148 * 16 ? ceil_div(items, 256) : 148 * 16;
+        hf_copy_kernel<<<grid, 256, 0, s>>>(rc, hole_list, mover_list, block_base + n_blocks, sz, stride, dl);
+        count_launches(1);
+    }
+    return launch_status();
+}
+
+extern "C" int oppb_step_end_dev(oppb_set_count* count, int32_t pending, const oppb_move_status* status,
+                                 oppb_step_record* records, int32_t n_records, void* stream) {
+    using namespace oppb;
+    if (!count || !status || pending < 0 || n_records < 0 || (n_records > 0 && !records)) return OPPB_ERR_ARG;
+    step_end_kernel<<<1, 1, 0, as_stream(stream)>>>(count, pending, status, records, n_records);
+    count_launches(1);
     return launch_status();
 }
 
@@ -292,23 +401,24 @@ extern "C" int oppb_hole_fill_static(int32_t size, int32_t remove_count, const u
     }
     cudaStream_t s = as_stream(stream);
     int32_t* scratch = nullptr;
-    const int rc = static_scratch(s, &scratch);
-    if (rc != OPPB_OK) return rc;
+    const int lookup = static_scratch(s, &scratch);
+    if (lookup != OPPB_OK) return lookup;
     const int64_t n_words = ceil_div(size, 32);
     const int n_blocks = ceil_div(n_words, kHfWords);  // <= kStaticMaxBlocks for any int32 size
     int* block_base = scratch;
     int32_t* hole_list = scratch + kStaticBaseWords;
     int32_t* mover_list = hole_list + kStaticListWords;
 
-    hf_count_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base);
+    const CountArg sz{size, nullptr, 0}, rc{remove_count, nullptr, 0};
+    hf_count_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, sz, n_words, block_base);
     scan_single_block_kernel<<<1, kScanBlock, 0, s>>>(block_base, n_blocks);
-    hf_emit_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, size, n_words, block_base, n_blocks, remove_count,
-                                                 hole_list, mover_list);
+    hf_emit_kernel<<<n_blocks, kHfBlock, 0, s>>>(remove_bits, sz, n_words, block_base, n_blocks, rc, hole_list,
+                                                 mover_list);
     count_launches(3);
     if (dl.total_cols > 0) {
         const int64_t threads = (int64_t)remove_count * dl.total_cols;
-        hf_copy_kernel<<<ceil_div(threads, 256), 256, 0, s>>>(remove_count, hole_list, mover_list,
-                                                             block_base + n_blocks, size, stride, dl);
+        hf_copy_kernel<<<ceil_div(threads, 256), 256, 0, s>>>(rc, hole_list, mover_list, block_base + n_blocks, sz,
+                                                             stride, dl);
         count_launches(1);
     }
     return launch_status();

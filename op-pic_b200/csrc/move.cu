@@ -42,14 +42,25 @@ static_assert(kSlots == kMoveBlock, "table init/flush assume one slot per thread
 enum : int { kDone = 0, kNeedMove = 1, kNeedRemove = 2, kFailed = 3 };
 
 struct PartArgs {
-    int32_t size;
+    int32_t size;         // the particle count; with count_dev, an upper bound of it
     int32_t stride;
     double* pos;          // written only by the fused push
     double* vel;          // fused push only
     double* lc;
     int32_t* p2c;
     uint32_t* remove_bits;
+    const int32_t* count_dev;  // oppb_set_count::size (device), or nullptr
+    int32_t pending;           // particles injected since *count_dev was set
 };
+
+// The particle count of a launch: the host's, or the device count plus the pending
+// injections, capped by the host's bound (include/oppb_graph.h).  Written by earlier
+// launches of the stream, so a plain load sees it.
+__device__ __forceinline__ int32_t live_count(const PartArgs& p) {
+    if (!p.count_dev) return p.size;
+    const int32_t n = *p.count_dev + p.pending;
+    return n < p.size ? n : p.size;
+}
 
 // Push prologue of the fused entry points: calculate_new_pos_vel_kernel
 // (apps/app_fempic/kernels.h:93-103) run on the particle's registers before its walk, the
@@ -118,7 +129,7 @@ __device__ __forceinline__ void cta_account(const PartArgs& p, oppb_move_status*
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned hole = __ballot_sync(kFullMask, active && final_cell == kRemoved);
     const unsigned rem = __ballot_sync(kFullMask, newly_removed);
-    if (lane == 0 && i < p.size) p.remove_bits[i >> 5] = hole;
+    if (lane == 0 && active) p.remove_bits[i >> 5] = hole;  // lane 0 active: the word holds live particles
     // Warp reductions in the integer reduce unit (shuffles would load the L1 data pipe the
     // visits are bound by).  The visit sum is taken in 16-bit halves so that 32 lanes
     // cannot overflow 32 bits whatever max_hops is.
@@ -339,14 +350,16 @@ __device__ __forceinline__ void push_prologue(const oppb_tet_mesh& m, const Part
 
 // ------------------------------------------------------------------ FP64 move
 
-template <int kDep, bool kPush, bool kSeed>
+template <int kDep, bool kPush, bool kSeed, bool kDevCount = false>
 __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     move_f64_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
                     PushArgs push, DhArgs dh) {
     __shared__ NodeTable table;
+    const int32_t n = kDevCount ? live_count(p) : p.size;
+    if (kDevCount && (int64_t)blockIdx.x * kMoveBlock >= n) return;  // beyond the device count (whole block)
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
-    const bool active = i < p.size;
+    const bool active = i < n;
     int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
     const int32_t cell0 = cell;
     int status = kDone;
@@ -418,14 +431,16 @@ struct Band {
     float tie;     // 2 * band
 };
 
-template <int kDep, bool kPush, bool kSeed>
+template <int kDep, bool kPush, bool kSeed, bool kDevCount = false>
 __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     move_mixed_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
                       Band band, PushArgs push, DhArgs dh) {
     __shared__ NodeTable table;
+    const int32_t n = kDevCount ? live_count(p) : p.size;
+    if (kDevCount && (int64_t)blockIdx.x * kMoveBlock >= n) return;  // beyond the device count (whole block)
     if (kDep == kDepTable) table_init(table);
     const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
-    const bool active = i < p.size;
+    const bool active = i < n;
     int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
     const int32_t cell0 = cell;
     int status = kDone;
@@ -592,8 +607,8 @@ int check_parts(const oppb_particles* p, bool need_bits) {
     return OPPB_OK;
 }
 
-PartArgs part_args(const oppb_particles* p) {
-    return PartArgs{p->size, p->stride, p->pos, p->vel, p->lc, p->p2c, p->remove_bits};
+PartArgs part_args(const oppb_particles* p, const int32_t* count_dev = nullptr, int32_t pending = 0) {
+    return PartArgs{p->size, p->stride, p->pos, p->vel, p->lc, p->p2c, p->remove_bits, count_dev, pending};
 }
 
 int replicas_for(size_t workspace_bytes, const void* workspace, int32_t n_nodes) {
@@ -647,10 +662,11 @@ Replicas make_replicas(double* node_charge, void* workspace, size_t workspace_by
 
 enum MoveKind { kMoveOnly, kMoveDepositF64, kMoveDepositMixed };
 
-template <int kKind, bool kPush, bool kSeed = false>
+template <int kKind, bool kPush, bool kSeed = false, bool kDevCount = false>
 int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
                 oppb_move_status* status, int32_t max_hops, double band, const PushArgs& push, void* workspace,
-                size_t ws_bytes, void* stream, const DhArgs& dh = DhArgs{}) {
+                size_t ws_bytes, void* stream, const DhArgs& dh = DhArgs{}, const int32_t* count_dev = nullptr,
+                int32_t pending = 0) {
     constexpr bool kMixed = kKind == kMoveDepositMixed;
     int rc = check_mesh(mesh, kMixed, kKind != kMoveOnly);
     if (rc) return rc;
@@ -664,7 +680,8 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     cudaStream_t s = as_stream(stream);
     if (cudaMemsetAsync(status, 0, sizeof(oppb_move_status), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
     if (parts->size == 0) return launch_status();
-    const PartArgs p = part_args(parts);
+    if (kDevCount != (count_dev != nullptr) || pending < 0) return OPPB_ERR_ARG;
+    const PartArgs p = part_args(parts, count_dev, pending);
     const int grid = ceil_div(parts->size, kMoveBlock);
     Replicas rep{};
     if (kKind != kMoveOnly) {
@@ -677,26 +694,26 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
     const float bf = (float)band;
     const Band bd{bf, -bf, 1.0f - bf, 1.0f + bf, 2.0f * bf};
     if constexpr (kKind == kMoveOnly)
-        move_f64_kernel<kDepNone, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops,
+        move_f64_kernel<kDepNone, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops,
                                                                            push, dh);
     else if constexpr (kKind == kMoveDepositF64) {
         if (table)
-            move_f64_kernel<kDepTable, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+            move_f64_kernel<kDepTable, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                                 max_hops, push, dh);
         else if (exact)
-            move_f64_kernel<kDepExact, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+            move_f64_kernel<kDepExact, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                                 max_hops, push, dh);
         else
-            move_f64_kernel<kDepWarp, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+            move_f64_kernel<kDepWarp, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                                max_hops, push, dh);
     } else if (exact)
-        move_mixed_kernel<kDepExact, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+        move_mixed_kernel<kDepExact, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                               max_hops, bd, push, dh);
     else if (table)
-        move_mixed_kernel<kDepTable, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+        move_mixed_kernel<kDepTable, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                               max_hops, bd, push, dh);
     else
-        move_mixed_kernel<kDepWarp, kPush, kSeed><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
+        move_mixed_kernel<kDepWarp, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                              max_hops, bd, push, dh);
     count_launches(1);
     rep.end(s);
@@ -715,18 +732,35 @@ int move_ex(const oppb_tet_mesh* mesh, const oppb_particles* parts, const oppb_m
     if (mixed && !o.deposit) return OPPB_ERR_ARG;    // the mixed move always deposits
     // The coefficients of oppb_push_f64 / oppb_push_mixed: q/m and dt, f32(q/m * dt) and f32(dt).
     const PushArgs push{o.qm, o.dt, (float)(o.qm * o.dt), (float)o.dt};
+    // The device count (oppb_set_count::size is its first member), or the host's parts->size.
+    const int32_t* cd = o.set_count ? reinterpret_cast<const int32_t*>(o.set_count) : nullptr;
+    const int32_t pd = o.pending;
+    if (cd) {  // device-counted launches: the deposit kernels, walks from the previous cell
+        if (kSeed || !o.deposit) return OPPB_ERR_ARG;
+        if (mixed)
+            return o.push ? launch_move<kMoveDepositMixed, true, false, true>(mesh, parts, node_charge, status,
+                                                                              max_hops, o.band, push, ws, ws_bytes,
+                                                                              stream, dh, cd, pd)
+                          : launch_move<kMoveDepositMixed, false, false, true>(mesh, parts, node_charge, status,
+                                                                               max_hops, o.band, push, ws, ws_bytes,
+                                                                               stream, dh, cd, pd);
+        return o.push ? launch_move<kMoveDepositF64, true, false, true>(mesh, parts, node_charge, status, max_hops,
+                                                                        0.0, push, ws, ws_bytes, stream, dh, cd, pd)
+                      : launch_move<kMoveDepositF64, false, false, true>(mesh, parts, node_charge, status, max_hops,
+                                                                         0.0, push, ws, ws_bytes, stream, dh, cd, pd);
+    }
     if (!o.deposit)
         return launch_move<kMoveOnly, false, kSeed>(mesh, parts, nullptr, status, max_hops, 0.0, push, nullptr, 0,
-                                                    stream, dh);
+                                                    stream, dh, cd, pd);
     if (mixed)
         return o.push ? launch_move<kMoveDepositMixed, true, kSeed>(mesh, parts, node_charge, status, max_hops,
-                                                                    o.band, push, ws, ws_bytes, stream, dh)
+                                                                    o.band, push, ws, ws_bytes, stream, dh, cd, pd)
                       : launch_move<kMoveDepositMixed, false, kSeed>(mesh, parts, node_charge, status, max_hops,
-                                                                     o.band, push, ws, ws_bytes, stream, dh);
+                                                                     o.band, push, ws, ws_bytes, stream, dh, cd, pd);
     return o.push ? launch_move<kMoveDepositF64, true, kSeed>(mesh, parts, node_charge, status, max_hops, 0.0,
-                                                              push, ws, ws_bytes, stream, dh)
+                                                              push, ws, ws_bytes, stream, dh, cd, pd)
                   : launch_move<kMoveDepositF64, false, kSeed>(mesh, parts, node_charge, status, max_hops, 0.0,
-                                                               push, ws, ws_bytes, stream, dh);
+                                                               push, ws, ws_bytes, stream, dh, cd, pd);
 }
 
 }  // namespace

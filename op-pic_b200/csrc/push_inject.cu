@@ -5,6 +5,7 @@
 #include <algorithm>
 
 #include "oppb_common.cuh"
+#include "oppb_graph.h"
 
 namespace oppb {
 namespace {
@@ -85,8 +86,11 @@ __global__ void fill_kernel(T* dst, int64_t count, T value) {
 }
 
 // Injection: face of injected particle k = first j with k < dist[j]; then
-// inject_ions_kernel (apps/app_fempic/kernels.h:63-90) plus the thermal velocity.
-__global__ void __launch_bounds__(kPushBlock) inject_kernel(int32_t start, int32_t count, int32_t stride,
+// inject_ions_kernel (apps/app_fempic/kernels.h:63-90) plus the thermal velocity.  With a
+// device count (cnt), start is cnt->size; a batch that would not fit in the stride writes
+// nothing and records OPPB_ERR_CAPACITY.
+__global__ void __launch_bounds__(kPushBlock) inject_kernel(oppb_set_count* cnt, int32_t start_host, int32_t count,
+                                                            int32_t stride,
                                                             int32_t n_faces, int32_t n_cells,
                                                             const int32_t* __restrict__ dist,
                                                             const int32_t* __restrict__ if2c,
@@ -96,6 +100,14 @@ __global__ void __launch_bounds__(kPushBlock) inject_kernel(int32_t start, int32
                                                             int32_t rdim, double ion_velocity, double qm, double dt,
                                                             double* pos, double* vel, int32_t* p2c) {
     const int64_t k = (int64_t)blockIdx.x * kPushBlock + threadIdx.x;
+    int32_t start = start_host;
+    if (cnt) {
+        start = cnt->size;
+        if ((int64_t)start + count > stride || start < 0) {
+            if (k == 0) atomicCAS(&cnt->error, 0, OPPB_ERR_CAPACITY);
+            return;
+        }
+    }
     if (k >= count) return;
     // Without a distribution the face index is already in p2c (opp_inc_part_count_with_distribution).
     const int face = dist ? face_of(dist, n_faces, k) : p2c[(int64_t)start + k];
@@ -179,8 +191,27 @@ extern "C" int oppb_inject_f64(const oppb_tet_mesh* mesh, const oppb_inlet* inle
     if ((int64_t)start + count > parts->stride) return OPPB_ERR_CAPACITY;
     if (count == 0) return OPPB_OK;
     inject_kernel<<<ceil_div(count, kPushBlock), kPushBlock, 0, as_stream(stream)>>>(
-        start, count, parts->stride, inlet->n_faces, mesh->n_cells, inlet->dist, inlet->if2c, inlet->geom, mesh->ef, rnd,
-        rnd_stride, rnd_dim, ion_velocity, qm, dt, parts->pos, parts->vel, parts->p2c);
+        nullptr, start, count, parts->stride, inlet->n_faces, mesh->n_cells, inlet->dist, inlet->if2c, inlet->geom,
+        mesh->ef, rnd, rnd_stride, rnd_dim, ion_velocity, qm, dt, parts->pos, parts->vel, parts->p2c);
+    count_launches(1);
+    return launch_status();
+}
+
+extern "C" int oppb_inject_dev(const oppb_tet_mesh* mesh, const oppb_inlet* inlet, const oppb_particles* parts,
+                               oppb_set_count* count, int32_t n_inject, const double* rnd, int32_t rnd_stride,
+                               int32_t rnd_dim, double ion_velocity, double qm, double dt, void* stream) {
+    using namespace oppb;
+    if (!mesh || !mesh->ef || !aligned(mesh->ef, 16) || !inlet || inlet->n_faces <= 0 || !inlet->if2c ||
+        !inlet->geom || !inlet->dist)
+        return OPPB_ERR_ARG;
+    if (!parts || !parts->pos || !parts->vel || !parts->p2c || !count || n_inject < 0 || parts->stride < 0)
+        return OPPB_ERR_ARG;
+    if (n_inject > 0 && (!rnd || rnd_stride < n_inject || (rnd_dim != 2 && rnd_dim != 5))) return OPPB_ERR_ARG;
+    if (n_inject > parts->stride) return OPPB_ERR_CAPACITY;
+    if (n_inject == 0) return OPPB_OK;
+    inject_kernel<<<ceil_div(n_inject, kPushBlock), kPushBlock, 0, as_stream(stream)>>>(
+        count, 0, n_inject, parts->stride, inlet->n_faces, mesh->n_cells, inlet->dist, inlet->if2c, inlet->geom,
+        mesh->ef, rnd, rnd_stride, rnd_dim, ion_velocity, qm, dt, parts->pos, parts->vel, parts->p2c);
     count_launches(1);
     return launch_status();
 }

@@ -10,10 +10,29 @@
 // sorted keys straight into the p2c swap buffer and the source indices (the
 // permutation) for the gather.
 
+#include "oppb_graph.h"
 #include "scan.cuh"
 
 namespace oppb {
 namespace {
+
+// The particle count of a sort: the host's, or (dev != nullptr) the device count plus `add`
+// capped by the host's value, which is then an upper bound (include/oppb_graph.h).  With
+// remove_dev, a zero remove count turns the sort into a plain copy into the swap buffers.
+struct SortCount {
+    int32_t host;
+    const int32_t* dev;
+    int32_t add;
+    const int32_t* remove_dev;
+};
+
+__device__ __forceinline__ int32_t sort_size(const SortCount& c) {
+    if (!c.dev) return c.host;
+    const int32_t v = *c.dev + c.add;
+    return v < 0 ? 0 : (v < c.host ? v : c.host);
+}
+
+__device__ __forceinline__ bool sort_is_copy(const SortCount& c) { return c.remove_dev && *c.remove_dev == 0; }
 
 constexpr int kSortBlock = 256;
 constexpr int kSortWarps = kSortBlock / 32;
@@ -27,20 +46,40 @@ __device__ __forceinline__ uint32_t cell_key(int32_t c, int32_t n_cells) {
     return ((uint32_t)c < (uint32_t)n_cells) ? (uint32_t)c : (uint32_t)n_cells;
 }
 
+// Shuffle key of particle j (Shuffle_All / Shuffle_Periodic): 30 random bits from a
+// splitmix64 hash of (seed, j) for a particle with a valid cell, 2^30 for a removed one, so
+// that removed particles still sort last.  The reference draws its keys with Thrust's
+// default engine seeded 123 (opp_lib/src/cuda/opp_particle_sorter.cu:40-54,195-201); only the
+// rule (random keys, removed last, stable sort) is kept, not the draws.
+constexpr uint32_t kShuffleRemoved = 1u << 30;
+
+__device__ __forceinline__ uint32_t shuffle_key(uint64_t seed, int64_t j, int32_t c, int32_t n_cells) {
+    if ((uint32_t)c >= (uint32_t)n_cells) return kShuffleRemoved;
+    uint64_t z = seed + 0x9e3779b97f4a7c15ull * (uint64_t)(j + 1);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    return (uint32_t)(z >> 34);
+}
+
 // Pass input: either raw p2c (first pass) or keys from the previous pass.
 struct PassIn {
     const int32_t* p2c;     // first pass only
     const uint32_t* keys;   // later passes
     const int32_t* vals;    // later passes (first pass: value = index)
+    uint64_t shuffle_seed;  // first pass: 0 = cell keys, else shuffle keys
 };
 
 __device__ __forceinline__ uint32_t load_key(const PassIn& in, int64_t j, int32_t n_cells) {
-    return in.p2c ? cell_key(in.p2c[j], n_cells) : in.keys[j];
+    if (!in.p2c) return in.keys[j];
+    const int32_t c = in.p2c[j];
+    return in.shuffle_seed ? shuffle_key(in.shuffle_seed, j, c, n_cells) : cell_key(c, n_cells);
 }
 
-__global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(PassIn in, int32_t size, int32_t n_cells,
+__global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(PassIn in, SortCount cnt, int32_t n_cells,
                                                                 int shift, int n_tiles, int* __restrict__ hist) {
     __shared__ int h[kRadix];
+    const int32_t size = sort_size(cnt);
     h[threadIdx.x] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kSortTile;
@@ -56,11 +95,13 @@ __global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(PassIn in, int32
 // offsets: exclusive scan of hist (digit-major), i.e. the first output slot of
 // (digit, tile).  keys_out/vals_out receive the pass result.  On the last pass
 // keys_out is the p2c swap buffer (removed key mapped back to the removed cell).
-__global__ void __launch_bounds__(kSortBlock, kScatterMinBlocks) radix_scatter_kernel(PassIn in, int32_t size, int32_t n_cells,
+__global__ void __launch_bounds__(kSortBlock, kScatterMinBlocks) radix_scatter_kernel(PassIn in, SortCount count, int32_t n_cells,
                                                                    int shift, int n_tiles,
                                                                    const int* __restrict__ offsets,
                                                                    uint32_t* __restrict__ keys_out,
                                                                    int32_t* __restrict__ vals_out, int last) {
+    const int32_t size = sort_size(count);
+    if (sort_is_copy(count) || (int64_t)blockIdx.x * kSortTile >= size) return;  // whole block
     __shared__ int cnt[kSortWarps][kRadix];
     __shared__ int tile_base[kRadix];
     __shared__ int scan_sm[kSortBlock / 32 + 1];
@@ -146,11 +187,16 @@ struct GatherCols {
 
 // dst[c][j] = src[c][perm[j]] for every column of every dat other than the key dat.
 // All loads of a particle are issued before its stores, so each thread keeps up to
-// kMaxCols loads in flight.
-__global__ void __launch_bounds__(256) gather_kernel(int32_t size, const int32_t* __restrict__ perm, GatherCols g) {
+// kMaxCols loads in flight.  When the sort is a copy (device count, no removal), perm is
+// not read (from = j) and the key column (key_src -> key_dst) is copied too.
+__global__ void __launch_bounds__(256) gather_kernel(SortCount cnt, const int32_t* __restrict__ perm, GatherCols g,
+                                                     const int32_t* __restrict__ key_src, int32_t* __restrict__ key_dst) {
+    const int32_t size = sort_size(cnt);
     const int64_t j = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (j >= size) return;
-    const int64_t from = perm[j];
+    const bool copy = sort_is_copy(cnt);
+    const int64_t from = copy ? j : perm[j];
+    if (copy && key_src) key_dst[j] = key_src[j];
     uint64_t v[kMaxCols];
 #pragma unroll
     for (int c = 0; c < kMaxCols; c++) {
@@ -210,21 +256,16 @@ extern "C" size_t oppb_sort_workspace_bytes(int32_t size, int32_t n_cells) {
     return oppb::sort_layout(size).total;
 }
 
-extern "C" int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride, int32_t n_dats, const oppb_dat* dats,
-                                 int32_t key_dat, int32_t* perm_out, void* workspace, size_t workspace_bytes,
-                                 void* stream) {
-    using namespace oppb;
-    if (size < 0 || n_cells <= 0 || n_cells >= kRemoved || stride < size || n_dats <= 0 || n_dats > kMaxDats ||
-        !dats || key_dat < 0 || key_dat >= n_dats)
-        return OPPB_ERR_ARG;
+namespace oppb {
+namespace {
+
+// The sort's launches for `size` particles (the host count, or the bound in device-count mode).
+// shuffle_seed != 0: sort by shuffle keys instead of cells; the key dat is then gathered like
+// the others.
+int launch_sort(const SortCount& cnt, int32_t size, int32_t n_cells, int32_t stride, int32_t n_dats,
+                const oppb_dat* dats, int32_t key_dat, int32_t* perm_out, void* workspace, cudaStream_t s,
+                uint64_t shuffle_seed = 0) {
     const oppb_dat& kd = dats[key_dat];
-    if (!kd.data || !kd.swap || kd.dim != 1 || kd.elem_bytes != 4) return OPPB_ERR_ARG;
-    for (int d = 0; d < n_dats; d++)
-        if (!dats[d].data || !dats[d].swap || dats[d].dim <= 0 || (dats[d].elem_bytes != 4 && dats[d].elem_bytes != 8))
-            return OPPB_ERR_ARG;
-    if (size == 0) return OPPB_OK;
-    if (!workspace || workspace_bytes < oppb_sort_workspace_bytes(size, n_cells)) return OPPB_ERR_WORKSPACE;
-    cudaStream_t s = as_stream(stream);
     const SortLayout L = sort_layout(size);
     char* ws = static_cast<char*>(workspace);
     uint32_t* keys[2] = {reinterpret_cast<uint32_t*>(ws + L.keys_a), reinterpret_cast<uint32_t*>(ws + L.keys_b)};
@@ -234,39 +275,120 @@ extern "C" int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride, 
     int* scan_tmp = reinterpret_cast<int*>(ws + L.scan);
 
     const int n_tiles = ceil_div(size, kSortTile);
-    const int passes = (key_bits(n_cells) + 7) / 8;
-    PassIn in{static_cast<const int32_t*>(kd.data), nullptr, nullptr};
+    const bool shuffle = shuffle_seed != 0;
+    const int passes = shuffle ? 4 : (key_bits(n_cells) + 7) / 8;  // shuffle keys: 31 bits
+    PassIn in{static_cast<const int32_t*>(kd.data), nullptr, nullptr, shuffle_seed};
     for (int p = 0; p < passes; p++) {
         const int shift = 8 * p;
         const bool last = (p == passes - 1);
-        uint32_t* ko = last ? static_cast<uint32_t*>(kd.swap) : keys[p & 1];
+        uint32_t* ko = (last && !shuffle) ? static_cast<uint32_t*>(kd.swap) : keys[p & 1];
         int32_t* vo = last ? perm : vals[p & 1];
-        radix_hist_kernel<<<n_tiles, kSortBlock, 0, s>>>(in, size, n_cells, shift, n_tiles, hist);
+        radix_hist_kernel<<<n_tiles, kSortBlock, 0, s>>>(in, cnt, n_cells, shift, n_tiles, hist);
         device_exclusive_scan(hist, hist, (int64_t)kRadix * n_tiles, scan_tmp, s);
-        radix_scatter_kernel<<<n_tiles, kSortBlock, 0, s>>>(in, size, n_cells, shift, n_tiles, hist, ko, vo,
-                                                            last ? 1 : 0);
+        radix_scatter_kernel<<<n_tiles, kSortBlock, 0, s>>>(in, cnt, n_cells, shift, n_tiles, hist, ko, vo,
+                                                            (last && !shuffle) ? 1 : 0);
         count_launches(2);
-        in = PassIn{nullptr, keys[p & 1], vals[p & 1]};
+        in = PassIn{nullptr, keys[p & 1], vals[p & 1], 0};
     }
     GatherCols g{};
     const int group = tuning().sort_gather_cols < kMaxCols ? tuning().sort_gather_cols : kMaxCols;
+    // The key column rides with the first gather launch (used only when the sort is a copy).
+    const int32_t* key_src = (cnt.remove_dev && !shuffle) ? static_cast<const int32_t*>(kd.data) : nullptr;
+    int32_t* key_dst = static_cast<int32_t*>(kd.swap);
     for (int d = 0; d < n_dats; d++) {
-        if (d == key_dat) continue;
+        if (d == key_dat && !shuffle) continue;
         for (int c = 0; c < dats[d].dim; c++) {
             const size_t off = (size_t)c * stride * dats[d].elem_bytes;
             g.src[g.n] = static_cast<const char*>(dats[d].data) + off;
             g.dst[g.n] = static_cast<char*>(dats[d].swap) + off;
             g.bytes[g.n] = dats[d].elem_bytes;
             if (++g.n == group) {
-                gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(size, perm, g);
+                gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(cnt, perm, g, key_src, key_dst);
                 count_launches(1);
                 g.n = 0;
+                key_src = nullptr;
             }
         }
     }
-    if (g.n > 0) {
-        gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(size, perm, g);
+    if (g.n > 0 || key_src) {
+        gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(cnt, perm, g, key_src, key_dst);
         count_launches(1);
     }
     return launch_status();
+}
+
+int check_sort_args(int32_t size, int32_t n_cells, int32_t stride, int32_t n_dats, const oppb_dat* dats,
+                    int32_t key_dat) {
+    if (size < 0 || n_cells <= 0 || n_cells >= kRemoved || stride < size || n_dats <= 0 || n_dats > kMaxDats ||
+        !dats || key_dat < 0 || key_dat >= n_dats)
+        return OPPB_ERR_ARG;
+    const oppb_dat& kd = dats[key_dat];
+    if (!kd.data || !kd.swap || kd.dim != 1 || kd.elem_bytes != 4) return OPPB_ERR_ARG;
+    for (int d = 0; d < n_dats; d++)
+        if (!dats[d].data || !dats[d].swap || dats[d].dim <= 0 || (dats[d].elem_bytes != 4 && dats[d].elem_bytes != 8))
+            return OPPB_ERR_ARG;
+    return OPPB_OK;
+}
+
+}  // namespace
+}  // namespace oppb
+
+extern "C" int oppb_sort_by_cell(int32_t size, int32_t n_cells, int32_t stride, int32_t n_dats, const oppb_dat* dats,
+                                 int32_t key_dat, int32_t* perm_out, void* workspace, size_t workspace_bytes,
+                                 void* stream) {
+    using namespace oppb;
+    const int rc = check_sort_args(size, n_cells, stride, n_dats, dats, key_dat);
+    if (rc) return rc;
+    if (size == 0) return OPPB_OK;
+    if (!workspace || workspace_bytes < oppb_sort_workspace_bytes(size, n_cells)) return OPPB_ERR_WORKSPACE;
+    return launch_sort(SortCount{size, nullptr, 0, nullptr}, size, n_cells, stride, n_dats, dats, key_dat, perm_out,
+                       workspace, as_stream(stream));
+}
+
+extern "C" size_t oppb_sort_dev_workspace_bytes(int32_t size_bound) {
+    if (size_bound < 0) return 0;
+    return oppb::sort_layout(size_bound).total;
+}
+
+extern "C" int oppb_sort_by_cell_dev(int32_t size_bound, const oppb_set_count* count, int32_t pending,
+                                     const oppb_move_status* status, int32_t n_cells, int32_t stride, int32_t n_dats,
+                                     const oppb_dat* dats, int32_t key_dat, void* workspace, size_t workspace_bytes,
+                                     void* stream) {
+    using namespace oppb;
+    const int rc = check_sort_args(size_bound, n_cells, stride, n_dats, dats, key_dat);
+    if (rc) return rc;
+    if (!count || !status || pending < 0) return OPPB_ERR_ARG;
+    if (size_bound == 0) return OPPB_OK;
+    if (!workspace || workspace_bytes < oppb_sort_dev_workspace_bytes(size_bound)) return OPPB_ERR_WORKSPACE;
+    const SortCount cnt{size_bound, &count->size, pending, &status->remove_count};
+    return launch_sort(cnt, size_bound, n_cells, stride, n_dats, dats, key_dat, nullptr, workspace,
+                       as_stream(stream));
+}
+
+extern "C" int oppb_shuffle(int32_t size, int32_t n_cells, int32_t stride, int32_t n_dats, const oppb_dat* dats,
+                            int32_t key_dat, uint64_t seed, int32_t* perm_out, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+    using namespace oppb;
+    const int rc = check_sort_args(size, n_cells, stride, n_dats, dats, key_dat);
+    if (rc) return rc;
+    if (seed == 0) return OPPB_ERR_ARG;
+    if (size == 0) return OPPB_OK;
+    if (!workspace || workspace_bytes < oppb_sort_workspace_bytes(size, n_cells)) return OPPB_ERR_WORKSPACE;
+    return launch_sort(SortCount{size, nullptr, 0, nullptr}, size, n_cells, stride, n_dats, dats, key_dat, perm_out,
+                       workspace, as_stream(stream), seed);
+}
+
+extern "C" int oppb_shuffle_dev(int32_t size_bound, const oppb_set_count* count, int32_t pending,
+                                const oppb_move_status* status, int32_t n_cells, int32_t stride, int32_t n_dats,
+                                const oppb_dat* dats, int32_t key_dat, uint64_t seed, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+    using namespace oppb;
+    const int rc = check_sort_args(size_bound, n_cells, stride, n_dats, dats, key_dat);
+    if (rc) return rc;
+    if (!count || !status || pending < 0 || seed == 0) return OPPB_ERR_ARG;
+    if (size_bound == 0) return OPPB_OK;
+    if (!workspace || workspace_bytes < oppb_sort_dev_workspace_bytes(size_bound)) return OPPB_ERR_WORKSPACE;
+    const SortCount cnt{size_bound, &count->size, pending, &status->remove_count};
+    return launch_sort(cnt, size_bound, n_cells, stride, n_dats, dats, key_dat, nullptr, workspace,
+                       as_stream(stream), seed);
 }

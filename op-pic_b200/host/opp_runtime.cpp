@@ -235,11 +235,17 @@ void opp_init(int argc, char** argv) {
     OPP_part_alloc_mult = (mult == DBL_MAX) ? 1.0 : mult;
     const std::string fill = opp_params->get<OPP_STRING>("opp_fill");
     const int period = opp_params->get<OPP_INT>("opp_fill_period");
+    // opp_init's parse (opp_lib/src/core/opp_lib_core.cpp:86-101); a value it does not know is
+    // refused here, where the reference would keep its default silently.
     if (fill == "HoleFill_All" || fill == "NOT FOUND") OPP_fill_type = OPP_HoleFill_All;
     else if (fill == "Sort_All") OPP_fill_type = OPP_Sort_All;
+    else if (fill == "Shuffle_All") OPP_fill_type = OPP_Shuffle_All;
     else if (fill == "Sort_Periodic") OPP_fill_type = OPP_Sort_Periodic;
-    else opp_abort("opp_fill " + fill + " is not supported on this backend");
-    if (OPP_fill_type == OPP_Sort_Periodic && period != INT_MAX && period >= 0) OPP_fill_period = period;
+    else if (fill == "Shuffle_Periodic") OPP_fill_type = OPP_Shuffle_Periodic;
+    else opp_abort("opp_fill " + fill + " is not a fill type");
+    if ((OPP_fill_type == OPP_Sort_Periodic || OPP_fill_type == OPP_Shuffle_Periodic) && period != INT_MAX &&
+        period >= 0)
+        OPP_fill_period = period;
     const int hops = opp_params->get<OPP_INT>("opp_move_max_hops");
     if (hops != INT_MAX && hops > 0) OPP_move_max_hops = hops;
     // B200 extension (absent from the reference's parameter files, default false): node-charge
@@ -588,8 +594,13 @@ bool opp_finalize_particle_move(opp_set set) {
     }
     set->particle_remove_count = st.remove_count;
     if (set->particle_remove_count <= 0) return false;
-    const bool sort = OPP_fill_type == OPP_Sort_All ||
-                      (OPP_fill_type == OPP_Sort_Periodic && OPP_main_loop_iter % OPP_fill_period == 0);
+    // The organize rule of opp_finalize_particle_move_core (opp_particle_organize_core.cpp:61-92).
+    const bool periodic = OPP_fill_type == OPP_Sort_Periodic || OPP_fill_type == OPP_Shuffle_Periodic;
+    const bool hole_fill = OPP_fill_type == OPP_HoleFill_All ||
+                           (periodic && (OPP_main_loop_iter % OPP_fill_period != 0 || OPP_comm_iteration != 0));
+    const bool sort = !hole_fill && (OPP_fill_type == OPP_Sort_All || OPP_fill_type == OPP_Sort_Periodic);
+    const bool shuffle = !hole_fill && (OPP_fill_type == OPP_Shuffle_All || OPP_fill_type == OPP_Shuffle_Periodic);
+    if (!hole_fill && !sort && !shuffle) opp_abort("OPP_fill_type is undefined");
     std::vector<oppb_dat> dats;
     int key = -1;
     for (opp_dat d : *set->particle_dats) {
@@ -600,6 +611,19 @@ bool opp_finalize_particle_move(opp_set set) {
         opp_profiler->start("Mv_sort_core");
         opp_particle_sort(set);
         opp_profiler->end("Mv_sort_core");
+    } else if (shuffle) {
+        // Random keys, removed particles last (oppb_shuffle); the seed follows the reference's
+        // RandomFunctor seed 123 and the iteration, so each shuffle draws new keys.
+        opp_profiler->start("Mv_shuffle_core");
+        if (key < 0) opp_abort("opp_finalize_particle_move: set has no mesh relation");
+        const int n_cells = set->cells_set ? set->cells_set->size : 0;
+        const uint64_t seed = (uint64_t(123) << 32) | (uint32_t)OPP_main_loop_iter | (uint64_t(1) << 63);
+        const size_t need = oppb_sort_workspace_bytes(set->size, n_cells);
+        check_oppb(oppb_shuffle(set->size, n_cells, stride_of(set), (int)dats.size(), dats.data(), key, seed, nullptr,
+                                oppb_rt::workspace(need), need, rt().stream),
+                   "oppb_shuffle");
+        for (opp_dat d : *set->particle_dats) std::swap(d->data_d, d->data_swap_d);
+        opp_profiler->end("Mv_shuffle_core");
     } else {
         opp_profiler->start("Mv_holefill_core");
         const size_t need = oppb_hole_fill_workspace_bytes(set->size, set->particle_remove_count);

@@ -41,6 +41,15 @@ class MoveStatus(C.Structure):
                 ("total_visits", c_u64), ("recheck_count", c_i32), ("reserved", c_i32)]
 
 
+class SetCount(C.Structure):
+    _fields_ = [("size", c_i32), ("error", c_i32), ("error_step", c_i32), ("steps", c_i32)]
+
+
+class StepRecord(C.Structure):
+    _fields_ = [("size_before_move", c_i32), ("removed", c_i32), ("size", c_i32), ("max_visits", c_i32),
+                ("total_visits", c_u64), ("recheck_count", c_i32), ("error", c_i32)]
+
+
 class Dat(C.Structure):
     _fields_ = [("data", c_vp), ("swap", c_vp), ("dim", c_i32), ("elem_bytes", c_i32)]
 
@@ -94,7 +103,8 @@ PRECISION_MIXED = 1
 
 class MoveOptions(C.Structure):
     _fields_ = [("precision", c_i32), ("deposit", c_i32), ("push", c_i32), ("reserved", c_i32),
-                ("qm", C.c_double), ("dt", C.c_double), ("band", C.c_double), ("dh", C.POINTER(DhGrid))]
+                ("qm", C.c_double), ("dt", C.c_double), ("band", C.c_double), ("dh", C.POINTER(DhGrid)),
+                ("set_count", c_vp), ("pending", c_i32), ("reserved2", c_i32)]
 
 
 class FieldSystem(C.Structure):
@@ -158,6 +168,18 @@ _SIGS = {
     "oppb_hole_fill_static": (C.c_int, [c_i32, c_i32, c_vp, c_i32, c_i32, P(Dat), c_vp]),
     "oppb_sort_workspace_bytes": (C.c_size_t, [c_i32, c_i32]),
     "oppb_sort_by_cell": (C.c_int, [c_i32, c_i32, c_i32, c_i32, P(Dat), c_i32, c_vp, c_vp, C.c_size_t, c_vp]),
+    "oppb_shuffle": (C.c_int, [c_i32, c_i32, c_i32, c_i32, P(Dat), c_i32, c_u64, c_vp, c_vp, C.c_size_t, c_vp]),
+    "oppb_inject_dev": (C.c_int, [P(TetMesh), P(Inlet), P(Particles), c_vp, c_i32, c_vp, c_i32, c_i32,
+                                  C.c_double, C.c_double, C.c_double, c_vp]),
+    "oppb_hole_fill_dev_workspace_bytes": (C.c_size_t, [c_i32]),
+    "oppb_hole_fill_dev": (C.c_int, [c_i32, c_vp, c_i32, c_vp, c_vp, c_i32, c_i32, P(Dat), c_vp, C.c_size_t,
+                                     c_vp]),
+    "oppb_sort_dev_workspace_bytes": (C.c_size_t, [c_i32]),
+    "oppb_sort_by_cell_dev": (C.c_int, [c_i32, c_vp, c_i32, c_vp, c_i32, c_i32, c_i32, P(Dat), c_i32, c_vp,
+                                        C.c_size_t, c_vp]),
+    "oppb_shuffle_dev": (C.c_int, [c_i32, c_vp, c_i32, c_vp, c_i32, c_i32, c_i32, P(Dat), c_i32, c_u64, c_vp,
+                                   C.c_size_t, c_vp]),
+    "oppb_step_end_dev": (C.c_int, [c_vp, c_i32, c_vp, c_vp, c_i32, c_vp]),
     "oppb_hex_mesh_pack": (C.c_int, [P(HexMesh), c_i32, c_vp, c_vp, c_vp]),
     "oppb_cabana_move_deposit": (C.c_int, [P(HexMesh), P(CabanaParticles), P(CabanaConsts), c_vp, c_i32, c_vp,
                                            c_i32, c_vp]),

@@ -238,6 +238,9 @@ class ParticleSet:
         return L.MoveStatus.from_buffer_copy(raw)
 
 
+FILL_MODES = ("HoleFill_All", "Sort_All", "Shuffle_All", "Sort_Periodic", "Shuffle_Periodic")
+
+
 @dataclass
 class StepTimes:
     move_ms: float = 0.0
@@ -251,7 +254,8 @@ class FemPIC:
 
     precision: 'f64' (bit-identical to the seq backend) or 'mixed' (FP32 push and tests
     with FP64 re-check; bit-identical cell decisions for the same positions).
-    fill: 'HoleFill_All' | 'Sort_All' | 'Sort_Periodic' as the reference's opp_fill.
+    fill: 'HoleFill_All' | 'Sort_All' | 'Sort_Periodic' | 'Shuffle_All' | 'Shuffle_Periodic' as the
+    reference's opp_fill (the shuffles sort by random keys, oppb_shuffle).
     """
 
     def __init__(self, hm: HostMesh, device: torch.device | str = "cuda", inject_per_step: int = 2000,
@@ -260,6 +264,8 @@ class FemPIC:
                  capacity: int = 0, max_hops: int = 4096, band: float = 1e-5, fused_deposit: bool = True,
                  fused_push: bool = True, direct_hop: float | None = None, dh_expansion=None,
                  field=None, spwt: float = 1.0, phi_inlet: float = 1.0, phi_fixed: float = 0.0):
+        if fill not in FILL_MODES:  # opp_finalize_particle_move_core aborts on an undefined fill type
+            raise ValueError(f"opp_fill {fill!r} is not one of {FILL_MODES}")
         if not torch.cuda.is_available():
             raise RuntimeError("FemPIC needs a CUDA device (there is no CPU fallback)")
         self.device = torch.device(device)
@@ -303,6 +309,11 @@ class FemPIC:
             self.spwt = float(spwt)
             self._field_graphs = {}
         self._pipeline(5, inject_per_step)
+        # Graph-captured steps (include/oppb_graph.h): the device count, its sync state, the
+        # captured graphs by (steps, phase, buffers, capacity) and a scratch count for warm-ups.
+        self.count_dev = torch.zeros(4, dtype=torch.int32, device=self.device)  # oppb_set_count
+        self._count_synced = False
+        self._graphs = {}
 
     # workspace shared by hole fill and sort (grown on demand)
     def _workspace(self, nbytes: int) -> torch.Tensor:
@@ -411,12 +422,21 @@ class FemPIC:
                                                               _ptr(self.node_charge), _ptr(ws), ws.numel(),
                                                               _stream_ptr(stream)))
 
+    def organize_kind(self) -> str:
+        """What a compaction at the current iteration does ('holefill', 'sort' or 'shuffle'):
+        opp_finalize_particle_move_core's rule (opp_lib/src/core/opp_particle_organize_core.cpp:49-95)."""
+        periodic = self.fill in ("Sort_Periodic", "Shuffle_Periodic")
+        if self.fill == "HoleFill_All" or (periodic and self.iter % self.fill_period != 0):
+            return "holefill"
+        return "sort" if self.fill.startswith("Sort") else "shuffle"
+
     def sort_now(self) -> bool:
-        if self.fill == "Sort_All":
-            return True
-        if self.fill == "Sort_Periodic":
-            return self.iter % self.fill_period == 0
-        return False
+        return self.organize_kind() == "sort"
+
+    def shuffle_seed(self) -> int:
+        """Seed of this iteration's shuffle keys (the reference seeds its RandomFunctor with 123,
+        opp_lib/src/cuda/opp_particle_sorter.cu:195-201; here 123 and the iteration)."""
+        return (123 << 32) | (self.iter & 0xFFFFFFFF) | (1 << 63)
 
     def finalize(self, remove_count: int, stream=None) -> str:
         """opp_finalize_particle_move: hole fill or cell sort, then size -= removed."""
@@ -425,19 +445,25 @@ class FemPIC:
         p = self.parts
         dats = p.dat_list()
         sp = _stream_ptr(stream)
-        if self.sort_now():
+        kind = self.organize_kind()
+        if kind == "sort":
             nbytes = self.lib.oppb_sort_workspace_bytes(p.size, self.mesh.n_cells)
             ws = self._workspace(nbytes)
             L.check("oppb_sort_by_cell", self.lib.oppb_sort_by_cell(
                 p.size, self.mesh.n_cells, p.capacity, len(p.DATS), dats, 3, None, _ptr(ws), ws.numel(), sp))
             p.swap_after_sort()
-            kind = "sort"
+        elif kind == "shuffle":
+            nbytes = self.lib.oppb_sort_workspace_bytes(p.size, self.mesh.n_cells)
+            ws = self._workspace(nbytes)
+            L.check("oppb_shuffle", self.lib.oppb_shuffle(
+                p.size, self.mesh.n_cells, p.capacity, len(p.DATS), dats, 3, self.shuffle_seed(), None, _ptr(ws),
+                ws.numel(), sp))
+            p.swap_after_sort()
         else:
             nbytes = self.lib.oppb_hole_fill_workspace_bytes(p.size, remove_count)
             ws = self._workspace(nbytes)
             L.check("oppb_hole_fill", self.lib.oppb_hole_fill(
                 p.size, remove_count, _ptr(p.bits), p.capacity, len(p.DATS), dats, _ptr(ws), ws.numel(), sp))
-            kind = "holefill"
         p.size -= remove_count
         return kind
 
@@ -463,6 +489,7 @@ class FemPIC:
         if st.error:
             raise L.OppbError(f"move (particle {st.error_index})", st.error)
         kind = self.finalize(st.remove_count, stream)
+        self._count_synced = False
         if not self.fused_deposit and self.precision == "f64":
             self.deposit(stream)
         if self.field is not None and self.field_enabled:
@@ -553,6 +580,195 @@ class FemPIC:
         copy.synchronize()
         cur.wait_stream(copy)
         return out
+
+    # ------------------------------------------------------------ graph-captured steps
+
+    def _bufs(self) -> tuple:
+        p = self.parts
+        return tuple(getattr(p, n) for n, _, _ in p.DATS) + tuple(getattr(p, n + "_swap") for n, _, _ in p.DATS)
+
+    def _set_bufs(self, bufs: tuple) -> None:
+        p, k = self.parts, len(self.parts.DATS)
+        for j, (n, _, _) in enumerate(p.DATS):
+            setattr(p, n, bufs[j])
+            setattr(p, n + "_swap", bufs[k + j])
+
+    def _graph_phase(self) -> int:
+        return self.iter % self.fill_period if self.fill.endswith("Periodic") else 0
+
+    def _step_dev(self, table: torch.Tensor, bound: int, records: torch.Tensor, n_records: int, stream=None,
+                  count=None, field: bool = True) -> None:
+        """One step on the device count (no host read): the launches of step() with the fused
+        push, sized from `bound`.  count: the oppb_set_count tensor (default self.count_dev)."""
+        p, m, lib = self.parts, self.mesh, self.lib
+        cnt = _ptr(self.count_dev if count is None else count)
+        st = _ptr(p.status)
+        sp = _stream_ptr(stream)
+        n_inj = int(table.shape[1])
+        self.zero_node_charge(stream)
+        v = p.view()
+        v.size = bound
+        L.check("oppb_inject_dev", lib.oppb_inject_dev(
+            C.byref(m.s), C.byref(m.inlet), C.byref(v), cnt, n_inj, _ptr(table), table.stride(0), table.shape[0],
+            self.ion_velocity, self.qm, self.dt, sp))
+        ws = self._deposit_ws()
+        o = L.MoveOptions(precision=L.PRECISION_MIXED if self.precision == "mixed" else L.PRECISION_F64,
+                          deposit=1, push=1, qm=self.qm, dt=self.dt, band=self.band, dh=None, set_count=cnt,
+                          pending=n_inj)
+        L.check("oppb_move_ex", lib.oppb_move_ex(C.byref(m.s), C.byref(v), C.byref(o), _ptr(self.node_charge), st,
+                                                 self.max_hops, _ptr(ws), ws.numel(), sp))
+        dats = p.dat_list()
+        kind = self.organize_kind()
+        cws = self._ws
+        if kind == "sort":
+            L.check("oppb_sort_by_cell_dev", lib.oppb_sort_by_cell_dev(
+                bound, cnt, n_inj, st, m.n_cells, p.capacity, len(p.DATS), dats, 3, _ptr(cws), cws.numel(), sp))
+            p.swap_after_sort()
+        elif kind == "shuffle":
+            L.check("oppb_shuffle_dev", lib.oppb_shuffle_dev(
+                bound, cnt, n_inj, st, m.n_cells, p.capacity, len(p.DATS), dats, 3, self.shuffle_seed(), _ptr(cws),
+                cws.numel(), sp))
+            p.swap_after_sort()
+        else:
+            L.check("oppb_hole_fill_dev", lib.oppb_hole_fill_dev(
+                bound, cnt, n_inj, st, _ptr(p.bits), p.capacity, len(p.DATS), dats, _ptr(cws), cws.numel(), sp))
+        L.check("oppb_step_end_dev", lib.oppb_step_end_dev(cnt, n_inj, st, _ptr(records), n_records, sp))
+        if field and self.field is not None and self.field_enabled:
+            self.field.launch(self.node_charge, self.n_vol, self.spwt, self.field_consts, self.mesh.ef, 4)
+        self.iter += 1
+
+    def _sync_count(self) -> None:
+        """Device count := host count (after host-sized steps)."""
+        if not self._count_synced:
+            self.count_dev.copy_(torch.tensor([self.parts.size, 0, 0, 0], dtype=torch.int32))
+            self._count_synced = True
+
+    def capture_steps(self, steps: int, n_inject: int | None = None, slack: float = 0.02) -> StepGraph:
+        """Captures `steps` whole steps, from the current iteration and particle buffers, as one
+        CUDA graph.  The capacity grows first when the count could exceed it (every particle
+        injected, none removed, plus `slack`)."""
+        if not self.fused_push:
+            raise ValueError("graph-captured steps need the fused push (fused_push=True)")
+        if self.dh is not None:
+            raise ValueError("graph-captured steps walk from the previous cell (no direct-hop seed)")
+        n_inj = self.inject_per_step if n_inject is None else int(n_inject)
+        p = self.parts
+        bound = int((p.size + steps * n_inj) * (1.0 + slack)) + 1
+        if bound > p.capacity:
+            p._alloc(max(bound, int(p.size + steps * n_inj * p.alloc_mult)))
+            self._graphs.clear()
+        bound = min(bound, p.capacity)
+        ws_bytes = max(self.lib.oppb_hole_fill_dev_workspace_bytes(bound),
+                       self.lib.oppb_sort_dev_workspace_bytes(bound))
+        self._workspace(ws_bytes)
+        self._deposit_ws()
+        tables = [torch.zeros((5, n_inj), dtype=torch.float64, device=self.device) for _ in range(steps)]
+        records = torch.zeros((steps, 8), dtype=torch.int32, device=self.device)
+        # Warm-up: one launch of every kernel the capture uses (the first launch of a kernel
+        # loads it), on a scratch count of -n_inj: the injection starts below 0 and writes
+        # nothing, and every later launch sees zero particles.
+        scratch = torch.zeros(4, dtype=torch.int32, device=self.device)
+        saved = (self._bufs(), self.iter, p.size, self.node_charge.clone(), p.status.clone())
+        for k in range(min(steps, max(1, self.fill_period if self.fill.endswith("Periodic") else 1))):
+            scratch.fill_(0)
+            scratch[0] = -n_inj
+            self._step_dev(tables[0], bound, records, steps, count=scratch, field=False)
+        if self.field is not None and self.field_enabled:
+            self.field.warm(self.node_charge, self.n_vol, self.spwt, self.field_consts, self.mesh.ef, 4)
+        self.node_charge.copy_(saved[3])
+        p.status.copy_(saved[4])
+        self._set_bufs(saved[0])
+        self.iter, p.size = saved[1], saved[2]
+        torch.cuda.synchronize(self.device)
+        self._sync_count()
+        launches0 = self.lib.oppb_kernel_launches()
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(device=self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                for k in range(steps):
+                    self._step_dev(tables[k], bound, records, steps)
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        launches = int(self.lib.oppb_kernel_launches() - launches0)
+        bufs_after = self._bufs()
+        self._set_bufs(saved[0])
+        self.iter, p.size = saved[1], saved[2]
+        return StepGraph(g, steps, bound, tables, records, saved[0], bufs_after, p.capacity, launches)
+
+    def graph_for(self, steps: int, n_inject: int | None = None) -> StepGraph:
+        """The captured graph for the next `steps` steps from here (captured when none fits)."""
+        n_inj = self.inject_per_step if n_inject is None else int(n_inject)
+        key = (steps, n_inj, self._graph_phase(), StepGraph.ptrs(self._bufs()), self.parts.capacity)
+        g = self._graphs.get(key)
+        if g is None or self.parts.size + steps * n_inj > g.bound:
+            g = self.capture_steps(steps, n_inj)
+            key = (steps, n_inj, self._graph_phase(), StepGraph.ptrs(self._bufs()), self.parts.capacity)
+            self._graphs[key] = g
+        return g
+
+    def replay(self, g: StepGraph, stream=None) -> list[dict]:
+        """Runs the steps of g (its tables as they are), then reads the count and the step records
+        back once.  Raises on a device error of any of the steps."""
+        if StepGraph.ptrs(g.bufs_before) != StepGraph.ptrs(self._bufs()) or g.capacity != self.parts.capacity:
+            raise ValueError("the graph was captured for other particle buffers")
+        self._sync_count()
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        with torch.cuda.stream(s):
+            g.graph.replay()
+        return self.replay_finish(g)
+
+    def replay_finish(self, g: StepGraph) -> list[dict]:
+        """After g.graph.replay() on the current stream (the device count in sync): reads the
+        count and the step records back and advances the host's view of the set."""
+        cnt = L.SetCount.from_buffer_copy(self.count_dev.cpu().numpy().tobytes())
+        raw = g.records.cpu().numpy().tobytes()
+        recs = [L.StepRecord.from_buffer_copy(raw[32 * k:32 * (k + 1)]) for k in range(g.steps)]
+        first = (cnt.steps - g.steps) % g.steps  # the ring position of this replay's first step
+        recs = [recs[(first + k) % g.steps] for k in range(g.steps)]
+        out = []
+        for k, r in enumerate(recs):
+            out.append({"iter": self.iter + k, "size_before_move": r.size_before_move, "removed": r.removed,
+                        "size": r.size, "visits": int(r.total_visits), "max_visits": r.max_visits,
+                        "rechecks": r.recheck_count, "error": r.error})
+        self.parts.size = cnt.size
+        self.iter += g.steps
+        self._set_bufs(g.bufs_after)
+        if cnt.error:
+            self.count_dev[1:3] = 0
+            raise L.OppbError(f"graph-captured step {cnt.error_step}", cnt.error)
+        self.last = out[-1]
+        return out
+
+    def run_graph(self, tables: list[torch.Tensor]) -> list[dict]:
+        """len(tables) steps from one graph replay; tables: device float64 [5][count] injection
+        tables (copied into the graph's own tables first)."""
+        g = self.graph_for(len(tables), int(tables[0].shape[1]))
+        for dst, src in zip(g.tables, tables):
+            if dst.data_ptr() != src.data_ptr():
+                dst.copy_(src)
+        return self.replay(g)
+
+
+class StepGraph:
+    """Whole FemPIC steps captured as one CUDA graph (include/oppb_graph.h): per step the node
+    charge reset, inject, push + move + deposit, hole fill / sort / shuffle, the step record and,
+    when on, the field phase, all sized from the device count.  `tables` are the device
+    injection tables the graph reads (step k reads tables[k]); `records` receive the steps'
+    oppb_step_record.  Valid while the particle count stays within `bound`, the particle
+    buffers and capacity are those of the capture and the step phase (iteration modulo the fill
+    period) is the same."""
+
+    def __init__(self, graph, steps: int, bound: int, tables, records, bufs_before, bufs_after, capacity: int,
+                 launches: int):
+        self.graph, self.steps, self.bound = graph, steps, bound
+        self.tables, self.records = tables, records
+        self.bufs_before, self.bufs_after, self.capacity = bufs_before, bufs_after, capacity
+        self.launches = launches  # library kernels per replay
+
+    @staticmethod
+    def ptrs(bufs) -> tuple:
+        return tuple(t.data_ptr() for t in bufs)
 
 
 def randoms_to_device(rnd_aos: np.ndarray, device) -> torch.Tensor:

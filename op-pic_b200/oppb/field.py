@@ -133,11 +133,10 @@ class FieldDevice:
     def status_host(self) -> L.FieldStatus:
         return L.FieldStatus.from_buffer_copy(self.status.cpu().numpy().tobytes())
 
-    def capture(self, den: torch.Tensor, n_vol: torch.Tensor, spwt: float, consts: FieldConstants,
-                ef: torch.Tensor, stride: int) -> torch.cuda.CUDAGraph:
-        """The field phase of a step (density, potential, field) as one CUDA graph."""
-        # First launches load the kernels: do them outside the capture, on scratch outputs
-        # (a solve with no CG iteration leaves D as it is; F1 is put back).
+    def warm(self, den: torch.Tensor, n_vol: torch.Tensor, spwt: float, consts: FieldConstants,
+             ef: torch.Tensor, stride: int) -> None:
+        """First launches load the kernels: run each once outside any capture, on scratch
+        outputs (a solve with no CG iteration leaves D as it is; F1 is put back)."""
         self.node_charge_density(den[:1].clone(), n_vol[:1], spwt)
         f1 = self.f1.clone()
         warm = FieldConstants(**{**consts.__dict__, "max_iter": 0})
@@ -145,13 +144,23 @@ class FieldDevice:
         self.f1.copy_(f1)
         self.electric_field(torch.empty_like(ef), stride)
         torch.cuda.synchronize(self.device)
+
+    def launch(self, den: torch.Tensor, n_vol: torch.Tensor, spwt: float, consts: FieldConstants,
+               ef: torch.Tensor, stride: int) -> None:
+        """The field phase's launches on the current stream: density, potential, field."""
+        self.node_charge_density(den, n_vol, spwt)
+        self.solve(den, consts)
+        self.electric_field(ef, stride)
+
+    def capture(self, den: torch.Tensor, n_vol: torch.Tensor, spwt: float, consts: FieldConstants,
+                ef: torch.Tensor, stride: int) -> torch.cuda.CUDAGraph:
+        """The field phase of a step (density, potential, field) as one CUDA graph."""
+        self.warm(den, n_vol, spwt, consts, ef, stride)
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream(device=self.device)
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
             with torch.cuda.graph(g, stream=s):
-                self.node_charge_density(den, n_vol, spwt)
-                self.solve(den, consts)
-                self.electric_field(ef, stride)
+                self.launch(den, n_vol, spwt, consts, ef, stride)
         torch.cuda.current_stream().wait_stream(s)
         return g

@@ -40,6 +40,15 @@ def steps(pos, vel, mdir, p2c, c2c, c_pos_ll, dt, extents, cell_width, n_steps, 
     return int(visits.value)
 
 
+def steps_job(args) -> tuple:
+    """One instance's n_steps in a worker process (args: pos, vel, mdir, p2c, c2c, c_pos_ll, dt,
+    extents, cell_width, n_steps); returns (pos, mdir, p2c, move calls of the last step)."""
+    pos, vel, mdir, p2c, c2c, c_pos_ll, dt, extents, cell_width, n_steps = args
+    pos, mdir, p2c = pos.copy(), mdir.copy(), p2c.copy()
+    v = steps(pos, vel, mdir, p2c, c2c, c_pos_ll, dt, extents, cell_width, n_steps)
+    return pos, mdir, p2c, v
+
+
 def run_reference(kind: str, nx, ny, cell_width, dt, pos, vel, mdir, p2c, c2c, c_pos_ll, n_steps,
                   threads: int | None = None) -> dict:
     """Run oracle/_ref/advec_ref_{seq,omp}: n_steps of update_pos + move.  Returns per-step wall

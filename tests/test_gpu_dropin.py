@@ -19,7 +19,8 @@ pytestmark = pytest.mark.gpu
 APP = Path(__file__).resolve().parent.parent / "op-pic_b200" / "lib" / "fempic_b200"
 
 
-@pytest.mark.parametrize("fill,period,steps", [("HoleFill_All", 10, 40), ("Sort_Periodic", 5, 30)])
+@pytest.mark.parametrize("fill,period,steps", [("HoleFill_All", 10, 200), ("Sort_Periodic", 10, 200),
+                                               ("Sort_Periodic", 5, 30)])
 def test_fempic_app_matches_oracle(tmp_path, fill, period, steps):
     hm = mesh()
     inject = 2000
@@ -147,3 +148,47 @@ def test_fempic_app_field_phase_matches_oracle(tmp_path):
     den = got["node_charge"]  # n_charge_den after compute_node_charge_density
     assert np.abs(den - o.node_charge).max() <= 1e-9 * np.abs(o.node_charge).max()
     assert np.abs(hm_o.c_ef - hm.c_ef).max() > 1e-6 * np.abs(hm.c_ef).max()  # the field phase changed the field
+
+
+def test_fempic_app_shuffle_holds_the_oracles_particles(tmp_path):
+    """opp_fill = Shuffle_Periodic through the drop-in runtime: the same sizes and removals as
+    the oracle's sorted run every step, and at the end the same particles (the seq backend's
+    shuffle sorts by cell; the GPU orders live particles by random keys)."""
+    hm = mesh()
+    inject, steps, period = 2000, 60, 4
+    dist = hm.inject_distribution(inject)
+    tables = [injection_randoms(13, s, inject, 0.1) for s in range(steps)]
+    R.write_case(tmp_path / "case.bin", hm, dist, steps, tables)
+    (tmp_path / "params.txt").write_text(R.params_text("Shuffle_Periodic", period, 2.0))
+    r = subprocess.run([str(APP), str(tmp_path / "params.txt"), str(tmp_path / "case.bin"), str(tmp_path / "out.bin")],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = R.read_output(tmp_path / "out.bin", hm.n_nodes)
+    o = O.OracleFemPIC(hm, dist, fill="Sort_Periodic", fill_period=period)
+    for s in range(steps):
+        out = o.step(tables[s])
+        rec = got["records"][s]
+        assert (int(rec["size"]), int(rec["removed"])) == (out["size"], out["removed"]), s
+    n = o.size
+
+    def rows(p2c, pos, vel, lc):
+        rec = np.concatenate([p2c.astype(np.int64)[:, None].view(np.uint64), pos.view(np.uint64),
+                              vel.view(np.uint64), lc.view(np.uint64)], axis=1)
+        return rec[np.lexsort(rec.T[::-1])]
+
+    np.testing.assert_array_equal(rows(got["p2c"], got["pos"], got["vel"], got["lc"]),
+                                  rows(o.p2c[:n], o.pos[:n], o.vel[:n], o.lc[:n]))
+    assert np.any(np.diff(got["p2c"]) < 0)  # live particles not in cell order
+    err = np.abs(got["node_charge"] - o.node_charge) / np.maximum(np.abs(o.node_charge), 1.0)
+    assert err.max() <= 1e-12
+
+
+def test_fempic_app_refuses_unknown_fill(tmp_path):
+    """An opp_fill value that is no fill type aborts at opp_init instead of running on."""
+    hm = mesh(4, 4, 8, 1.0, 1.0, 2.0)
+    dist = hm.inject_distribution(100)
+    R.write_case(tmp_path / "case.bin", hm, dist, 2, [injection_randoms(1, s, 100, 0.1) for s in range(2)])
+    (tmp_path / "params.txt").write_text(R.params_text("Shuffle_Sometimes", 4, 2.0))
+    r = subprocess.run([str(APP), str(tmp_path / "params.txt"), str(tmp_path / "case.bin"), str(tmp_path / "out.bin")],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and "fill" in (r.stdout + r.stderr)

@@ -93,3 +93,80 @@ def test_fullsize_mixed_cells_equal_fp64(big_mesh):
     (c_m, q_m, r_m, v_m), (c_f, q_f, r_f, v_f) = res["mixed"], res["f64"]
     assert torch.equal(c_m, c_f) and r_m == r_f and v_m == v_f
     assert float((q_m - q_f).abs().max() / q_f.abs().max()) <= 1e-5
+
+
+@pytest.fixture(scope="module")
+def steady_slice(big_mesh):
+    """Config 2's steady state: 300 steps of 250,000 ions (Sort_Periodic every 10) on the
+    2,654,208-tet mesh, one more injection and push, then a contiguous slice of 1,000,000
+    particles from the middle of the set: host copies of its positions and start cells."""
+    sim = FemPIC(big_mesh, DEV, inject_per_step=INJECT, fill="Sort_Periodic", fill_period=10, capacity=70_000_000)
+    gen = torch.Generator(device=DEV)
+    gen.manual_seed(0)
+    rnd = torch.empty((5, INJECT), dtype=torch.float64, device=DEV)
+    for _ in range(301):
+        rnd[0:2].uniform_(0.0, 1.0, generator=gen)
+        rnd[2:5].normal_(0.0, 0.1, generator=gen)
+        if sim.iter < 300:
+            sim.step(rnd)
+        else:
+            sim.inject(rnd)
+            sim.push()
+    n = sim.parts.size
+    k = 1_000_000
+    a = (n - k) // 2
+    state = {"n": n, "pos": sim.parts.pos[:, a:a + k].T.contiguous().cpu().numpy(),
+             "p2c": sim.parts.p2c[0, a:a + k].contiguous().cpu().numpy()}
+    del sim
+    torch.cuda.empty_cache()
+    return state
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_fullsize_steady_state_slice_bit_exact(big_mesh, steady_slice, precision):
+    """One steady-state move + deposit on 1,000,000 particles of config 2 (from a 57M-particle
+    set): cells, removals and visit counts equal the oracle's; FP64 weights bit for bit (mixed:
+    within 1e-5); node charges within 1e-12 relative (mixed: 1e-5 of the largest)."""
+    from oppb.fempic import DeviceMesh, ParticleSet
+    from oracle import oracle as O
+
+    assert steady_slice["n"] > 50_000_000
+    pos, p2c0 = steady_slice["pos"], steady_slice["p2c"]
+    k = len(p2c0)
+    dm = DeviceMesh(big_mesh, DEV, mixed=precision == "mixed")
+    ps = ParticleSet(DEV, k)
+    ps.size = k
+    ps.pos[:, :k] = torch.from_numpy(pos.T.copy()).to(DEV)
+    ps.p2c[0, :k] = torch.from_numpy(p2c0).to(DEV)
+    charge = torch.zeros(big_mesh.n_nodes, dtype=torch.float64, device=DEV)
+    nb = L.load().oppb_deposit_workspace_bytes(big_mesh.n_nodes)
+    ws = torch.empty(max(nb, 1), dtype=torch.uint8, device=DEV)
+    v = ps.view()
+    if precision == "f64":
+        rc = L.load().oppb_move_deposit_f64(C.byref(dm.s), C.byref(v), charge.data_ptr(), ps.status.data_ptr(), 4096,
+                                            ws.data_ptr(), nb, None)
+    else:
+        rc = L.load().oppb_move_deposit_mixed(C.byref(dm.s), C.byref(v), charge.data_ptr(), ps.status.data_ptr(),
+                                              4096, 1e-5, ws.data_ptr(), nb, None)
+    L.check("move_deposit", rc)
+    torch.cuda.synchronize()
+    st = ps.status_host()
+    got = ps.host_aos()
+
+    p2c = p2c0.copy()
+    lc = np.zeros((k, 4))
+    removed, visits, _ = O.move(pos, lc, p2c, big_mesh.c2c, big_mesh.c_vol, big_mesh.c_det, n=k)
+    keep = p2c != O.REMOVED
+    q = np.zeros(big_mesh.n_nodes)
+    O.deposit(np.ascontiguousarray(lc[keep]), np.ascontiguousarray(p2c[keep]), big_mesh.c2n, q)
+
+    assert st.error == 0 and st.remove_count == removed and int(st.total_visits) == visits
+    np.testing.assert_array_equal(got["p2c"], p2c)
+    qg = charge.cpu().numpy()
+    if precision == "f64":
+        np.testing.assert_array_equal(got["lc"][keep].view(np.uint64), lc[keep].view(np.uint64))
+        assert (np.abs(qg - q) / np.maximum(np.abs(q), 1.0)).max() <= 1e-12
+    else:
+        assert np.abs(got["lc"][keep] - lc[keep]).max() <= 1e-5
+        assert np.abs(qg - q).max() / np.abs(q).max() <= 1e-5
+    assert visits > k

@@ -263,8 +263,10 @@ def _run_both(precision, fill, steps, inject, seed=0, period=5, fused_push=True)
 @pytest.mark.parametrize("fused_push", [True, False])
 @pytest.mark.parametrize("fill", ["HoleFill_All", "Sort_Periodic"])
 def test_fempic_steps_f64(fill, fused_push):
+    """Config 1 at its own length: 200 steps of 2,000 ions on the 10x10x40-hex mesh (the count
+    reaches its plateau and removals through the far wall start), against the oracle."""
     last = None
-    for s, sim, orc in _run_both("f64", fill, 60, 2000, fused_push=fused_push):
+    for s, sim, orc in _run_both("f64", fill, 200, 2000, fused_push=fused_push, period=10):
         if s % 10 == 9 or s == 0:
             got = sim.parts.host_aos()
             n = orc.size
@@ -290,10 +292,11 @@ def test_fempic_steps_unfused_deposit():
 
 @pytest.mark.parametrize("fused_push", [True, False])
 def test_fempic_steps_mixed(fused_push):
-    """Mixed precision: same cells, counts and hop totals as the oracle running the same
-    FP32 push with FP64 cell decisions; weights and node charges within stated bounds."""
+    """Mixed precision (config 3, its 200 steps): same cells, counts and hop totals as the oracle
+    running the same FP32 push with FP64 cell decisions; weights and node charges within stated
+    bounds."""
     rechecks = 0
-    for s, sim, orc in _run_both("mixed", "HoleFill_All", 40, 2000, seed=2, fused_push=fused_push):
+    for s, sim, orc in _run_both("mixed", "HoleFill_All", 200, 2000, seed=2, fused_push=fused_push):
         rechecks += sim.last["rechecks"]
         if s % 10 == 9:
             got = sim.parts.host_aos()
