@@ -134,7 +134,12 @@ typedef struct oppb_tuning {
     int32_t advec_items; /* NESO-advection step: 256-particle work items per block pass, i.e.
                             particles per thread in flight (1, 2 or 4; default 2) */
     int32_t sort_gather_cols; /* cell sort: particle-dat columns gathered per launch (1..16, default 16) */
-    int32_t reserved[4];
+    int32_t move_lanes;  /* lanes per particle of the FP64 move: 1 (0 reads as 1) = a particle per thread,
+                            32 per warp; 2 = a particle per lane pair, 16 per warp, each lane reading one
+                            64-B half of the cell record and computing two of the four lambdas */
+    int32_t move_occupancy; /* lane-pair FP64 move: CTAs per SM it is compiled for, 8 (0 reads as 8;
+                               32 registers a thread) or 5 (48 registers, no spills) */
+    int32_t reserved[2];
 } oppb_tuning;
 
 /* Set / read the tuning used by subsequent launches (OPPB_ERR_ARG on unknown values). */

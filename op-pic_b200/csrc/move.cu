@@ -406,6 +406,158 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
     deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, l);
 }
 
+// ------------------------------------------------ FP64 move, two lanes per particle
+//
+// oppb_tuning.move_lanes = 2.  A cell visit of the one-lane kernel is five 256-bit loads by
+// one lane, each touching its own L1 line when the warp's lanes sit in different cells, so
+// the L1 data pipe serves five wavefronts per visit.  Here a lane pair walks one particle:
+// lane h reads the half [8h, 8h+8) of the 128-B det record (vertices 2h and 2h+1, two
+// 256-bit loads) and 16 B of the nav record (h = 0: coef and c2c[0..1]; h = 1: c2c[2..3]),
+// and computes lambda_2h and lambda_2h+1 with the reference's expression; both lanes of a
+// pair read the same lines, so a visit costs three wavefronts.  The pair agrees on the
+// inside test with a vote, gathers the other two lambdas by shuffles for the first-index
+// argmin, and takes the neighbour from the lane that holds it: the decisions and lambdas
+// are bit-identical to move_f64_kernel's.
+//
+// The CTA works in three phases.  (1) Thread t loads (and pushes) particle t with coalesced
+// accesses into shared memory.  (2) The 128 pairs take particles from a CTA counter until
+// the CTA's 256 are walked, so a long walk does not hold the other lanes of its warp idle.
+// (3) Thread t stores particle t's result and runs the accounting and deposit of the
+// one-lane kernel.
+
+constexpr int kInfoVisits = 0x3fffffff, kInfoRemoved = 1 << 30, kInfoFailed = 1 << 31;
+
+// One lambda of the reference expression coef * (((d0 - d1 x) + d2 y) - d3 z).
+__device__ __forceinline__ double lambda_f64(double coef, double d0, double d1, double d2, double d3, double x,
+                                             double y, double z) {
+    double t = __dsub_rn(d0, __dmul_rn(d1, x));
+    t = __dadd_rn(t, __dmul_rn(d2, y));
+    t = __dsub_rn(t, __dmul_rn(d3, z));
+    return __dmul_rn(coef, t);
+}
+
+__device__ __forceinline__ bool in_band_f64(double l) { return (l > -kTol) && (__dsub_rn(l, 1.0) < kTol); }
+
+template <int kDep, bool kPush, bool kDevCount, int kOcc>
+__global__ void __launch_bounds__(kMoveBlock, kOcc)
+    move_f64_pair_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
+                         PushArgs push) {
+    __shared__ NodeTable table;
+    __shared__ double s_x[3][kMoveBlock];
+    __shared__ double s_l[4][kMoveBlock];
+    __shared__ int32_t s_cell[kMoveBlock];
+    __shared__ int32_t s_cell0[kMoveBlock];
+    __shared__ int32_t s_info[kMoveBlock];
+    __shared__ int s_next;
+    const int32_t n = kDevCount ? live_count(p) : p.size;
+    const int64_t base = (int64_t)blockIdx.x * kMoveBlock;
+    if (kDevCount && base >= n) return;  // beyond the device count (whole block)
+    if (kDep == kDepTable) table_init(table);
+    const int t = threadIdx.x;
+    {
+    const int64_t i = base + t;
+    const bool active = i < n;
+    const int32_t cell0 = active ? ld_stream(p.p2c + i) : kRemoved;
+    // (1) load and push
+    if (active && cell0 != kRemoved) {
+        double x = ld_stream(p.pos + i);
+        double y = ld_stream(p.pos + p.stride + i);
+        double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
+        if (kPush && (uint32_t)cell0 < (uint32_t)m.n_cells) push_prologue<false>(m, p, push, i, cell0, x, y, z);
+        s_x[0][t] = x;
+        s_x[1][t] = y;
+        s_x[2][t] = z;
+    }
+    s_cell[t] = cell0;
+    s_cell0[t] = cell0;
+    s_info[t] = 0;
+    if (t == 0) s_next = 0;
+    }
+    __syncthreads();
+    // (2) pairs walk the CTA's particles
+    {
+        const int count = (int64_t)n - base < kMoveBlock ? (int)((int64_t)n - base) : kMoveBlock;
+        const int lane = t & 31;
+        const int h = lane & 1;
+        const int src0 = lane & 30;
+        const unsigned pm = 3u << src0;
+        for (;;) {
+            int slot = 0;
+            if (h == 0) slot = atomicAdd(&s_next, 1);
+            slot = __shfl_sync(pm, slot, src0);
+            if (slot >= count) break;
+            int32_t cell = s_cell[slot];
+            if (cell == kRemoved) continue;
+            double la = 0.0, lb = 0.0;  // lambda_2h, lambda_2h+1
+            int visits = 0, err = 0;
+            bool removed = false;
+            for (;;) {
+                if ((uint32_t)cell >= (uint32_t)m.n_cells) {
+                    err = OPPB_ERR_CELL_RANGE;
+                    break;
+                }
+                const double* d = m.det + (int64_t)cell * 16 + 8 * h;
+                double a0, b0, g0, d0, a1, b1, g1, d1;
+                ldg256(d, a0, b0, g0, d0);
+                ldg256(d + 4, a1, b1, g1, d1);
+                const double2 nv = ldg_d2(m.nav + (int64_t)cell * 4 + 2 * h);
+                const double coef = __shfl_sync(pm, nv.x, src0);
+                // the position from shared memory at every visit: registers are what the walk is short of
+                const double x = s_x[0][slot], y = s_x[1][slot], z = s_x[2][slot];
+                la = lambda_f64(coef, a0, b0, g0, d0, x, y, z);
+                lb = lambda_f64(coef, a1, b1, g1, d1, x, y, z);
+                visits++;
+                if (__all_sync(pm, in_band_f64(la) && in_band_f64(lb))) break;
+                const double oa = __shfl_xor_sync(pm, la, 1), ob = __shfl_xor_sync(pm, lb, 1);
+                const double l[4] = {h ? oa : la, h ? ob : lb, h ? la : oa, h ? lb : ob};
+                const int mi = argmin4(l);
+                // c2c[0..1] are lane 0's nv.y, c2c[2..3] lane 1's nv.x.
+                const double pair_bits = __shfl_sync(pm, h ? nv.x : nv.y, src0 + (mi >> 1));
+                const long long b = __double_as_longlong(pair_bits);
+                const int32_t next = (mi & 1) ? (int32_t)(b >> 32) : (int32_t)(b & 0xffffffffll);
+                if (next < 0) {
+                    cell = kRemoved;
+                    removed = true;
+                    break;
+                }
+                cell = next;
+                if (visits >= max_hops) {
+                    err = OPPB_ERR_HOP_LIMIT;
+                    break;
+                }
+            }
+            s_l[2 * h][slot] = la;
+            s_l[2 * h + 1][slot] = lb;
+            if (h == 0) {
+                s_cell[slot] = cell;
+                s_info[slot] = visits | (removed ? kInfoRemoved : 0) | (err ? kInfoFailed : 0);
+                if (err) raise_error(st, err, (int32_t)(base + slot));
+            }
+        }
+    }
+    __syncthreads();
+    // (3) results, accounting, deposit
+    const int64_t i = base + t;
+    const bool active = i < n;
+    const int32_t cell0 = s_cell0[t];
+    int visits = 0;
+    bool newly_removed = false, failed = false;
+    int32_t cell = cell0;
+    double l[4] = {0.0, 0.0, 0.0, 0.0};
+    if (active && cell0 != kRemoved) {
+        const int info = s_info[t];
+        visits = info & kInfoVisits;
+        newly_removed = (info & kInfoRemoved) != 0;
+        failed = (info & kInfoFailed) != 0;
+        cell = s_cell[t];
+#pragma unroll
+        for (int k = 0; k < 4; k++) l[k] = s_l[k][t];
+        store_result(p, i, l, visits, cell, cell0);
+    }
+    cta_account(p, st, i, active, cell, newly_removed, visits, 0);
+    deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && !newly_removed && !failed, cell, l);
+}
+
 // -------------------------------------------------------- mixed FP32 / FP64 move
 //
 // lambda_i(x) = c_i + g_i . (x - o) for i = 0..2 with o = f32(vertex 0), c_i, g_i in f32,
@@ -662,6 +814,18 @@ Replicas make_replicas(double* node_charge, void* workspace, size_t workspace_by
 
 enum MoveKind { kMoveOnly, kMoveDepositF64, kMoveDepositMixed };
 
+// The pair kernel for the tuned deposit, compiled for kOcc resident CTAs per SM.
+template <bool kPush, bool kDevCount, int kOcc>
+void launch_pair(int grid, cudaStream_t s, bool table, bool exact, const oppb_tet_mesh& m, const PartArgs& p,
+                 const DepositArgs& d, oppb_move_status* st, int32_t max_hops, const PushArgs& push) {
+    if (table)
+        move_f64_pair_kernel<kDepTable, kPush, kDevCount, kOcc><<<grid, kMoveBlock, 0, s>>>(m, p, d, st, max_hops, push);
+    else if (exact)
+        move_f64_pair_kernel<kDepExact, kPush, kDevCount, kOcc><<<grid, kMoveBlock, 0, s>>>(m, p, d, st, max_hops, push);
+    else
+        move_f64_pair_kernel<kDepWarp, kPush, kDevCount, kOcc><<<grid, kMoveBlock, 0, s>>>(m, p, d, st, max_hops, push);
+}
+
 template <int kKind, bool kPush, bool kSeed = false, bool kDevCount = false>
 int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
                 oppb_move_status* status, int32_t max_hops, double band, const PushArgs& push, void* workspace,
@@ -697,7 +861,13 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
         move_f64_kernel<kDepNone, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops,
                                                                            push, dh);
     else if constexpr (kKind == kMoveDepositF64) {
-        if (table)
+        if (!kSeed && tuning().move_lanes == 2) {  // a particle per lane pair
+            if (tuning().move_occupancy == 5)
+                launch_pair<kPush, kDevCount, 5>(grid, s, table, exact, *mesh, p, rep.args, status, max_hops, push);
+            else
+                launch_pair<kPush, kDevCount, kMinBlocks>(grid, s, table, exact, *mesh, p, rep.args, status, max_hops,
+                                                          push);
+        } else if (table)
             move_f64_kernel<kDepTable, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                                 max_hops, push, dh);
         else if (exact)

@@ -56,7 +56,7 @@ class Dat(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("advec_items", c_i32), ("sort_gather_cols", c_i32),
-                ("reserved", c_i32 * 4)]
+                ("move_lanes", c_i32), ("move_occupancy", c_i32), ("reserved", c_i32 * 2)]
 
 
 DEPOSIT_WARP_ATOMIC = 0
@@ -237,7 +237,8 @@ def check(fn: str, status: int) -> None:
 
 
 def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_items: int | None = None,
-               sort_gather_cols: int | None = None) -> None:
+               sort_gather_cols: int | None = None, move_lanes: int | None = None,
+               move_occupancy: int | None = None) -> None:
     t = Tuning()
     load().oppb_get_tuning(C.byref(t))
     if deposit is not None:
@@ -248,6 +249,10 @@ def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_it
         t.advec_items = advec_items
     if sort_gather_cols is not None:
         t.sort_gather_cols = sort_gather_cols
+    if move_lanes is not None:
+        t.move_lanes = move_lanes
+    if move_occupancy is not None:
+        t.move_occupancy = move_occupancy
     check("oppb_set_tuning", load().oppb_set_tuning(C.byref(t)))
 
 

@@ -1,13 +1,16 @@
 """The launch choices of the FemPIC path, picked by timing them on the live state.
 
-The move + deposit launch has two choices (oppb_tuning): the deposit strategy (warp-matched
+The move + deposit launch has four choices (oppb_tuning): the FP64 move's lanes per particle
+(one, 32 particles per warp, or a lane pair, 16 per warp) and, for the pair kernel, the CTAs per
+SM it is compiled for (8 at 32 registers a thread, 5 at 48); the deposit strategy (warp-matched
 FP64 atomics, or a per-CTA shared-memory node table) and how many node-sum copies the atomics
-are spread over; the cell sort has one (particle-dat columns gathered per launch).  tune_move
+are spread over.  The cell sort has one (particle-dat columns gathered per launch).  tune_move
 and tune_sort time every candidate on the simulation's current particle state, restoring a
 snapshot of the particle dats before each trial so that every candidate sees the same input,
 then keep the fastest as the process-wide tuning.  The choice of a trial is the median of
-its repetitions.  The sort interval is not tuned: it is the reference's Sort_Periodic period,
-which fixes the particle order the results are compared in.
+its repetitions.  tune_sort_period times whole sort cycles (the steps between two cell sorts)
+for candidate Sort_Periodic periods from a snapshot of the state and reports the cost per
+particle-step of each; results stay bit-exact for any period (the oracle runs the same one).
 """
 from __future__ import annotations
 
@@ -21,7 +24,9 @@ import torch
 from oppb import _lib as L
 
 MOVE_CANDIDATES = [(dep, rep) for dep in (L.DEPOSIT_WARP_ATOMIC, L.DEPOSIT_CTA_TABLE) for rep in (1, 4, 8, 16)]
+LANE_CANDIDATES = [(1, 8), (2, 8), (2, 5)]  # (move_lanes, move_occupancy)
 SORT_CANDIDATES = [16, 10, 5]
+PERIOD_CANDIDATES = [5, 10, 20]
 
 
 @dataclass
@@ -111,6 +116,111 @@ def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None
     finally:
         snap.restore()
     L.set_tuning(deposit=res.choice[0], replicas=res.choice[1])
+    return res
+
+
+def tune_lanes(sim, candidates=None, reps: int = 3, with_push: bool | None = None) -> TuneResult:
+    """Lanes per particle and compiled occupancy of the FP64 move + deposit launch (the mixed
+    kernel has one lane per particle: nothing to tune there), timed as tune_move times its
+    candidates, with the deposit choice in force.  Sets the fastest; sim's state is left as found."""
+    if sim.precision != "f64":
+        return TuneResult(choice=(1, 8))
+    before = L.Tuning()
+    L.load().oppb_get_tuning(C.byref(before))
+    cands = candidates or LANE_CANDIDATES
+    if not snapshot_fits(sim):
+        return TuneResult(choice=(before.move_lanes, before.move_occupancy))
+    snap = ParticleSnapshot(sim)
+    fused = sim.fused_push if with_push is None else with_push
+
+    def run(c) -> float:
+        L.set_tuning(move_lanes=c[0], move_occupancy=c[1])
+        snap.restore()
+        if fused:
+            return _timed(sim.push_move)
+        sim.push()
+        return _timed(sim.move)
+
+    try:
+        res = pick(cands, run, reps)
+    except Exception:
+        L.load().oppb_set_tuning(C.byref(before))
+        raise
+    finally:
+        snap.restore()
+    L.set_tuning(move_lanes=res.choice[0], move_occupancy=res.choice[1])
+    return res
+
+
+class StateSnapshot:
+    """The whole particle state of a FemPIC sim (count, iteration, dats over [0, size), the
+    buffer roles), restored before each trial of a multi-step measurement."""
+
+    def __init__(self, sim):
+        self.sim = sim
+        p = sim.parts
+        self.size, self.iter, self.period = p.size, sim.iter, sim.fill_period
+        self.bufs = sim._bufs()
+        self.saved = {name: getattr(p, name)[:, :p.size].clone() for name, _, _ in p.DATS}
+
+    def restore(self) -> None:
+        sim, p = self.sim, self.sim.parts
+        sim._set_bufs(self.bufs)
+        for name, t in self.saved.items():
+            getattr(p, name)[:, :t.shape[1]].copy_(t)
+        p.size, sim.iter, sim.fill_period = self.size, self.iter, self.period
+        sim._count_synced = False
+        sim.zero_node_charge()
+
+
+def state_snapshot_fits(sim, steps: int, headroom: float = 1.25) -> bool:
+    """Whether a StateSnapshot fits, and the state can grow by `steps` injections within capacity."""
+    p = sim.parts
+    return snapshot_fits(sim, headroom) and p.size + steps * sim.inject_per_step <= p.capacity
+
+
+def tune_sort_period(sim, tables, candidates=None) -> TuneResult:
+    """Cost of a Sort_Periodic cycle per particle-step for each candidate period P: from a
+    snapshot of the state, P steps (hole fills, then the cell sort on the cycle's last step),
+    timed over the move + compaction launches as the bench times its steps; tables: device
+    injection tables, used in turn.  times_ms holds nanoseconds per particle-step (the
+    comparison the choice is made on).  The period is reported, not set: sim.fill_period and
+    the state are left as found."""
+    cands = candidates or PERIOD_CANDIDATES
+    if not sim.fill.startswith("Sort") or not state_snapshot_fits(sim, max(cands)):
+        return TuneResult(choice=sim.fill_period)
+    snap = StateSnapshot(sim)
+    s = torch.cuda.current_stream()
+
+    def run(period) -> float:
+        snap.restore()
+        sim.fill_period = period
+        sim.iter = period * (1 + sim.iter // period) - period + 1  # the cycle ends with the sort step
+        ps, t = 0, 0.0
+        for k in range(period):
+            sim.inject(tables[k % len(tables)])
+            sim.zero_node_charge()
+            n = sim.parts.size
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record(s)
+            sim.push_move() if sim.fused_push else (sim.push(), sim.move())
+            e[1].record(s)
+            st = sim.parts.status_host()
+            if st.error:
+                raise L.OppbError("move", st.error)
+            e[2].record(s)
+            sim.finalize(st.remove_count)
+            e[3].record(s)
+            e[3].synchronize()
+            sim.iter += 1
+            ps += n
+            t += e[0].elapsed_time(e[1]) + e[2].elapsed_time(e[3])
+        return 1e6 * t / ps  # ns per particle-step
+
+    try:
+        res = pick(cands, run, reps=1)
+    finally:
+        snap.restore()
     return res
 
 
