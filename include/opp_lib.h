@@ -9,12 +9,30 @@
 
 #include <cuda_runtime_api.h>
 
+// The standard headers the reference's opp_lib.h brings in transitively (opp_defs.h,
+// opp_util.h, opp_params.h, opp_profiler.h): app headers written against it, such as the
+// FemPIC mesh loader, rely on them.
+#include <algorithm>
+#include <array>
+#include <cfloat>
+#include <chrono>
+#include <cinttypes>
 #include <climits>
+#include <cmath>
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <iomanip>
+#include <iostream>
+#include <limits>
 #include <map>
 #include <memory>
+#include <random>
+#include <sstream>
+#include <stack>
 #include <string>
 #include <vector>
 
@@ -41,6 +59,10 @@ typedef std::string OPP_STRING;
 #define OPP_ARG_MAP 2
 
 #define OPP_RUN_ON_ROOT(command) if (OPP_rank == OPP_ROOT command)
+// Early returns of app functions on ranks outside the run (opp_defs.h:184-187).
+#define OPP_RETURN_IF_INVALID_PROCESS if (OPP_rank < 0) return;
+#define OPP_RETURN_ZERO_IF_INVALID_PROCESS if (OPP_rank < 0) return 0;
+#define OPP_RETURN_EMPTY_IF_INVALID_PROCESS if (OPP_rank < 0) return "";
 
 enum opp_iterate_type { OPP_ITERATE_ALL = 1, OPP_ITERATE_INJECTED };
 enum opp_move_status { OPP_MOVE_DONE = 0, OPP_NEED_MOVE, OPP_NEED_REMOVE };
@@ -209,6 +231,11 @@ extern double OPP_part_alloc_mult;
 extern int OPP_iter_start;
 extern int OPP_iter_end;
 extern int OPP_move_max_hops;       // bound on cell visits per particle and move
+// Communication and hop statistics the apps' logs print (opp_defs.h:428-439); one GPU has no
+// communication rounds, so they stay 0.
+extern int OPP_max_comm_iteration;
+extern int OPP_part_comm_count_per_iter;
+extern int OPP_move_moreX_hops;
 extern std::vector<opp_set> opp_sets;
 extern std::vector<opp_map> opp_maps;
 extern std::vector<opp_dat> opp_dats;
@@ -283,6 +310,18 @@ int opp_mpi_halo_exchanges_grouped(opp_set set, int nargs, opp_arg* args, Device
 void opp_mpi_halo_wait_all(int nargs, opp_arg* args);
 void opp_set_dirtybit_grouped(int nargs, opp_arg* args, DeviceType device);
 inline int64_t opp_get_global_value(int64_t value) { return value; }
+// Sum, maximum and minimum over ranks (opp_util.h:274): on one GPU, the value three times.
+inline void opp_get_global_values(const int64_t value, int64_t& gbl_value, int64_t& gbl_max, int64_t& gbl_min) {
+    gbl_value = gbl_max = gbl_min = value;
+}
+
+// printf-formatted value (opp_util.h:85).
+template <typename T>
+std::string str(T value, std::string format) {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, format.c_str(), value);
+    return std::string(buf);
+}
 
 // --------------------------------------------------------- B200 extensions
 // Device-resident packed mesh and scratch shared by the generated-loop entry points.

@@ -52,7 +52,9 @@ extern "C" {
  *   ef    [n_cells][4]  f64 : cell electric field x,y,z + pad
  *   geo32 [n_cells][16] f32 : mixed path, for vertices 0..2 {lambda_i(o), dlambda_i/dx,
  *                             dlambda_i/dy, dlambda_i/dz} about origin o, then o = vertex 0
- *                             rounded to f32 (3 floats) and one zero word; lambda_3 is
+ *                             rounded to f32 (3 floats) and G, the rounded-up sum of the nine
+ *                             |dlambda_i/dx_j| (the FP32 error bound's factor; +inf when the
+ *                             rows' |lambda_i(o)| sum above 1.001); lambda_3 is
  *                             1 - lambda_0 - lambda_1 - lambda_2 (may be NULL)
  *   nav32 [n_cells][8] 32-bit: mixed path origin o (3 floats), one unused word,
  *                             c2c[0..3] as int32 (may be NULL) */

@@ -71,14 +71,22 @@ __global__ void pack_kernel(PackIn in, oppb_tet_mesh m, int32_t* invalid_out) {
             const float oy = (float)in.n_pos[ps + nd.x];
             const float oz = (float)in.n_pos[2 * ps + nd.x];
             reinterpret_cast<float4*>(m.nav32 + c * 8)[0] = make_float4(ox, oy, oz, 0.0f);
-            reinterpret_cast<float4*>(m.geo32 + c * 16)[3] = make_float4(ox, oy, oz, 0.0f);
+            // The record's last word bounds the rows' gradients: G = sum_ij |g_ij| of the stored
+            // f32 values, rounded up, so that S = sum_i (|c_i| + sum_j |g_ij| |d_j|) <= 1.001 +
+            // G max_j |d_j|; a cell whose sum_i |c_i| exceeds 1.001 (c_i = lambda_i(o) with o its
+            // vertex 0 is 1, 0, 0 to rounding) gets G = +inf, so all its visits are re-checked.
+            double gsum = 0.0, csum = 0.0;
 #pragma unroll
             for (int i = 0; i < 3; i++) {
                 const double a = d[4 * i], b = d[4 * i + 1], g = d[4 * i + 2], e = d[4 * i + 3];
                 const double li = cf * (((a - b * (double)ox) + g * (double)oy) - e * (double)oz);
-                reinterpret_cast<float4*>(m.geo32 + c * 16)[i] =
-                    make_float4((float)li, (float)(-cf * b), (float)(cf * g), (float)(-cf * e));
+                const float4 row = make_float4((float)li, (float)(-cf * b), (float)(cf * g), (float)(-cf * e));
+                reinterpret_cast<float4*>(m.geo32 + c * 16)[i] = row;
+                csum += fabs((double)row.x);
+                gsum += fabs((double)row.y) + fabs((double)row.z) + fabs((double)row.w);
             }
+            const float gbound = csum <= 1.001 ? __double2float_ru(gsum * (1.0 + 0x1p-20)) : __int_as_float(0x7f800000);
+            reinterpret_cast<float4*>(m.geo32 + c * 16)[3] = make_float4(ox, oy, oz, gbound);
         }
     }
     if (invalid_out) {

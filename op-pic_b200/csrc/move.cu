@@ -566,12 +566,15 @@ __global__ void __launch_bounds__(kMoveBlock, kOcc)
 // FP32 error of lambda_0..2 is below 6u S_i (rounding of c, g, d and of the three FMAs),
 // and that of lambda_3 below 6u (S_0 + S_1 + S_2) + 3u (1 + S_0 + S_1 + S_2) (the three
 // subtractions), so below 9u (1 + S) with S = S_0 + S_1 + S_2.  For S <= kMaxS = 16 every
-// error is below 9.2e-6 < band = 1e-5.  A decision is taken in FP32 only when every
+// error is below 9.2e-6 < band = 1e-5.  S is bounded per visit by 1.001 + G max_j |d_j|,
+// G the cell's rounded-up sum of |g_ij| (the record's last word, +inf for a cell whose
+// sum of |c_i| exceeds 1.001), evaluated with one FMA and compared with kMaxS less 2^-20 of
+// it, which covers that FMA's rounding.  A decision is taken in FP32 only when every
 // threshold (-1e-10, 1+1e-10) and, outside the cell, every argmin tie is at least `band`
-// away and S <= kMaxS; otherwise the visit is recomputed with the FP64 reference
-// expression.  Hence every decision equals the FP64 one.
+// away and the bound is within kMaxS; otherwise the visit is recomputed with the FP64
+// reference expression.  Hence every decision equals the FP64 one.
 
-constexpr float kMaxS = 16.0f;
+constexpr float kMaxS = 16.0f * (1.0f - 0x1p-20f);
 
 // The band's thresholds, precomputed on the host: kernel parameters live in the constant
 // bank and are used as instruction operands without occupying registers.
@@ -624,14 +627,13 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
             const float dx = (float)(x - (double)g1[4]);
             const float dy = (float)(y - (double)g1[5]);
             const float dz = (float)(z - (double)g1[6]);
+            const float ssum = fmaf(g1[7], fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))), 1.001f);
             const float rows[12] = {g0[0], g0[1], g0[2], g0[3], g0[4], g0[5], g0[6], g0[7],
                                     g1[0], g1[1], g1[2], g1[3]};
-            float ssum = 0.0f;
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 const float c0 = rows[4 * k], gx = rows[4 * k + 1], gy = rows[4 * k + 2], gz = rows[4 * k + 3];
                 lf[k] = fmaf(gz, dz, fmaf(gy, dy, fmaf(gx, dx, c0)));
-                ssum += fabsf(c0) + fabsf(gx) * fabsf(dx) + fabsf(gy) * fabsf(dy) + fabsf(gz) * fabsf(dz);
             }
             lf[3] = ((1.0f - lf[0]) - lf[1]) - lf[2];
             // Classify in FP32.

@@ -22,6 +22,9 @@ int OPP_rank = 0;
 int OPP_comm_size = 1;
 int OPP_main_loop_iter = 0;
 int OPP_comm_iteration = 0;
+int OPP_max_comm_iteration = 0;
+int OPP_part_comm_count_per_iter = 0;
+int OPP_move_moreX_hops = 0;
 int OPP_fill_period = 4;
 opp_fill_type OPP_fill_type = OPP_HoleFill_All;
 double OPP_part_alloc_mult = 1.0;

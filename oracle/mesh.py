@@ -167,3 +167,51 @@ def area_distribution(if_area: np.ndarray, total: int) -> np.ndarray:
         cum = total if f == n - 1 else int(r) + (1 if x - r >= 0.5 else 0)  # llround: halves away from 0
         dist[f] = min(cum, total)
     return np.maximum.accumulate(dist)
+
+
+def write_box_files(dims, out_dir) -> dict:
+    """The box as the app's text mesh files (the formats LoadVolumeMesh and LoadSurfaceMesh
+    read, apps/app_fempic/minifempic_funcs.h:230-270,477-520), the same text the reference
+    harness writes: mesh.dat (node list in mm, 304 tetrahedra), inlet.dat (the z=0 nodes and the
+    203 inlet triangles), wall.dat (the z=lz nodes).  Returns the three paths."""
+    from pathlib import Path
+
+    nx, ny, nz, lx, ly, lz = dims
+    out = Path(out_dir)
+    NX, NY = nx + 1, ny + 1
+
+    def coords(n, l):
+        h = l / n
+        x = [float(i) * h for i in range(n + 1)]
+        x[n] = l
+        return [repr(v * 1000.0) for v in x]
+
+    cx, cy, cz = coords(nx, lx), coords(ny, ly), coords(nz, lz)
+    nid = lambda i, j, k: i + NX * (j + NY * k) + 1  # noqa: E731
+    node = lambda i, j, k: f"{nid(i, j, k)} {cx[i]} {cy[j]} {cz[k]}"  # noqa: E731
+    lines = [f"{NX * NY * (nz + 1)} {6 * nx * ny * nz}"]
+    lines += [node(i, j, k) for k in range(nz + 1) for j in range(NY) for i in range(NX)]
+    e = 1
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                for a, b, _ in _PERM:
+                    o1 = [0, 0, 0]
+                    o1[a] = 1
+                    o2 = list(o1)
+                    o2[b] = 1
+                    lines.append(f"{e} 304 {nid(i, j, k)} {nid(i + o1[0], j + o1[1], k + o1[2])} "
+                                 f"{nid(i + o2[0], j + o2[1], k + o2[2])} {nid(i + 1, j + 1, k + 1)}")
+                    e += 1
+    (out / "mesh.dat").write_text("\n".join(lines) + "\n")
+    lines = [f"{NX * NY} {2 * nx * ny}"] + [node(i, j, 0) for j in range(NY) for i in range(NX)]
+    e = 1
+    for j in range(ny):
+        for i in range(nx):
+            n000, n100, n010, n110 = nid(i, j, 0), nid(i + 1, j, 0), nid(i, j + 1, 0), nid(i + 1, j + 1, 0)
+            lines += [f"{e} 203 {n000} {n110} {n100}", f"{e + 1} 203 {n000} {n010} {n110}"]
+            e += 2
+    (out / "inlet.dat").write_text("\n".join(lines) + "\n")
+    lines = [f"{NX * NY} 0"] + [node(i, j, nz) for j in range(NY) for i in range(NX)]
+    (out / "wall.dat").write_text("\n".join(lines) + "\n")
+    return {"global_mesh": out / "mesh.dat", "inlet_mesh": out / "inlet.dat", "wall_mesh": out / "wall.dat"}

@@ -4,6 +4,7 @@ and matches the oracle: identical sizes and removals per step, identical final p
 state (cells, positions, velocities, weights), node charges within 1e-12 relative."""
 from __future__ import annotations
 
+import re
 import subprocess
 from pathlib import Path
 
@@ -192,3 +193,68 @@ def test_fempic_app_refuses_unknown_fill(tmp_path):
     r = subprocess.run([str(APP), str(tmp_path / "params.txt"), str(tmp_path / "case.bin"), str(tmp_path / "out.bin")],
                        capture_output=True, text=True, timeout=120)
     assert r.returncode != 0 and "fill" in (r.stdout + r.stderr)
+
+
+REF_MAIN = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "fempic_opp_dropin"
+LOG_LINE = re.compile(r"ts: (\d+)\s+np: (\d+) \((\d+) added, (\d+) removed\)\s+max c_ef: (\S+) max n_pot: (\S+)")
+
+
+@pytest.mark.skipif(not REF_MAIN.exists(), reason="the reference's generated main was not built (oracle/Makefile)")
+@pytest.mark.parametrize("fill,period", [("HoleFill_All", 10), ("Sort_Periodic", 5)])
+def test_reference_generated_main_runs_on_the_dropin(tmp_path, fill, period):
+    """The reference's own generated FemPIC main, apps_codegen/app_fempic_cg/fempic_opp.cpp,
+    compiled unmodified against include/ and linked with libopp_b200.so (oracle/Makefile): its
+    mesh from the app's text files through its own load_mesh(), its injection from its own
+    init_inject_distributions and rand_file, the field phase every step (FESolver on the GPU),
+    the physical constants of fempic_defs.h.  Its per-step log (particles, added, removed, max
+    c_ef, max n_pot) against the oracle running the same step with the same field phase."""
+    from oracle import field as F
+    from oracle import mesh as OM
+
+    # 0.08 per step along z: ions reach the far wall from step ~50; ~10 per inlet face per step
+    dims, steps = (10, 10, 40, 1.0, 1.0, 4.0), 70
+    n0, vion, temp, wall, spwt, dt = 1e9, 1e6, 1e6, 1.0, 4e4, 8e-8
+    files = OM.write_box_files(dims, tmp_path)
+    rand = np.random.default_rng(3).random((1000, 2))
+    (tmp_path / "rand.dat").write_text("1000 2\n" + "".join(f"{a!r} {b!r}\n" for a, b in rand))
+    (tmp_path / "params.txt").write_text(
+        f"REAL plasma_den = {n0}\nREAL ion_velocity = {vion}\nREAL electron_temperature = {temp}\n"
+        f"REAL wall_potential = {wall}\nREAL spwt = {spwt}\nINT charge_multiple = 1\nINT num_steps = {steps}\n"
+        f"REAL dt = {dt}\nREAL grid_spacing = 0.1\nBOOL print_final = true\n"
+        f"STRING global_mesh = {files['global_mesh']}\nSTRING inlet_mesh = {files['inlet_mesh']}\n"
+        f"STRING wall_mesh = {files['wall_mesh']}\nSTRING rand_file = {tmp_path / 'rand.dat'}\n"
+        f"STRING opp_fill = {fill}\nINT opp_fill_period = {period}\nREAL opp_allocation_multiple = 11\n"
+        "BOOL opp_global_move = false\nBOOL opp_profile_all = false\n")
+    r = subprocess.run([str(REF_MAIN), str(tmp_path / "params.txt")], capture_output=True, text=True, timeout=600,
+                       cwd=tmp_path)
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
+    log = [LOG_LINE.search(line) for line in r.stdout.splitlines()]
+    log = [(int(m[1]), int(m[2]), int(m[3]), int(m[4]), float(m[5]), float(m[6])) for m in log if m]
+    assert [x[0] for x in log] == list(range(steps))
+
+    # The oracle: the loader's mesh (pinned by tests/test_mesh_ref_cpu.py), init_inject_distributions'
+    # counts (plasma_den * ion_velocity * area * dt / spwt, truncated, per face), the rand_file's
+    # pairs restarting at every face, no thermal velocity, charge / mass = QE / (2 AMU).
+    qe, amu, kb, eps0 = 1.602e-19, 1.660538921e-27, 8.617333262e-5, 8.8541878e-12
+    m = OM.box_mesh(*dims)
+    per_face = [int(n0 * vion * a * dt / spwt + 0.0) for a in m.if_area]
+    dist = np.cumsum(per_face).astype(np.int32)
+    inject = int(dist[-1])
+    start = np.concatenate([[0], dist[:-1]])
+    face = np.searchsorted(dist, np.arange(inject), side="right")
+    table = np.zeros((inject, 5))
+    table[:, 0:2] = rand[np.arange(inject) - start[face]]
+    bnd = np.where(m.n_type == OM.FIXED, -1.0 * wall, 0.0)  # init_boundary_pot_kernel
+    fs = F.FieldSystem(m.n_pos, m.n_type, bnd, m.c2n)
+    consts = F.FieldConsts(n0=n0, phi0=0.0, kte=kb * temp, qe=qe, eps0=eps0, max_iter=10000)
+    o = O.OracleFemPIC(m, dist, ion_velocity=vion, qm=(1 * qe) / (2 * amu), dt=dt, fill=fill, fill_period=period,
+                       field=(fs, consts, spwt, m.n_vol))
+    removed = 0
+    for s in range(steps):
+        out = o.step(table)
+        ts, np_, added, rem, max_cef, max_pot = log[s]
+        assert (np_, added, rem) == (out["size"], inject, out["removed"]), s
+        removed += rem
+        assert abs(max_cef - max(0.0, float(m.c_ef.max()))) <= 1e-9 * max(1.0, abs(max_cef)), s
+        assert abs(max_pot - float(np.abs(o.potential).max())) <= 1e-9 * max(1.0, abs(max_pot)), s
+    assert removed > 0 and log[-1][1] > 50_000
