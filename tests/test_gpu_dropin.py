@@ -216,7 +216,7 @@ def test_reference_generated_main_runs_on_the_dropin(tmp_path, fill, period):
     n0, vion, temp, wall, spwt, dt = 1e9, 1e6, 1e6, 1.0, 4e4, 8e-8
     files = OM.write_box_files(dims, tmp_path)
     rand = np.random.default_rng(3).random((1000, 2))
-    (tmp_path / "rand.dat").write_text("1000 2\n" + "".join(f"{a!r} {b!r}\n" for a, b in rand))
+    (tmp_path / "rand.dat").write_text("1000 2\n" + "".join(f"{float(a)!r} {float(b)!r}\n" for a, b in rand))
     (tmp_path / "params.txt").write_text(
         f"REAL plasma_den = {n0}\nREAL ion_velocity = {vion}\nREAL electron_temperature = {temp}\n"
         f"REAL wall_potential = {wall}\nREAL spwt = {spwt}\nINT charge_multiple = 1\nINT num_steps = {steps}\n"
