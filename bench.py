@@ -337,9 +337,11 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
         for t in g.tables:
             device_randoms(t)
         e0, e1 = E(), E()
+        torch.cuda.profiler.start()  # profiler range: the replays (for `ncu --profile-from-start off`)
         e0.record(s)
         g.graph.replay()
         e1.record(s)
+        torch.cuda.profiler.stop()
         recs = sim.replay_finish(g)
         ps_g += sum(r["size_before_move"] for r in recs)
         t_g += e0.elapsed_time(e1)
