@@ -141,7 +141,10 @@ typedef struct oppb_tuning {
                             64-B half of the cell record and computing two of the four lambdas */
     int32_t move_occupancy; /* lane-pair FP64 move: CTAs per SM it is compiled for, 8 (0 reads as 8;
                                32 registers a thread) or 5 (48 registers, no spills) */
-    int32_t reserved[2];
+    int32_t sort_scatter;   /* cell sort / shuffle: 0 = gather every dat by destination (scattered
+                               reads, coalesced writes), 1 = scatter by source (coalesced reads,
+                               scattered writes); the same result */
+    int32_t reserved[1];
 } oppb_tuning;
 
 /* Set / read the tuning used by subsequent launches (OPPB_ERR_ARG on unknown values). */

@@ -99,7 +99,8 @@ __global__ void __launch_bounds__(kSortBlock, kScatterMinBlocks) radix_scatter_k
                                                                    int shift, int n_tiles,
                                                                    const int* __restrict__ offsets,
                                                                    uint32_t* __restrict__ keys_out,
-                                                                   int32_t* __restrict__ vals_out, int last) {
+                                                                   int32_t* __restrict__ vals_out, int last,
+                                                                   int32_t* __restrict__ inv_out) {
     const int32_t size = sort_size(count);
     if (sort_is_copy(count) || (int64_t)blockIdx.x * kSortTile >= size) return;  // whole block
     __shared__ int cnt[kSortWarps][kRadix];
@@ -172,6 +173,7 @@ __global__ void __launch_bounds__(kSortBlock, kScatterMinBlocks) radix_scatter_k
         else
             keys_out[dest] = k;
         vals_out[dest] = sv[t];
+        if (inv_out) inv_out[sv[t]] = (int32_t)dest;  // the scatter form's destination of each source
     }
 }
 
@@ -218,6 +220,40 @@ __global__ void __launch_bounds__(256) gather_kernel(SortCount cnt, const int32_
     }
 }
 
+// The scatter form of the dat move (oppb_tuning.sort_scatter): thread i reads every column of
+// source particle i (coalesced) and writes it to its destination inv[i] (scattered 8-B and 4-B
+// stores, merged into whole sectors in L2 when neighbouring destinations arrive close in time);
+// the gather form reads scattered and writes coalesced.  Same result.
+__global__ void __launch_bounds__(256) scatter_cols_kernel(SortCount cnt, const int32_t* __restrict__ inv, GatherCols g,
+                                                           const int32_t* __restrict__ key_src,
+                                                           int32_t* __restrict__ key_dst) {
+    const int32_t size = sort_size(cnt);
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i >= size) return;
+    const bool copy = sort_is_copy(cnt);
+    const int64_t to = copy ? i : inv[i];
+    if (copy && key_src) key_dst[i] = key_src[i];
+    uint64_t v[kMaxCols];
+#pragma unroll
+    for (int c = 0; c < kMaxCols; c++) {
+        if (c < g.n) {
+            if (g.bytes[c] == 8)
+                v[c] = (uint64_t)__ldcs(reinterpret_cast<const long long*>(g.src[c]) + i);
+            else
+                v[c] = (uint32_t)__ldcs(reinterpret_cast<const int*>(g.src[c]) + i);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kMaxCols; c++) {
+        if (c < g.n) {
+            if (g.bytes[c] == 8)
+                reinterpret_cast<long long*>(g.dst[c])[to] = (long long)v[c];
+            else
+                reinterpret_cast<int*>(g.dst[c])[to] = (int)v[c];
+        }
+    }
+}
+
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 int key_bits(int32_t n_cells) {
@@ -227,7 +263,7 @@ int key_bits(int32_t n_cells) {
 }
 
 struct SortLayout {
-    size_t keys_a, vals_a, keys_b, vals_b, perm, hist, scan, total;
+    size_t keys_a, vals_a, keys_b, vals_b, perm, inv, hist, scan, total;
 };
 
 SortLayout sort_layout(int32_t size) {
@@ -241,6 +277,7 @@ SortLayout sort_layout(int32_t size) {
     L.keys_b = o; o += align256(4 * n);
     L.vals_b = o; o += align256(4 * n);
     L.perm = o;   o += align256(4 * n);
+    L.inv = o;    o += align256(4 * n);
     L.hist = o;   o += align256(4 * hist_n);
     L.scan = o;   o += align256(4 * scan_scratch_ints((int64_t)hist_n));
     L.total = o;
@@ -271,6 +308,8 @@ int launch_sort(const SortCount& cnt, int32_t size, int32_t n_cells, int32_t str
     uint32_t* keys[2] = {reinterpret_cast<uint32_t*>(ws + L.keys_a), reinterpret_cast<uint32_t*>(ws + L.keys_b)};
     int32_t* vals[2] = {reinterpret_cast<int32_t*>(ws + L.vals_a), reinterpret_cast<int32_t*>(ws + L.vals_b)};
     int32_t* perm = perm_out ? perm_out : reinterpret_cast<int32_t*>(ws + L.perm);
+    const bool scatter = tuning().sort_scatter != 0;
+    int32_t* inv = scatter ? reinterpret_cast<int32_t*>(ws + L.inv) : nullptr;
     int* hist = reinterpret_cast<int*>(ws + L.hist);
     int* scan_tmp = reinterpret_cast<int*>(ws + L.scan);
 
@@ -286,7 +325,7 @@ int launch_sort(const SortCount& cnt, int32_t size, int32_t n_cells, int32_t str
         radix_hist_kernel<<<n_tiles, kSortBlock, 0, s>>>(in, cnt, n_cells, shift, n_tiles, hist);
         device_exclusive_scan(hist, hist, (int64_t)kRadix * n_tiles, scan_tmp, s);
         radix_scatter_kernel<<<n_tiles, kSortBlock, 0, s>>>(in, cnt, n_cells, shift, n_tiles, hist, ko, vo,
-                                                            (last && !shuffle) ? 1 : 0);
+                                                            (last && !shuffle) ? 1 : 0, last ? inv : nullptr);
         count_launches(2);
         in = PassIn{nullptr, keys[p & 1], vals[p & 1], 0};
     }
@@ -303,7 +342,10 @@ int launch_sort(const SortCount& cnt, int32_t size, int32_t n_cells, int32_t str
             g.dst[g.n] = static_cast<char*>(dats[d].swap) + off;
             g.bytes[g.n] = dats[d].elem_bytes;
             if (++g.n == group) {
-                gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(cnt, perm, g, key_src, key_dst);
+                if (scatter)
+                    scatter_cols_kernel<<<ceil_div(size, 256), 256, 0, s>>>(cnt, inv, g, key_src, key_dst);
+                else
+                    gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(cnt, perm, g, key_src, key_dst);
                 count_launches(1);
                 g.n = 0;
                 key_src = nullptr;
@@ -311,7 +353,10 @@ int launch_sort(const SortCount& cnt, int32_t size, int32_t n_cells, int32_t str
         }
     }
     if (g.n > 0 || key_src) {
-        gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(cnt, perm, g, key_src, key_dst);
+        if (scatter)
+            scatter_cols_kernel<<<ceil_div(size, 256), 256, 0, s>>>(cnt, inv, g, key_src, key_dst);
+        else
+            gather_kernel<<<ceil_div(size, 256), 256, 0, s>>>(cnt, perm, g, key_src, key_dst);
         count_launches(1);
     }
     return launch_status();

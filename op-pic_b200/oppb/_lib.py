@@ -56,7 +56,7 @@ class Dat(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("advec_items", c_i32), ("sort_gather_cols", c_i32),
-                ("move_lanes", c_i32), ("move_occupancy", c_i32), ("reserved", c_i32 * 2)]
+                ("move_lanes", c_i32), ("move_occupancy", c_i32), ("sort_scatter", c_i32), ("reserved", c_i32 * 1)]
 
 
 DEPOSIT_WARP_ATOMIC = 0
@@ -238,7 +238,7 @@ def check(fn: str, status: int) -> None:
 
 def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_items: int | None = None,
                sort_gather_cols: int | None = None, move_lanes: int | None = None,
-               move_occupancy: int | None = None) -> None:
+               move_occupancy: int | None = None, sort_scatter: int | None = None) -> None:
     t = Tuning()
     load().oppb_get_tuning(C.byref(t))
     if deposit is not None:
@@ -253,6 +253,8 @@ def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_it
         t.move_lanes = move_lanes
     if move_occupancy is not None:
         t.move_occupancy = move_occupancy
+    if sort_scatter is not None:
+        t.sort_scatter = sort_scatter
     check("oppb_set_tuning", load().oppb_set_tuning(C.byref(t)))
 
 

@@ -25,7 +25,7 @@ from oppb import _lib as L
 
 MOVE_CANDIDATES = [(dep, rep) for dep in (L.DEPOSIT_WARP_ATOMIC, L.DEPOSIT_CTA_TABLE) for rep in (1, 4, 8, 16)]
 LANE_CANDIDATES = [(1, 8), (2, 8), (2, 5)]  # (move_lanes, move_occupancy)
-SORT_CANDIDATES = [16, 10, 5]
+SORT_CANDIDATES = [(16, 0), (10, 0), (5, 0), (16, 1), (10, 1)]  # (columns per launch, scatter form)
 PERIOD_CANDIDATES = [5, 10, 20]
 
 
@@ -237,19 +237,20 @@ def time_move(sim, deposit: int, replicas: int = 1, reps: int = 3, with_push: bo
 
 
 def tune_sort(sim, candidates=None, reps: int = 3) -> TuneResult:
-    """Columns per gather launch of the cell sort, timed on sim's current (unsorted) state; the
-    sort writes into the swap buffers only, so the state is not changed."""
+    """Columns per launch and form (gather by destination, or scatter by source) of the cell
+    sort's dat move, timed on sim's current (unsorted) state; the sort writes into the swap
+    buffers only, so the state is not changed."""
     p = sim.parts
     lib = sim.lib
     nbytes = lib.oppb_sort_workspace_bytes(p.size, sim.mesh.n_cells)
     ws = sim._workspace(nbytes)
     dats = p.dat_list()
 
-    def run(cols) -> float:
-        L.set_tuning(sort_gather_cols=cols)
+    def run(c) -> float:
+        L.set_tuning(sort_gather_cols=c[0], sort_scatter=c[1])
         return _timed(lambda: L.check("oppb_sort_by_cell", lib.oppb_sort_by_cell(
             p.size, sim.mesh.n_cells, p.capacity, len(p.DATS), dats, 3, None, ws.data_ptr(), ws.numel(), None)))
 
     res = pick(candidates or SORT_CANDIDATES, run, reps)
-    L.set_tuning(sort_gather_cols=res.choice)
+    L.set_tuning(sort_gather_cols=res.choice[0], sort_scatter=res.choice[1])
     return res

@@ -4,7 +4,7 @@ from __future__ import annotations
 
 import pytest
 
-from oppb.autotune import MOVE_CANDIDATES, SORT_CANDIDATES, pick
+from oppb.autotune import LANE_CANDIDATES, MOVE_CANDIDATES, PERIOD_CANDIDATES, SORT_CANDIDATES, pick
 
 
 def test_pick_smallest_median():
@@ -30,7 +30,23 @@ def test_pick_ties_and_errors():
 
 def test_candidate_sets():
     assert len(set(MOVE_CANDIDATES)) == len(MOVE_CANDIDATES) == 8
-    assert all(1 <= c <= 16 for c in SORT_CANDIDATES) and SORT_CANDIDATES[0] == 16
+    assert all(1 <= c <= 16 and f in (0, 1) for c, f in SORT_CANDIDATES) and SORT_CANDIDATES[0] == (16, 0)
+    assert LANE_CANDIDATES[0] == (1, 8) and all(lanes in (1, 2) and occ in (5, 8) for lanes, occ in LANE_CANDIDATES)
+    assert 10 in PERIOD_CANDIDATES
+
+
+def test_tuning_fields_validated():
+    """oppb_set_tuning accepts the documented values of every field and refuses others."""
+    from oppb import _lib as L
+
+    L.set_tuning(move_lanes=2, move_occupancy=5, sort_scatter=1)
+    t = L.Tuning()
+    L.load().oppb_get_tuning(t)
+    assert (t.move_lanes, t.move_occupancy, t.sort_scatter) == (2, 5, 1)
+    for kw in (dict(move_lanes=3), dict(move_occupancy=6), dict(sort_scatter=2)):
+        with pytest.raises(L.OppbError):
+            L.set_tuning(**kw)
+    L.set_tuning(move_lanes=1, move_occupancy=8, sort_scatter=0)
 
 
 def test_snapshot_fits_counts_live_columns(monkeypatch):

@@ -221,9 +221,16 @@ def test_hole_fill_matches_oracle(n, frac, seed):
     assert not (got["p2c"][:m] == REMOVED).any()
 
 
+@pytest.fixture(params=[0, 1], ids=["gather", "scatter"])
+def sort_form(request):
+    L.set_tuning(sort_scatter=request.param)
+    yield request.param
+    L.set_tuning(sort_scatter=0)
+
+
 @pytest.mark.parametrize("n,n_cells,frac,seed", [(1, 24000, 0.0, 0), (4096, 24000, 0.1, 1), (4097, 200, 0.2, 2),
                                                  (1_000_000, 2_654_208, 0.01, 3), (333_333, 24000, 0.0, 4)])
-def test_sort_matches_oracle(n, n_cells, frac, seed):
+def test_sort_matches_oracle(n, n_cells, frac, seed, sort_form):
     rng = np.random.default_rng(seed)
     pos, vel, lc, _ = _state(n, seed, 0.0)
     p2c = rng.integers(0, n_cells, n).astype(np.int32)
@@ -503,4 +510,4 @@ def test_autotune_leaves_state_and_picks_valid(precision):
     for name in ("pos", "vel", "lc", "p2c"):
         np.testing.assert_array_equal(ga[name].view(np.uint8), gb[name].view(np.uint8), err_msg=name)
     _charge_close(a.node_charge.cpu().numpy(), b.node_charge.cpu().numpy(), CHARGE_RTOL)
-    L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC, replicas=8, sort_gather_cols=16)  # defaults for later tests
+    L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC, replicas=8, sort_gather_cols=16, sort_scatter=0)  # defaults
