@@ -32,6 +32,7 @@ extern "C" {
 #define OPPB_ERR_CAPACITY    6  /* injection would exceed the set capacity          */
 #define OPPB_ERR_NO_DEVICE   7  /* no CUDA device visible                           */
 #define OPPB_ERR_SCRATCH_LIMIT 8 /* request larger than a fixed in-library scratch  */
+#define OPPB_ERR_WAIT_LIMIT  9  /* device: a bounded wait for an asynchronous copy ran out */
 
 /* Cell index of a removed particle: MAX_CELL_INDEX in opp_lib/include/opp_defs.h:150. */
 #define OPPB_REMOVED_CELL 2147483647
@@ -144,7 +145,10 @@ typedef struct oppb_tuning {
     int32_t sort_scatter;   /* cell sort / shuffle: 0 = gather every dat by destination (scattered
                                reads, coalesced writes), 1 = scatter by source (coalesced reads,
                                scattered writes); the same result */
-    int32_t reserved[1];
+    int32_t move_stage;     /* FP64 move, one lane per particle: 0 = each visit's cell record read by
+                               the lane's own 256-bit loads; 1 = staged into shared memory by bulk
+                               asynchronous copies (cp.async.bulk, one per record half, completed on
+                               a warp's mbarrier) and read from there; the same results */
 } oppb_tuning;
 
 /* Set / read the tuning used by subsequent launches (OPPB_ERR_ARG on unknown values). */

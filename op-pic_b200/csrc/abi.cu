@@ -7,7 +7,7 @@
 namespace oppb {
 namespace {
 std::atomic<uint64_t> g_launches{0};
-oppb_tuning g_tuning = {OPPB_DEPOSIT_WARP_ATOMIC, 8, 2, 16, 1, 8, 0, {0}};
+oppb_tuning g_tuning = {OPPB_DEPOSIT_WARP_ATOMIC, 8, 2, 16, 1, 8, 0, 0};
 }  // namespace
 void count_launches(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 const oppb_tuning& tuning() { return g_tuning; }
@@ -25,6 +25,7 @@ extern "C" int oppb_set_tuning(const oppb_tuning* t) {
     if (t->move_lanes < 0 || t->move_lanes > 2) return OPPB_ERR_ARG;
     if (t->move_occupancy != 0 && t->move_occupancy != 5 && t->move_occupancy != 8) return OPPB_ERR_ARG;
     if (t->sort_scatter != 0 && t->sort_scatter != 1) return OPPB_ERR_ARG;
+    if (t->move_stage != 0 && t->move_stage != 1) return OPPB_ERR_ARG;
     oppb::g_tuning = *t;
     if (oppb::g_tuning.move_lanes == 0) oppb::g_tuning.move_lanes = 1;
     if (oppb::g_tuning.move_occupancy == 0) oppb::g_tuning.move_occupancy = 8;
@@ -48,6 +49,7 @@ extern "C" const char* oppb_status_string(int status) {
         case OPPB_ERR_CAPACITY: return "particle set capacity exceeded";
         case OPPB_ERR_NO_DEVICE: return "no CUDA device";
         case OPPB_ERR_SCRATCH_LIMIT: return "request exceeds the fixed scratch of an allocation-free entry point";
+        case OPPB_ERR_WAIT_LIMIT: return "a bounded wait for an asynchronous copy ran out";
         default: return "unknown status";
     }
 }

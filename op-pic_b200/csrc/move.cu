@@ -558,6 +558,155 @@ __global__ void __launch_bounds__(kMoveBlock, kOcc)
     deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && !newly_removed && !failed, cell, l);
 }
 
+// ------------------------------------ FP64 move, cell records staged by bulk async copies
+//
+// oppb_tuning.move_stage = 1.  The one-lane walk, with each visit's 160-B cell record (the
+// 128-B det record and the 32-B nav record) brought into the lane's slot of shared memory by
+// two bulk asynchronous copies (cp.async.bulk, handled by the copy engine rather than the L1
+// load pipe that bounds the 256-bit-load kernel) instead of five 256-bit loads.  A warp visits
+// in lock step: lane 0 posts the expected bytes of the warp's active lanes on the warp's
+// mbarrier, every active lane issues its two copies, the warp waits on the barrier's phase,
+// and each lane reads its record from shared memory (a 176-B slot stride, so that eight lanes'
+// 128-bit reads hit distinct banks) and evaluates it with the reference expression.  Every
+// wait is bounded: a wait that runs out records OPPB_ERR_WAIT_LIMIT, waits once more (bounded)
+// for the copies in flight and ends the walks.  Decisions, lambdas and counts are
+// bit-identical to move_f64_kernel's.
+
+constexpr int kStageOcc = 4;            // CTAs per SM: 45 KB of record slots each
+constexpr int kStageSlot = 22;          // doubles per lane slot: 160 B of record + 16 B of padding
+constexpr long kStagePolls = 1L << 20;  // bound on the barrier polls of one visit (each suspends <= 1 us)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t arrivals) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(arrivals) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, 1000;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bulk copy of `bytes` (a multiple of 16; both addresses 16-B aligned) from global memory into
+// this CTA's shared memory, completing `bytes` transactions on the mbarrier.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Polls the warp's barrier for `parity`, at most kStagePolls times; the result is the warp's.
+__device__ __forceinline__ bool warp_wait_phase(uint64_t* bar, uint32_t parity) {
+    bool done = false;
+    for (long k = 0; k < kStagePolls && !done; k++) done = __all_sync(kFullMask, mbar_try_wait(bar, parity));
+    return done;
+}
+
+template <int kDep, bool kPush, bool kDevCount>
+__global__ void __launch_bounds__(kMoveBlock, kStageOcc)
+    move_f64_stage_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
+                          PushArgs push) {
+    __shared__ NodeTable table;
+    __shared__ __align__(16) double s_rec[kMoveBlock * kStageSlot];
+    __shared__ __align__(8) uint64_t s_bar[kMoveBlock / 32];
+    const int32_t n = kDevCount ? live_count(p) : p.size;
+    if (kDevCount && (int64_t)blockIdx.x * kMoveBlock >= n) return;  // beyond the device count (whole block)
+    if (kDep == kDepTable) table_init(table);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t* bar = &s_bar[warp];
+    if (lane == 0) mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncwarp();
+    const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
+    const bool active = i < n;
+    int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
+    const int32_t cell0 = cell;
+    int status = kDone, visits = 0, err = 0;
+    double l[4] = {0.0, 0.0, 0.0, 0.0};
+    double x = 0.0, y = 0.0, z = 0.0;
+    bool walking = active && cell != kRemoved;
+    if (walking) {
+        x = ld_stream(p.pos + i);
+        y = ld_stream(p.pos + p.stride + i);
+        z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
+        if (kPush && (uint32_t)cell < (uint32_t)m.n_cells) push_prologue<false>(m, p, push, i, cell, x, y, z);
+    }
+    double* slot = s_rec + threadIdx.x * kStageSlot;
+    uint32_t parity = 0;
+    for (;;) {
+        if (walking && (uint32_t)cell >= (uint32_t)m.n_cells) {
+            err = OPPB_ERR_CELL_RANGE;
+            walking = false;
+        }
+        const unsigned wm = __ballot_sync(kFullMask, walking);
+        if (!wm) break;
+        if (lane == 0) mbar_arrive_expect_tx(bar, 160u * (uint32_t)__popc(wm));
+        if (walking) {
+            // this lane's reads of its slot (the previous visit) come before the copy's writes
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bulk_copy_g2s(slot, m.det + (int64_t)cell * 16, 128, bar);
+            bulk_copy_g2s(slot + 16, m.nav + (int64_t)cell * 4, 32, bar);
+        }
+        if (!warp_wait_phase(bar, parity)) {
+            if (lane == 0) raise_error(st, OPPB_ERR_WAIT_LIMIT, (int32_t)i);
+            warp_wait_phase(bar, parity);  // the copies in flight, once more (bounded)
+            if (walking) err = OPPB_ERR_WAIT_LIMIT;
+            break;
+        }
+        parity ^= 1u;
+        if (walking) {
+            const double2* r = reinterpret_cast<const double2*>(slot);
+            const double2 coef_n01 = r[8], n23_pad = r[9];
+            const double coef = coef_n01.x;
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                const double2 ab = r[2 * v], gd = r[2 * v + 1];
+                double t = __dsub_rn(ab.x, __dmul_rn(ab.y, x));
+                t = __dadd_rn(t, __dmul_rn(gd.x, y));
+                t = __dsub_rn(t, __dmul_rn(gd.y, z));
+                l[v] = __dmul_rn(coef, t);
+            }
+            visits++;
+            if (inside_f64(l)) {
+                walking = false;
+            } else {
+                const int mi = argmin4(l);
+                const long long b = __double_as_longlong(mi < 2 ? coef_n01.y : n23_pad.x);
+                const int32_t next = (mi & 1) ? (int32_t)(b >> 32) : (int32_t)(b & 0xffffffffll);
+                if (next < 0) {
+                    cell = kRemoved;
+                    status = kNeedRemove;
+                    walking = false;
+                } else {
+                    cell = next;
+                    if (visits >= max_hops) {
+                        err = OPPB_ERR_HOP_LIMIT;
+                        walking = false;
+                    }
+                }
+            }
+        }
+    }
+    if (err) {
+        if (err != OPPB_ERR_WAIT_LIMIT) raise_error(st, err, (int32_t)i);
+        status = kFailed;
+    }
+    if (active && cell0 != kRemoved) store_result(p, i, l, visits, cell, cell0);
+    cta_account(p, st, i, active, cell, status == kNeedRemove, visits, 0);
+    deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, l);
+}
+
 // -------------------------------------------------------- mixed FP32 / FP64 move
 //
 // lambda_i(x) = c_i + g_i . (x - o) for i = 0..2 with o = f32(vertex 0), c_i, g_i in f32,
@@ -863,7 +1012,17 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
         move_f64_kernel<kDepNone, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops,
                                                                            push, dh);
     else if constexpr (kKind == kMoveDepositF64) {
-        if (!kSeed && tuning().move_lanes == 2) {  // a particle per lane pair
+        if (!kSeed && tuning().move_lanes != 2 && tuning().move_stage == 1) {  // records staged by bulk copies
+            if (table)
+                move_f64_stage_kernel<kDepTable, kPush, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args,
+                                                                                              status, max_hops, push);
+            else if (exact)
+                move_f64_stage_kernel<kDepExact, kPush, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args,
+                                                                                              status, max_hops, push);
+            else
+                move_f64_stage_kernel<kDepWarp, kPush, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args,
+                                                                                             status, max_hops, push);
+        } else if (!kSeed && tuning().move_lanes == 2) {  // a particle per lane pair
             if (tuning().move_occupancy == 5)
                 launch_pair<kPush, kDevCount, 5>(grid, s, table, exact, *mesh, p, rep.args, status, max_hops, push);
             else

@@ -19,6 +19,7 @@ OPPB_ERR_CELL_RANGE = 5
 OPPB_ERR_CAPACITY = 6
 OPPB_ERR_NO_DEVICE = 7
 OPPB_ERR_SCRATCH_LIMIT = 8
+OPPB_ERR_WAIT_LIMIT = 9
 HOLE_FILL_STATIC_MAX_REMOVES = 1048576
 REMOVED_CELL = 2147483647
 
@@ -56,7 +57,7 @@ class Dat(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("advec_items", c_i32), ("sort_gather_cols", c_i32),
-                ("move_lanes", c_i32), ("move_occupancy", c_i32), ("sort_scatter", c_i32), ("reserved", c_i32 * 1)]
+                ("move_lanes", c_i32), ("move_occupancy", c_i32), ("sort_scatter", c_i32), ("move_stage", c_i32)]
 
 
 DEPOSIT_WARP_ATOMIC = 0
@@ -238,7 +239,8 @@ def check(fn: str, status: int) -> None:
 
 def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_items: int | None = None,
                sort_gather_cols: int | None = None, move_lanes: int | None = None,
-               move_occupancy: int | None = None, sort_scatter: int | None = None) -> None:
+               move_occupancy: int | None = None, sort_scatter: int | None = None,
+               move_stage: int | None = None) -> None:
     t = Tuning()
     load().oppb_get_tuning(C.byref(t))
     if deposit is not None:
@@ -255,6 +257,8 @@ def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_it
         t.move_occupancy = move_occupancy
     if sort_scatter is not None:
         t.sort_scatter = sort_scatter
+    if move_stage is not None:
+        t.move_stage = move_stage
     check("oppb_set_tuning", load().oppb_set_tuning(C.byref(t)))
 
 

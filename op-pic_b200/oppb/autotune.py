@@ -1,8 +1,9 @@
 """The launch choices of the FemPIC path, picked by timing them on the live state.
 
-The move + deposit launch has four choices (oppb_tuning): the FP64 move's lanes per particle
-(one, 32 particles per warp, or a lane pair, 16 per warp) and, for the pair kernel, the CTAs per
-SM it is compiled for (8 at 32 registers a thread, 5 at 48); the deposit strategy (warp-matched
+The move + deposit launch has five choices (oppb_tuning): the FP64 move's lanes per particle
+(one, 32 particles per warp, or a lane pair, 16 per warp), for the pair kernel the CTAs per SM
+it is compiled for (8 at 32 registers a thread, 5 at 48), for the one-lane kernel whether the
+cell records are staged into shared memory by bulk asynchronous copies; the deposit strategy (warp-matched
 FP64 atomics, or a per-CTA shared-memory node table) and how many node-sum copies the atomics
 are spread over.  The cell sort has one (particle-dat columns gathered per launch).  tune_move
 and tune_sort time every candidate on the simulation's current particle state, restoring a
@@ -24,7 +25,7 @@ import torch
 from oppb import _lib as L
 
 MOVE_CANDIDATES = [(dep, rep) for dep in (L.DEPOSIT_WARP_ATOMIC, L.DEPOSIT_CTA_TABLE) for rep in (1, 4, 8, 16)]
-LANE_CANDIDATES = [(1, 8), (2, 8), (2, 5)]  # (move_lanes, move_occupancy)
+LANE_CANDIDATES = [(1, 8, 0), (1, 8, 1), (2, 8, 0), (2, 5, 0)]  # (move_lanes, move_occupancy, move_stage)
 SORT_CANDIDATES = [(16, 0), (10, 0), (5, 0), (16, 1), (10, 1)]  # (columns per launch, scatter form)
 PERIOD_CANDIDATES = [5, 10, 20]
 
@@ -124,17 +125,17 @@ def tune_lanes(sim, candidates=None, reps: int = 3, with_push: bool | None = Non
     kernel has one lane per particle: nothing to tune there), timed as tune_move times its
     candidates, with the deposit choice in force.  Sets the fastest; sim's state is left as found."""
     if sim.precision != "f64":
-        return TuneResult(choice=(1, 8))
+        return TuneResult(choice=(1, 8, 0))
     before = L.Tuning()
     L.load().oppb_get_tuning(C.byref(before))
     cands = candidates or LANE_CANDIDATES
     if not snapshot_fits(sim):
-        return TuneResult(choice=(before.move_lanes, before.move_occupancy))
+        return TuneResult(choice=(before.move_lanes, before.move_occupancy, before.move_stage))
     snap = ParticleSnapshot(sim)
     fused = sim.fused_push if with_push is None else with_push
 
     def run(c) -> float:
-        L.set_tuning(move_lanes=c[0], move_occupancy=c[1])
+        L.set_tuning(move_lanes=c[0], move_occupancy=c[1], move_stage=c[2])
         snap.restore()
         if fused:
             return _timed(sim.push_move)
@@ -148,7 +149,7 @@ def tune_lanes(sim, candidates=None, reps: int = 3, with_push: bool | None = Non
         raise
     finally:
         snap.restore()
-    L.set_tuning(move_lanes=res.choice[0], move_occupancy=res.choice[1])
+    L.set_tuning(move_lanes=res.choice[0], move_occupancy=res.choice[1], move_stage=res.choice[2])
     return res
 
 

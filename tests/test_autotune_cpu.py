@@ -31,7 +31,8 @@ def test_pick_ties_and_errors():
 def test_candidate_sets():
     assert len(set(MOVE_CANDIDATES)) == len(MOVE_CANDIDATES) == 8
     assert all(1 <= c <= 16 and f in (0, 1) for c, f in SORT_CANDIDATES) and SORT_CANDIDATES[0] == (16, 0)
-    assert LANE_CANDIDATES[0] == (1, 8) and all(lanes in (1, 2) and occ in (5, 8) for lanes, occ in LANE_CANDIDATES)
+    assert LANE_CANDIDATES[0] == (1, 8, 0)
+    assert all(lanes in (1, 2) and occ in (5, 8) and stage in (0, 1) for lanes, occ, stage in LANE_CANDIDATES)
     assert 10 in PERIOD_CANDIDATES
 
 
@@ -39,14 +40,14 @@ def test_tuning_fields_validated():
     """oppb_set_tuning accepts the documented values of every field and refuses others."""
     from oppb import _lib as L
 
-    L.set_tuning(move_lanes=2, move_occupancy=5, sort_scatter=1)
+    L.set_tuning(move_lanes=2, move_occupancy=5, sort_scatter=1, move_stage=1)
     t = L.Tuning()
     L.load().oppb_get_tuning(t)
-    assert (t.move_lanes, t.move_occupancy, t.sort_scatter) == (2, 5, 1)
-    for kw in (dict(move_lanes=3), dict(move_occupancy=6), dict(sort_scatter=2)):
+    assert (t.move_lanes, t.move_occupancy, t.sort_scatter, t.move_stage) == (2, 5, 1, 1)
+    for kw in (dict(move_lanes=3), dict(move_occupancy=6), dict(sort_scatter=2), dict(move_stage=2)):
         with pytest.raises(L.OppbError):
             L.set_tuning(**kw)
-    L.set_tuning(move_lanes=1, move_occupancy=8, sort_scatter=0)
+    L.set_tuning(move_lanes=1, move_occupancy=8, sort_scatter=0, move_stage=0)
 
 
 def test_snapshot_fits_counts_live_columns(monkeypatch):

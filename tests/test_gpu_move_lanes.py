@@ -1,8 +1,10 @@
-"""The FP64 move with two lanes per particle (oppb_tuning.move_lanes = 2, compiled for 8 or 5
-resident CTAs per SM): cells, weights, removals, visit counts and the removal bitmap bit-exact
-against the oracle, as the one-lane kernel; node charges within 1e-12 relative (FP64
-atomics), and bit for bit equal across lane modes in the deterministic deposit; the fused
-push, the device-count launch and the error paths (hop limit, bad cell) included."""
+"""The FP64 move's variants: two lanes per particle (oppb_tuning.move_lanes = 2, compiled for 8
+or 5 resident CTAs per SM) and one lane with each visit's cell record staged into shared memory
+by bulk asynchronous copies (move_stage = 1).  Cells, weights, removals, visit counts and the
+removal bitmap bit-exact against the oracle, as the default kernel; node charges within 1e-12
+relative (FP64 atomics), and bit for bit equal to the default kernel's in the deterministic
+deposit; the fused push, the device-count launch and the error paths (hop limit, bad cell)
+included."""
 from __future__ import annotations
 
 import ctypes as C
@@ -20,11 +22,15 @@ pytestmark = pytest.mark.gpu
 DEV = torch.device("cuda:0")
 
 
-@pytest.fixture(params=[(2, 8), (2, 5)], ids=["pair-occ8", "pair-occ5"])
+DEFAULT = (1, 8, 0)  # (move_lanes, move_occupancy, move_stage)
+
+
+@pytest.fixture(params=[(1, 8, 1), (2, 8, 0), (2, 5, 0)], ids=["staged", "pair-occ8", "pair-occ5"])
 def pair_lanes(request):
-    L.set_tuning(move_lanes=request.param[0], move_occupancy=request.param[1])
+    lanes, occ, stage = request.param
+    L.set_tuning(move_lanes=lanes, move_occupancy=occ, move_stage=stage)
     yield request.param
-    L.set_tuning(move_lanes=1, move_occupancy=8)
+    L.set_tuning(move_lanes=DEFAULT[0], move_occupancy=DEFAULT[1], move_stage=DEFAULT[2])
 
 
 def _particles(hm, n, seed):
@@ -82,17 +88,18 @@ def test_pair_exact_deposit_equals_one_lane_bit_for_bit(pair_lanes):
     hm = mesh()
     dm = DeviceMesh(hm, DEV, mixed=False)
     out = {}
-    for lanes in (1, 2):
-        L.set_tuning(deposit=L.DEPOSIT_EXACT, move_lanes=lanes)
+    for variant in (DEFAULT, pair_lanes):
+        L.set_tuning(deposit=L.DEPOSIT_EXACT, move_lanes=variant[0], move_occupancy=variant[1], move_stage=variant[2])
         try:
             _, _, ps = _particles(hm, 200_000, 9)
             charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
             L.check("move_deposit", _move_deposit(dm, ps, hm, charge))
             torch.cuda.synchronize()
         finally:
-            L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=pair_lanes[0])
-        out[lanes] = charge.cpu().numpy()
-    np.testing.assert_array_equal(out[1].view(np.uint64), out[2].view(np.uint64))
+            L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=pair_lanes[0], move_occupancy=pair_lanes[1],
+                         move_stage=pair_lanes[2])
+        out[variant] = charge.cpu().numpy()
+    np.testing.assert_array_equal(out[DEFAULT].view(np.uint64), out[pair_lanes].view(np.uint64))
 
 
 def test_pair_fempic_steps_match_oracle(pair_lanes):
