@@ -184,13 +184,14 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     log(f"[{precision}] fill {CFG['fill_steps']} steps in {time.time() - t0:.1f}s, size {sim.parts.size}")
     for _ in range(warmup):
         sim.step(device_randoms(rnd_buf))
-    # Launch choices (FP64 move lanes per particle and occupancy, deposit strategy, node-sum
-    # copies, sort gather columns) timed on this state before the timed steps; the state is
-    # restored after each trial.  The sort interval's trials (whole sort cycles) are reported;
-    # the timed steps keep the workload's period.
-    from oppb.autotune import tune_lanes, tune_move, tune_sort, tune_sort_period
-    tuned = {"lanes": tune_lanes(sim, with_push=False).report(), "move": tune_move(sim, with_push=False).report(),
-             "sort": tune_sort(sim).report()}
+    # Launch choices (FP64 move lanes per particle, occupancy and record staging, deposit
+    # strategy, node-sum copies, block shape, the sort's dat move) timed on this state before
+    # the timed steps; the state is restored after each trial.  The sort interval's trials
+    # (whole sort cycles) are reported; the timed steps keep the workload's period.
+    from oppb.autotune import tune_block, tune_lanes, tune_move, tune_sort, tune_sort_period
+    tuned = {"lanes": tune_lanes(sim, with_push=False).report(), "move": tune_move(sim, with_push=False).report()}
+    tuned["block"] = tune_block(sim, with_push=False).report()
+    tuned["sort"] = tune_sort(sim).report()
     period_tables = [device_randoms(torch.empty_like(rnd_buf)) for _ in range(4)]
     sp = tune_sort_period(sim, period_tables)
     tuned["sort_interval"] = {"ns_per_particle_step": {str(k): v for k, v in sp.times_ms.items()},
@@ -201,6 +202,7 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     t_exact = time_move(sim, L.DEPOSIT_EXACT, with_push=False)
     tuned["deterministic_deposit_ms"] = t_exact if t_exact == t_exact else None  # NaN: not measured
     log(f"[{precision}] autotune lanes {tuned['lanes']['choice']} move {tuned['move']['choice']} "
+        f"block {tuned['block']['choice']} "
         f"sort cols {tuned['sort']['choice']} sort interval {tuned['sort_interval']}")
     # Inputs of the timed steps generated before timing (device-resident).
     tables = [device_randoms(torch.empty_like(rnd_buf)) for _ in range(min(steps, 16))]
@@ -538,8 +540,9 @@ def arm_ours(args) -> dict:
                            "fused_steps": mixed["fused_steps"]},
         "graph_step": {"mixed": mixed["graph_step"], "f64": f64["graph_step"]},
         "mixed_over_plain": mixed["job_value"] / f64["job_value"],
-        "autotune": {"what": "move launch (FP64 lanes per particle and occupancy, deposit strategy, node-sum "
-                             "copies) and sort gather columns, median of 3 timed trials on the warmed-up state; "
+        "autotune": {"what": "move launch (FP64 lanes per particle, occupancy and record staging; deposit "
+                             "strategy and node-sum copies; block shape) and the sort's dat move (columns per "
+                             "launch, gather or scatter), median of 3 timed trials on the warmed-up state; "
                              "sort interval: one timed sort cycle per candidate period from the same state",
                      "f64": f64["autotune"], "mixed": mixed["autotune"]},
         "roofline": {"bound": "hbm", "kernel": "move_mixed_kernel (move + fused deposit)",

@@ -149,6 +149,10 @@ typedef struct oppb_tuning {
                                the lane's own 256-bit loads; 1 = staged into shared memory by bulk
                                asynchronous copies (cp.async.bulk, one per record half, completed on
                                a warp's mbarrier) and read from there; the same results */
+    int32_t move_block;     /* threads per CTA of the one-lane FP64 and mixed moves with the warp-grouped
+                               deposit: 128, 256 (0 reads as 256) or 512, with 2048 / move_block CTAs
+                               resident per SM (32 registers a thread); the other deposits, the lane-pair
+                               and the staged kernels use 256.  The same results */
 } oppb_tuning;
 
 /* Set / read the tuning used by subsequent launches (OPPB_ERR_ARG on unknown values). */

@@ -34,6 +34,7 @@ namespace {
 
 constexpr int kMoveBlock = 256;
 constexpr int kMinBlocks = 8;          // 8 x 256 threads per SM: 32 registers per thread
+constexpr int kThreadsPerSm = kMoveBlock * kMinBlocks;  // every block shape keeps 32 registers a thread
 constexpr int kSlots = 256;            // shared node-sum table (power of two, one slot per thread)
 constexpr int kMaxProbe = 16;          // linear-probe bound; beyond it the sum goes straight to global
 constexpr int kDepNone = 0, kDepWarp = 1, kDepTable = 2, kDepExact = 3;
@@ -121,9 +122,11 @@ __device__ __noinline__ void recheck_f64(const oppb_tet_mesh& m, int32_t c, doub
 // added to the status with one atomic per counter per CTA.  Every CTA updates the same
 // few status words, so per-warp atomics there serialise in L2 and cost as much as a
 // large share of the move itself.  Every thread of the CTA must call it.
+template <int kBlock = kMoveBlock>
 __device__ __forceinline__ void cta_account(const PartArgs& p, oppb_move_status* st, int64_t i, bool active,
                                             int32_t final_cell, bool newly_removed, int visits, int rechecks) {
-    constexpr int kWarps = kMoveBlock / 32;
+    constexpr int kWarps = kBlock / 32;
+    static_assert(kWarps >= 1 && kWarps <= 32 && (kWarps & (kWarps - 1)) == 0, "a power-of-two warp count");
     __shared__ unsigned long long s_sum[kWarps];
     __shared__ int s_cnt[kWarps][3];  // removed, max visits, rechecks
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -350,15 +353,18 @@ __device__ __forceinline__ void push_prologue(const oppb_tet_mesh& m, const Part
 
 // ------------------------------------------------------------------ FP64 move
 
-template <int kDep, bool kPush, bool kSeed, bool kDevCount = false>
-__global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
+// kBlock: threads per CTA (oppb_tuning.move_block; 256 for the CTA-table deposit, whose
+// node table has one slot per thread), with 2048 / kBlock CTAs resident per SM.
+template <int kDep, bool kPush, bool kSeed, bool kDevCount = false, int kBlock = kMoveBlock>
+__global__ void __launch_bounds__(kBlock, kThreadsPerSm / kBlock)
     move_f64_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
                     PushArgs push, DhArgs dh) {
+    static_assert(kBlock == kMoveBlock || kDep != kDepTable, "the node table is sized for 256 threads");
     __shared__ NodeTable table;
     const int32_t n = kDevCount ? live_count(p) : p.size;
-    if (kDevCount && (int64_t)blockIdx.x * kMoveBlock >= n) return;  // beyond the device count (whole block)
+    if (kDevCount && (int64_t)blockIdx.x * kBlock >= n) return;  // beyond the device count (whole block)
     if (kDep == kDepTable) table_init(table);
-    const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < n;
     int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
     const int32_t cell0 = cell;
@@ -402,7 +408,7 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
         }
         store_result(p, i, l, visits, cell, cell0);
     }
-    cta_account(p, st, i, active, cell, status == kNeedRemove, visits, 0);
+    cta_account<kBlock>(p, st, i, active, cell, status == kNeedRemove, visits, 0);
     deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, l);
 }
 
@@ -735,15 +741,16 @@ struct Band {
     float tie;     // 2 * band
 };
 
-template <int kDep, bool kPush, bool kSeed, bool kDevCount = false>
-__global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
+template <int kDep, bool kPush, bool kSeed, bool kDevCount = false, int kBlock = kMoveBlock>
+__global__ void __launch_bounds__(kBlock, kThreadsPerSm / kBlock)
     move_mixed_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
                       Band band, PushArgs push, DhArgs dh) {
+    static_assert(kBlock == kMoveBlock || kDep != kDepTable, "the node table is sized for 256 threads");
     __shared__ NodeTable table;
     const int32_t n = kDevCount ? live_count(p) : p.size;
-    if (kDevCount && (int64_t)blockIdx.x * kMoveBlock >= n) return;  // beyond the device count (whole block)
+    if (kDevCount && (int64_t)blockIdx.x * kBlock >= n) return;  // beyond the device count (whole block)
     if (kDep == kDepTable) table_init(table);
-    const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < n;
     int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
     const int32_t cell0 = cell;
@@ -845,7 +852,7 @@ __global__ void __launch_bounds__(kMoveBlock, kMinBlocks)
         status = kFailed;
     }
     if (active && cell0 != kRemoved) store_result(p, i, lf, visits, cell, cell0);
-    cta_account(p, st, i, active, cell, status == kNeedRemove, visits, rechecks);
+    cta_account<kBlock>(p, st, i, active, cell, status == kNeedRemove, visits, rechecks);
     deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, lf);
 }
 
@@ -977,6 +984,37 @@ void launch_pair(int grid, cudaStream_t s, bool table, bool exact, const oppb_te
         move_f64_pair_kernel<kDepWarp, kPush, kDevCount, kOcc><<<grid, kMoveBlock, 0, s>>>(m, p, d, st, max_hops, push);
 }
 
+// The one-lane kernels with the warp-grouped deposit at block shape kBlock.
+template <bool kMixed, bool kPush, bool kSeed, bool kDevCount, int kBlock>
+void launch_warp_shape(int32_t size, cudaStream_t s, const oppb_tet_mesh& m, const PartArgs& p,
+                       const DepositArgs& d, oppb_move_status* st, int32_t max_hops, const Band& bd,
+                       const PushArgs& push, const DhArgs& dh) {
+    const int grid = ceil_div(size, kBlock);
+    if constexpr (kMixed)
+        move_mixed_kernel<kDepWarp, kPush, kSeed, kDevCount, kBlock><<<grid, kBlock, 0, s>>>(m, p, d, st, max_hops,
+                                                                                            bd, push, dh);
+    else
+        move_f64_kernel<kDepWarp, kPush, kSeed, kDevCount, kBlock><<<grid, kBlock, 0, s>>>(m, p, d, st, max_hops,
+                                                                                          push, dh);
+}
+
+// ... at the tuned block shape (oppb_tuning.move_block).
+template <bool kMixed, bool kPush, bool kSeed, bool kDevCount>
+void launch_warp(int32_t size, cudaStream_t s, const oppb_tet_mesh& m, const PartArgs& p, const DepositArgs& d,
+                 oppb_move_status* st, int32_t max_hops, const Band& bd, const PushArgs& push, const DhArgs& dh) {
+    switch (tuning().move_block) {
+        case 128:
+            launch_warp_shape<kMixed, kPush, kSeed, kDevCount, 128>(size, s, m, p, d, st, max_hops, bd, push, dh);
+            break;
+        case 512:
+            launch_warp_shape<kMixed, kPush, kSeed, kDevCount, 512>(size, s, m, p, d, st, max_hops, bd, push, dh);
+            break;
+        default:
+            launch_warp_shape<kMixed, kPush, kSeed, kDevCount, kMoveBlock>(size, s, m, p, d, st, max_hops, bd, push,
+                                                                           dh);
+    }
+}
+
 template <int kKind, bool kPush, bool kSeed = false, bool kDevCount = false>
 int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* node_charge,
                 oppb_move_status* status, int32_t max_hops, double band, const PushArgs& push, void* workspace,
@@ -1035,8 +1073,8 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
             move_f64_kernel<kDepExact, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                                 max_hops, push, dh);
         else
-            move_f64_kernel<kDepWarp, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
-                                                                               max_hops, push, dh);
+            launch_warp<false, kPush, kSeed, kDevCount>(parts->size, s, *mesh, p, rep.args, status, max_hops, bd, push,
+                                                        dh);
     } else if (exact)
         move_mixed_kernel<kDepExact, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                               max_hops, bd, push, dh);
@@ -1044,8 +1082,7 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
         move_mixed_kernel<kDepTable, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
                                                                               max_hops, bd, push, dh);
     else
-        move_mixed_kernel<kDepWarp, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status,
-                                                                             max_hops, bd, push, dh);
+        launch_warp<true, kPush, kSeed, kDevCount>(parts->size, s, *mesh, p, rep.args, status, max_hops, bd, push, dh);
     count_launches(1);
     rep.end(s);
     return launch_status();

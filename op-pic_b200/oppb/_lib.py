@@ -57,7 +57,8 @@ class Dat(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("advec_items", c_i32), ("sort_gather_cols", c_i32),
-                ("move_lanes", c_i32), ("move_occupancy", c_i32), ("sort_scatter", c_i32), ("move_stage", c_i32)]
+                ("move_lanes", c_i32), ("move_occupancy", c_i32), ("sort_scatter", c_i32), ("move_stage", c_i32),
+                ("move_block", c_i32)]
 
 
 DEPOSIT_WARP_ATOMIC = 0
@@ -240,7 +241,7 @@ def check(fn: str, status: int) -> None:
 def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_items: int | None = None,
                sort_gather_cols: int | None = None, move_lanes: int | None = None,
                move_occupancy: int | None = None, sort_scatter: int | None = None,
-               move_stage: int | None = None) -> None:
+               move_stage: int | None = None, move_block: int | None = None) -> None:
     t = Tuning()
     load().oppb_get_tuning(C.byref(t))
     if deposit is not None:
@@ -259,6 +260,8 @@ def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_it
         t.sort_scatter = sort_scatter
     if move_stage is not None:
         t.move_stage = move_stage
+    if move_block is not None:
+        t.move_block = move_block
     check("oppb_set_tuning", load().oppb_set_tuning(C.byref(t)))
 
 

@@ -1,17 +1,19 @@
 """The launch choices of the FemPIC path, picked by timing them on the live state.
 
-The move + deposit launch has five choices (oppb_tuning): the FP64 move's lanes per particle
-(one, 32 particles per warp, or a lane pair, 16 per warp), for the pair kernel the CTAs per SM
-it is compiled for (8 at 32 registers a thread, 5 at 48), for the one-lane kernel whether the
-cell records are staged into shared memory by bulk asynchronous copies; the deposit strategy (warp-matched
-FP64 atomics, or a per-CTA shared-memory node table) and how many node-sum copies the atomics
-are spread over.  The cell sort has one (particle-dat columns gathered per launch).  tune_move
-and tune_sort time every candidate on the simulation's current particle state, restoring a
-snapshot of the particle dats before each trial so that every candidate sees the same input,
-then keep the fastest as the process-wide tuning.  The choice of a trial is the median of
-its repetitions.  tune_sort_period times whole sort cycles (the steps between two cell sorts)
-for candidate Sort_Periodic periods from a snapshot of the state and reports the cost per
-particle-step of each; results stay bit-exact for any period (the oracle runs the same one).
+The move + deposit launch has six choices (oppb_tuning): the FP64 move's lanes per particle
+(one, 32 particles per warp, or a lane pair, 16 per warp), for the pair kernel the CTAs per
+SM it is compiled for (8 at 32 registers a thread, 5 at 48), for the one-lane kernel whether
+the cell records are staged into shared memory by bulk asynchronous copies; the deposit
+strategy (warp-matched FP64 atomics, or a per-CTA shared-memory node table), how many
+node-sum copies the atomics are spread over, and the block shape of the one-lane kernels
+(128, 256 or 512 threads).  The cell sort has two (particle-dat columns moved per launch,
+gather by destination or scatter by source).  tune_move, tune_lanes, tune_block and tune_sort
+time every candidate on the simulation's current particle state, restoring a snapshot of the
+particle dats before each trial so that every candidate sees the same input, then keep the
+fastest as the process-wide tuning.  The choice of a trial is the median of its repetitions.
+tune_sort_period times whole sort cycles (the steps between two cell sorts) for candidate
+Sort_Periodic periods from a snapshot of the state and reports the cost per particle-step of
+each; results stay bit-exact for any period (the oracle runs the same one).
 """
 from __future__ import annotations
 
@@ -26,6 +28,7 @@ from oppb import _lib as L
 
 MOVE_CANDIDATES = [(dep, rep) for dep in (L.DEPOSIT_WARP_ATOMIC, L.DEPOSIT_CTA_TABLE) for rep in (1, 4, 8, 16)]
 LANE_CANDIDATES = [(1, 8, 0), (1, 8, 1), (2, 8, 0), (2, 5, 0)]  # (move_lanes, move_occupancy, move_stage)
+BLOCK_CANDIDATES = [256, 128, 512]  # threads per CTA of the one-lane move kernels
 SORT_CANDIDATES = [(16, 0), (10, 0), (5, 0), (16, 1), (10, 1)]  # (columns per launch, scatter form)
 PERIOD_CANDIDATES = [5, 10, 20]
 
@@ -87,22 +90,23 @@ def _timed(fn) -> float:
     return e0.elapsed_time(e1)
 
 
-def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None) -> TuneResult:
-    """Deposit strategy x node-sum copies for sim's move + deposit launch, on sim's current
-    state, pushed as a step pushes it (so the walks have a step's hops): timed with the push as
-    its prologue when with_push (default: when sim fuses the push), else the move launch alone
-    after an untimed push.  Sets the fastest; sim's state is left as found."""
+def _tune_walk(sim, cands, apply, current, reps: int, with_push: bool | None) -> TuneResult:
+    """Times each candidate of the move + deposit launch on sim's current state, pushed as a step
+    pushes it: with the push as its prologue when with_push (default: when sim fuses the push),
+    else the move launch alone after an untimed push.  apply(c) sets candidate c's tuning;
+    current(t) reads a tuning's choice.  Sets the fastest; sim's state is left as found.  When
+    the state's snapshot does not fit in device memory, nothing is timed and the current choice
+    (or the first candidate) is kept."""
     before = L.Tuning()
     L.load().oppb_get_tuning(C.byref(before))
-    cands = candidates or MOVE_CANDIDATES
-    if not snapshot_fits(sim):  # keep the current choice rather than run out of device memory
-        cur = (before.deposit, before.replicas)
+    if not snapshot_fits(sim):
+        cur = current(before)
         return TuneResult(choice=cur if cur in cands else cands[0])
     snap = ParticleSnapshot(sim)
     fused = sim.fused_push if with_push is None else with_push
 
     def run(c) -> float:
-        L.set_tuning(deposit=c[0], replicas=c[1])
+        apply(c)
         snap.restore()
         if fused:
             return _timed(sim.push_move)
@@ -116,41 +120,46 @@ def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None
         raise
     finally:
         snap.restore()
-    L.set_tuning(deposit=res.choice[0], replicas=res.choice[1])
+    apply(res.choice)
     return res
+
+
+def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None) -> TuneResult:
+    """Deposit strategy x node-sum copies for sim's move + deposit launch."""
+    return _tune_walk(sim, candidates or MOVE_CANDIDATES, lambda c: L.set_tuning(deposit=c[0], replicas=c[1]),
+                      lambda t: (t.deposit, t.replicas), reps, with_push)
 
 
 def tune_lanes(sim, candidates=None, reps: int = 3, with_push: bool | None = None) -> TuneResult:
-    """Lanes per particle and compiled occupancy of the FP64 move + deposit launch (the mixed
-    kernel has one lane per particle: nothing to tune there), timed as tune_move times its
-    candidates, with the deposit choice in force.  Sets the fastest; sim's state is left as found."""
+    """Lanes per particle, compiled occupancy and record staging of the FP64 move + deposit
+    launch (the mixed kernel has one lane per particle: nothing to tune there), with the deposit
+    choice in force."""
     if sim.precision != "f64":
         return TuneResult(choice=(1, 8, 0))
-    before = L.Tuning()
-    L.load().oppb_get_tuning(C.byref(before))
-    cands = candidates or LANE_CANDIDATES
-    if not snapshot_fits(sim):
-        return TuneResult(choice=(before.move_lanes, before.move_occupancy, before.move_stage))
-    snap = ParticleSnapshot(sim)
-    fused = sim.fused_push if with_push is None else with_push
+    return _tune_walk(sim, candidates or LANE_CANDIDATES,
+                      lambda c: L.set_tuning(move_lanes=c[0], move_occupancy=c[1], move_stage=c[2]),
+                      lambda t: (t.move_lanes, t.move_occupancy, t.move_stage), reps, with_push)
 
-    def run(c) -> float:
-        L.set_tuning(move_lanes=c[0], move_occupancy=c[1], move_stage=c[2])
-        snap.restore()
-        if fused:
-            return _timed(sim.push_move)
-        sim.push()
-        return _timed(sim.move)
 
-    try:
-        res = pick(cands, run, reps)
-    except Exception:
-        L.load().oppb_set_tuning(C.byref(before))
-        raise
-    finally:
-        snap.restore()
-    L.set_tuning(move_lanes=res.choice[0], move_occupancy=res.choice[1], move_stage=res.choice[2])
-    return res
+def block_shape_applies(t: L.Tuning, precision: str) -> bool:
+    """Whether oppb_tuning.move_block shapes the launch: the one-lane kernels with the
+    warp-grouped deposit (the CTA table is sized for 256 threads, the exact deposit, the
+    lane-pair and the staged kernels run 256)."""
+    if t.deposit != L.DEPOSIT_WARP_ATOMIC:
+        return False
+    return precision != "f64" or (t.move_lanes in (0, 1) and t.move_stage == 0)
+
+
+def tune_block(sim, candidates=None, reps: int = 3, with_push: bool | None = None) -> TuneResult:
+    """Threads per CTA of the one-lane move + deposit launch (2048 / block CTAs per SM, 32
+    registers a thread either way), with the deposit and lane choices in force; nothing is timed
+    when those choices do not use the one-lane warp-deposit kernel."""
+    t = L.Tuning()
+    L.load().oppb_get_tuning(C.byref(t))
+    if not block_shape_applies(t, sim.precision):
+        return TuneResult(choice=t.move_block or 256)
+    return _tune_walk(sim, candidates or BLOCK_CANDIDATES, lambda c: L.set_tuning(move_block=c),
+                      lambda t: t.move_block, reps, with_push)
 
 
 class StateSnapshot:

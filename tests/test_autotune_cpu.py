@@ -4,7 +4,8 @@ from __future__ import annotations
 
 import pytest
 
-from oppb.autotune import LANE_CANDIDATES, MOVE_CANDIDATES, PERIOD_CANDIDATES, SORT_CANDIDATES, pick
+from oppb.autotune import (BLOCK_CANDIDATES, LANE_CANDIDATES, MOVE_CANDIDATES, PERIOD_CANDIDATES, SORT_CANDIDATES,
+                            block_shape_applies, pick)
 
 
 def test_pick_smallest_median():
@@ -34,20 +35,38 @@ def test_candidate_sets():
     assert LANE_CANDIDATES[0] == (1, 8, 0)
     assert all(lanes in (1, 2) and occ in (5, 8) and stage in (0, 1) for lanes, occ, stage in LANE_CANDIDATES)
     assert 10 in PERIOD_CANDIDATES
+    assert BLOCK_CANDIDATES[0] == 256 and sorted(BLOCK_CANDIDATES) == [128, 256, 512]
 
 
 def test_tuning_fields_validated():
     """oppb_set_tuning accepts the documented values of every field and refuses others."""
     from oppb import _lib as L
 
-    L.set_tuning(move_lanes=2, move_occupancy=5, sort_scatter=1, move_stage=1)
+    L.set_tuning(move_lanes=2, move_occupancy=5, sort_scatter=1, move_stage=1, move_block=512)
     t = L.Tuning()
     L.load().oppb_get_tuning(t)
-    assert (t.move_lanes, t.move_occupancy, t.sort_scatter, t.move_stage) == (2, 5, 1, 1)
-    for kw in (dict(move_lanes=3), dict(move_occupancy=6), dict(sort_scatter=2), dict(move_stage=2)):
+    assert (t.move_lanes, t.move_occupancy, t.sort_scatter, t.move_stage, t.move_block) == (2, 5, 1, 1, 512)
+    for kw in (dict(move_lanes=3), dict(move_occupancy=6), dict(sort_scatter=2), dict(move_stage=2),
+               dict(move_block=64), dict(move_block=384), dict(move_block=1024)):
         with pytest.raises(L.OppbError):
             L.set_tuning(**kw)
-    L.set_tuning(move_lanes=1, move_occupancy=8, sort_scatter=0, move_stage=0)
+    L.set_tuning(move_block=0)  # 0 reads as the default
+    L.load().oppb_get_tuning(t)
+    assert t.move_block == 256
+    L.set_tuning(move_lanes=1, move_occupancy=8, sort_scatter=0, move_stage=0, move_block=256)
+
+
+def test_block_shape_applies_to_the_one_lane_warp_deposit():
+    """move_block shapes the one-lane kernels with the warp-grouped deposit only."""
+    from oppb import _lib as L
+
+    t = L.Tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=1, move_stage=0, move_block=128)
+    assert block_shape_applies(t, "f64") and block_shape_applies(t, "mixed")
+    assert not block_shape_applies(L.Tuning(deposit=L.DEPOSIT_CTA_TABLE, move_lanes=1), "mixed")
+    assert not block_shape_applies(L.Tuning(deposit=L.DEPOSIT_EXACT, move_lanes=1), "f64")
+    assert not block_shape_applies(L.Tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=2), "f64")
+    assert not block_shape_applies(L.Tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=1, move_stage=1), "f64")
+    assert block_shape_applies(L.Tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=2), "mixed")
 
 
 def test_snapshot_fits_counts_live_columns(monkeypatch):
