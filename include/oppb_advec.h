@@ -34,6 +34,21 @@ typedef struct oppb_advec_instance {
     double  extents[2];
 } oppb_advec_instance;
 
+/* Direct-hop seed of one instance (the global move of the reference's move loop,
+ * opp_dev_checkForGlobalMove2D_kernel with opp_dev_findStructuredCellIndex2D,
+ * opp_lib/include/device_kernels/cuda_inline_kernels.h): the map of its grid (device,
+ * filled by oppb_dh_build_quad), the grid's lower corner, 1/spacing and box counts.  Before a
+ * particle's walk, box (x, y) = ((pos - min) * inv_spacing truncated toward zero, negative
+ * giving 0); a box at or past the count on either axis, or one without a cell, removes the
+ * particle (p2c = OPPB_REMOVED_CELL, counted in status->remove_count), else the walk starts
+ * from the box's cell. */
+typedef struct oppb_advec_dh {
+    const int32_t* map;
+    double  min[2];
+    double  inv_spacing;
+    int64_t dims[2];
+} oppb_advec_dh;
+
 /* A batch.  instances: device array [n_instances].  tile_prefix: device array
  * [n_instances + 1], the first 256-particle work item of each instance (prefix sum of
  * ceil(n_parts / 256)).  Blocks take items in order, a chunk at a time, from work_counter,
@@ -53,6 +68,8 @@ typedef struct oppb_advec_batch {
     int32_t* p2c;              /* p2c [stride] */
     int32_t* work_counter;     /* device scratch, one int32: the launch hands out work items in
                                   order from it (the launcher zeroes it on the launch's stream) */
+    const oppb_advec_dh* dh;   /* device array [n_instances], or NULL: walks start from p2c.
+                                  Particles at OPPB_REMOVED_CELL are skipped either way. */
 } oppb_advec_batch;
 
 /* Packs one instance's c_pos_ll (SoA [2][ld]) and c2c_map (SoA [4][ld]) into
@@ -62,7 +79,8 @@ int oppb_advec_pack_cells(double* cells, int32_t cell_offset, int32_t n_cells, i
 
 /* update_pos_kernel then move_kernel for every particle of every instance, fused per
  * particle (the position stays in registers), in one persistent launch.  Bit-identical to
- * the seq backend running the two loops on each instance.  status is accumulated into, not
+ * the seq backend running the two loops on each instance (with opp_global_move on, when
+ * batch->dh is set).  status is accumulated into, not
  * cleared (zero it before a sequence of steps, e.g. one captured CUDA graph of many steps):
  * total_visits / max_visits count move calls; the first hop-bound overrun or out-of-range
  * cell sets error / error_index (index into the concatenated dats). */

@@ -1,4 +1,5 @@
-/* C ABI of the direct-hop (DH) seed of the FemPIC move: OP-PIC's structured cell mapper
+/* C ABI of the direct-hop (DH) seed of the FemPIC move (and, at the end, of the 2-D grids of
+ * the NESO-advection move): OP-PIC's structured cell mapper
  * (opp_lib/include/opp_direct_hop_core.h CellMapper, seq build
  * opp_lib/src/seq/opp_direct_hop_seq.cpp) and the global-move pre-pass of the move loop
  * (apps_codegen/app_fempic_cg/seq/move_kernel_loop.hpp:112-131, CUDA
@@ -63,6 +64,29 @@ int oppb_dh_grid_init(const double* n_pos, int32_t n_nodes, double spacing, cons
  * once to read the number of (cell, box) pairs; call again with that much. */
 int oppb_dh_build(const oppb_tet_mesh* mesh, const double* n_pos, oppb_dh_grid* grid, void* workspace,
                   size_t ws_bytes, size_t* ws_needed, void* stream);
+
+/* ------------------------------------------------------- 2-D grids (NESO advection)
+ * The global move of the advection app (apps_codegen/app_neso_advection_mdir_cg/advec_opp.cpp:
+ * 97-103: BoundingBox(c_pos_ll, DIM, expansion), opp_init_direct_hop_cg; CUDA pre-pass
+ * opp_dev_checkForGlobalMove2D_kernel).  The grid has one box along z (min = max = 0). */
+
+/* Host: BoundingBox(pos, 2, expansion) of host AoS [n][2] points (the cells' lower-left
+ * corners c_pos_ll in the app): z stays 0, x/y widened as oppb_dh_bounding_box widens them. */
+int oppb_dh_bounding_box_2d(const double* pos, int32_t n, const double expansion[3], double min_out[3],
+                            double max_out[3]);
+
+/* Host: oppb_dh_bounding_box_2d then oppb_dh_grid_from_box (dims[2] = 1). */
+int oppb_dh_grid_init_2d(const double* pos, int32_t n, double spacing, const double expansion[3],
+                         oppb_dh_grid* grid);
+
+/* Device: fills grid->map for the square cells of one advection instance (generateStructuredMesh,
+ * as oppb_dh_build, with the app's all-cell checker, apps_codegen/app_neso_advection_mdir_cg/
+ * seq/move_kernel_loop.hpp:194-219: the lowest-index cell whose move_kernel call ends with
+ * MOVE_DONE, i.e. with 0 <= p - c_pos_ll <= cell_width on both axes).  cells: the instance's
+ * first packed record ({c_pos_ll, c2c}, include/oppb_advec.h), device, 32-byte aligned.
+ * Workspace as oppb_dh_build.  OPPB_ERR_ARG unless grid->dims[2] == 1. */
+int oppb_dh_build_quad(const double* cells, int32_t n_cells, double cell_width, oppb_dh_grid* grid,
+                       void* workspace, size_t ws_bytes, size_t* ws_needed, void* stream);
 
 /* ------------------------------------------------------------- general move entry point */
 

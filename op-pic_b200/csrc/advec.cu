@@ -11,7 +11,8 @@
 // then y), reading one 32-byte cell record {c_pos_ll, c2c} per call.  This file is compiled
 // with -fmad=false and the periodic wrap uses the library's FMOD (a - b * trunc(a / b),
 // opp_lib/include/opp_util.h:48) with a correctly rounded divide, so positions, directions and
-// cells are bit-identical to the seq backend.
+// cells are bit-identical to the seq backend.  With the global move on (batch.dh), each walk
+// starts from the cell of the direct-hop grid box holding the updated position.
 
 #include "oppb_advec.h"
 #include "oppb_common.cuh"
@@ -89,16 +90,30 @@ __device__ __forceinline__ int move_particle(const double* __restrict__ cells, i
 
 constexpr int kChunkItems = 8;  // work items a block takes from the counter at once
 
+// Direct-hop seed (oppb_advec_dh): the cell of the grid box holding (x, y), or kRemoved
+// outside the grid or in a box without a cell.  Each box coordinate is (pos - min) * (1/h)
+// truncated by a round-toward-zero conversion that saturates (negative and NaN give 0), the
+// conversion the reference's (size_t) cast compiles to.
+__device__ __forceinline__ int32_t dh_seed_2d(const oppb_advec_dh& g, double x, double y) {
+    const unsigned long long ix = __double2ull_rz(__dmul_rn(__dsub_rn(x, __ldg(&g.min[0])), __ldg(&g.inv_spacing)));
+    const unsigned long long iy = __double2ull_rz(__dmul_rn(__dsub_rn(y, __ldg(&g.min[1])), __ldg(&g.inv_spacing)));
+    const unsigned long long dx = (unsigned long long)__ldg(&g.dims[0]), dy = (unsigned long long)__ldg(&g.dims[1]);
+    if (ix >= dx || iy >= dy) return kRemoved;
+    return __ldg(g.map + (int64_t)(ix + dx * iy));
+}
+
 // A block takes a chunk of work items from the batch's counter (so items are processed in
 // order across the whole GPU) and walks it kItems items per pass (one particle of each per
 // thread), so every thread has kItems independent particles' loads in flight.
-template <int kMode, int kItems>
+template <int kMode, int kItems, bool kSeed>
 __global__ void __launch_bounds__(kAdvBlock) advec_kernel(oppb_advec_batch b, oppb_move_status* st,
                                                           int32_t max_hops) {
     static_assert(kChunkItems % kItems == 0, "a chunk is a whole number of passes");
+    static_assert(!kSeed || kMode != kUpdateOnly, "the seed belongs to the move");
     __shared__ int s_chunk;
     unsigned long long my_calls = 0;
     int my_max = 0;
+    int my_removed = 0;
     int cursor = 0;
     const int64_t sd = b.stride;
     for (;;) {
@@ -153,6 +168,14 @@ __global__ void __launch_bounds__(kAdvBlock) advec_kernel(oppb_advec_batch b, op
                 if (kMode != kUpdateOnly) {
                     if (cell[k] == kRemoved) continue;
                     const int32_t cell0 = cell[k];
+                    if (kSeed) {  // the global-move pre-pass, after the update as in the reference
+                        cell[k] = dh_seed_2d(b.dh[inst[k]], x[k], y[k]);
+                        if (cell[k] == kRemoved) {
+                            st_stream(b.p2c + i, kRemoved);
+                            my_removed++;
+                            continue;
+                        }
+                    }
                     int err = 0;
                     const int calls = move_particle(b.cells, __ldg(&I.cell_offset), __ldg(&I.n_cells), x[k], y[k], mx[k],
                                                     my[k], cell[k], __ldg(&I.cell_width), ex, ey, max_hops, err);
@@ -170,24 +193,29 @@ __global__ void __launch_bounds__(kAdvBlock) advec_kernel(oppb_advec_batch b, op
     // One atomic per counter per block: the grid is persistent, so this is a few hundred.
     __shared__ unsigned long long s_calls[kAdvWarps];
     __shared__ int s_max[kAdvWarps];
+    __shared__ int s_removed[kAdvWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) my_calls += __shfl_xor_sync(kFullMask, my_calls, o);
     my_max = (int)__reduce_max_sync(kFullMask, (unsigned)my_max);
+    if (kSeed) my_removed = (int)__reduce_add_sync(kFullMask, (unsigned)my_removed);
     if (lane == 0) {
         s_calls[warp] = my_calls;
         s_max[warp] = my_max;
+        s_removed[warp] = my_removed;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long c = 0;
-        int m = 0;
+        int m = 0, r = 0;
         for (int k = 0; k < kAdvWarps; k++) {
             c += s_calls[k];
             m = max(m, s_max[k]);
+            r += s_removed[k];
         }
         if (c) atomicAdd(reinterpret_cast<unsigned long long*>(&st->total_visits), c);
         if (m) atomicMax(&st->max_visits, m);
+        if (kSeed && r) atomicAdd(&st->remove_count, r);
     }
 }
 
@@ -207,7 +235,7 @@ __global__ void __launch_bounds__(256) advec_pack_kernel(double* cells, int32_t 
 }
 
 // Persistent grid: resident blocks of the kernel on every SM (cached per device and variant).
-template <int kMode, int kItems>
+template <int kMode, int kItems, bool kSeed>
 int persistent_grid(int n_blocks_needed) {
     static int cached[64] = {0};
     int dev = 0;
@@ -215,16 +243,27 @@ int persistent_grid(int n_blocks_needed) {
     if (!cached[dev]) {
         int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, advec_kernel<kMode, kItems>, kAdvBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, advec_kernel<kMode, kItems, kSeed>, kAdvBlock, 0);
         cached[dev] = sms * (per_sm > 0 ? per_sm : 1);
     }
     return n_blocks_needed < cached[dev] ? n_blocks_needed : cached[dev];
 }
 
-template <int kMode, int kItems>
+template <int kMode, int kItems, bool kSeed>
 void launch_items(const oppb_advec_batch* b, oppb_move_status* status, int32_t max_hops, cudaStream_t s) {
-    const int grid = persistent_grid<kMode, kItems>(ceil_div(b->n_work, kChunkItems));
-    advec_kernel<kMode, kItems><<<grid, kAdvBlock, 0, s>>>(*b, status, max_hops);
+    const int grid = persistent_grid<kMode, kItems, kSeed>(ceil_div(b->n_work, kChunkItems));
+    advec_kernel<kMode, kItems, kSeed><<<grid, kAdvBlock, 0, s>>>(*b, status, max_hops);
+}
+
+template <int kMode, bool kSeed>
+void launch_seeded(const oppb_advec_batch* b, oppb_move_status* status, int32_t max_hops, cudaStream_t s) {
+    const int items = tuning().advec_items;
+    if (items == 4)
+        launch_items<kMode, 4, kSeed>(b, status, max_hops, s);
+    else if (items == 1)
+        launch_items<kMode, 1, kSeed>(b, status, max_hops, s);
+    else
+        launch_items<kMode, 2, kSeed>(b, status, max_hops, s);
 }
 
 int check_batch(const oppb_advec_batch* b) {
@@ -243,13 +282,14 @@ int launch_advec(const oppb_advec_batch* b, oppb_move_status* status, int32_t ma
     if (b->n_work == 0) return OPPB_OK;
     cudaStream_t s = as_stream(stream);
     if (cudaMemsetAsync(b->work_counter, 0, sizeof(int32_t), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
-    const int items = tuning().advec_items;
-    if (items == 4)
-        launch_items<kMode, 4>(b, status, max_hops, s);
-    else if (items == 1)
-        launch_items<kMode, 1>(b, status, max_hops, s);
-    else
-        launch_items<kMode, 2>(b, status, max_hops, s);
+    if constexpr (kMode != kUpdateOnly) {
+        if (b->dh)
+            launch_seeded<kMode, true>(b, status, max_hops, s);
+        else
+            launch_seeded<kMode, false>(b, status, max_hops, s);
+    } else {
+        launch_seeded<kMode, false>(b, status, max_hops, s);
+    }
     count_launches(1);
     return launch_status();
 }

@@ -1,5 +1,6 @@
-// Direct-hop (DH) structured grid of the FemPIC move (include/oppb_dh.h): the host set-up of
-// the grid (OP-PIC's BoundingBox and CellMapper::init_host) and its build on the GPU.
+// Direct-hop (DH) structured grid of the FemPIC move and of the 2-D NESO-advection move
+// (include/oppb_dh.h): the host set-up of the grid (OP-PIC's BoundingBox and
+// CellMapper::init_host) and its build on the GPU.
 //
 // The reference fills the map on the host by testing, for each grid box, every mesh cell in
 // index order until one contains the query point (opp_lib/src/seq/opp_direct_hop_seq.cpp:
@@ -14,6 +15,11 @@
 // A cell accepts a point only within the 1e-10 tolerance of its barycentric weights, far
 // inside the widening, and the bin of a coordinate is monotone in it, so every accepting
 // cell is among the candidates of the point's box: the lowest accepting index is found.
+// The advection mesh's square cells go through the same two kernels with the app's
+// all-cell checker (apps_codegen/app_neso_advection_mdir_cg/seq/move_kernel_loop.hpp:
+// 194-219): a square accepts a point when the move kernel's FP64 differences p - ll lie in
+// [0, cell_width] on both axes, i.e. at most one rounding beyond the square, again far inside
+// the widening.  A 2-D grid has one box along z (min = max = 0), where every z bin is 0.
 
 #include <cfloat>
 #include <cmath>
@@ -48,22 +54,65 @@ __device__ __forceinline__ int64_t bin_of(const GridArgs& g, int d, double v) {
     return (int64_t)t;
 }
 
-// Node bounding box of cell c, widened; false for a cell with a node index out of range.
-__device__ __forceinline__ bool cell_bins(const oppb_tet_mesh& m, const double* npos, int32_t c, const GridArgs& g,
-                                          int64_t b0[3], int64_t b1[3]) {
-    const int4 nd = ldg_i4(m.c2n + (int64_t)c * 4);
-    const int n[4] = {nd.x, nd.y, nd.z, nd.w};
-    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+// Tetrahedra of the FemPIC mesh: node bounding boxes, and the move kernel's FP64 barycentric
+// test (apps_codegen/app_fempic_cg/seq/move_kernel_loop.hpp:170-198).
+struct TetCells {
+    oppb_tet_mesh m;
+    const double* npos;  // SoA [3][n_nodes]
+    __device__ int32_t count() const { return m.n_cells; }
+    // Node bounding box of cell c; false for a cell with a node index out of range.
+    __device__ bool bounds(int32_t c, double lo[3], double hi[3]) const {
+        const int4 nd = ldg_i4(m.c2n + (int64_t)c * 4);
+        const int n[4] = {nd.x, nd.y, nd.z, nd.w};
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        if ((uint32_t)n[k] >= (uint32_t)m.n_nodes) return false;
+        for (int d = 0; d < 3; d++) lo[d] = DBL_MAX, hi[d] = -DBL_MAX;
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const double v = __ldg(npos + (int64_t)d * m.n_nodes + n[k]);
-            lo[d] = fmin(lo[d], v);
-            hi[d] = fmax(hi[d], v);
+        for (int k = 0; k < 4; k++) {
+            if ((uint32_t)n[k] >= (uint32_t)m.n_nodes) return false;
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const double v = __ldg(npos + (int64_t)d * m.n_nodes + n[k]);
+                lo[d] = fmin(lo[d], v);
+                hi[d] = fmax(hi[d], v);
+            }
         }
+        return true;
     }
+    __device__ bool holds(int32_t c, const double p[3]) const {
+        double l[4];
+        int nb[4];
+        visit_f64(m, c, p[0], p[1], p[2], l, nb);
+        return inside_f64(l);
+    }
+};
+
+// Squares of one NESO-advection instance (packed records {c_pos_ll x, y, c2c}, include/oppb_advec.h):
+// the square [ll, ll + w]^2 at z = 0, and move_kernel's in-cell test of its first call
+// (apps/app_neso_advection/kernels.h move_kernel, step 2 on both axes).
+struct QuadCells {
+    const double* cells;  // the instance's first record, [n][4]
+    int32_t n;
+    double w;             // CONST_cell_width
+    __device__ int32_t count() const { return n; }
+    __device__ bool bounds(int32_t c, double lo[3], double hi[3]) const {
+        const double2 ll = ldg_d2(cells + (int64_t)c * 4);
+        lo[0] = ll.x, lo[1] = ll.y, lo[2] = 0.0;
+        hi[0] = ll.x + w, hi[1] = ll.y + w, hi[2] = 0.0;
+        return true;
+    }
+    __device__ bool holds(int32_t c, const double p[3]) const {
+        const double2 ll = ldg_d2(cells + (int64_t)c * 4);
+        const double dx = __dsub_rn(p[0], ll.x), dy = __dsub_rn(p[1], ll.y);
+        return (dx >= 0.0) && (dx <= w) && (dy >= 0.0) && (dy <= w);
+    }
+};
+
+// Bounding box of cell c, widened; false for a cell with a node index out of range.
+template <class Cells>
+__device__ __forceinline__ bool cell_bins(const Cells& cs, int32_t c, const GridArgs& g, int64_t b0[3],
+                                          int64_t b1[3]) {
+    double lo[3], hi[3];
+    if (!cs.bounds(c, lo, hi)) return false;
     const double ext = fmax(fmax(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]);
     const double w = kBinWiden * ext;
 #pragma unroll
@@ -76,13 +125,12 @@ __device__ __forceinline__ bool cell_bins(const oppb_tet_mesh& m, const double* 
 
 // kMode 0: add the number of (cell, box) pairs to *pairs; 1: count the cells of every box;
 // 2: write each cell into its boxes' lists.
-template <int kMode>
-__global__ void __launch_bounds__(kDhBlock) dh_bin_kernel(oppb_tet_mesh m, const double* npos, GridArgs g,
-                                                          unsigned long long* pairs, int* counts, int* cursor,
-                                                          int* list) {
+template <int kMode, class Cells>
+__global__ void __launch_bounds__(kDhBlock) dh_bin_kernel(Cells cs, GridArgs g, unsigned long long* pairs,
+                                                          int* counts, int* cursor, int* list) {
     const int32_t c = (int32_t)(blockIdx.x * kDhBlock + threadIdx.x);
     int64_t b0[3], b1[3];
-    const bool ok = c < m.n_cells && cell_bins(m, npos, c, g, b0, b1);
+    const bool ok = c < cs.count() && cell_bins(cs, c, g, b0, b1);
     if (kMode == 0) {
         unsigned long long s =
             ok ? (unsigned long long)((b1[0] - b0[0] + 1) * (b1[1] - b0[1] + 1) * (b1[2] - b0[2] + 1)) : 0ull;
@@ -103,24 +151,24 @@ __global__ void __launch_bounds__(kDhBlock) dh_bin_kernel(oppb_tet_mesh m, const
             }
 }
 
-// Lowest-index cell whose FP64 barycentric test (the move kernel's) accepts p, or kRemoved.
-__device__ int32_t first_cell(const oppb_tet_mesh& m, const GridArgs& g, const int* offsets, const int* list,
+// Lowest-index cell whose test (the move kernel's) accepts p, or kRemoved.
+template <class Cells>
+__device__ int32_t first_cell(const Cells& cs, const GridArgs& g, const int* offsets, const int* list,
                               const double p[3]) {
     const int64_t b = bin_of(g, 0, p[0]) + g.dims[0] * (bin_of(g, 1, p[1]) + g.dims[1] * bin_of(g, 2, p[2]));
     int32_t best = kRemoved;
     for (int k = offsets[b]; k < offsets[b + 1]; k++) {
         const int32_t c = list[k];
-        if (c >= best) continue;
-        double l[4];
-        int nb[4];
-        visit_f64(m, c, p[0], p[1], p[2], l, nb);
-        if (inside_f64(l)) best = c;
+        if (c < best && cs.holds(c, p)) best = c;
     }
     return best;
 }
 
-// One thread per grid box: generateStructuredMesh steps 1 and 3 for the box.
-__global__ void __launch_bounds__(kDhBlock) dh_query_kernel(oppb_tet_mesh m, GridArgs g, const int* offsets,
+// One thread per grid box: generateStructuredMesh steps 1 and 3 for the box.  On a 2-D grid
+// the z nudge repeats the x/y query and the upper z corners clamp onto the lower ones, so the
+// answer is the 2-D one (the reference's 4 corners).
+template <class Cells>
+__global__ void __launch_bounds__(kDhBlock) dh_query_kernel(Cells cs, GridArgs g, const int* offsets,
                                                             const int* list, int32_t* map, int64_t size) {
     const int64_t idx = (int64_t)blockIdx.x * kDhBlock + threadIdx.x;
     if (idx >= size) return;
@@ -135,14 +183,14 @@ __global__ void __launch_bounds__(kDhBlock) dh_query_kernel(oppb_tet_mesh m, Gri
         q[d] = (__dadd_rn(corner[d], g.h) <= g.max[d]) ? __dadd_rn(corner[d], __dmul_rn(g.h, 0.5))
                                                        : __dmul_rn(__dadd_rn(corner[d], g.max[d]), 0.5);
     }
-    int32_t cid = first_cell(m, g, offsets, list, q);
+    int32_t cid = first_cell(cs, g, offsets, list, q);
     // Not found: nudge the centroid by h/100 along x, then y, then z (cumulative, :172-183).
     const double nudge = __ddiv_rn(g.h, 100.0);
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         if (cid != kRemoved) break;
         q[d] = __dadd_rn(q[d], nudge);
-        cid = first_cell(m, g, offsets, list, q);
+        cid = first_cell(cs, g, offsets, list, q);
     }
     if (cid == kRemoved) {
         // Step 3 (:214-246): the lowest cell holding one of the box's 8 corners, each corner
@@ -154,7 +202,7 @@ __global__ void __launch_bounds__(kDhBlock) dh_query_kernel(oppb_tet_mesh m, Gri
                 const double t = ((k >> d) & 1) ? __dadd_rn(corner[d], g.h) : corner[d];
                 v[d] = (t > g.max[d]) ? g.max[d] : t;
             }
-            const int32_t c = first_cell(m, g, offsets, list, v);
+            const int32_t c = first_cell(cs, g, offsets, list, v);
             if (c < cid) cid = c;
         }
     }
@@ -226,13 +274,13 @@ extern "C" int oppb_dh_grid_init(const double* n_pos, int32_t n_nodes, double sp
     return rc ? rc : oppb_dh_grid_from_box(mn, mx, spacing, g);
 }
 
-extern "C" int oppb_dh_build(const oppb_tet_mesh* mesh, const double* n_pos, oppb_dh_grid* grid, void* workspace,
-                             size_t ws_bytes, size_t* ws_needed, void* stream) {
-    using namespace oppb;
-    if (!mesh || !n_pos || !grid || !grid->map || mesh->n_cells <= 0 || mesh->n_nodes <= 0) return OPPB_ERR_ARG;
-    if (!mesh->det || !mesh->nav || !mesh->c2n || !aligned(mesh->det, 32) || !aligned(mesh->nav, 32) ||
-        !aligned(mesh->c2n, 16))
-        return OPPB_ERR_ARG;
+namespace oppb {
+namespace {
+
+// The build common to both meshes: bin the cells, then query every box.
+template <class Cells>
+int build_map(const Cells& cs, int32_t n_cells, oppb_dh_grid* grid, void* workspace, size_t ws_bytes,
+              size_t* ws_needed, void* stream) {
     if (grid->size <= 0 || grid->size > 2147483646 || !(grid->spacing > 0.0) ||
         grid->size != grid->dims[0] * grid->dims[1] * grid->dims[2])
         return OPPB_ERR_ARG;
@@ -243,9 +291,9 @@ extern "C" int oppb_dh_build(const oppb_tet_mesh* mesh, const double* n_pos, opp
     cudaStream_t s = as_stream(stream);
     unsigned long long* d_pairs = nullptr;
     if (cudaGetSymbolAddress(reinterpret_cast<void**>(&d_pairs), g_dh_pairs) != cudaSuccess) return OPPB_ERR_LAUNCH;
-    const int cell_grid = ceil_div(mesh->n_cells, kDhBlock);
+    const int cell_grid = ceil_div(n_cells, kDhBlock);
     if (cudaMemsetAsync(d_pairs, 0, sizeof(unsigned long long), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
-    dh_bin_kernel<0><<<cell_grid, kDhBlock, 0, s>>>(*mesh, n_pos, g, d_pairs, nullptr, nullptr, nullptr);
+    dh_bin_kernel<0><<<cell_grid, kDhBlock, 0, s>>>(cs, g, d_pairs, nullptr, nullptr, nullptr);
     count_launches(1);
     unsigned long long pairs = 0;
     if (cudaMemcpyAsync(&pairs, d_pairs, sizeof pairs, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -267,13 +315,63 @@ extern "C" int oppb_dh_build(const oppb_tet_mesh* mesh, const double* n_pos, opp
     w += align256(sizeof(int) * (size_t)(pairs ? pairs : 1));
     int* scratch = reinterpret_cast<int*>(w);
     if (cudaMemsetAsync(offsets, 0, sizeof(int) * (size_t)(n + 1), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
-    dh_bin_kernel<1><<<cell_grid, kDhBlock, 0, s>>>(*mesh, n_pos, g, nullptr, offsets, nullptr, nullptr);
+    dh_bin_kernel<1><<<cell_grid, kDhBlock, 0, s>>>(cs, g, nullptr, offsets, nullptr, nullptr);
     count_launches(1);
     device_exclusive_scan(offsets, offsets, n + 1, scratch, s);  // offsets[n] = pairs
     if (cudaMemcpyAsync(cursor, offsets, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
         return OPPB_ERR_LAUNCH;
-    dh_bin_kernel<2><<<cell_grid, kDhBlock, 0, s>>>(*mesh, n_pos, g, nullptr, nullptr, cursor, list);
-    dh_query_kernel<<<ceil_div(n, kDhBlock), kDhBlock, 0, s>>>(*mesh, g, offsets, list, grid->map, n);
+    dh_bin_kernel<2><<<cell_grid, kDhBlock, 0, s>>>(cs, g, nullptr, nullptr, cursor, list);
+    dh_query_kernel<<<ceil_div(n, kDhBlock), kDhBlock, 0, s>>>(cs, g, offsets, list, grid->map, n);
     count_launches(2);
     return launch_status();
+}
+
+}  // namespace
+}  // namespace oppb
+
+extern "C" int oppb_dh_build(const oppb_tet_mesh* mesh, const double* n_pos, oppb_dh_grid* grid, void* workspace,
+                             size_t ws_bytes, size_t* ws_needed, void* stream) {
+    using namespace oppb;
+    if (!mesh || !n_pos || !grid || !grid->map || mesh->n_cells <= 0 || mesh->n_nodes <= 0) return OPPB_ERR_ARG;
+    if (!mesh->det || !mesh->nav || !mesh->c2n || !aligned(mesh->det, 32) || !aligned(mesh->nav, 32) ||
+        !aligned(mesh->c2n, 16))
+        return OPPB_ERR_ARG;
+    return build_map(TetCells{*mesh, n_pos}, mesh->n_cells, grid, workspace, ws_bytes, ws_needed, stream);
+}
+
+extern "C" int oppb_dh_bounding_box_2d(const double* pos, int32_t n, const double expansion[3], double min_out[3],
+                                       double max_out[3]) {
+    if (!pos || !expansion || !min_out || !max_out || n <= 0) return OPPB_ERR_ARG;
+    // BoundingBox(pos, 2, expansion) (opp_lib/include/opp_direct_hop_core.h:70-120): z stays
+    // 0; the x/y widening reads the expansion's x for both minima and its y for both maxima.
+    double mn[2] = {DBL_MAX, DBL_MAX}, mx[2] = {DBL_MIN, DBL_MIN};
+    for (int32_t i = 0; i < n; i++)
+        for (int d = 0; d < 2; d++) {
+            const double v = pos[2 * (int64_t)i + d];
+            mn[d] = (mn[d] < v) ? mn[d] : v;  // std::min(v, mn)
+            mx[d] = (v < mx[d]) ? mx[d] : v;  // std::max(v, mx)
+        }
+    mn[0] -= (expansion[0] + oppb::kBoundOffset);
+    mn[1] -= (expansion[0] + oppb::kBoundOffset);
+    mx[0] += (expansion[1] - oppb::kBoundOffset);
+    mx[1] += (expansion[1] - oppb::kBoundOffset);
+    min_out[0] = mn[0], min_out[1] = mn[1], min_out[2] = 0.0;
+    max_out[0] = mx[0], max_out[1] = mx[1], max_out[2] = 0.0;
+    return OPPB_OK;
+}
+
+extern "C" int oppb_dh_grid_init_2d(const double* pos, int32_t n, double spacing, const double expansion[3],
+                                    oppb_dh_grid* g) {
+    double mn[3], mx[3];
+    const int rc = oppb_dh_bounding_box_2d(pos, n, expansion, mn, mx);
+    return rc ? rc : oppb_dh_grid_from_box(mn, mx, spacing, g);
+}
+
+extern "C" int oppb_dh_build_quad(const double* cells, int32_t n_cells, double cell_width, oppb_dh_grid* grid,
+                                  void* workspace, size_t ws_bytes, size_t* ws_needed, void* stream) {
+    using namespace oppb;
+    if (!cells || !aligned(cells, 32) || n_cells <= 0 || !grid || !grid->map || !(cell_width > 0.0) ||
+        grid->dims[2] != 1)
+        return OPPB_ERR_ARG;
+    return build_map(QuadCells{cells, n_cells, cell_width}, n_cells, grid, workspace, ws_bytes, ws_needed, stream);
 }

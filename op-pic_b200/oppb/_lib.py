@@ -91,7 +91,11 @@ class AdvecInstance(C.Structure):
 class AdvecBatch(C.Structure):
     _fields_ = [("n_instances", c_i32), ("n_work", c_i32), ("instances", c_vp), ("tile_prefix", c_vp),
                 ("cells", c_vp), ("stride", c_i64), ("pos", c_vp), ("vel", c_vp), ("mdir", c_vp), ("p2c", c_vp),
-                ("work_counter", c_vp)]
+                ("work_counter", c_vp), ("dh", c_vp)]
+
+
+class AdvecDh(C.Structure):
+    _fields_ = [("map", c_vp), ("min", C.c_double * 2), ("inv_spacing", C.c_double), ("dims", c_i64 * 2)]
 
 
 class DhGrid(C.Structure):
@@ -193,6 +197,9 @@ _SIGS = {
     "oppb_advec_move": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
     "oppb_dh_grid_init": (C.c_int, [c_vp, c_i32, C.c_double, c_vp, P(DhGrid)]),
     "oppb_dh_build": (C.c_int, [P(TetMesh), c_vp, P(DhGrid), c_vp, C.c_size_t, P(C.c_size_t), c_vp]),
+    "oppb_dh_bounding_box_2d": (C.c_int, [c_vp, c_i32, c_vp, c_vp, c_vp]),
+    "oppb_dh_grid_init_2d": (C.c_int, [c_vp, c_i32, C.c_double, c_vp, P(DhGrid)]),
+    "oppb_dh_build_quad": (C.c_int, [c_vp, c_i32, C.c_double, P(DhGrid), c_vp, C.c_size_t, P(C.c_size_t), c_vp]),
     "oppb_move_ex": (C.c_int, [P(TetMesh), P(Particles), P(MoveOptions), c_vp, c_vp, c_i32, c_vp, C.c_size_t,
                                c_vp]),
     "oppb_field_setup": (C.c_int, [P(FemPICMesh), P(FieldSystem)]),

@@ -8,7 +8,8 @@ Host-side set-up mirrors the reference app where the particle path needs it:
   particles   init_particles' construction: positions uniform inside every cell (cell order),
               normal velocities, move direction (1, 1); seeded numpy generator
   AdvecBatch  device buffers of many instances concatenated, the instance table, the step
-              launch and its CUDA-graph capture
+              launch and its CUDA-graph capture; the global move (opp_global_move with
+              opp_init_direct_hop_cg, advec_opp.cpp:97-103) as each instance's direct-hop grid
   shard_instances  the split of an ensemble over GPUs: instances are independent, so each
               rank advances its own subset in its own persistent launch, with no collective
               on the data path
@@ -126,6 +127,49 @@ class AdvecBatchDevice:
                                   _ptr(self.cells), cap, _ptr(self.pos), _ptr(self.vel), _ptr(self.mdir),
                                   _ptr(self.p2c), _ptr(self.counter))
         self.n_total = n_total
+        self.dh_grids: list = []  # per instance (L.DhGrid, map tensor), once enable_direct_hop ran
+        self._dh_table = None
+
+    def enable_direct_hop(self, grid_spacing, expansion=None) -> None:
+        """The app's global move: every instance gets the direct-hop grid of its mesh
+        (BoundingBox(c_pos_ll, 2, expansion), expansion (2 cell widths, 2 cell widths, 0) as in
+        advec_opp.cpp, the map built on the GPU) and its walks start from the grid's seed.
+        grid_spacing: one value for all instances, or one per instance."""
+        spacings = list(grid_spacing) if np.ndim(grid_spacing) else [grid_spacing] * len(self.meshes)
+        if len(spacings) != len(self.meshes):
+            raise ValueError("one grid spacing per instance")
+        dh = (L.AdvecDh * len(self.meshes))()
+        self.dh_grids = []
+        ws = None
+        for k, (m, spacing) in enumerate(zip(self.meshes, spacings)):
+            ex = (C.c_double * 3)(*(expansion if expansion is not None else (2 * m.cell_width, 2 * m.cell_width, 0.0)))
+            ll = np.ascontiguousarray(m.c_pos_ll, dtype=np.float64)
+            g = L.DhGrid()
+            L.check("oppb_dh_grid_init_2d", self.lib.oppb_dh_grid_init_2d(ll.ctypes.data, m.n_cells, spacing, ex,
+                                                                          C.byref(g)))
+            gmap = torch.empty(int(g.size), dtype=torch.int32, device=self.device)
+            g.map = gmap.data_ptr()
+            cells = self.cells.data_ptr() + 32 * self.cell_offsets[k]
+            need = C.c_size_t(0)
+            for _ in range(2):  # the first call may only size the workspace
+                rc = self.lib.oppb_dh_build_quad(cells, m.n_cells, m.cell_width, C.byref(g), _ptr(ws),
+                                                 0 if ws is None else ws.numel(), C.byref(need), None)
+                if rc != L.OPPB_ERR_WORKSPACE:
+                    break
+                ws = torch.empty(int(need.value), dtype=torch.uint8, device=self.device)
+            L.check("oppb_dh_build_quad", rc)
+            dh[k] = L.AdvecDh(g.map, (C.c_double * 2)(g.min[0], g.min[1]), g.inv_spacing,
+                              (L.c_i64 * 2)(g.dims[0], g.dims[1]))
+            self.dh_grids.append((g, gmap))
+        self._dh_table = torch.frombuffer(bytearray(bytes(dh)), dtype=torch.uint8).to(self.device)
+        self.batch.dh = self._dh_table.data_ptr()
+        torch.cuda.synchronize(self.device)
+
+    def disable_direct_hop(self) -> None:
+        """Walks start from p2c again."""
+        self.batch.dh = None
+        self._dh_table = None
+        self.dh_grids = []
 
     def set_instance(self, k: int, pos, vel, mdir, p2c) -> None:
         """Upload one instance's host AoS particles."""
@@ -201,6 +245,8 @@ class AdvecBatchDevice:
             pre = torch.tensor([0, (n + WORK_ITEM - 1) // WORK_ITEM], dtype=torch.int32, device=self.device)
             b = L.AdvecBatch(1, int(pre[1].item()), _ptr(inst), _ptr(pre), _ptr(self.cells), self.capacity,
                              _ptr(self.pos), _ptr(self.vel), _ptr(self.mdir), _ptr(self.p2c), _ptr(self.counter))
+            if self._dh_table is not None:
+                b.dh = self._dh_table.data_ptr() + k * C_.sizeof(L.AdvecDh)
             out.append((b, (inst, pre)))
         return out
 

@@ -18,6 +18,18 @@ def _lib() -> C.CDLL:
         lib.oracle_advec_steps.restype = C.c_int
         lib.oracle_advec_steps.argtypes = [i32, vp, vp, vp, vp, vp, vp, C.c_double, vp, C.c_double, i32, i32,
                                            C.POINTER(C.c_int64)]
+        lib.oracle_advec_steps_dh.restype = C.c_int
+        lib.oracle_advec_steps_dh.argtypes = [i32, vp, vp, vp, vp, vp, vp, C.c_double, vp, C.c_double, i32, i32,
+                                              vp, vp, C.c_double, vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        lib.oracle_advec_move_dh.restype = C.c_int
+        lib.oracle_advec_move_dh.argtypes = [i32, vp, vp, vp, vp, vp, vp, C.c_double, i32, vp, vp, C.c_double, vp,
+                                             C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        lib.oracle_advec_dh_grid_init.restype = C.c_int
+        lib.oracle_advec_dh_grid_init.argtypes = [i32, vp, C.c_double, vp, vp, vp]
+        lib.oracle_advec_dh_build.restype = None
+        lib.oracle_advec_dh_build.argtypes = [i32, vp, C.c_double, vp, vp, C.c_double, vp, vp]
+        lib.oracle_advec_dh_seed.restype = i32
+        lib.oracle_advec_dh_seed.argtypes = [i32, vp, vp, vp, C.c_double, vp, vp]
         lib._advec_bound = True
     return lib
 
@@ -40,6 +52,68 @@ def steps(pos, vel, mdir, p2c, c2c, c_pos_ll, dt, extents, cell_width, n_steps, 
     return int(visits.value)
 
 
+class DhGrid:
+    """The direct-hop grid of a 2-D advection mesh: box = {min x, y, z, max x, y, z} (z = 0),
+    dims (X, Y, 1), spacing, and the map (x fastest), as the oracle builds it."""
+
+    def __init__(self, box, dims, spacing, map_):
+        self.box, self.dims, self.spacing, self.map = box, dims, spacing, map_
+        self.inv = 1.0 / spacing
+
+
+def dh_grid(c_pos_ll, spacing: float, expansion) -> tuple[np.ndarray, np.ndarray]:
+    """BoundingBox(c_pos_ll, 2, expansion) and the CellMapper's box counts: (box[6], dims[3])."""
+    ll = np.ascontiguousarray(c_pos_ll, dtype=np.float64)
+    ex = np.ascontiguousarray(expansion, dtype=np.float64)
+    box, dims = np.zeros(6), np.zeros(3, np.int64)
+    if _lib().oracle_advec_dh_grid_init(len(ll), _p(ll), spacing, _p(ex), _p(box), _p(dims)) != 0:
+        raise ValueError("grid too large")
+    return box, dims
+
+
+def dh_build(c_pos_ll, cell_width: float, extents, spacing: float, expansion) -> DhGrid:
+    """The reference's structured map of the mesh, by its own search over all cells per query."""
+    ll = np.ascontiguousarray(c_pos_ll, dtype=np.float64)
+    box, dims = dh_grid(ll, spacing, expansion)
+    ext = np.ascontiguousarray(extents, dtype=np.float64)
+    m = np.zeros(int(dims[0] * dims[1]), np.int32)
+    _lib().oracle_advec_dh_build(len(ll), _p(ll), cell_width, _p(ext), _p(box), spacing, _p(dims), _p(m))
+    return DhGrid(box, dims, spacing, m)
+
+
+def dh_seed(pos, p2c, g: DhGrid) -> int:
+    """The global-move pre-pass in place (pos [n,2], p2c [n]); returns the particles removed."""
+    return int(_lib().oracle_advec_dh_seed(len(p2c), _p(pos), _p(p2c), _p(g.box), g.inv, _p(g.dims), _p(g.map)))
+
+
+def steps_dh(pos, vel, mdir, p2c, c2c, c_pos_ll, dt, extents, cell_width, n_steps, g: DhGrid,
+             max_hops=1 << 20) -> tuple[int, int]:
+    """steps() with every move starting from the direct-hop seed; returns (move calls of the
+    last step, particles removed by the pre-pass)."""
+    ext = np.ascontiguousarray(extents, dtype=np.float64)
+    visits, removed = C.c_int64(0), C.c_int64(0)
+    rc = _lib().oracle_advec_steps_dh(len(p2c), _p(pos), _p(vel), _p(mdir), _p(p2c), _p(c2c), _p(c_pos_ll), dt,
+                                      _p(ext), cell_width, n_steps, max_hops, _p(g.map), _p(g.box), g.inv,
+                                      _p(g.dims), C.byref(visits), C.byref(removed))
+    if rc != 0:
+        raise RuntimeError("oracle: a particle exceeded max_hops")
+    return int(visits.value), int(removed.value)
+
+
+def move(pos, mdir, p2c, c2c, c_pos_ll, extents, cell_width, g: DhGrid | None = None,
+         max_hops=1 << 20) -> tuple[int, int]:
+    """The move loop alone, in place (mdir, p2c), from the direct-hop seed when g is given;
+    returns (move calls, particles removed by the pre-pass)."""
+    ext = np.ascontiguousarray(extents, dtype=np.float64)
+    visits, removed = C.c_int64(0), C.c_int64(0)
+    args = (None, None, 0.0, None) if g is None else (_p(g.map), _p(g.box), g.inv, _p(g.dims))
+    rc = _lib().oracle_advec_move_dh(len(p2c), _p(pos), _p(mdir), _p(p2c), _p(c2c), _p(c_pos_ll), _p(ext),
+                                     cell_width, max_hops, *args, C.byref(visits), C.byref(removed))
+    if rc != 0:
+        raise RuntimeError("oracle: a particle exceeded max_hops")
+    return int(visits.value), int(removed.value)
+
+
 def steps_job(args) -> tuple:
     """One instance's n_steps in a worker process (args: pos, vel, mdir, p2c, c2c, c_pos_ll, dt,
     extents, cell_width, n_steps); returns (pos, mdir, p2c, move calls of the last step)."""
@@ -50,9 +124,11 @@ def steps_job(args) -> tuple:
 
 
 def run_reference(kind: str, nx, ny, cell_width, dt, pos, vel, mdir, p2c, c2c, c_pos_ll, n_steps,
-                  threads: int | None = None) -> dict:
+                  threads: int | None = None, dh_spacing: float | None = None) -> dict:
     """Run oracle/_ref/advec_ref_{seq,omp}: n_steps of update_pos + move.  Returns per-step wall
-    times and the final pos, mdir, p2c."""
+    times and the final pos, mdir, p2c; with dh_spacing, the global move is on (the app's
+    opp_init_direct_hop_cg with that grid spacing and an expansion of two cell widths in x and
+    y) and the result also holds the reference's grid: dims, box and map."""
     import os
     import subprocess
     import tempfile
@@ -65,17 +141,19 @@ def run_reference(kind: str, nx, ny, cell_width, dt, pos, vel, mdir, p2c, c2c, c
         raise FileNotFoundError(exe)
     n = len(p2c)
     hdr = np.zeros(1, dtype=[("magic", "S8"), ("ints", "<i4", 4), ("dbl", "<f8", 2)])
-    hdr["magic"] = b"OPPBADV1"
+    hdr["magic"] = b"OPPBADV1" if dh_spacing is None else b"OPPBADV2"
     hdr["ints"] = [nx, ny, n, n_steps]
     hdr["dbl"] = [dt, cell_width]
     with tempfile.TemporaryDirectory() as d:
         d = Path(d)
         with open(d / "case.bin", "wb") as f:
             f.write(hdr.tobytes())
+            if dh_spacing is not None:
+                f.write(np.array([1, 0], "<i4").tobytes() + np.array([dh_spacing], "<f8").tobytes())
             for a, t in ((c2c, "<i4"), (c_pos_ll, "<f8"), (pos, "<f8"), (vel, "<f8"), (mdir, "<i4"),
                          (p2c, "<i4")):
                 f.write(np.ascontiguousarray(a, dtype=t).tobytes())
-        (d / "params.txt").write_text(params_text("HoleFill_All", 10, 2.0))
+        (d / "params.txt").write_text(params_text("HoleFill_All", 10, 2.0, global_move=dh_spacing is not None))
         env = dict(os.environ)
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
@@ -95,5 +173,10 @@ def run_reference(kind: str, nx, ny, cell_width, dt, pos, vel, mdir, p2c, c2c, c
     ns = int(take("<i4", 1)[0])
     times = take("<f8", ns)
     size = int(take("<i4", 1)[0])
-    return {"times": times, "pos": take("<f8", size * 2).reshape(size, 2), "mdir": take("<i4", size * 2).reshape(size, 2),
-            "p2c": take("<i4", size)}
+    out = {"times": times, "pos": take("<f8", size * 2).reshape(size, 2),
+           "mdir": take("<i4", size * 2).reshape(size, 2), "p2c": take("<i4", size)}
+    if dh_spacing is not None:
+        dims = take("<i8", 3)
+        out["dims"], out["box"] = dims, take("<f8", 6)
+        out["map"] = take("<i4", int(dims.prod()))
+    return out

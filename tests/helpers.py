@@ -34,3 +34,21 @@ def random_particles(hm: HostMesh, n: int, seed: int, spread: float = 0.05, far_
     on = rng.random(n) < 0.01
     pos[on] = hm.n_pos[hm.c2n[cells[on], 0]]
     return np.ascontiguousarray(pos), cells
+
+
+def advec_edge_particles(m, ppc: int, v_sd: float, seed: int):
+    """NESO-advection particles (oppb.advec.particles) with a quarter resting on their cell's
+    lower x edge and a quarter on its lower y edge: points two cells share, where the walk's
+    start cell (the direct-hop seed or the previous cell) decides the final one.  Returns AoS
+    pos, vel, mdir, p2c."""
+    from oppb.advec import particles
+
+    pos, vel, mdir, p2c = particles(m, ppc, v_sd, seed)
+    rng = np.random.default_rng(seed + 1)
+    ia = rng.choice(len(p2c), len(p2c) // 4, replace=False)
+    ib = rng.choice(len(p2c), len(p2c) // 4, replace=False)
+    pos[ia, 0] = m.c_pos_ll[p2c[ia], 0]
+    pos[ib, 1] = m.c_pos_ll[p2c[ib], 1]
+    vel[ia] = 0.0
+    vel[ib] = 0.0
+    return pos, vel, mdir, p2c

@@ -198,3 +198,147 @@ def test_ensemble_of_64_over_500_steps_under_graph_matches_oracle():
     pool.join()
     assert sum(len(h[3]) for h in host) > 5_000_000
     _assert_same(dev, [{"pos": r[0], "mdir": r[1], "p2c": r[2]} for r in ref])
+
+
+# ------------------------------------------------------------------ direct hop (global move)
+
+GOLDEN_DH = Path(__file__).resolve().parent / "golden" / "advec_dh_9x8.npz"
+# (nx, ny, cell_width, grid spacing): spacings that align with the cells, straddle their
+# edges, or are coarser than a cell
+DH_MESHES = [(9, 8, 1.0, 0.7), (13, 9, 0.5, 0.5), (7, 11, 1.0, 0.3), (10, 6, 0.25, 0.4), (5, 19, 0.8, 1.9),
+             (64, 48, 1.0, 0.45)]
+
+
+def test_dh_maps_match_oracle():
+    """oppb_dh_build_quad (the cells binned into the grid boxes, one query thread per box)
+    gives the oracle's map (the reference's search over all cells per query), and the grid's
+    counts and bounds are the oracle's, for every instance of a batch."""
+    meshes = [AdvecMesh(nx, ny, cw) for nx, ny, cw, _ in DH_MESHES]
+    for m, (_, _, cw, gs) in zip(meshes, DH_MESHES):
+        dev = AdvecBatchDevice([m], [1], [0.5], DEV)
+        dev.enable_direct_hop(gs)
+        g, gmap = dev.dh_grids[0]
+        ref = OA.dh_build(m.c_pos_ll, cw, m.extents, gs, (2 * cw, 2 * cw, 0.0))
+        assert list(g.dims) == list(ref.dims)
+        np.testing.assert_array_equal(np.array(list(g.min) + list(g.max)).view(np.uint64), ref.box.view(np.uint64))
+        np.testing.assert_array_equal(gmap.cpu().numpy(), ref.map, err_msg=str((m.nx, m.ny, cw, gs)))
+
+
+def test_dh_matches_reference_golden():
+    """The global move on, as the reference ran it (golden fixture): map, then 7 steps with
+    particles on cell edges that the seed moves to the neighbouring cell."""
+    z = np.load(GOLDEN_DH)
+    cw = float(z["cell_width"])
+    m = AdvecMesh(int(z["nx"]), int(z["ny"]), cw)
+    dev = AdvecBatchDevice([m], [len(z["p2c"])], [float(z["dt"])], DEV)
+    dev.set_instance(0, z["pos"], z["vel"], z["mdir"], z["p2c"])
+    dev.enable_direct_hop(float(z["grid_spacing"]))
+    np.testing.assert_array_equal(dev.dh_grids[0][1].cpu().numpy(), z["ref_map"])
+    dev.zero_status()
+    for _ in range(int(z["steps"])):
+        dev.step()
+    torch.cuda.synchronize()
+    got = dev.host_instance(0)
+    np.testing.assert_array_equal(got["pos"].view(np.uint64), z["ref_pos"].view(np.uint64))
+    np.testing.assert_array_equal(got["mdir"], z["ref_mdir"])
+    np.testing.assert_array_equal(got["p2c"], z["ref_p2c"])
+    assert dev.status_host().remove_count == 0
+
+
+def test_dh_batch_steps_match_oracle_and_graph():
+    """A batch of the meshes above with edge particles: 12 steps with the seed, as launches and
+    as replays of a 4-step CUDA graph, against the oracle per instance (positions, directions,
+    cells, move calls)."""
+    from helpers import advec_edge_particles
+
+    meshes = [AdvecMesh(nx, ny, cw) for nx, ny, cw, _ in DH_MESHES]
+    host = [advec_edge_particles(m, 9, 0.7, 300 + k) for k, m in enumerate(meshes)]
+    dts = [0.45] * len(meshes)
+    devs = []
+    for _ in range(2):
+        d = AdvecBatchDevice(meshes, [len(h[3]) for h in host], dts, DEV)
+        for k, h in enumerate(host):
+            d.set_instance(k, *h)
+        devs.append(d)
+    for d in devs:  # every instance with its own spacing
+        d.enable_direct_hop([gs for _, _, _, gs in DH_MESHES])
+    steps = 12
+    a, b = devs
+    a.zero_status()
+    b.zero_status()
+    for _ in range(steps):
+        a.step()
+    b.step()
+    g = b.capture(4)
+    for _ in range((steps - 1) // 4):
+        g.replay()
+    for _ in range((steps - 1) % 4):
+        b.step()
+    torch.cuda.synchronize()
+    ref, visits = [], 0
+    for m, h, (_, _, cw, gs), dt in zip(meshes, host, DH_MESHES, dts):
+        pos, vel, mdir, p2c = (x.copy() for x in h)
+        grid = OA.dh_build(m.c_pos_ll, cw, m.extents, gs, (2 * cw, 2 * cw, 0.0))
+        for _ in range(steps):
+            v, r = OA.steps_dh(pos, vel, mdir, p2c, m.c2c, m.c_pos_ll, dt, m.extents, cw, 1, grid)
+            visits += v
+            assert r == 0
+        ref.append({"pos": pos, "mdir": mdir, "p2c": p2c})
+    sa, sb = a.status_host(), b.status_host()
+    assert sa.error == 0 and int(sa.total_visits) == visits and sa.remove_count == 0
+    assert int(sb.total_visits) == visits
+    _assert_same(a, ref)
+    _assert_same(b, ref)
+
+
+def test_dh_move_only_removes_outside_the_grid():
+    """oppb_advec_move with the seed: positions past the grid on either axis, or in a box
+    without a cell, are removed (p2c = REMOVED, counted), particles already removed are
+    skipped, the others walk from the seed as the oracle's move loop does."""
+    m = AdvecMesh(12, 10, 1.0)
+    pos, vel, mdir, p2c = particles(m, 6, 0.0, 8)
+    n = len(p2c)
+    rng = np.random.default_rng(3)
+    pos += rng.normal(0.0, 1.5, pos.shape)  # away from their cells (multi-hop walks)
+    pos[:, 0] = np.clip(pos[:, 0], 0.0, 11.999)
+    pos[:, 1] = np.clip(pos[:, 1], 0.0, 9.999)
+    pos[0] = (1e9, 3.0)    # past the grid in x
+    pos[1] = (3.0, 1e9)    # past the grid in y
+    pos[2] = (-1.7, 3.0)   # inside the grid, in a box left of the mesh: no cell
+    pos[3] = (-1e9, -1e9)  # truncates to box (0, 0): no cell
+    p2c[4] = 2147483647    # already removed: skipped
+    dev = AdvecBatchDevice([m], [n], [0.5], DEV)
+    dev.set_instance(0, pos, vel, mdir, p2c)
+    dev.enable_direct_hop(0.6)
+    dev.zero_status()
+    dev.move()
+    torch.cuda.synchronize()
+    st = dev.status_host()
+    g = OA.dh_build(m.c_pos_ll, 1.0, m.extents, 0.6, (2.0, 2.0, 0.0))
+    P, M, C2 = pos.copy(), mdir.copy(), p2c.copy()
+    visits, removed = OA.move(P, M, C2, m.c2c, m.c_pos_ll, m.extents, 1.0, g)
+    got = dev.host_instance(0)
+    assert st.error == 0 and st.remove_count == removed == 4
+    assert int(st.total_visits) == visits
+    np.testing.assert_array_equal(got["p2c"], C2)
+    np.testing.assert_array_equal(got["mdir"], M)
+    assert list(np.flatnonzero(C2 == 2147483647)) == [0, 1, 2, 3, 4]
+
+
+def test_dh_disabled_walks_from_p2c_again():
+    m = AdvecMesh(9, 8, 1.0)
+    from helpers import advec_edge_particles
+
+    pos, vel, mdir, p2c = advec_edge_particles(m, 10, 0.5, 11)
+    dev = AdvecBatchDevice([m], [len(p2c)], [0.5], DEV)
+    dev.set_instance(0, pos, vel, mdir, p2c)
+    dev.enable_direct_hop(0.7)
+    dev.disable_direct_hop()
+    for _ in range(3):
+        dev.step()
+    torch.cuda.synchronize()
+    P, M, C2 = pos.copy(), mdir.copy(), p2c.copy()
+    OA.steps(P, vel, M, C2, m.c2c, m.c_pos_ll, 0.5, m.extents, 1.0, 3)
+    got = dev.host_instance(0)
+    np.testing.assert_array_equal(got["p2c"], C2)
+    np.testing.assert_array_equal(got["pos"].view(np.uint64), P.view(np.uint64))
