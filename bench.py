@@ -357,25 +357,40 @@ def run_precision(hm, dev, precision: str, steps: int, warmup: int, seed: int, s
     if e2e_steps:
         # End to end through the public API (FemPIC.run_steps): every step's injection table
         # goes up from pinned host memory and its node charges (plus the move status) come
-        # back; the copies run on a second stream and overlap the neighbouring steps.
+        # back; the copies run on a second stream and overlap the neighbouring steps.  The
+        # same steps through FemPIC.run_graph_host (graph replays of one sort cycle, the count
+        # read back once a replay) are reported beside it.
         host_tables = [torch.from_numpy(np.ascontiguousarray(injection_randoms(seed + 7, k, CFG["inject"],
                                                                                 CFG["sigma"]).T)).pin_memory()
                        for k in range(e2e_steps)]
         charges_out = [torch.empty(hm.n_nodes, dtype=torch.float64).pin_memory() for _ in range(e2e_steps)]
+
+        def timed(call) -> tuple[float, list]:
+            torch.cuda.synchronize()
+            e0, e1 = E(), E()
+            e0.record(s)
+            recs = call(host_tables, charges_out)
+            e1.record(s)
+            e1.synchronize()
+            return e0.elapsed_time(e1), recs
+
         for _ in range(max(1, warmup)):  # untimed warm-up calls of the same API, 3 steps each
             sim.run_steps(host_tables[:3], charges_out[:3])
-        torch.cuda.synchronize()
-        e0, e1 = E(), E()
-        e0.record(s)
-        recs = sim.run_steps(host_tables, charges_out)
-        e1.record(s)
-        e1.synchronize()
-        t_e2e = e0.elapsed_time(e1)
+        t_e2e, recs = timed(sim.run_steps)
+        # The graph path's warm-up captures its graphs for both buffer parities of a sort cycle.
+        per = CFG["period"]
+        k = 2 * per if e2e_steps >= 2 * per else e2e_steps
+        sim.run_graph_host(host_tables[:k], charges_out[:k])
+        t_graph, recs_graph = timed(sim.run_graph_host)
         n_e2e = sum(r["size_before_move"] for r in recs)
+        n_graph = sum(r["size_before_move"] for r in recs_graph)
         out["e2e"] = {"value": n_e2e / (t_e2e / 1e3), "unit": UNIT,
                       "h2d_bytes_per_step": int(host_tables[0].numel() * 8),
                       "d2h_bytes_per_step": int(charges_out[0].numel() * 8 + 32), "steps": e2e_steps,
-                      "what": "whole step (inject, push + move + deposit, compaction) through FemPIC.run_steps"}
+                      "what": "whole step (inject, push + move + deposit, compaction) through FemPIC.run_steps",
+                      "graph_replays": {"value": n_graph / (t_graph / 1e3), "unit": UNIT,
+                                        "what": "the same steps through FemPIC.run_graph_host: replays of one sort "
+                                                "cycle, the count and step records read back once a replay"}}
 
     if cpu_sample:
         # One more step up to the push, then a contiguous slice of the particles as the
@@ -1172,7 +1187,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["oppb", "reference"], default="oppb")
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--fill-steps", type=int, default=CFG["fill_steps"], help="steps to reach the steady state")

@@ -31,6 +31,7 @@ LANE_CANDIDATES = [(1, 8, 0), (1, 8, 1), (2, 8, 0), (2, 5, 0)]  # (move_lanes, m
 BLOCK_CANDIDATES = [256, 128, 512]  # threads per CTA of the one-lane move kernels
 SORT_CANDIDATES = [(16, 0), (10, 0), (5, 0), (16, 1), (10, 1)]  # (columns per launch, scatter form)
 PERIOD_CANDIDATES = [5, 10, 20]
+MARGIN = 0.01  # a move-launch candidate replaces the default only when more than 1 % faster
 
 
 @dataclass
@@ -42,15 +43,20 @@ class TuneResult:
         return {"choice": str(self.choice), "ms": {str(k): v for k, v in self.times_ms.items()}}
 
 
-def pick(candidates, run: Callable[[object], float], reps: int = 3) -> TuneResult:
+def pick(candidates, run: Callable[[object], float], reps: int = 3, margin: float = 0.0) -> TuneResult:
     """Times run(candidate) reps times per candidate (each call returns milliseconds) and returns
-    the candidate with the smallest median; ties go to the earlier candidate."""
+    the candidate with the smallest median; ties go to the earlier candidate.  With margin > 0
+    the first candidate (the default) is kept unless the fastest beats it by more than that
+    fraction, so that trial noise does not flip the choice."""
     if not candidates:
         raise ValueError("no candidates")
     res = TuneResult(choice=None)
     for c in candidates:
         res.times_ms[c] = statistics.median(run(c) for _ in range(reps))
     res.choice = min(candidates, key=lambda c: (res.times_ms[c], candidates.index(c)))
+    first = candidates[0]
+    if res.times_ms[res.choice] > res.times_ms[first] * (1.0 - margin):
+        res.choice = first
     return res
 
 
@@ -114,7 +120,7 @@ def _tune_walk(sim, cands, apply, current, reps: int, with_push: bool | None) ->
         return _timed(sim.move)
 
     try:
-        res = pick(cands, run, reps)
+        res = pick(cands, run, reps, margin=MARGIN)
     except Exception:
         L.load().oppb_set_tuning(C.byref(before))
         raise

@@ -314,6 +314,7 @@ class FemPIC:
         self.count_dev = torch.zeros(4, dtype=torch.int32, device=self.device)  # oppb_set_count
         self._count_synced = False
         self._graphs = {}
+        self._gio = {}  # run_graph_host's staging buffers and events
 
     # workspace shared by hole fill and sort (grown on demand)
     def _workspace(self, nbytes: int) -> torch.Tensor:
@@ -597,9 +598,10 @@ class FemPIC:
         return self.iter % self.fill_period if self.fill.endswith("Periodic") else 0
 
     def _step_dev(self, table: torch.Tensor, bound: int, records: torch.Tensor, n_records: int, stream=None,
-                  count=None, field: bool = True) -> None:
+                  count=None, field: bool = True, charge_out: torch.Tensor | None = None) -> None:
         """One step on the device count (no host read): the launches of step() with the fused
-        push, sized from `bound`.  count: the oppb_set_count tensor (default self.count_dev)."""
+        push, sized from `bound`.  count: the oppb_set_count tensor (default self.count_dev);
+        charge_out: a device buffer that receives the step's node charges (a copy)."""
         p, m, lib = self.parts, self.mesh, self.lib
         cnt = _ptr(self.count_dev if count is None else count)
         st = _ptr(p.status)
@@ -633,6 +635,8 @@ class FemPIC:
             L.check("oppb_hole_fill_dev", lib.oppb_hole_fill_dev(
                 bound, cnt, n_inj, st, _ptr(p.bits), p.capacity, len(p.DATS), dats, _ptr(cws), cws.numel(), sp))
         L.check("oppb_step_end_dev", lib.oppb_step_end_dev(cnt, n_inj, st, _ptr(records), n_records, sp))
+        if charge_out is not None:
+            charge_out.copy_(self.node_charge)
         if field and self.field is not None and self.field_enabled:
             self.field.launch(self.node_charge, self.n_vol, self.spwt, self.field_consts, self.mesh.ef, 4)
         self.iter += 1
@@ -643,10 +647,12 @@ class FemPIC:
             self.count_dev.copy_(torch.tensor([self.parts.size, 0, 0, 0], dtype=torch.int32))
             self._count_synced = True
 
-    def capture_steps(self, steps: int, n_inject: int | None = None, slack: float = 0.02) -> StepGraph:
+    def capture_steps(self, steps: int, n_inject: int | None = None, slack: float = 0.02,
+                      keep_charges: bool = False) -> StepGraph:
         """Captures `steps` whole steps, from the current iteration and particle buffers, as one
         CUDA graph.  The capacity grows first when the count could exceed it (every particle
-        injected, none removed, plus `slack`)."""
+        injected, none removed, plus `slack`).  keep_charges: every step also copies its node
+        charges into the graph's `charges[k]`."""
         if not self.fused_push:
             raise ValueError("graph-captured steps need the fused push (fused_push=True)")
         if self.dh is not None:
@@ -664,6 +670,8 @@ class FemPIC:
         self._deposit_ws()
         tables = [torch.zeros((5, n_inj), dtype=torch.float64, device=self.device) for _ in range(steps)]
         records = torch.zeros((steps, 8), dtype=torch.int32, device=self.device)
+        charges = torch.zeros((steps, self.node_charge.numel()), dtype=torch.float64, device=self.device) \
+            if keep_charges else None
         # Warm-up: one launch of every kernel the capture uses (the first launch of a kernel
         # loads it), on a scratch count of -n_inj: the injection starts below 0 and writes
         # nothing, and every later launch sees zero particles.
@@ -688,30 +696,34 @@ class FemPIC:
         with torch.cuda.stream(s):
             with torch.cuda.graph(g, stream=s):
                 for k in range(steps):
-                    self._step_dev(tables[k], bound, records, steps)
+                    self._step_dev(tables[k], bound, records, steps, charge_out=None if charges is None else charges[k])
         torch.cuda.current_stream(self.device).wait_stream(s)
         launches = int(self.lib.oppb_kernel_launches() - launches0)
         bufs_after = self._bufs()
         self._set_bufs(saved[0])
         self.iter, p.size = saved[1], saved[2]
-        return StepGraph(g, steps, bound, tables, records, saved[0], bufs_after, p.capacity, launches)
+        return StepGraph(g, steps, bound, tables, records, saved[0], bufs_after, p.capacity, launches, charges,
+                         self.node_charge.data_ptr())
 
-    def graph_for(self, steps: int, n_inject: int | None = None) -> StepGraph:
+    def _graph_key(self, steps: int, n_inj: int, keep_charges: bool) -> tuple:
+        return (steps, n_inj, self._graph_phase(), StepGraph.ptrs(self._bufs()), self.parts.capacity,
+                self.node_charge.data_ptr(), keep_charges)
+
+    def graph_for(self, steps: int, n_inject: int | None = None, keep_charges: bool = False) -> StepGraph:
         """The captured graph for the next `steps` steps from here (captured when none fits)."""
         n_inj = self.inject_per_step if n_inject is None else int(n_inject)
-        key = (steps, n_inj, self._graph_phase(), StepGraph.ptrs(self._bufs()), self.parts.capacity)
-        g = self._graphs.get(key)
+        g = self._graphs.get(self._graph_key(steps, n_inj, keep_charges))
         if g is None or self.parts.size + steps * n_inj > g.bound:
-            g = self.capture_steps(steps, n_inj)
-            key = (steps, n_inj, self._graph_phase(), StepGraph.ptrs(self._bufs()), self.parts.capacity)
-            self._graphs[key] = g
+            g = self.capture_steps(steps, n_inj, keep_charges=keep_charges)
+            self._graphs[self._graph_key(steps, n_inj, keep_charges)] = g
         return g
 
     def replay(self, g: StepGraph, stream=None) -> list[dict]:
         """Runs the steps of g (its tables as they are), then reads the count and the step records
         back once.  Raises on a device error of any of the steps."""
-        if StepGraph.ptrs(g.bufs_before) != StepGraph.ptrs(self._bufs()) or g.capacity != self.parts.capacity:
-            raise ValueError("the graph was captured for other particle buffers")
+        if StepGraph.ptrs(g.bufs_before) != StepGraph.ptrs(self._bufs()) or g.capacity != self.parts.capacity or \
+                g.node_charge_ptr != self.node_charge.data_ptr():
+            raise ValueError("the graph was captured for other particle or node-charge buffers")
         self._sync_count()
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         with torch.cuda.stream(s):
@@ -749,6 +761,87 @@ class FemPIC:
                 dst.copy_(src)
         return self.replay(g)
 
+    def run_graph_host(self, host_tables: list[torch.Tensor], charges_out: list[torch.Tensor] | None = None,
+                       steps_per_graph: int | None = None) -> list[dict]:
+        """run_steps' contract (host tables in, every step's node charges out) on graph-captured
+        steps: the steps go in chunks of steps_per_graph (default: the fill period of a
+        periodic fill, else 10), each one replay of a captured graph that also copies every
+        step's node charges aside; the count and the step records come back once per chunk.
+        host_tables: pinned CPU float64 [5][count] tables, one count for all steps;
+        charges_out: pinned CPU float64 [n_nodes] tensors, one per step (or None).  A second
+        stream moves the next chunk's tables up and the last chunk's charges down while a
+        chunk runs.  Returns the per-step records; every copy has completed on return, and
+        node_charge holds the last step's charges."""
+        n = len(host_tables)
+        if n == 0:
+            return []
+        if charges_out is not None and len(charges_out) != n:
+            raise ValueError("charges_out needs one tensor per step")
+        rows, n_inj = host_tables[0].shape
+        if any(t.shape != host_tables[0].shape for t in host_tables):
+            raise ValueError("graph-captured steps inject the same count every step")
+        S = steps_per_graph or (self.fill_period if self.fill.endswith("Periodic") else 10)
+        chunks = [list(range(c, min(c + S, n))) for c in range(0, n, S)]
+        cur = torch.cuda.current_stream(self.device)
+        p = self._pipeline(rows, n_inj)
+        copy = p["copy"]
+        io = self._graph_io(S, rows, n_inj)
+        t_ready, t_free, c_ready, c_free = io["table_ready"], io["table_free"], io["charge_ready"], io["charge_free"]
+        for e in t_free + c_free:
+            e.record(cur)
+
+        def upload(c: int) -> None:  # chunk c's tables into staging set c % 2, on the copy stream
+            b = c % 2
+            with torch.cuda.stream(copy):
+                copy.wait_event(t_free[b])
+                for k, j in enumerate(chunks[c]):
+                    io["tables"][b][k].copy_(host_tables[j], non_blocking=True)
+                t_ready[b].record(copy)
+
+        upload(0)
+        out = []
+        for c, idx in enumerate(chunks):
+            b = c % 2
+            g = self.graph_for(len(idx), n_inj, keep_charges=True)
+            if c + 1 < len(chunks):
+                upload(c + 1)
+            cur.wait_event(t_ready[b])
+            for k in range(len(idx)):
+                g.tables[k].copy_(io["tables"][b][k])
+            t_free[b].record(cur)
+            self._sync_count()
+            g.graph.replay()
+            cur.wait_event(c_free[b])  # the previous download from this staging set is done
+            io["charges"][b][:len(idx)].copy_(g.charges)
+            c_ready[b].record(cur)
+            if charges_out is not None:
+                with torch.cuda.stream(copy):
+                    copy.wait_event(c_ready[b])
+                    for k, j in enumerate(idx):
+                        charges_out[j].copy_(io["charges"][b][k], non_blocking=True)
+                    c_free[b].record(copy)
+            else:
+                c_free[b].record(cur)
+            out.extend(self.replay_finish(g))
+        copy.synchronize()
+        cur.wait_stream(copy)
+        return out
+
+    def _graph_io(self, steps: int, rows: int, cols: int) -> dict:
+        """run_graph_host's device staging (two sets of `steps` injection tables and of `steps`
+        node-charge buffers) and its events, made once per shape."""
+        key = (steps, rows, cols)
+        io = self._gio.get(key)
+        if io is None:
+            ev = lambda: torch.cuda.Event()  # noqa: E731
+            nn = self.node_charge.numel()
+            io = self._gio[key] = {
+                "tables": [torch.empty((steps, rows, cols), dtype=torch.float64, device=self.device) for _ in range(2)],
+                "charges": [torch.empty((steps, nn), dtype=torch.float64, device=self.device) for _ in range(2)],
+                "table_ready": [ev(), ev()], "table_free": [ev(), ev()],
+                "charge_ready": [ev(), ev()], "charge_free": [ev(), ev()]}
+        return io
+
 
 class StepGraph:
     """Whole FemPIC steps captured as one CUDA graph (include/oppb_graph.h): per step the node
@@ -760,11 +853,13 @@ class StepGraph:
     period) is the same."""
 
     def __init__(self, graph, steps: int, bound: int, tables, records, bufs_before, bufs_after, capacity: int,
-                 launches: int):
+                 launches: int, charges=None, node_charge_ptr: int = 0):
         self.graph, self.steps, self.bound = graph, steps, bound
         self.tables, self.records = tables, records
         self.bufs_before, self.bufs_after, self.capacity = bufs_before, bufs_after, capacity
         self.launches = launches  # library kernels per replay
+        self.charges = charges  # [steps][n_nodes] per-step node charges (keep_charges), else None
+        self.node_charge_ptr = node_charge_ptr
 
     @staticmethod
     def ptrs(bufs) -> tuple:

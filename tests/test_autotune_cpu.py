@@ -23,6 +23,14 @@ def test_pick_smallest_median():
     assert res.report()["choice"] == "b"
 
 
+def test_pick_margin_keeps_the_default_within_noise():
+    times = {"d": 2.000, "a": 1.995, "b": 2.5}
+    assert pick(["d", "a", "b"], lambda c: times[c], reps=1, margin=0.01).choice == "d"
+    assert pick(["d", "a", "b"], lambda c: times[c], reps=1).choice == "a"
+    times["a"] = 1.9
+    assert pick(["d", "a", "b"], lambda c: times[c], reps=1, margin=0.01).choice == "a"
+
+
 def test_pick_ties_and_errors():
     assert pick([(1, 8), (0, 4)], lambda c: 1.0, reps=1).choice == (1, 8)
     with pytest.raises(ValueError):

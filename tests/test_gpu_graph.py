@@ -213,3 +213,43 @@ def test_shuffle_removed_last_and_permutation():
         assert np.any(np.diff(pm[:live]) < 0)  # not the identity: shuffled
         perms.append(pm)
     np.testing.assert_array_equal(perms[0], perms[1])
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_run_graph_host_equals_run_steps(precision):
+    """FemPIC.run_graph_host (graph replays of 10 steps, staging copies on a second stream, every
+    step's node charges copied aside inside the graph) against FemPIC.run_steps on the same
+    pinned host tables: 25 steps (chunks of 10, 10 and 5), the same per-step counts and visits,
+    the same particle dats bit for bit, every step's node charges within 1e-12; then a second
+    call that replays the graphs it captured."""
+    hm = mesh()
+    kw = dict(inject_per_step=INJECT, precision=precision, fill="Sort_Periodic", fill_period=10)
+    a, b = FemPIC(hm, DEV, **kw), FemPIC(hm, DEV, **kw)
+    n = 25
+    host = [torch.from_numpy(np.ascontiguousarray(injection_randoms(6, k, INJECT, 0.1).T)).pin_memory()
+            for k in range(2 * n)]
+    ca = [torch.empty(hm.n_nodes, dtype=torch.float64).pin_memory() for _ in range(2 * n)]
+    cb = [torch.empty(hm.n_nodes, dtype=torch.float64).pin_memory() for _ in range(2 * n)]
+    key = ("size_before_move", "removed", "size", "visits", "max_visits", "rechecks")
+    for half in range(2):
+        sl = slice(half * n, (half + 1) * n)
+        ra = a.run_steps(host[sl], ca[sl])
+        graphs_before = len(b._graphs)
+        rb = b.run_graph_host(host[sl], cb[sl])
+        assert [tuple(x[k] for k in key) for x in ra] == [tuple(x[k] for k in key) for x in rb], half
+        for k in range(sl.start, sl.stop):
+            _charge_close(cb[k].numpy(), ca[k].numpy())
+        _charge_close(b.node_charge.cpu().numpy(), ca[sl.stop - 1].numpy())
+        _same_dats(a, b)
+        assert a.iter == b.iter and a.parts.size == b.parts.size
+    assert len(b._graphs) >= graphs_before  # the second call reuses or adds graphs, never fewer
+    assert b.parts.size > 40_000
+
+
+def test_run_graph_host_rejects_mixed_counts():
+    hm = mesh()
+    sim = FemPIC(hm, DEV, inject_per_step=INJECT)
+    t = [torch.zeros((5, INJECT), dtype=torch.float64).pin_memory(),
+         torch.zeros((5, INJECT + 1), dtype=torch.float64).pin_memory()]
+    with pytest.raises(ValueError):
+        sim.run_graph_host(t)
