@@ -153,6 +153,9 @@ typedef struct oppb_tuning {
                                deposit: 128, 256 (0 reads as 256) or 512, with 2048 / move_block CTAs
                                resident per SM (32 registers a thread); the other deposits, the lane-pair
                                and the staged kernels use 256.  The same results */
+    int32_t cabana_occupancy; /* CabanaPIC move + deposit: resident CTAs per SM it is compiled for:
+                                 0 = the compiler's register count, 4 (default; 64 registers a
+                                 thread) or 5 (48 registers, small spills).  The same results */
 } oppb_tuning;
 
 /* Set / read the tuning used by subsequent launches (OPPB_ERR_ARG on unknown values). */

@@ -320,8 +320,11 @@ struct ConstsF32 {
     float qdt_2mc, cdx, cdy, cdz;
 };
 
-template <bool kF32Mom>
-__global__ void __launch_bounds__(kCabBlock) cabana_move_deposit_kernel(HexArgs m, CabParts p,
+// kOcc: resident CTAs per SM the kernel is compiled for (oppb_tuning.cabana_occupancy): 0 = the
+// compiler's register count (FP64 form 76 registers, 3 CTAs per SM; FP32-momentum form 64, 4),
+// 4 (64 registers, no spills) or 5 (48 registers, about 100 B of spills a thread).
+template <bool kF32Mom, int kOcc>
+__global__ void __launch_bounds__(kCabBlock, kOcc > 0 ? kOcc : 1) cabana_move_deposit_kernel(HexArgs m, CabParts p,
                                                                         oppb_cabana_consts k, ConstsF32 kf,
                                                                         double* acc, int32_t acc_stride,
                                                                         oppb_move_status* st, int32_t max_hops) {
@@ -498,7 +501,11 @@ int launch_cabana(const oppb_hex_mesh* mesh, const oppb_cabana_particles* parts,
     // FP32 constants: the round-to-nearest FP32 values of the FP64 ones.
     const ConstsF32 kf{(float)consts->qdt_2mc, (float)consts->cdt_d[0], (float)consts->cdt_d[1],
                        (float)consts->cdt_d[2]};
-    cabana_move_deposit_kernel<kF32Mom><<<ceil_div(parts->size, kCabBlock), kCabBlock, 0, s>>>(
+    const int occ = tuning().cabana_occupancy;
+    auto kernel = occ == 5   ? cabana_move_deposit_kernel<kF32Mom, 5>
+                  : occ == 4 ? cabana_move_deposit_kernel<kF32Mom, 4>
+                             : cabana_move_deposit_kernel<kF32Mom, 0>;
+    kernel<<<ceil_div(parts->size, kCabBlock), kCabBlock, 0, s>>>(
         m, p, *consts, kf, acc, acc_stride, status, max_hops);
     count_launches(1);
     return launch_status();

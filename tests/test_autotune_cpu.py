@@ -55,12 +55,17 @@ def test_tuning_fields_validated():
     L.load().oppb_get_tuning(t)
     assert (t.move_lanes, t.move_occupancy, t.sort_scatter, t.move_stage, t.move_block) == (2, 5, 1, 1, 512)
     for kw in (dict(move_lanes=3), dict(move_occupancy=6), dict(sort_scatter=2), dict(move_stage=2),
-               dict(move_block=64), dict(move_block=384), dict(move_block=1024)):
+               dict(move_block=64), dict(move_block=384), dict(move_block=1024), dict(cabana_occupancy=3),
+               dict(cabana_occupancy=8)):
         with pytest.raises(L.OppbError):
             L.set_tuning(**kw)
     L.set_tuning(move_block=0)  # 0 reads as the default
     L.load().oppb_get_tuning(t)
     assert t.move_block == 256
+    L.set_tuning(cabana_occupancy=5)
+    L.load().oppb_get_tuning(t)
+    assert t.cabana_occupancy == 5
+    L.set_tuning(cabana_occupancy=4)
     L.set_tuning(move_lanes=1, move_occupancy=8, sort_scatter=0, move_stage=0, move_block=256)
 
 

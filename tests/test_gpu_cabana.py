@@ -1,7 +1,8 @@
 """Parity of the CabanaPIC move + current deposit kernel (through the C ABI) with the oracle
 and with the reference's own outputs (golden fixture): positions, momenta, streaks, cells
 and call counts bit-exact; the 12 accumulators, summed with FP64 atomics in a different
-order, within CUR_RTOL of the largest accumulator magnitude."""
+order, within CUR_RTOL of the largest accumulator magnitude.  Each test runs on the kernel
+compiled with the compiler's register count and for 4 and 5 resident CTAs per SM."""
 from __future__ import annotations
 
 from pathlib import Path
@@ -18,6 +19,14 @@ pytestmark = pytest.mark.gpu
 DEV = torch.device("cuda:0")
 CUR_RTOL = 1e-12
 GOLDEN = Path(__file__).resolve().parent / "golden" / "cabana_4x5x6.npz"
+
+
+@pytest.fixture(autouse=True, params=[0, 4, 5], ids=["occ-default", "occ4", "occ5"])
+def occupancy(request):
+    """Every test runs on every compilation of the kernel (oppb_tuning.cabana_occupancy)."""
+    L.set_tuning(cabana_occupancy=request.param)
+    yield request.param
+    L.set_tuning(cabana_occupancy=4)
 
 
 class _K:
