@@ -308,7 +308,7 @@ int oppb_hole_fill(int32_t size, int32_t remove_count, const uint32_t* remove_bi
  * not pay cudaMalloc/cudaFree's implicit device-wide synchronisation.  Same arguments and
  * same result as oppb_hole_fill, bit for bit.
  *
- * Its scratch is a fixed array inside the library, about 8.1 MiB on every GPU that loads
+ * Its scratch is a fixed array inside the library, about 8.5 MiB on every GPU that loads
  * the library, held until the process exits; remove_count above
  * OPPB_HOLE_FILL_STATIC_MAX_REMOVES returns OPPB_ERR_SCRATCH_LIMIT and changes nothing.
  * The first call on each device looks the array's device address up with that device

@@ -21,8 +21,10 @@ namespace oppb {
 namespace {
 
 constexpr int kHfBlock = 256;
-constexpr int kHfWordsPerThread = 8;
-constexpr int kHfWords = kHfBlock * kHfWordsPerThread;  // words per block (65,536 particles)
+// Two bitmap words (64 particles) a thread: the threads over the last live particles emit the
+// movers bit by bit, so this bounds the longest thread of the emit kernel.
+constexpr int kHfWordsPerThread = 2;
+constexpr int kHfWords = kHfBlock * kHfWordsPerThread;  // words per block (16,384 particles)
 constexpr int kMaxDats = 16;
 
 struct DatList {
@@ -133,7 +135,9 @@ __global__ void __launch_bounds__(kHfBlock) hf_emit_kernel(const uint32_t* __res
 }
 
 // One (pair, column) per thread and pass of a grid-stride loop: copies the element of column
-// col of the mover to the hole.
+// col of the mover to the hole.  The pair index runs fastest, so a warp reads consecutive
+// entries of the two lists and, the movers being the last live particles in descending order,
+// neighbouring elements of one column; only the writes to the holes scatter.
 __global__ void hf_copy_kernel(CountArg pairs_arg, const int32_t* __restrict__ hole_list,
                                const int32_t* __restrict__ mover_list, const int* __restrict__ totals,
                                CountArg size_arg, int32_t stride, DatList dats) {
@@ -143,8 +147,8 @@ __global__ void hf_copy_kernel(CountArg pairs_arg, const int32_t* __restrict__ h
     const int64_t n_items = n_pairs_max * dats.total_cols;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_items;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = t / dats.total_cols;
-        const int col = (int)(t - k * dats.total_cols);
+        const int col = (int)(t / n_pairs_max);
+        const int64_t k = t - (int64_t)col * n_pairs_max;
         if (k >= H || k >= size - H) continue;
         const int32_t to = hole_list[k], from = mover_list[k];
         if (from <= to) continue;
@@ -330,10 +334,10 @@ extern "C" int oppb_step_end_dev(oppb_set_count* count, int32_t pending, const o
 namespace oppb {
 namespace {
 
-constexpr int64_t kStaticMaxBlocks = (((int64_t)INT_MAX + 31) / 32 + kHfWords - 1) / kHfWords;  // 32,768
+constexpr int64_t kStaticMaxBlocks = (((int64_t)INT_MAX + 31) / 32 + kHfWords - 1) / kHfWords;  // 131,072
 constexpr int64_t kStaticBaseWords = (kStaticMaxBlocks + 1 + 63) / 64 * 64;  // whole 256-B lines
 constexpr int64_t kStaticListWords = OPPB_HOLE_FILL_STATIC_MAX_REMOVES;
-constexpr int64_t kStaticWords = kStaticBaseWords + 2 * kStaticListWords;  // about 8.1 MiB
+constexpr int64_t kStaticWords = kStaticBaseWords + 2 * kStaticListWords;  // about 8.5 MiB
 
 }  // namespace
 

@@ -58,17 +58,41 @@ __global__ void __launch_bounds__(kScanBlock) scan_tile_sums_kernel(const int* _
     if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
-// In-place exclusive scan of a[0,n) by one block; a[n] receives the total.
+// In-place exclusive scan of a[0,n) by one block, kScanTile values a pass (coalesced loads into
+// shared memory, kScanItems consecutive values a thread); a[n] receives the total.
 __global__ void __launch_bounds__(kScanBlock) scan_single_block_kernel(int* a, int n) {
+    __shared__ int tile[kScanTile];
     __shared__ int sm[kScanBlock / 32 + 1];
     int carry = 0;
-    for (int base = 0; base < n; base += kScanBlock) {
-        const int j = base + threadIdx.x;
-        const int v = (j < n) ? a[j] : 0;
+    for (int base = 0; base < n; base += kScanTile) {
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            const int j = base + k * kScanBlock + threadIdx.x;
+            tile[k * kScanBlock + threadIdx.x] = (j < n) ? a[j] : 0;
+        }
+        __syncthreads();
+        int vals[kScanItems];
+        int s = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            vals[k] = tile[threadIdx.x * kScanItems + k];
+            s += vals[k];
+        }
         int total;
-        const int ex = block_exclusive_scan(v, sm, &total);
-        if (j < n) a[j] = carry + ex;
+        int run = block_exclusive_scan(s, sm, &total) + carry;
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            tile[threadIdx.x * kScanItems + k] = run;
+            run += vals[k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            const int j = base + k * kScanBlock + threadIdx.x;
+            if (j < n) a[j] = tile[k * kScanBlock + threadIdx.x];
+        }
         carry += total;
+        __syncthreads();  // the next pass overwrites the tile
     }
     if (threadIdx.x == 0) a[n] = carry;
 }
