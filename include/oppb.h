@@ -156,6 +156,13 @@ typedef struct oppb_tuning {
     int32_t cabana_occupancy; /* CabanaPIC move + deposit: resident CTAs per SM it is compiled for:
                                  0 = the compiler's register count, 4 (default; 64 registers a
                                  thread) or 5 (48 registers, small spills).  The same results */
+    int32_t move_walk32;      /* FP64 move + deposit: 1 = walk on the mixed path's FP32 records (each
+                                 inside test and argmin decided in FP32 or, near a threshold, by the
+                                 FP64 expression, so equal to the FP64 decision) and evaluate the FP64
+                                 lambdas once at the last cell), compiled for 8 CTAs per SM; 2 = the
+                                 same compiled for 6; used when the mesh holds geo32 and nav32
+                                 (else the plain FP64 kernel runs).  0 (default) = the FP64 walk.
+                                 The same results either way, bit for bit */
 } oppb_tuning;
 
 /* Set / read the tuning used by subsequent launches (OPPB_ERR_ARG on unknown values). */

@@ -7,7 +7,7 @@
 namespace oppb {
 namespace {
 std::atomic<uint64_t> g_launches{0};
-oppb_tuning g_tuning = {OPPB_DEPOSIT_WARP_ATOMIC, 8, 2, 16, 1, 8, 0, 0, 256, 4};
+oppb_tuning g_tuning = {OPPB_DEPOSIT_WARP_ATOMIC, 8, 2, 16, 1, 8, 0, 0, 256, 4, 0};
 }  // namespace
 void count_launches(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
 const oppb_tuning& tuning() { return g_tuning; }
@@ -29,6 +29,7 @@ extern "C" int oppb_set_tuning(const oppb_tuning* t) {
     if (t->move_block != 0 && t->move_block != 128 && t->move_block != 256 && t->move_block != 512)
         return OPPB_ERR_ARG;
     if (t->cabana_occupancy != 0 && t->cabana_occupancy != 4 && t->cabana_occupancy != 5) return OPPB_ERR_ARG;
+    if (t->move_walk32 < 0 || t->move_walk32 > 2) return OPPB_ERR_ARG;
     oppb::g_tuning = *t;
     if (oppb::g_tuning.move_lanes == 0) oppb::g_tuning.move_lanes = 1;
     if (oppb::g_tuning.move_occupancy == 0) oppb::g_tuning.move_occupancy = 8;

@@ -856,6 +856,132 @@ __global__ void __launch_bounds__(kBlock, kThreadsPerSm / kBlock)
     deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, lf);
 }
 
+// ------------------------------------------------ FP64 move on FP32 walk decisions
+//
+// oppb_tuning.move_walk32 = 1 (FP64 move + deposit, on a mesh that also holds the mixed
+// path's records).  The walk is move_mixed_kernel's: every inside test and argmin is decided
+// from the 64-B FP32 record, or, inside the band, by the FP64 reference expression, so each
+// decision is the FP64 one and the particle visits the FP64 kernel's cells.  The FP64
+// lambdas are then evaluated once, with the reference expression, at the last cell visited
+// (the cell the particle ends in, or the one it left the mesh from): p_lc, p2c, the deposit,
+// the removals and the visit counts are move_f64_kernel's bit for bit (its recheck count stays
+// 0, as the FP64 kernel's).  A visit costs two 256-bit loads instead of five; the last cell
+// five more.
+constexpr float kWalk32Band = 1e-5f;  // above the FP32 lambdas' proven error (9.2e-6)
+
+// kOcc: resident CTAs per SM it is compiled for, 8 (32 registers, 24 B of spills) or 6 (39
+// registers, 8 B).
+template <int kDep, bool kPush, bool kSeed, bool kDevCount = false, int kOcc = kMinBlocks>
+__global__ void __launch_bounds__(kMoveBlock, kOcc)
+    move_walk32_kernel(oppb_tet_mesh m, PartArgs p, DepositArgs dep, oppb_move_status* st, int32_t max_hops,
+                       PushArgs push, DhArgs dh) {
+    __shared__ NodeTable table;
+    const int32_t n = kDevCount ? live_count(p) : p.size;
+    if (kDevCount && (int64_t)blockIdx.x * kMoveBlock >= n) return;  // beyond the device count (whole block)
+    if (kDep == kDepTable) table_init(table);
+    const int64_t i = (int64_t)blockIdx.x * kMoveBlock + threadIdx.x;
+    const bool active = i < n;
+    int32_t cell = active ? ld_stream(p.p2c + i) : kRemoved;
+    const int32_t cell0 = cell;
+    int32_t last = cell;  // the cell of the last visit
+    int status = kDone;
+    int visits = 0;
+    int err = 0;
+    double l[4] = {0.0, 0.0, 0.0, 0.0};
+    double lr[4];  // the rare FP64 re-evaluation inside the band (written out of line)
+    const float bl = kWalk32Band, bneg = -kWalk32Band, bin = 1.0f - kWalk32Band, bout = 1.0f + kWalk32Band,
+                btie = 2.0f * kWalk32Band;
+    if (active && cell != kRemoved) {
+        double x = ld_stream(p.pos + i);
+        double y = ld_stream(p.pos + p.stride + i);
+        double z = ld_stream(p.pos + 2 * (int64_t)p.stride + i);
+        if (kPush && (uint32_t)cell < (uint32_t)m.n_cells) push_prologue<false>(m, p, push, i, cell, x, y, z);
+        if (kSeed) {  // the walk starts from the grid box's cell (after the push, as the reference)
+            cell = dh_seed(dh, x, y, z);
+            if (cell == kRemoved) status = kNeedRemove;
+        }
+        while (!kSeed || cell != kRemoved) {
+            if ((uint32_t)cell >= (uint32_t)m.n_cells) {
+                err = OPPB_ERR_CELL_RANGE;
+                break;
+            }
+            last = cell;
+            visits++;
+            float g0[8], g1[8];  // rows 0..2, then the origin
+            ldg256(m.geo32 + (int64_t)cell * 16, g0);
+            ldg256(m.geo32 + (int64_t)cell * 16 + 8, g1);
+            const float dx = (float)(x - (double)g1[4]);
+            const float dy = (float)(y - (double)g1[5]);
+            const float dz = (float)(z - (double)g1[6]);
+            const float ssum = fmaf(g1[7], fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))), 1.001f);
+            const float rows[12] = {g0[0], g0[1], g0[2], g0[3], g0[4], g0[5], g0[6], g0[7],
+                                    g1[0], g1[1], g1[2], g1[3]};
+            float lf[4];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const float c0 = rows[4 * k], gx = rows[4 * k + 1], gy = rows[4 * k + 2], gz = rows[4 * k + 3];
+                lf[k] = fmaf(gz, dz, fmaf(gy, dy, fmaf(gx, dx, c0)));
+            }
+            lf[3] = ((1.0f - lf[0]) - lf[1]) - lf[2];
+            // The mixed kernel's classification (its comment states the error bound).
+            bool clear_in = ssum <= kMaxS;
+            bool clear_out = false;
+            bool ambiguous = !(ssum <= kMaxS);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                clear_in = clear_in && (lf[k] >= bl) && (lf[k] <= bin);
+                clear_out = clear_out || (lf[k] <= bneg) || (lf[k] >= bout);
+            }
+            int mi = 0;
+            if (!clear_in && !ambiguous) {
+                if (!clear_out) {
+                    ambiguous = true;
+                } else {
+                    float mv = lf[0];
+#pragma unroll
+                    for (int k = 1; k < 4; k++)
+                        if (lf[k] < mv) {
+                            mv = lf[k];
+                            mi = k;
+                        }
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if (k != mi && !(lf[k] - mv > btie)) ambiguous = true;
+                }
+            }
+            bool in = clear_in;
+            if (ambiguous) {
+                recheck_f64(m, cell, x, y, z, lr);
+                in = inside_f64(lr);
+                if (!in) mi = argmin4(lr);
+            }
+            if (in) break;
+            const int32_t next = __ldg(reinterpret_cast<const int32_t*>(m.nav32 + (int64_t)cell * 8 + 4) + mi);
+            if (next < 0) {
+                cell = kRemoved;
+                status = kNeedRemove;
+                break;
+            }
+            cell = next;
+            if (visits >= max_hops) {
+                err = OPPB_ERR_HOP_LIMIT;
+                break;
+            }
+        }
+        if (visits > 0) {  // the FP64 lambdas of the last cell visited, as move_f64_kernel leaves them
+            int nb[4];
+            visit_f64(m, last, x, y, z, l, nb);
+        }
+        if (err) {
+            raise_error(st, err, (int32_t)i);
+            status = kFailed;
+        }
+        store_result(p, i, l, visits, cell, cell0);
+    }
+    cta_account(p, st, i, active, cell, status == kNeedRemove, visits, 0);
+    deposit_epilogue<kDep>(m, table, dep, active && cell0 != kRemoved && status == kDone, cell, l);
+}
+
 // ------------------------------------------------------------- standalone deposit
 
 template <int kDep>
@@ -984,6 +1110,22 @@ void launch_pair(int grid, cudaStream_t s, bool table, bool exact, const oppb_te
         move_f64_pair_kernel<kDepWarp, kPush, kDevCount, kOcc><<<grid, kMoveBlock, 0, s>>>(m, p, d, st, max_hops, push);
 }
 
+// The FP32-walk FP64 kernel for the tuned deposit, compiled for kOcc resident CTAs per SM.
+template <bool kPush, bool kSeed, bool kDevCount, int kOcc>
+void launch_walk32(int grid, cudaStream_t s, bool table, bool exact, const oppb_tet_mesh& m, const PartArgs& p,
+                   const DepositArgs& d, oppb_move_status* st, int32_t max_hops, const PushArgs& push,
+                   const DhArgs& dh) {
+    if (table)
+        move_walk32_kernel<kDepTable, kPush, kSeed, kDevCount, kOcc><<<grid, kMoveBlock, 0, s>>>(m, p, d, st, max_hops,
+                                                                                               push, dh);
+    else if (exact)
+        move_walk32_kernel<kDepExact, kPush, kSeed, kDevCount, kOcc><<<grid, kMoveBlock, 0, s>>>(m, p, d, st, max_hops,
+                                                                                               push, dh);
+    else
+        move_walk32_kernel<kDepWarp, kPush, kSeed, kDevCount, kOcc><<<grid, kMoveBlock, 0, s>>>(m, p, d, st, max_hops,
+                                                                                              push, dh);
+}
+
 // The one-lane kernels with the warp-grouped deposit at block shape kBlock.
 template <bool kMixed, bool kPush, bool kSeed, bool kDevCount, int kBlock>
 void launch_warp_shape(int32_t size, cudaStream_t s, const oppb_tet_mesh& m, const PartArgs& p,
@@ -1050,7 +1192,15 @@ int launch_move(const oppb_tet_mesh* mesh, const oppb_particles* parts, double* 
         move_f64_kernel<kDepNone, kPush, kSeed, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args, status, max_hops,
                                                                            push, dh);
     else if constexpr (kKind == kMoveDepositF64) {
-        if (!kSeed && tuning().move_lanes != 2 && tuning().move_stage == 1) {  // records staged by bulk copies
+        if (tuning().move_walk32 != 0 && mesh->geo32 && mesh->nav32 && aligned(mesh->geo32, 32) &&
+            aligned(mesh->nav32, 32)) {  // walk on the FP32 records, FP64 lambdas at the last cell
+            if (tuning().move_walk32 == 2)
+                launch_walk32<kPush, kSeed, kDevCount, 6>(grid, s, table, exact, *mesh, p, rep.args, status,
+                                                          max_hops, push, dh);
+            else
+                launch_walk32<kPush, kSeed, kDevCount, kMinBlocks>(grid, s, table, exact, *mesh, p, rep.args, status,
+                                                                   max_hops, push, dh);
+        } else if (!kSeed && tuning().move_lanes != 2 && tuning().move_stage == 1) {  // records staged by bulk copies
             if (table)
                 move_f64_stage_kernel<kDepTable, kPush, kDevCount><<<grid, kMoveBlock, 0, s>>>(*mesh, p, rep.args,
                                                                                               status, max_hops, push);

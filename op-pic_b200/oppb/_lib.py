@@ -58,7 +58,7 @@ class Dat(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("deposit", c_i32), ("replicas", c_i32), ("advec_items", c_i32), ("sort_gather_cols", c_i32),
                 ("move_lanes", c_i32), ("move_occupancy", c_i32), ("sort_scatter", c_i32), ("move_stage", c_i32),
-                ("move_block", c_i32), ("cabana_occupancy", c_i32)]
+                ("move_block", c_i32), ("cabana_occupancy", c_i32), ("move_walk32", c_i32)]
 
 
 DEPOSIT_WARP_ATOMIC = 0
@@ -249,7 +249,7 @@ def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_it
                sort_gather_cols: int | None = None, move_lanes: int | None = None,
                move_occupancy: int | None = None, sort_scatter: int | None = None,
                move_stage: int | None = None, move_block: int | None = None,
-               cabana_occupancy: int | None = None) -> None:
+               cabana_occupancy: int | None = None, move_walk32: int | None = None) -> None:
     t = Tuning()
     load().oppb_get_tuning(C.byref(t))
     if deposit is not None:
@@ -272,6 +272,8 @@ def set_tuning(deposit: int | None = None, replicas: int | None = None, advec_it
         t.move_block = move_block
     if cabana_occupancy is not None:
         t.cabana_occupancy = cabana_occupancy
+    if move_walk32 is not None:
+        t.move_walk32 = move_walk32
     check("oppb_set_tuning", load().oppb_set_tuning(C.byref(t)))
 
 

@@ -27,7 +27,8 @@ import torch
 from oppb import _lib as L
 
 MOVE_CANDIDATES = [(dep, rep) for dep in (L.DEPOSIT_WARP_ATOMIC, L.DEPOSIT_CTA_TABLE) for rep in (1, 4, 8, 16)]
-LANE_CANDIDATES = [(1, 8, 0), (1, 8, 1), (2, 8, 0), (2, 5, 0)]  # (move_lanes, move_occupancy, move_stage)
+# (move_lanes, move_occupancy, move_stage, move_walk32)
+LANE_CANDIDATES = [(1, 8, 0, 0), (1, 8, 0, 1), (1, 8, 0, 2), (1, 8, 1, 0), (2, 8, 0, 0), (2, 5, 0, 0)]
 BLOCK_CANDIDATES = [256, 128, 512]  # threads per CTA of the one-lane move kernels
 SORT_CANDIDATES = [(16, 0), (10, 0), (5, 0), (16, 1), (10, 1)]  # (columns per launch, scatter form)
 PERIOD_CANDIDATES = [5, 10, 20]
@@ -137,23 +138,23 @@ def tune_move(sim, candidates=None, reps: int = 3, with_push: bool | None = None
 
 
 def tune_lanes(sim, candidates=None, reps: int = 3, with_push: bool | None = None) -> TuneResult:
-    """Lanes per particle, compiled occupancy and record staging of the FP64 move + deposit
-    launch (the mixed kernel has one lane per particle: nothing to tune there), with the deposit
-    choice in force."""
+    """Lanes per particle, compiled occupancy, record staging and FP32 walk of the FP64 move +
+    deposit launch (the mixed kernel has one lane per particle: nothing to tune there), with the
+    deposit choice in force."""
     if sim.precision != "f64":
-        return TuneResult(choice=(1, 8, 0))
+        return TuneResult(choice=(1, 8, 0, 0))
     return _tune_walk(sim, candidates or LANE_CANDIDATES,
-                      lambda c: L.set_tuning(move_lanes=c[0], move_occupancy=c[1], move_stage=c[2]),
-                      lambda t: (t.move_lanes, t.move_occupancy, t.move_stage), reps, with_push)
+                      lambda c: L.set_tuning(move_lanes=c[0], move_occupancy=c[1], move_stage=c[2], move_walk32=c[3]),
+                      lambda t: (t.move_lanes, t.move_occupancy, t.move_stage, t.move_walk32), reps, with_push)
 
 
 def block_shape_applies(t: L.Tuning, precision: str) -> bool:
     """Whether oppb_tuning.move_block shapes the launch: the one-lane kernels with the
     warp-grouped deposit (the CTA table is sized for 256 threads, the exact deposit, the
-    lane-pair and the staged kernels run 256)."""
+    lane-pair, staged and FP32-walk kernels run 256)."""
     if t.deposit != L.DEPOSIT_WARP_ATOMIC:
         return False
-    return precision != "f64" or (t.move_lanes in (0, 1) and t.move_stage == 0)
+    return precision != "f64" or (t.move_lanes in (0, 1) and t.move_stage == 0 and t.move_walk32 == 0)
 
 
 def tune_block(sim, candidates=None, reps: int = 3, with_push: bool | None = None) -> TuneResult:

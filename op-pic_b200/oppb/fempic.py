@@ -272,7 +272,9 @@ class FemPIC:
         self.hm = hm
         self.inject_per_step = inject_per_step
         self.dist_host = hm.inject_distribution(inject_per_step)
-        self.mesh = DeviceMesh(hm, self.device, mixed=(precision == "mixed"), dist=self.dist_host)
+        # The mixed path's FP32 records are packed for both precisions: the FP64 move can walk on
+        # them (oppb_tuning.move_walk32).
+        self.mesh = DeviceMesh(hm, self.device, mixed=True, dist=self.dist_host)
         self.parts = ParticleSet(self.device, capacity, alloc_mult)
         self.ion_velocity, self.qm, self.dt = ion_velocity, qm, dt
         if precision not in ("f64", "mixed"):

@@ -40,8 +40,10 @@ def test_pick_ties_and_errors():
 def test_candidate_sets():
     assert len(set(MOVE_CANDIDATES)) == len(MOVE_CANDIDATES) == 8
     assert all(1 <= c <= 16 and f in (0, 1) for c, f in SORT_CANDIDATES) and SORT_CANDIDATES[0] == (16, 0)
-    assert LANE_CANDIDATES[0] == (1, 8, 0)
-    assert all(lanes in (1, 2) and occ in (5, 8) and stage in (0, 1) for lanes, occ, stage in LANE_CANDIDATES)
+    assert LANE_CANDIDATES[0] == (1, 8, 0, 0)
+    assert all(lanes in (1, 2) and occ in (5, 8) and stage in (0, 1) and w in (0, 1, 2)
+               for lanes, occ, stage, w in LANE_CANDIDATES)
+    assert (1, 8, 0, 1) in LANE_CANDIDATES
     assert 10 in PERIOD_CANDIDATES
     assert BLOCK_CANDIDATES[0] == 256 and sorted(BLOCK_CANDIDATES) == [128, 256, 512]
 
@@ -56,7 +58,7 @@ def test_tuning_fields_validated():
     assert (t.move_lanes, t.move_occupancy, t.sort_scatter, t.move_stage, t.move_block) == (2, 5, 1, 1, 512)
     for kw in (dict(move_lanes=3), dict(move_occupancy=6), dict(sort_scatter=2), dict(move_stage=2),
                dict(move_block=64), dict(move_block=384), dict(move_block=1024), dict(cabana_occupancy=3),
-               dict(cabana_occupancy=8)):
+               dict(cabana_occupancy=8), dict(move_walk32=3)):
         with pytest.raises(L.OppbError):
             L.set_tuning(**kw)
     L.set_tuning(move_block=0)  # 0 reads as the default
@@ -79,6 +81,7 @@ def test_block_shape_applies_to_the_one_lane_warp_deposit():
     assert not block_shape_applies(L.Tuning(deposit=L.DEPOSIT_EXACT, move_lanes=1), "f64")
     assert not block_shape_applies(L.Tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=2), "f64")
     assert not block_shape_applies(L.Tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=1, move_stage=1), "f64")
+    assert not block_shape_applies(L.Tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=1, move_walk32=1), "f64")
     assert block_shape_applies(L.Tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=2), "mixed")
 
 

@@ -1,6 +1,7 @@
 """The FP64 move's variants: two lanes per particle (oppb_tuning.move_lanes = 2, compiled for 8
-or 5 resident CTAs per SM) and one lane with each visit's cell record staged into shared memory
-by bulk asynchronous copies (move_stage = 1).  Cells, weights, removals, visit counts and the
+or 5 resident CTAs per SM), one lane with each visit's cell record staged into shared memory
+by bulk asynchronous copies (move_stage = 1), and the walk on the mixed path's FP32 records with
+the FP64 lambdas evaluated at the last cell (move_walk32 = 1).  Cells, weights, removals, visit counts and the
 removal bitmap bit-exact against the oracle, as the default kernel; node charges within 1e-12
 relative (FP64 atomics), and bit for bit equal to the default kernel's in the deterministic
 deposit; the fused push, the device-count launch and the error paths (hop limit, bad cell)
@@ -22,15 +23,19 @@ pytestmark = pytest.mark.gpu
 DEV = torch.device("cuda:0")
 
 
-DEFAULT = (1, 8, 0)  # (move_lanes, move_occupancy, move_stage)
+DEFAULT = (1, 8, 0, 0)  # (move_lanes, move_occupancy, move_stage, move_walk32)
 
 
-@pytest.fixture(params=[(1, 8, 1), (2, 8, 0), (2, 5, 0)], ids=["staged", "pair-occ8", "pair-occ5"])
+def _set(v):
+    L.set_tuning(move_lanes=v[0], move_occupancy=v[1], move_stage=v[2], move_walk32=v[3])
+
+
+@pytest.fixture(params=[(1, 8, 1, 0), (2, 8, 0, 0), (2, 5, 0, 0), (1, 8, 0, 1), (1, 8, 0, 2)],
+                ids=["staged", "pair-occ8", "pair-occ5", "walk32-occ8", "walk32-occ6"])
 def pair_lanes(request):
-    lanes, occ, stage = request.param
-    L.set_tuning(move_lanes=lanes, move_occupancy=occ, move_stage=stage)
+    _set(request.param)
     yield request.param
-    L.set_tuning(move_lanes=DEFAULT[0], move_occupancy=DEFAULT[1], move_stage=DEFAULT[2])
+    _set(DEFAULT)
 
 
 def _particles(hm, n, seed):
@@ -56,7 +61,7 @@ def test_pair_move_deposit_matches_oracle(pair_lanes, deposit, n, seed):
     L.set_tuning(deposit=deposit)
     try:
         hm = mesh()
-        dm = DeviceMesh(hm, DEV, mixed=False)
+        dm = DeviceMesh(hm, DEV, mixed=True)
         pos, p2c, ps = _particles(hm, n, seed)
         charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
         L.check("move_deposit", _move_deposit(dm, ps, hm, charge))
@@ -86,18 +91,19 @@ def test_pair_exact_deposit_equals_one_lane_bit_for_bit(pair_lanes):
     """OPPB_DEPOSIT_EXACT sums integers: the node charges of the lane-pair kernel equal the
     one-lane kernel's bit for bit on the same particles."""
     hm = mesh()
-    dm = DeviceMesh(hm, DEV, mixed=False)
+    dm = DeviceMesh(hm, DEV, mixed=True)
     out = {}
     for variant in (DEFAULT, pair_lanes):
-        L.set_tuning(deposit=L.DEPOSIT_EXACT, move_lanes=variant[0], move_occupancy=variant[1], move_stage=variant[2])
+        L.set_tuning(deposit=L.DEPOSIT_EXACT)
+        _set(variant)
         try:
             _, _, ps = _particles(hm, 200_000, 9)
             charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
             L.check("move_deposit", _move_deposit(dm, ps, hm, charge))
             torch.cuda.synchronize()
         finally:
-            L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC, move_lanes=pair_lanes[0], move_occupancy=pair_lanes[1],
-                         move_stage=pair_lanes[2])
+            L.set_tuning(deposit=L.DEPOSIT_WARP_ATOMIC)
+            _set(pair_lanes)
         out[variant] = charge.cpu().numpy()
     np.testing.assert_array_equal(out[DEFAULT].view(np.uint64), out[pair_lanes].view(np.uint64))
 
@@ -139,7 +145,7 @@ def test_pair_graph_steps_equal_direct(pair_lanes):
 def test_pair_errors_reported(pair_lanes):
     """A bad start cell and the hop limit raise their error word with the particle index."""
     hm = mesh()
-    dm = DeviceMesh(hm, DEV, mixed=False)
+    dm = DeviceMesh(hm, DEV, mixed=True)
     pos, p2c, ps = _particles(hm, 600, 3)
     ps.p2c[0, 417] = hm.n_cells + 5
     charge = torch.zeros(hm.n_nodes, dtype=torch.float64, device=DEV)
