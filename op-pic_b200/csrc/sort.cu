@@ -187,6 +187,26 @@ struct GatherCols {
     int32_t bytes[kMaxCols];
 };
 
+// L2 eviction policies (createpolicy, sm_80+): the gathered sources are reused by neighbouring
+// destinations (a 32-B sector holds four particles of one column that end up within a few
+// hundred thousand destinations of each other), so their lines are kept in L2 ahead of the
+// streaming destination writes and the permutation, which are touched once.
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ long long ld_keep(const long long* p, uint64_t pol) {
+    long long v;
+    asm("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_keep(const int* p, uint64_t pol) {
+    int v;
+    asm("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 // dst[c][j] = src[c][perm[j]] for every column of every dat other than the key dat.
 // All loads of a particle are issued before its stores, so each thread keeps up to
 // kMaxCols loads in flight.  When the sort is a copy (device count, no removal), perm is
@@ -197,16 +217,17 @@ __global__ void __launch_bounds__(256) gather_kernel(SortCount cnt, const int32_
     const int64_t j = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (j >= size) return;
     const bool copy = sort_is_copy(cnt);
-    const int64_t from = copy ? j : perm[j];
+    const int64_t from = copy ? j : __ldcs(perm + j);
     if (copy && key_src) key_dst[j] = key_src[j];
+    const uint64_t keep = l2_policy_evict_last();
     uint64_t v[kMaxCols];
 #pragma unroll
     for (int c = 0; c < kMaxCols; c++) {
         if (c < g.n) {
             if (g.bytes[c] == 8)
-                v[c] = (uint64_t)__ldg(reinterpret_cast<const long long*>(g.src[c]) + from);
+                v[c] = (uint64_t)ld_keep(reinterpret_cast<const long long*>(g.src[c]) + from, keep);
             else
-                v[c] = (uint32_t)__ldg(reinterpret_cast<const int*>(g.src[c]) + from);
+                v[c] = (uint32_t)ld_keep(reinterpret_cast<const int*>(g.src[c]) + from, keep);
         }
     }
 #pragma unroll
