@@ -982,8 +982,11 @@ ADV_WORKLOAD = ("NESO-advection ensemble: 64 independent periodic square meshes,
 # Per step: read pos 16 + vel 16 + mdir 8 + p2c 4, write pos 16 + mdir 8 B per particle; 32 B per cell record.
 ADV_BYTES_PER_PARTICLE = 68
 ADV_BYTES_PER_CELL = 32
-# DRAM bytes per particle of one full-size launch (ncu, profiles/advec_kernel_neso_ensemble_64.txt).
-ADV_MEASURED_DRAM_BYTES_PER_PARTICLE = 76.2
+# DRAM bytes per particle of one launch (ncu, profiles/advec_kernel_neso_ensemble_64.txt): a
+# 19.2M-particle, 8-instance capture, scaled by the particle count (traffic grows with it).
+ADV_MEASURED_DRAM_BYTES_PER_PARTICLE = 69.7
+ADV_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of an 8-instance, 19.2M-particle launch, "
+                      "per particle x particles")
 
 
 def run_advec(dev, steps: int, warmup: int, cpu: bool, rank: int = 0, world: int = 1) -> dict:
@@ -1078,7 +1081,7 @@ def run_advec(dev, steps: int, warmup: int, cpu: bool, rank: int = 0, world: int
            "autotune": {"advec_items": {str(k): v for k, v in sweep.items()}, "chosen": best},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": achieved / peaks["hbm_gbs"], "bytes_per_launch": bytes_step,
-                        "traffic": ADV_MEASURED_DRAM_BYTES_PER_PARTICLE * n, "traffic_source": TRAFFIC_SOURCE,
+                        "traffic": ADV_MEASURED_DRAM_BYTES_PER_PARTICLE * n, "traffic_source": ADV_TRAFFIC_SOURCE,
                         "what": "rank 0's persistent launch over its shard"}}
     if cpu and rank == 0:
         out["cpu_baseline"] = advec_cpu_baseline()

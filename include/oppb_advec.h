@@ -22,13 +22,18 @@ extern "C" {
 
 /* One instance: its particles [part_offset, part_offset + n_parts) of the concatenated dats,
  * its cells [cell_offset, cell_offset + n_cells) of the packed cell records, and its
- * CONST_dt, CONST_cell_width, CONST_extents (advec_opp.cpp). */
+ * CONST_dt, CONST_cell_width, CONST_extents (advec_opp.cpp).  grid_nx > 0 declares the cells
+ * the periodic grid_nx x (n_cells / grid_nx) grid of the app's init_mesh (advec_misc.h:115-141:
+ * cell x + nx y with c_pos_ll = (x w, y w) and the VOXEL_MAP neighbours), as
+ * oppb_advec_check_grid verifies: the move then computes each cell's corner and neighbours
+ * from its index instead of reading its record (the same values, bit for bit).  0 = read the
+ * records. */
 typedef struct oppb_advec_instance {
     int64_t part_offset;
     int32_t n_parts;
     int32_t cell_offset;
     int32_t n_cells;
-    int32_t reserved;
+    int32_t grid_nx;
     double  dt;
     double  cell_width;
     double  extents[2];
@@ -76,6 +81,14 @@ typedef struct oppb_advec_batch {
  * cells[cell_offset .. cell_offset + n_cells). */
 int oppb_advec_pack_cells(double* cells, int32_t cell_offset, int32_t n_cells, int32_t ld,
                           const double* c_pos_ll, const int32_t* c2c, void* stream);
+
+/* Writes to *mismatches (device int32) the number of cells of one instance whose packed record
+ * (cells + 4 * cell_offset, n_cells records) differs in any bit from the periodic nx-wide grid's
+ * corner (x w, y w) and neighbours; 0 means the instance may set grid_nx = nx.  No counterpart
+ * in the reference (its move always reads c_pos_ll and c_c_map).  OPPB_ERR_ARG unless
+ * n_cells is a multiple of nx. */
+int oppb_advec_check_grid(const double* cells, int32_t cell_offset, int32_t n_cells, int32_t nx,
+                          double cell_width, int32_t* mismatches, void* stream);
 
 /* update_pos_kernel then move_kernel for every particle of every instance, fused per
  * particle (the position stays in registers), in one persistent launch.  Bit-identical to

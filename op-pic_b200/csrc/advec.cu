@@ -88,6 +88,58 @@ __device__ __forceinline__ int move_particle(const double* __restrict__ cells, i
     }
 }
 
+// move_kernel's hops on an instance whose cells are the periodic nx x ny grid of the app's
+// init_mesh (apps_codegen/app_neso_advection_mdir_cg/advec_misc.h:115-141): the corner
+// (ix w, iy w) and the VOXEL_MAP neighbours (advec_defs.h:46-54) computed from the cell
+// index instead of read from the record, which oppb_advec_check_grid found equal to them bit
+// for bit.  The walk keeps (ix, iy) and steps them with the periodic wrap; the arithmetic
+// and the decisions are move_particle's.
+__device__ __forceinline__ int move_particle_grid(int32_t nx, int32_t n_cells, double x, double y, int& mx, int& my,
+                                                  int32_t& cell, double cw, double ex, double ey, int32_t max_hops,
+                                                  int& err) {
+    if ((uint32_t)cell >= (uint32_t)n_cells) {
+        err = OPPB_ERR_CELL_RANGE;
+        return 0;
+    }
+    const int32_t ny = n_cells / nx;
+    int32_t iy = cell / nx;
+    int32_t ix = cell - iy * nx;
+    int calls = 0;
+    for (;;) {
+        calls++;
+        const double dx = x - (double)ix * cw;  // c_pos_ll = (x * cell_width, y * cell_width)
+        const double dy = y - (double)iy * cw;
+        if (calls == 1) {  // OPP_DO_ONCE
+            const bool xp = ((dx > cw) && (ex > 2 * dx - cw)) || ((dx < 0) && (ex < cw - 2 * dx));
+            const bool yp = ((dy > cw) && (ey > 2 * dy - cw)) || ((dy < 0) && (ey < cw - 2 * dy));
+            mx = xp ? 1 : -1;
+            my = yp ? 1 : -1;
+        }
+        bool hop = false;
+        if ((dx >= 0.0) && (dx <= cw)) {
+            mx = 0;
+        } else if (mx != 0) {
+            ix = mx > 0 ? (ix + 1 >= nx ? 0 : ix + 1) : (ix - 1 < 0 ? nx - 1 : ix - 1);  // xu_y : xd_y
+            hop = true;
+        }
+        if (!hop) {
+            if ((dy >= 0.0) && (dy <= cw)) {
+                my = 0;
+            } else if (my != 0) {
+                iy = my > 0 ? (iy + 1 >= ny ? 0 : iy + 1) : (iy - 1 < 0 ? ny - 1 : iy - 1);  // x_yu : x_yd
+                hop = true;
+            }
+        }
+        if (!hop) break;
+        if (calls >= max_hops) {
+            err = OPPB_ERR_HOP_LIMIT;
+            break;
+        }
+    }
+    cell = ix + nx * iy;
+    return calls;
+}
+
 constexpr int kChunkItems = 8;  // work items a block takes from the counter at once
 
 // Direct-hop seed (oppb_advec_dh): the cell of the grid box holding (x, y), or kRemoved
@@ -167,7 +219,6 @@ __global__ void __launch_bounds__(kAdvBlock) advec_kernel(oppb_advec_batch b, op
                 }
                 if (kMode != kUpdateOnly) {
                     if (cell[k] == kRemoved) continue;
-                    const int32_t cell0 = cell[k];
                     if (kSeed) {  // the global-move pre-pass, after the update as in the reference
                         cell[k] = dh_seed_2d(b.dh[inst[k]], x[k], y[k]);
                         if (cell[k] == kRemoved) {
@@ -177,12 +228,18 @@ __global__ void __launch_bounds__(kAdvBlock) advec_kernel(oppb_advec_batch b, op
                         }
                     }
                     int err = 0;
-                    const int calls = move_particle(b.cells, __ldg(&I.cell_offset), __ldg(&I.n_cells), x[k], y[k], mx[k],
-                                                    my[k], cell[k], __ldg(&I.cell_width), ex, ey, max_hops, err);
+                    const int32_t gnx = __ldg(&I.grid_nx);
+                    const int calls =
+                        gnx > 0 ? move_particle_grid(gnx, __ldg(&I.n_cells), x[k], y[k], mx[k], my[k], cell[k],
+                                                     __ldg(&I.cell_width), ex, ey, max_hops, err)
+                                : move_particle(b.cells, __ldg(&I.cell_offset), __ldg(&I.n_cells), x[k], y[k], mx[k],
+                                                my[k], cell[k], __ldg(&I.cell_width), ex, ey, max_hops, err);
                     if (err) raise_error(st, err, (int32_t)i);
                     st_stream(b.mdir + i, mx[k]);
                     st_stream(b.mdir + sd + i, my[k]);
-                    if (cell[k] != cell0) st_stream(b.p2c + i, cell[k]);
+                    // Every processed particle's cell is stored, changed or not: a warp then
+                    // writes whole sectors of p2c, which DRAM takes without reading them first.
+                    st_stream(b.p2c + i, cell[k]);
                     my_calls += (unsigned long long)calls;
                     my_max = max(my_max, calls);
                 }
@@ -232,6 +289,24 @@ __global__ void __launch_bounds__(256) advec_pack_kernel(double* cells, int32_t 
     r.z = __longlong_as_double(((long long)(uint32_t)nb[1] << 32) | (uint32_t)nb[0]);
     r.w = __longlong_as_double(((long long)(uint32_t)nb[3] << 32) | (uint32_t)nb[2]);
     reinterpret_cast<double4*>(cells)[(int64_t)cell_offset + c] = r;
+}
+
+// Counts the cells whose packed record differs, in any bit, from the periodic grid's corner and
+// neighbours (move_particle_grid).
+__global__ void __launch_bounds__(256) advec_check_grid_kernel(const double* cells, int32_t n_cells, int32_t nx,
+                                                               double cw, int32_t* mismatches) {
+    const int32_t c = (int32_t)(blockIdx.x * 256 + threadIdx.x);
+    if (c >= n_cells) return;
+    const int32_t ny = n_cells / nx, iy = c / nx, ix = c - iy * nx;
+    const int32_t xd = (ix - 1 < 0 ? nx - 1 : ix - 1) + nx * iy, xu = (ix + 1 >= nx ? 0 : ix + 1) + nx * iy;
+    const int32_t yd = ix + nx * (iy - 1 < 0 ? ny - 1 : iy - 1), yu = ix + nx * (iy + 1 >= ny ? 0 : iy + 1);
+    double llx, lly, n01, n23;
+    ldg256(cells + (int64_t)c * 4, llx, lly, n01, n23);
+    const bool same = __double_as_longlong(llx) == __double_as_longlong((double)ix * cw) &&
+                      __double_as_longlong(lly) == __double_as_longlong((double)iy * cw) &&
+                      __double_as_longlong(n01) == (long long)(((unsigned long long)(uint32_t)xu << 32) | (uint32_t)xd) &&
+                      __double_as_longlong(n23) == (long long)(((unsigned long long)(uint32_t)yu << 32) | (uint32_t)yd);
+    if (!same) atomicAdd(mismatches, 1);
 }
 
 // Persistent grid: resident blocks of the kernel on every SM (cached per device and variant).
@@ -304,6 +379,20 @@ extern "C" int oppb_advec_pack_cells(double* cells, int32_t cell_offset, int32_t
         return OPPB_ERR_ARG;
     advec_pack_kernel<<<ceil_div(n_cells, 256), 256, 0, as_stream(stream)>>>(cells, cell_offset, n_cells, ld,
                                                                              c_pos_ll, c2c);
+    count_launches(1);
+    return launch_status();
+}
+
+extern "C" int oppb_advec_check_grid(const double* cells, int32_t cell_offset, int32_t n_cells, int32_t nx,
+                                     double cell_width, int32_t* mismatches, void* stream) {
+    using namespace oppb;
+    if (!cells || !aligned(cells, 32) || cell_offset < 0 || n_cells <= 0 || nx <= 0 || n_cells % nx != 0 ||
+        !mismatches)
+        return OPPB_ERR_ARG;
+    cudaStream_t s = as_stream(stream);
+    if (cudaMemsetAsync(mismatches, 0, sizeof(int32_t), s) != cudaSuccess) return OPPB_ERR_LAUNCH;
+    advec_check_grid_kernel<<<ceil_div(n_cells, 256), 256, 0, s>>>(cells + (int64_t)cell_offset * 4, n_cells, nx,
+                                                                   cell_width, mismatches);
     count_launches(1);
     return launch_status();
 }

@@ -85,7 +85,7 @@ class CabanaConsts(C.Structure):
 
 class AdvecInstance(C.Structure):
     _fields_ = [("part_offset", c_i64), ("n_parts", c_i32), ("cell_offset", c_i32), ("n_cells", c_i32),
-                ("reserved", c_i32), ("dt", C.c_double), ("cell_width", C.c_double), ("extents", C.c_double * 2)]
+                ("grid_nx", c_i32), ("dt", C.c_double), ("cell_width", C.c_double), ("extents", C.c_double * 2)]
 
 
 class AdvecBatch(C.Structure):
@@ -193,6 +193,7 @@ _SIGS = {
                                                  c_vp, c_i32, c_vp]),
     "oppb_advec_pack_cells": (C.c_int, [c_vp, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp]),
     "oppb_advec_step": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
+    "oppb_advec_check_grid": (C.c_int, [c_vp, c_i32, c_i32, c_i32, C.c_double, c_vp, c_vp]),
     "oppb_advec_update_pos": (C.c_int, [P(AdvecBatch), c_vp]),
     "oppb_advec_move": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
     "oppb_dh_grid_init": (C.c_int, [c_vp, c_i32, C.c_double, c_vp, P(DhGrid)]),

@@ -88,7 +88,10 @@ class AdvecBatchDevice:
     (SoA [2][capacity]), packed cell records, the instance table and work-item prefix.
     There is no CPU fallback."""
 
-    def __init__(self, meshes: list[AdvecMesh], counts: list[int], dts: list[float], device):
+    def __init__(self, meshes: list[AdvecMesh], counts: list[int], dts: list[float], device, grid: bool = True):
+        """grid: verify each instance's packed cells against the periodic grid of the app's
+        init_mesh (oppb_advec_check_grid) and, where they match bit for bit, let the move
+        compute corners and neighbours instead of reading the records."""
         if not torch.cuda.is_available():
             raise RuntimeError("AdvecBatchDevice needs a CUDA device (there is no CPU fallback)")
         self.device = torch.device(device)
@@ -121,6 +124,16 @@ class AdvecBatchDevice:
             prefix.append(prefix[-1] + (n + WORK_ITEM - 1) // WORK_ITEM)
             po += n
             co += m.n_cells
+        self.grid_nx = [0] * len(meshes)
+        if grid:
+            mism = torch.zeros(max(1, len(meshes)), dtype=torch.int32, device=self.device)
+            for k, m in enumerate(meshes):
+                L.check("oppb_advec_check_grid", self.lib.oppb_advec_check_grid(
+                    _ptr(self.cells), self.cell_offsets[k], m.n_cells, m.nx, m.cell_width, _ptr(mism) + 4 * k, None))
+            for k, bad in enumerate(mism.cpu().tolist()[:len(meshes)]):
+                if bad == 0:
+                    self.grid_nx[k] = meshes[k].nx
+                    table[k].grid_nx = meshes[k].nx
         self.instances = torch.frombuffer(bytearray(bytes(table)), dtype=torch.uint8).to(self.device)
         self.tile_prefix = torch.tensor(prefix, dtype=torch.int32, device=self.device)
         self.batch = L.AdvecBatch(len(meshes), prefix[-1], _ptr(self.instances), _ptr(self.tile_prefix),

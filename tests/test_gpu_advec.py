@@ -24,10 +24,10 @@ INSTANCES = [(13, 9, 0.7, 0.35, 30, 2.0), (40, 17, 1.0, 0.5, 7, 0.6), (7, 33, 0.
              (64, 64, 1.0, 0.5, 50, 0.5), (4, 4, 1.0, 0.8, 3, 4.0)]
 
 
-def _build(specs, seed0=0):
+def _build(specs, seed0=0, grid=True):
     meshes = [AdvecMesh(nx, ny, cw) for nx, ny, cw, _, _, _ in specs]
     host = [particles(m, ppc, v_sd, seed0 + k) for k, (m, (_, _, _, _, ppc, v_sd)) in enumerate(zip(meshes, specs))]
-    dev = AdvecBatchDevice(meshes, [len(h[3]) for h in host], [s[3] for s in specs], DEV)
+    dev = AdvecBatchDevice(meshes, [len(h[3]) for h in host], [s[3] for s in specs], DEV, grid=grid)
     for k, h in enumerate(host):
         dev.set_instance(k, *h)
     return meshes, host, dev
@@ -51,9 +51,13 @@ def _assert_same(dev, ref):
         np.testing.assert_array_equal(got["p2c"], r["p2c"], err_msg=f"p2c {k}")
 
 
-def test_batch_step_matches_oracle_per_instance():
+@pytest.mark.parametrize("grid", [True, False], ids=["grid", "records"])
+def test_batch_step_matches_oracle_per_instance(grid):
+    """Cells verified as the periodic grid (corners and neighbours computed) and read from
+    their records: the same results, the oracle's."""
     steps = 6
-    meshes, host, dev = _build(INSTANCES)
+    meshes, host, dev = _build(INSTANCES, grid=grid)
+    assert dev.grid_nx == ([m.nx for m in meshes] if grid else [0] * len(meshes))
     dev.zero_status()
     for _ in range(steps):
         dev.step()
@@ -245,7 +249,8 @@ def test_dh_matches_reference_golden():
     assert dev.status_host().remove_count == 0
 
 
-def test_dh_batch_steps_match_oracle_and_graph():
+@pytest.mark.parametrize("grid", [True, False], ids=["grid", "records"])
+def test_dh_batch_steps_match_oracle_and_graph(grid):
     """A batch of the meshes above with edge particles: 12 steps with the seed, as launches and
     as replays of a 4-step CUDA graph, against the oracle per instance (positions, directions,
     cells, move calls)."""
@@ -256,7 +261,7 @@ def test_dh_batch_steps_match_oracle_and_graph():
     dts = [0.45] * len(meshes)
     devs = []
     for _ in range(2):
-        d = AdvecBatchDevice(meshes, [len(h[3]) for h in host], dts, DEV)
+        d = AdvecBatchDevice(meshes, [len(h[3]) for h in host], dts, DEV, grid=grid)
         for k, h in enumerate(host):
             d.set_instance(k, *h)
         devs.append(d)
@@ -342,3 +347,42 @@ def test_dh_disabled_walks_from_p2c_again():
     got = dev.host_instance(0)
     np.testing.assert_array_equal(got["p2c"], C2)
     np.testing.assert_array_equal(got["pos"].view(np.uint64), P.view(np.uint64))
+
+
+def test_check_grid_rejects_a_perturbed_mesh():
+    """oppb_advec_check_grid counts every cell whose record differs from the periodic grid (a
+    corner one ulp off, a neighbour changed).  An instance with a perturbed corner keeps reading
+    its records, and its steps equal the oracle's on that mesh, next to a clean instance on the
+    grid path."""
+    specs = [(9, 7, 1.0, 0.5, 20, 0.8), (11, 6, 0.5, 0.3, 20, 1.2)]
+    meshes = [AdvecMesh(nx, ny, cw) for nx, ny, cw, _, _, _ in specs]
+    m = meshes[1]
+    m.c_pos_ll[17, 0] = np.nextafter(m.c_pos_ll[17, 0], 10.0)
+    host = [particles(mm, s[4], s[5], 70 + k) for k, (mm, s) in enumerate(zip(meshes, specs))]
+    dev = AdvecBatchDevice(meshes, [len(h[3]) for h in host], [s[3] for s in specs], DEV)
+    assert dev.grid_nx == [9, 0]
+    for k, h in enumerate(host):
+        dev.set_instance(k, *h)
+    for _ in range(5):
+        dev.step()
+    torch.cuda.synchronize()
+    ref, _ = _oracle(meshes, host, specs, 5)
+    _assert_same(dev, ref)
+    # A changed neighbour, checked on its own packed copy of the clean mesh.
+    m2 = AdvecMesh(11, 6, 0.5)
+    c2c = m2.c2c.copy()
+    c2c[40, 1] = c2c[40, 0]
+    cells = torch.zeros(m2.n_cells * 4, dtype=torch.float64, device=DEV)
+    mism = torch.zeros(1, dtype=torch.int32, device=DEV)
+    lib = L.load()
+    for cc, want in ((m2.c2c, 0), (c2c, 1)):
+        ll = torch.from_numpy(np.ascontiguousarray(m2.c_pos_ll.T)).to(DEV)
+        nb = torch.from_numpy(np.ascontiguousarray(cc.T)).to(DEV)
+        L.check("pack", lib.oppb_advec_pack_cells(cells.data_ptr(), 0, m2.n_cells, m2.n_cells, ll.data_ptr(),
+                                                  nb.data_ptr(), None))
+        L.check("check", lib.oppb_advec_check_grid(cells.data_ptr(), 0, m2.n_cells, m2.nx, m2.cell_width,
+                                                   mism.data_ptr(), None))
+        assert int(mism.item()) == want
+    with pytest.raises(L.OppbError):  # n_cells not a multiple of nx
+        L.check("check", lib.oppb_advec_check_grid(cells.data_ptr(), 0, m2.n_cells, 7, m2.cell_width,
+                                                   mism.data_ptr(), None))
