@@ -27,7 +27,12 @@ extern "C" {
  * (:178-210: NORMAL and OPEN nodes are unknowns, numbered in node order; INLET and FIXED
  * nodes are Dirichlet), pre_assembly (:330-391: K and F0 from 2x2x2 Gauss points, both
  * scaled by 1/SCALLING^2) and enrich_cell_shape_deriv (:474-499: c_sd = NX / SCALLING).
- * K is CSR over the unknowns with columns ascending in each row.  Arrays are malloc-owned. */
+ * K is CSR over the unknowns with columns ascending in each row.  Arrays are malloc-owned.
+ * When K's entries lie on at most OPPB_FIELD_MAX_DIAG diagonals (column - row offsets) that
+ * hold no more than 1.5 nnz values in all, K is also given by diagonals: dia_val[j * neq + r] =
+ * K[r][r + dia_off[j]] (0 where K has no entry), offsets ascending; else n_diag = 0.  A box
+ * mesh in node order has 15 diagonals. */
+#define OPPB_FIELD_MAX_DIAG 16
 typedef struct oppb_field_system {
     int32_t  n_nodes, n_cells, neq;
     int32_t* node_to_eq;   /* [n_nodes] equation of a node, -1 for a Dirichlet node        */
@@ -40,6 +45,9 @@ typedef struct oppb_field_system {
     double*  k_val;        /* [nnz]                                                         */
     double*  f0;           /* [neq]                                                         */
     int64_t  nnz;
+    int32_t  n_diag;                        /* 0 = no diagonal form                      */
+    int32_t  dia_off[OPPB_FIELD_MAX_DIAG];
+    double*  dia_val;                       /* [n_diag][neq], or NULL                    */
 } oppb_field_system;
 
 int oppb_field_setup(const oppb_fempic_mesh* mesh, oppb_field_system* out);
@@ -69,6 +77,9 @@ typedef struct oppb_field_device {
     double* d;                /* [neq] Newton iterate D (dLocal), zero at start            */
     double* f1;               /* [neq] F1, accumulated over calls as the reference's f1Local */
     double* work;             /* oppb_field_work_doubles(neq) doubles                       */
+    int32_t n_diag;           /* K by diagonals (oppb_field_system), 0 = CSR only: the CG's */
+    int32_t dia_off[OPPB_FIELD_MAX_DIAG]; /* products then read the diagonals, coalesced   */
+    const double* dia_val;    /* [n_diag][neq]; the same sums, term by term in column order */
 } oppb_field_device;
 
 /* Doubles of work space a device system needs. */

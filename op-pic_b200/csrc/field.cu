@@ -53,6 +53,10 @@ struct FieldArgs {
     // constants
     double n0, phi0, kte, qe, eps0, rtol, atol;
     int32_t max_iter;
+    // K by diagonals (n_diag > 0): dia_val[j * neq + r] = K[r][r + dia_off[j]], offsets ascending.
+    int32_t n_diag;
+    int32_t dia_off[OPPB_FIELD_MAX_DIAG];
+    const double* dia_val;
 };
 
 // Sum of v over the block, returned to every thread (fixed order: deterministic).
@@ -92,6 +96,23 @@ __device__ __forceinline__ double shape_na(int a, int i, int j, int k) {
 // rewritten between grid barriers).
 template <bool kDiag>
 __device__ __forceinline__ double row_dot(const FieldArgs& a, int64_t u, double du, const double* v) {
+    if (a.n_diag > 0) {
+        // By diagonals: neighbouring rows read neighbouring values of every diagonal and of v,
+        // so a warp's loads are coalesced.  Offsets ascend, so the nonzero terms are added in
+        // the CSR row's column order; the zeros of a diagonal where the row has no entry add
+        // +0 or -0 to a sum that starts at +0 and so is never -0, which leaves it unchanged.
+        double s = 0.0;
+#pragma unroll 4
+        for (int j = 0; j < a.n_diag; j++) {
+            const int32_t off = a.dia_off[j];
+            const int64_t c = u + off;
+            double kv = __ldg(a.dia_val + (int64_t)j * a.neq + u);
+            if (kDiag && off == 0) kv = du;
+            const double vc = (c >= 0 && c < a.neq) ? v[c] : 0.0;
+            s += kv * vc;
+        }
+        return s;
+    }
     int64_t k = __ldg(a.k_rowptr + u);
     const int64_t end = __ldg(a.k_rowptr + u + 1);
     double s = 0.0;
@@ -403,6 +424,10 @@ extern "C" int oppb_field_solve(const oppb_field_device* f, const oppb_field_con
     a.partial_b = w + 8 * n + kMaxCoopBlocks;
     a.n0 = c->n0, a.phi0 = c->phi0, a.kte = c->kte, a.qe = c->qe, a.eps0 = c->eps0;
     a.rtol = c->rtol, a.atol = c->atol, a.max_iter = c->max_iter;
+    if (f->n_diag < 0 || f->n_diag > OPPB_FIELD_MAX_DIAG || (f->n_diag > 0 && !f->dia_val)) return OPPB_ERR_ARG;
+    a.n_diag = f->n_diag;
+    for (int j = 0; j < OPPB_FIELD_MAX_DIAG; j++) a.dia_off[j] = f->dia_off[j];
+    a.dia_val = f->dia_val;
     void* args[] = {&a};
     if (cudaLaunchCooperativeKernel((const void*)field_newton_kernel, dim3(blocks), dim3(kFieldBlock), args, 0,
                                     as_stream(stream)) != cudaSuccess)

@@ -157,6 +157,32 @@ extern "C" int oppb_field_setup(const oppb_fempic_mesh* mp, oppb_field_system* o
     s.k_rowptr[neq] = at;
     s.nnz = nnz;
     for (int32_t r = 0; r < neq; r++) s.f0[r] *= scalar2;
+    // The diagonal form, when K's entries lie on few diagonals.
+    std::vector<int32_t> offs;
+    bool banded = true;
+    for (int32_t r = 0; r < neq && banded; r++)
+        for (int64_t k = s.k_rowptr[r]; k < s.k_rowptr[r + 1]; k++) {
+            const int32_t o = s.k_col[k] - r;
+            if (std::find(offs.begin(), offs.end(), o) == offs.end()) {
+                if ((int)offs.size() == OPPB_FIELD_MAX_DIAG) {
+                    banded = false;
+                    break;
+                }
+                offs.push_back(o);
+            }
+        }
+    if (banded && !offs.empty() && (double)offs.size() * neq <= 1.5 * (double)nnz) {
+        std::sort(offs.begin(), offs.end());
+        s.n_diag = (int32_t)offs.size();
+        for (int j = 0; j < s.n_diag; j++) s.dia_off[j] = offs[(size_t)j];
+        s.dia_val = alloc<double>((size_t)s.n_diag * neq);
+        for (int64_t q = 0; q < (int64_t)s.n_diag * neq; q++) s.dia_val[q] = 0.0;
+        for (int32_t r = 0; r < neq; r++)
+            for (int64_t k = s.k_rowptr[r]; k < s.k_rowptr[r + 1]; k++) {
+                const int j = (int)(std::lower_bound(offs.begin(), offs.end(), s.k_col[k] - r) - offs.begin());
+                s.dia_val[(int64_t)j * neq + r] = s.k_val[k];
+            }
+    }
     *out = s;
     return OPPB_OK;
 }
@@ -172,5 +198,6 @@ extern "C" void oppb_field_system_free(oppb_field_system* s) {
     std::free(s->k_col);
     std::free(s->k_val);
     std::free(s->f0);
+    std::free(s->dia_val);
     *s = oppb_field_system{};
 }

@@ -80,6 +80,9 @@ FESolver::FESolver(const opp_map c2n_map, const opp_dat n_type, const opp_dat n_
     d.k_col = I.keep(upload(s.k_col, nnz));
     d.k_val = I.keep(upload(s.k_val, nnz));
     d.f0 = I.keep(upload(s.f0, neq));
+    d.n_diag = s.n_diag;
+    for (int j = 0; j < OPPB_FIELD_MAX_DIAG; j++) d.dia_off[j] = s.dia_off[j];
+    d.dia_val = s.n_diag > 0 ? I.keep(upload(s.dia_val, (size_t)s.n_diag * neq)) : nullptr;
     oppb_field_system_free(&s);  // s is zeroed: sizes below come from the copies taken above
     const std::vector<double> zeros(neq ? neq : 1, 0.0);
     d.d = I.keep(upload(zeros.data(), zeros.size()));   // D (dLocal) starts at 0

@@ -116,7 +116,8 @@ class MoveOptions(C.Structure):
 class FieldSystem(C.Structure):
     _fields_ = [("n_nodes", c_i32), ("n_cells", c_i32), ("neq", c_i32), ("node_to_eq", c_ip), ("c2n", c_ip),
                 ("det_j", c_dp), ("c_sd", c_dp), ("n_bnd_pot", c_dp), ("k_rowptr", C.POINTER(c_i64)),
-                ("k_col", c_ip), ("k_val", c_dp), ("f0", c_dp), ("nnz", c_i64)]
+                ("k_col", c_ip), ("k_val", c_dp), ("f0", c_dp), ("nnz", c_i64), ("n_diag", c_i32),
+                ("dia_off", c_i32 * 16), ("dia_val", c_dp)]
 
 
 class FieldConsts(C.Structure):
@@ -128,7 +129,8 @@ class FieldConsts(C.Structure):
 class FieldDevice(C.Structure):
     _fields_ = [("n_nodes", c_i32), ("n_cells", c_i32), ("neq", c_i32), ("reserved", c_i32),
                 ("node_to_eq", c_vp), ("c2n", c_vp), ("det_j", c_vp), ("n_bnd_pot", c_vp), ("k_rowptr", c_vp),
-                ("k_col", c_vp), ("k_val", c_vp), ("f0", c_vp), ("d", c_vp), ("f1", c_vp), ("work", c_vp)]
+                ("k_col", c_vp), ("k_val", c_vp), ("f0", c_vp), ("d", c_vp), ("f1", c_vp), ("work", c_vp),
+                ("n_diag", c_i32), ("dia_off", c_i32 * 16), ("dia_val", c_vp)]
 
 
 class FieldStatus(C.Structure):

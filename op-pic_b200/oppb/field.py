@@ -52,7 +52,8 @@ def _ptr(t: torch.Tensor | None) -> int | None:
 
 def host_system(hm, n_bnd_pot: np.ndarray) -> dict:
     """FESolver's set-up on the host (oppb_field_setup): node_to_eq, det_j, c_sd [nc][4][3],
-    K as CSR (k_rowptr, k_col, k_val) and f0, as numpy arrays."""
+    K as CSR (k_rowptr, k_col, k_val), K by diagonals when banded (dia_off [n_diag],
+    dia_val [n_diag][neq]; n_diag = 0 otherwise) and f0, as numpy arrays."""
     lib = L.load()
     n_pos = np.ascontiguousarray(hm.n_pos, np.float64)
     n_type = np.ascontiguousarray(hm.n_type, np.int32)
@@ -76,7 +77,10 @@ def host_system(hm, n_bnd_pot: np.ndarray) -> dict:
                 "node_to_eq": take(sys_.node_to_eq, nn, np.int32), "det_j": take(sys_.det_j, nc, np.float64),
                 "c_sd": take(sys_.c_sd, nc * 12, np.float64).reshape(nc, 4, 3),
                 "k_rowptr": take(sys_.k_rowptr, neq + 1, np.int64), "k_col": take(sys_.k_col, nnz, np.int32),
-                "k_val": take(sys_.k_val, nnz, np.float64), "f0": take(sys_.f0, neq, np.float64)}
+                "k_val": take(sys_.k_val, nnz, np.float64), "f0": take(sys_.f0, neq, np.float64),
+                "dia_off": np.array(list(sys_.dia_off)[:sys_.n_diag], np.int32),
+                "dia_val": take(sys_.dia_val, sys_.n_diag * neq, np.float64).reshape(sys_.n_diag, neq)
+                if sys_.n_diag else np.zeros((0, neq))}
     finally:
         lib.oppb_field_system_free(C.byref(sys_))
 
@@ -104,9 +108,20 @@ class FieldDevice:
         self.work = torch.zeros(int(lib.oppb_field_work_doubles(neq)), dtype=torch.float64, device=dev)
         self.status = torch.zeros(3, dtype=torch.float64, device=dev)        # oppb_field_status (24 B)
         self.potential = torch.zeros(nn, dtype=torch.float64, device=dev)
+        self.dia_off = h["dia_off"]
+        self.d_dia = t(h["dia_val"]) if len(self.dia_off) else None
         self.s = L.FieldDevice(nn, nc, neq, 0, _ptr(self.d_node_to_eq), _ptr(self.d_c2n), _ptr(self.d_det_j),
                                _ptr(self.d_bnd), _ptr(self.d_rowptr), _ptr(self.d_col), _ptr(self.d_val),
                                _ptr(self.d_f0), _ptr(self.d), _ptr(self.f1), _ptr(self.work))
+        self.set_diagonal_form(True)
+
+    def set_diagonal_form(self, on: bool) -> None:
+        """Whether the CG's products read K by diagonals (when K has that form) or as CSR."""
+        n = len(self.dia_off) if on and self.d_dia is not None else 0
+        self.s.n_diag = n
+        for j in range(16):
+            self.s.dia_off[j] = int(self.dia_off[j]) if j < n else 0
+        self.s.dia_val = _ptr(self.d_dia) if n else None
 
     @staticmethod
     def _stream(stream):

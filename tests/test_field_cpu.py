@@ -38,6 +38,20 @@ def test_setup_matches_oracle(dims):
     assert abs(k - k.T).max() <= 1e-12 * abs(k).max()
     assert (o.det_j < 0).all() and (k.diagonal() < 0).all()
     np.testing.assert_allclose(o.c_sd.sum(axis=1), 0.0, atol=1e-9 * np.abs(o.c_sd).max())
+    # K by diagonals: the box mesh's K lies on 15 diagonals (the form is kept when they hold at
+    # most 1.5 nnz values, so not on the smallest mesh), and the diagonal form holds K's entries
+    # at their offsets and zeros elsewhere
+    off, dia = h["dia_off"], h["dia_val"]
+    if 15 * h["neq"] > 1.5 * h["nnz"]:
+        assert len(off) == 0
+        return
+    assert len(off) == 15 and np.all(np.diff(off) > 0) and dia.shape == (15, h["neq"])
+    dense_from_dia = np.zeros_like(dia)
+    rows = np.repeat(np.arange(h["neq"]), np.diff(h["k_rowptr"]))
+    j = np.searchsorted(off, h["k_col"] - rows)
+    assert np.all(off[j] == h["k_col"] - rows)
+    dense_from_dia[j, rows] = h["k_val"]
+    np.testing.assert_array_equal(dia.view(np.uint64), dense_from_dia.view(np.uint64))
 
 
 def test_loops_match_reference_golden():

@@ -109,6 +109,30 @@ def test_solve_repeats_and_graph_replay():
         _close(ef, out[0][1], 1e-11)
 
 
+@pytest.mark.parametrize("dims", [(8, 8, 24, 1.0, 1.0, 3.0), (48, 48, 192, 1.0, 1.0, 4.0)])
+def test_diagonal_form_equals_csr(dims):
+    """The CG's products by diagonals add the same terms in the same order as the CSR rows, so
+    one Newton step from the same state agrees with the CSR one as two CSR solves agree with
+    each other (the F1 / J-diagonal atomics reorder between runs): same iteration count within
+    one, potential within 1e-12."""
+    hm = HostMesh(*dims, solve_field=False)
+    bnd = boundary_potential(hm.n_type, 1.0, 0.0)
+    rng = np.random.default_rng(3)
+    ion = torch.from_numpy(rng.random(hm.n_nodes)).to(DEV)
+    c = FieldConstants(n0=50.0, phi0=0.0, kte=1.0, qe=1.0, eps0=1.0)
+    out = []
+    for diag in (False, True):
+        fd = FieldDevice(hm, DEV, bnd)
+        assert len(fd.dia_off) == 15
+        fd.set_diagonal_form(diag)
+        pot = fd.solve(ion, c).cpu().numpy()
+        st = fd.status_host()
+        assert st.converged == 1
+        out.append((pot, st.iterations))
+    assert abs(out[0][1] - out[1][1]) <= 1 and out[0][1] > 10
+    _close(out[1][0], out[0][0], 1e-12)
+
+
 def test_full_size_solve_matches_oracle():
     """The 48x48x192-hex mesh (463,393 nodes): one Newton step against the oracle."""
     hm = HostMesh(48, 48, 192, 1.0, 1.0, 4.0, solve_field=False)
