@@ -1,7 +1,8 @@
 """Edge cases of the particle entry points: an empty particle set through every launcher (each
 returns OPPB_OK, leaves the move status and the node charges at zero and launches nothing
 that writes), a cell sort whose keys need a fourth radix pass and one whose keys fit one
-bit, and hole fills whose holes sit only at the tail or only at the head."""
+bit, hole fills whose holes sit only at the tail or only at the head, and one over more bitmap
+blocks than one pass of the single-block scan takes."""
 from __future__ import annotations
 
 import ctypes as C
@@ -139,3 +140,35 @@ def test_hole_fill_holes_at_one_end(where):
     for k, name in enumerate(("pos", "vel", "lc", "p2c")):
         np.testing.assert_array_equal(got[name][: n - r].view(np.uint8), dats[k][: n - r].view(np.uint8),
                                       err_msg=name)
+
+
+def test_hole_fill_many_bitmap_blocks():
+    """A hole fill over 70M particles: more bitmap blocks (4,273 of 16,384 particles) than the
+    single-block scan takes in one 4,096-value pass, so the block counts are scanned in two
+    passes.  Two int32 dats (the cells and each particle's index) against the pairing rule:
+    the k-th hole in ascending order takes the k-th live particle from the back while that one
+    lies behind it."""
+    n, r = 70_000_003, 7_001
+    rng = np.random.default_rng(21)
+    holes = np.sort(rng.choice(n, r, replace=False))
+    p2c = (np.arange(n, dtype=np.int64) % 1000).astype(np.int32)
+    p2c[holes] = REMOVED
+    ident = np.arange(n, dtype=np.int32)
+    bits = np.packbits((p2c == REMOVED).astype(np.uint8), bitorder="little")
+    words = np.zeros((n + 31) // 32 * 4, np.uint8)
+    words[: len(bits)] = bits
+    d_p2c, d_ident = torch.from_numpy(p2c).to(DEV), torch.from_numpy(ident).to(DEV)
+    d_bits = torch.from_numpy(words.view(np.int32)).to(DEV)
+    dats = (L.Dat * 2)(L.Dat(d_p2c.data_ptr(), None, 1, 4), L.Dat(d_ident.data_ptr(), None, 1, 4))
+    lib = L.load()
+    ws = _ws(lib.oppb_hole_fill_workspace_bytes(n, r))
+    L.check("hole_fill", lib.oppb_hole_fill(n, r, d_bits.data_ptr(), n, 2, dats, ws.data_ptr(), ws.numel(), None))
+    got_p2c, got_ident = d_p2c.cpu().numpy(), d_ident.cpu().numpy()
+    live_back = np.flatnonzero(p2c != REMOVED)[::-1][:r]
+    keep = live_back > holes
+    want_p2c, want_ident = p2c.copy(), ident.copy()
+    want_p2c[holes[keep]] = p2c[live_back[keep]]
+    want_ident[holes[keep]] = ident[live_back[keep]]
+    np.testing.assert_array_equal(got_p2c[: n - r], want_p2c[: n - r])
+    np.testing.assert_array_equal(got_ident[: n - r], want_ident[: n - r])
+    assert not (got_p2c[: n - r] == REMOVED).any()
