@@ -252,6 +252,12 @@ opp_set opp_decl_particle_set(int size, char const* name, opp_set cells_set);
 opp_set opp_decl_particle_set(char const* name, opp_set cells_set);
 opp_map opp_decl_map(opp_set from, opp_set to, int dim, int* imap, char const* name);
 opp_dat opp_decl_dat(opp_set set, int dim, opp_data_type dtype, void* data, char const* name);
+// From a text file: a "size dim" header, then `size` rows of `dim` values (at least the set's
+// size rows; dim 1-4 for int, 1-4 or 16 for double), as opp_load_from_file_core reads it
+// (opp_lib/src/core/opp_lib_file_core.cpp:180-281; opp_lib/src/cuda/opp_cuda.cu:361-385).
+// A missing or malformed file ends the program with status -1, as there.
+opp_map opp_decl_map_txt(opp_set from, opp_set to, int dim, const char* file_name, char const* name);
+opp_dat opp_decl_dat_txt(opp_set set, int dim, opp_data_type dtype, const char* file_name, char const* name);
 
 void opp_decl_const_impl(int dim, int size, char* data, const char* name);
 template <typename T>
@@ -303,12 +309,36 @@ T* opp_get_data(opp_dat dat) {
     return (T*)dat->data;
 }
 OPP_INT* opp_get_data(opp_map map);
+// Text dumps in the reference CUDA backend's format and place (opp_lib/src/cuda/opp_cuda.cu:458-481,
+// opp_lib/src/core/opp_lib_file_core.cpp:35-178): files/<prefix>_cuda_<suffix> for a dat and
+// files/<prefix>_cuda0__<suffix> for a map, a "size dim -- exec nonexec" header, one row per
+// element (" %2.25lE" per double, -0 written, and left in the host copy, as +0; " %d" per
+// int), then the two import_exec_below / import_non_exec_below marker lines.  A file that
+// cannot be opened ends the program with status 2, as there.
 void opp_print_dat_to_txtfile(opp_dat dat, const char* file_prefix, const char* file_suffix);
+void opp_print_map_to_txtfile(opp_map map, const char* file_prefix, const char* file_suffix);
+// The dat's values on stdout (opp_dump_dat_core, opp_lib_file_core.cpp:103-131): "\t %+2.25lE"
+// per double and a "\t\n" per row.  The reference names its other dump types "real" and
+// "integer", so an int dat ends the program there (message, status 0); it does here too.
+void opp_dump_dat(opp_dat data);
+// The dat with its host copy current (opp_cuda.cu:484-499); particle dats are refused.
+opp_dat opp_fetch_data(opp_dat dat);
 
-// One-GPU build: halo exchanges and global reductions are identities.
+// One-GPU build: halo exchanges, double-indirect reductions and mesh colouring are identities
+// (the reference defines them only for MPI builds, opp_lib/src/mpi/).
 int opp_mpi_halo_exchanges_grouped(opp_set set, int nargs, opp_arg* args, DeviceType device);
+int opp_mpi_halo_exchanges(opp_set set, int nargs, opp_arg* args);
+void opp_mpi_halo_exchange(opp_arg* arg, int exec_flag);
 void opp_mpi_halo_wait_all(int nargs, opp_arg* args);
+void opp_mpi_force_halo_update_if_dirty(opp_set set, std::vector<opp_dat> dats, DeviceType device);
 void opp_set_dirtybit_grouped(int nargs, opp_arg* args, DeviceType device);
+// An OPP_INC through a particle's cell map (opp_lib/src/mpi/opp_mpi_utils.cpp:537-544).
+bool is_double_indirect_reduction(opp_arg& arg);
+void opp_init_double_indirect_reductions(int nargs, opp_arg* args);
+void opp_exchange_double_indirect_reductions(int nargs, opp_arg* args);
+void opp_complete_double_indirect_reductions(int nargs, opp_arg* args);
+void opp_colour_cartesian_mesh(const int ndim, std::vector<int> cell_counts, opp_dat cell_index,
+                               const opp_dat cell_colors, const int cell_ghosts = 0);
 inline int64_t opp_get_global_value(int64_t value) { return value; }
 // Sum, maximum and minimum over ranks (opp_util.h:274): on one GPU, the value three times.
 inline void opp_get_global_values(const int64_t value, int64_t& gbl_value, int64_t& gbl_max, int64_t& gbl_min) {

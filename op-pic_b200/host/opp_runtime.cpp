@@ -371,14 +371,61 @@ opp_dat new_dat(opp_set set, int dim, const char* type, int elem, const char* na
 opp_dat opp_decl_dat(opp_set set, int dim, opp_data_type dtype, void* data, char const* name) {
     const bool is_int = (dtype == DT_INT);
     opp_dat d = new_dat(set, dim, is_int ? "int" : "double", is_int ? 4 : 8, name);
-    if (data && !set->is_particle) {
-        std::memcpy(d->data, data, (size_t)set->size * d->size);
-        upload(d, set->size);
-    } else if (data) {
+    if (data) {
         std::memcpy(d->data, data, (size_t)set->size * d->size);
         upload(d, set->size);
     }
     return d;
+}
+
+namespace {
+// `rows` rows of `dim` values from a text file with a "size dim" header (size >= rows), as
+// opp_load_from_file_core reads it: the dims it has formats for (int 1-4, double 1-4 and 16);
+// a missing file, a header that does not fit or a value that does not parse ends the program
+// with status -1 after the reference's message.
+std::vector<char> load_txt(const char* file_name, int rows, int dim, bool is_double) {
+    std::FILE* fp = std::fopen(file_name, "r");
+    if (!fp) {
+        std::printf("\topp_load_from_file - Unable to open file %s\n", file_name);
+        std::exit(-1);
+    }
+    int fsize = -1, fdim = -1;
+    if (std::fscanf(fp, "%d %d\n", &fsize, &fdim) != 2) {
+        std::printf("\topp_load_from_file - error reading file data from %s\n", file_name);
+        std::exit(-1);
+    }
+    if (fsize < rows || fdim != dim) {
+        std::printf("\topp_load_from_file - dim and/or set_size issue in file %s\n", file_name);
+        std::exit(-1);
+    }
+    const bool dim_ok = (dim >= 1 && dim <= 4) || (is_double && dim == 16);
+    std::vector<char> out((size_t)std::max(rows, 1) * std::max(dim, 1) * (is_double ? 8 : 4));
+    for (int n = 0; n < rows; n++) {
+        bool ok = dim_ok;
+        for (int j = 0; ok && j < dim; j++) {
+            const size_t k = (size_t)n * dim + j;
+            ok = is_double ? std::fscanf(fp, " %lf", reinterpret_cast<double*>(out.data()) + k) == 1
+                           : std::fscanf(fp, " %d", reinterpret_cast<int*>(out.data()) + k) == 1;
+        }
+        if (!ok) {
+            opp_printf("opp_load_from_file", "Error reading %s from %s at index %d", is_double ? "Double" : "Int",
+                       file_name, n);
+            std::exit(-1);
+        }
+    }
+    std::fclose(fp);
+    return out;
+}
+}  // namespace
+
+opp_dat opp_decl_dat_txt(opp_set set, int dim, opp_data_type dtype, const char* file_name, char const* name) {
+    std::vector<char> v = load_txt(file_name, set->size, dim, dtype != DT_INT);
+    return opp_decl_dat(set, dim, dtype, v.data(), name);
+}
+
+opp_map opp_decl_map_txt(opp_set from, opp_set to, int dim, const char* file_name, char const* name) {
+    std::vector<char> v = load_txt(file_name, from->size, dim, false);
+    return opp_decl_map(from, to, dim, reinterpret_cast<int*>(v.data()), name);
 }
 
 opp_map opp_decl_map(opp_set from, opp_set to, int dim, int* imap, char const* name) {
@@ -703,21 +750,95 @@ OPP_INT* opp_get_data(opp_map map) {
     return map->map;
 }
 
-void opp_print_dat_to_txtfile(opp_dat dat, const char* prefix, const char* suffix) {
-    opp_download_dat(dat);
-    const std::string file = std::string(prefix) + "_" + suffix;
+namespace {
+// opp_print_dat_to_txtfile_core / opp_print_map_to_txtfile_core's file: files/<prefix>_<suffix>,
+// the header, `rows` rows written by row(fp, i), and the marker lines after the set's own rows
+// and after its exec halo (both after the last row on one GPU, where the halos are empty).
+template <class Row>
+void write_txt(const std::string& prefix, const char* suffix, int size, int dim, int exec, int nonexec, int rows,
+               Row row) {
+    const std::string file = "files/" + prefix + "_" + suffix;
     std::FILE* f = std::fopen(file.c_str(), "w");
-    if (!f) opp_abort("cannot write " + file);
-    std::fprintf(f, "%d %d -- %d %d\n", dat->set->size, dat->dim, dat->set->size, 0);
-    const bool is_int = std::strcmp(dat->type, "int") == 0;
-    for (int i = 0; i < dat->set->size; i++) {
-        for (int d = 0; d < dat->dim; d++) {
-            if (is_int) std::fprintf(f, " %d", reinterpret_cast<int*>(dat->data)[(size_t)i * dat->dim + d]);
-            else std::fprintf(f, " %2.25lE", reinterpret_cast<double*>(dat->data)[(size_t)i * dat->dim + d]);
-        }
+    if (!f) {
+        opp_printf("opp_print_dat_to_txtfile_core", "can't open file %s\n", file.c_str());
+        std::exit(2);
+    }
+    std::fprintf(f, "%d %d -- %d %d\n", size, dim, exec, nonexec);
+    for (int i = 0; i < rows; i++) {
+        row(f, i);
         std::fprintf(f, "\n");
+        if (i + 1 == size) std::fprintf(f, "import_exec_below ****************************************\n");
+        if (i + 1 == size + exec) std::fprintf(f, "import_non_exec_below ****************************************\n");
     }
     std::fclose(f);
+}
+
+void print_dat_txt(opp_dat dat, const std::string& prefix, const char* suffix) {
+    opp_set s = dat->set;
+    const bool is_double = std::strcmp(dat->type, "double") == 0;
+    write_txt(prefix, suffix, s->size, dat->dim, s->exec_size, s->nonexec_size,
+              s->size + s->exec_size + s->nonexec_size, [&](std::FILE* f, int i) {
+                  for (int j = 0; j < dat->dim; j++) {
+                      const size_t k = (size_t)i * dat->dim + j;
+                      if (is_double) {
+                          // -0 is written, and left in the host copy, as +0 (as the reference does)
+                          double& v = reinterpret_cast<double*>(dat->data)[k];
+                          if (v == 0.0) v = 0.0;
+                          std::fprintf(f, " %2.25lE", v);
+                      } else {
+                          std::fprintf(f, " %d", reinterpret_cast<const int*>(dat->data)[k]);
+                      }
+                  }
+              });
+}
+}  // namespace
+
+void opp_print_dat_to_txtfile(opp_dat dat, const char* prefix, const char* suffix) {
+    opp_download_dat(dat);
+    print_dat_txt(dat, std::string(prefix) + "_cuda", suffix);
+}
+
+void opp_print_map_to_txtfile(opp_map map, const char* prefix, const char* suffix) {
+    const std::string pre = std::string(prefix) + "_cuda0_";
+    if (map->from->is_particle) {  // the mesh relation dat, its device copy brought back first
+        opp_download_dat(map->p2c_dat);
+        print_dat_txt(map->p2c_dat, pre, suffix);
+        return;
+    }
+    opp_set s = map->from;
+    write_txt(pre, suffix, s->size, map->dim, s->exec_size, s->nonexec_size, s->size + s->exec_size,
+              [&](std::FILE* f, int i) {
+                  for (int j = 0; j < map->dim; j++) std::fprintf(f, " %d", map->map[(size_t)i * map->dim + j]);
+              });
+}
+
+void opp_dump_dat(opp_dat dat) {
+    check_cuda(cudaStreamSynchronize(rt().stream), "dump sync");
+    opp_download_dat(dat);
+    std::fflush(stdout);
+    if (dat) {
+        const bool is_double = std::strncmp("double", dat->type, 6) == 0;
+        for (int i = 0; i < dat->set->size; i++) {
+            for (int j = 0; j < dat->dim; j++) {
+                if (!is_double) {
+                    std::printf("\topp_dump_dat_core Unsupported type for dumping %s\n", dat->type);
+                    std::exit(0);
+                }
+                std::printf("\t %+2.25lE", reinterpret_cast<const double*>(dat->data)[(size_t)i * dat->dim + j]);
+            }
+            std::printf("\t\n");
+        }
+    }
+    std::fflush(stdout);
+}
+
+opp_dat opp_fetch_data(opp_dat dat) {
+    if (dat->set->is_particle) {
+        opp_printf("opp_fetch_data", "Error Cannot rearrange particle dats");
+        opp_abort();
+    }
+    opp_download_dat(dat);
+    return dat;
 }
 
 int opp_mpi_halo_exchanges_grouped(opp_set, int nargs, opp_arg* args, DeviceType) {
@@ -725,7 +846,22 @@ int opp_mpi_halo_exchanges_grouped(opp_set, int nargs, opp_arg* args, DeviceType
         if (args[i].argtype == OPP_ARG_DAT && args[i].dat) oppb_rt::sync_host_to_device(args[i].dat);
     return 0;
 }
+int opp_mpi_halo_exchanges(opp_set set, int nargs, opp_arg* args) {
+    opp_mpi_halo_exchanges_grouped(set, nargs, args, Device_GPU);
+    return set->size;
+}
+void opp_mpi_halo_exchange(opp_arg*, int) {}
 void opp_mpi_halo_wait_all(int, opp_arg*) {}
+void opp_mpi_force_halo_update_if_dirty(opp_set, std::vector<opp_dat> dats, DeviceType) {
+    for (opp_dat d : dats) oppb_rt::sync_host_to_device(d);
+}
+bool is_double_indirect_reduction(opp_arg& arg) {
+    return arg.argtype == OPP_ARG_DAT && arg.p2c_map != nullptr && arg.idx != -1 && arg.acc == OPP_INC;
+}
+void opp_init_double_indirect_reductions(int, opp_arg*) {}
+void opp_exchange_double_indirect_reductions(int, opp_arg*) {}
+void opp_complete_double_indirect_reductions(int, opp_arg*) {}
+void opp_colour_cartesian_mesh(const int, std::vector<int>, opp_dat, const opp_dat, const int) {}
 void opp_set_dirtybit_grouped(int nargs, opp_arg* args, DeviceType) {
     for (int i = 0; i < nargs; i++)
         if (args[i].argtype == OPP_ARG_DAT && args[i].dat && args[i].acc != OPP_READ)
