@@ -236,6 +236,26 @@ extern int OPP_move_max_hops;       // bound on cell visits per particle and mov
 extern int OPP_max_comm_iteration;
 extern int OPP_part_comm_count_per_iter;
 extern int OPP_move_moreX_hops;
+// The rest of opp_defs.h:417-450 with the reference's defaults (opp_lib_core.cpp:45-69).
+// OPP_maps_base_index = 1 makes opp_decl_map take 1-based maps (each entry less 1 on
+// declaration); OPP_gpu_threads_per_block holds the parameter file's opp_threads_per_block and
+// OPP_gpu_direct its opp_gpu_direct (informational: the kernels' launch shapes come from
+// oppb_tuning); OPP_mpi_part_alloc_mult and OPP_dh_data_dump are set from the command line
+// (OPP_MPI_ALLOC_MULT=, OPP_DH_DATA_DUMP=) as there; the others stay at their one-rank values.
+extern double OPP_hybrid_balance;
+extern int OPP_maps_base_index;
+extern int OPP_auto_soa;
+extern int OPP_gpu_direct;
+extern int OPP_mpi_part_alloc_mult;
+extern int* OPP_mesh_relation_data;
+extern int* OPP_mesh_relation_data_d;
+extern int OPP_gpu_threads_per_block;
+extern size_t OPP_gpu_shared_mem_per_block;
+extern int OPP_part_cells_set_size;
+extern bool OPP_dh_data_dump;
+extern bool useGlobalMove;  // set by opp_init_direct_hop_cg when opp_global_move is on
+extern size_t opp_maxSavedDHGrid[3];
+extern size_t opp_minSavedDHGrid[3];
 extern std::vector<opp_set> opp_sets;
 extern std::vector<opp_map> opp_maps;
 extern std::vector<opp_dat> opp_dats;

@@ -169,7 +169,8 @@ void opp_init_direct_hop_cg(double grid_spacing, const opp_dat c_gbl_id, const o
                             opp_map c2c_map, opp_map p2c_map, opp_arg arg0, opp_arg arg1, opp_arg arg2,
                             opp_arg arg3) {
     (void)p2c_map, (void)arg0, (void)arg1;
-    if (!opp_params->get<OPP_BOOL>("opp_global_move")) return;
+    useGlobalMove = opp_params->get<OPP_BOOL>("opp_global_move");
+    if (!useGlobalMove) return;
     opp_profiler->start("Setup_Mover");
     opp_set cells = c2c_map->from;
     if (c_gbl_id) {

@@ -24,13 +24,29 @@ int OPP_main_loop_iter = 0;
 int OPP_comm_iteration = 0;
 int OPP_max_comm_iteration = 0;
 int OPP_part_comm_count_per_iter = 0;
-int OPP_move_moreX_hops = 0;
-int OPP_fill_period = 4;
+int OPP_move_moreX_hops = -1;
+int OPP_fill_period = 2;
 opp_fill_type OPP_fill_type = OPP_HoleFill_All;
 double OPP_part_alloc_mult = 1.0;
 int OPP_iter_start = 0;
 int OPP_iter_end = 0;
+// The reference's -1 leaves its walks unbounded; a kernel here stops a walk after this many
+// cell visits and reports OPPB_ERR_HOP_LIMIT (opp_move_max_hops in the parameter file sets it).
 int OPP_move_max_hops = 4096;
+double OPP_hybrid_balance = 1.0;
+int OPP_maps_base_index = 0;
+int OPP_auto_soa = 1;  // device dats are SoA, as the CUDA backend sets it in opp_init
+int OPP_gpu_direct = 0;
+int OPP_mpi_part_alloc_mult = 1;
+int* OPP_mesh_relation_data = nullptr;
+int* OPP_mesh_relation_data_d = nullptr;
+int OPP_gpu_threads_per_block = 32;  // OPP_DEFAULT_GPU_THREADS_PER_BLOCK
+size_t OPP_gpu_shared_mem_per_block = 0;
+int OPP_part_cells_set_size = 0;
+bool OPP_dh_data_dump = false;
+bool useGlobalMove = false;
+size_t opp_maxSavedDHGrid[3];
+size_t opp_minSavedDHGrid[3];
 std::vector<opp_set> opp_sets;
 std::vector<opp_map> opp_maps;
 std::vector<opp_dat> opp_dats;
@@ -246,8 +262,8 @@ void opp_init(int argc, char** argv) {
     else if (fill == "Sort_Periodic") OPP_fill_type = OPP_Sort_Periodic;
     else if (fill == "Shuffle_Periodic") OPP_fill_type = OPP_Shuffle_Periodic;
     else opp_abort("opp_fill " + fill + " is not a fill type");
-    if ((OPP_fill_type == OPP_Sort_Periodic || OPP_fill_type == OPP_Shuffle_Periodic) && period != INT_MAX &&
-        period >= 0)
+    // A missing opp_fill_period reads as INT_MAX, which the reference takes as the period too.
+    if ((OPP_fill_type == OPP_Sort_Periodic || OPP_fill_type == OPP_Shuffle_Periodic) && period >= 0)
         OPP_fill_period = period;
     const int hops = opp_params->get<OPP_INT>("opp_move_max_hops");
     if (hops != INT_MAX && hops > 0) OPP_move_max_hops = hops;
@@ -259,13 +275,30 @@ void opp_init(int argc, char** argv) {
         t.deposit = OPPB_DEPOSIT_EXACT;
         if (oppb_set_tuning(&t) != OPPB_OK) opp_abort("oppb_set_tuning");
     }
+    const int tpb = opp_params->get<OPP_INT>("opp_threads_per_block");
+    if (tpb > 0 && tpb < INT_MAX) OPP_gpu_threads_per_block = tpb;
+    const int gpu_direct = opp_params->get<OPP_INT>("opp_gpu_direct");
+    if (gpu_direct > 0 && gpu_direct < INT_MAX) OPP_gpu_direct = gpu_direct;
+    // opp_set_args_core (opp_lib_core.cpp:149-184): the first of its keys an argument holds.
     for (int n = 1; n < argc; n++) {
-        const char* p = std::strstr(argv[n], "OPP_ALLOC_MULT=");
-        if (p) OPP_part_alloc_mult = std::atof(p + 15);
+        char tmp[64] = {0};
+        if (const char* p = std::strstr(argv[n], "OPP_ALLOC_MULT=")) {
+            std::strncpy(tmp, p, 17);
+            OPP_part_alloc_mult = std::atof(tmp + 15);
+        } else if (const char* q = std::strstr(argv[n], "OPP_MPI_ALLOC_MULT=")) {
+            std::strncpy(tmp, q, 21);
+            OPP_mpi_part_alloc_mult = std::atoi(tmp + 19);
+        } else if (const char* r = std::strstr(argv[n], "OPP_DH_DATA_DUMP=")) {
+            std::strncpy(tmp, r, 18);
+            OPP_dh_data_dump = std::atoi(tmp + 17) != 0;
+        }
     }
     int devices = 0;
     if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) opp_abort("no CUDA device");
     check_cuda(cudaSetDevice(0), "cudaSetDevice");
+    cudaDeviceProp prop{};
+    check_cuda(cudaGetDeviceProperties(&prop, 0), "cudaGetDeviceProperties");
+    OPP_gpu_shared_mem_per_block = prop.sharedMemPerBlock;
     check_cuda(cudaStreamCreateWithFlags(&rt().stream, cudaStreamNonBlocking), "stream");
     rt().status = reinterpret_cast<oppb_move_status*>(dev_alloc(sizeof(oppb_move_status)));
     rt().invalid = reinterpret_cast<int32_t*>(dev_alloc(sizeof(int32_t)));
@@ -429,6 +462,14 @@ opp_map opp_decl_map_txt(opp_set from, opp_set to, int dim, const char* file_nam
 }
 
 opp_map opp_decl_map(opp_set from, opp_set to, int dim, int* imap, char const* name) {
+    // A 1-based map (OPP_maps_base_index = 1) is taken 0-based, as opp_decl_map_core does
+    // (opp_lib/src/core/opp_lib_core.cpp:261-264); the caller's array is not changed.
+    std::vector<int> rebased;
+    if (imap && OPP_maps_base_index == 1) {
+        rebased.assign(imap, imap + (size_t)from->size * dim);
+        for (int& v : rebased) v--;
+        imap = rebased.data();
+    }
     opp_map m = new opp_map_core{};
     m->index = (int)opp_maps.size();
     m->from = from;
@@ -814,9 +855,9 @@ void opp_print_map_to_txtfile(opp_map map, const char* prefix, const char* suffi
 
 void opp_dump_dat(opp_dat dat) {
     check_cuda(cudaStreamSynchronize(rt().stream), "dump sync");
-    opp_download_dat(dat);
     std::fflush(stdout);
     if (dat) {
+        opp_download_dat(dat);
         const bool is_double = std::strncmp("double", dat->type, 6) == 0;
         for (int i = 0; i < dat->set->size; i++) {
             for (int j = 0; j < dat->dim; j++) {
@@ -841,10 +882,17 @@ opp_dat opp_fetch_data(opp_dat dat) {
     return dat;
 }
 
-int opp_mpi_halo_exchanges_grouped(opp_set, int nargs, opp_arg* args, DeviceType) {
-    for (int i = 0; i < nargs; i++)
-        if (args[i].argtype == OPP_ARG_DAT && args[i].dat) oppb_rt::sync_host_to_device(args[i].dat);
-    return 0;
+// One rank: no halo, so the loop runs over the set's own elements (the reference's return value
+// without MPI, opp_lib/src/cuda/opp_cuda_halo.cu:318-353); the dats of the loop's arguments are
+// brought current on the side that runs it: the host copy for a Device_CPU loop, the device copy
+// for a Device_GPU loop.
+int opp_mpi_halo_exchanges_grouped(opp_set set, int nargs, opp_arg* args, DeviceType device) {
+    for (int i = 0; i < nargs; i++) {
+        if (args[i].argtype != OPP_ARG_DAT || !args[i].dat) continue;
+        if (device == Device_CPU) opp_download_dat(args[i].dat);
+        else oppb_rt::sync_host_to_device(args[i].dat);
+    }
+    return set->size;
 }
 int opp_mpi_halo_exchanges(opp_set set, int nargs, opp_arg* args) {
     opp_mpi_halo_exchanges_grouped(set, nargs, args, Device_GPU);

@@ -21,7 +21,7 @@ PARAMS = ("STRING opp_fill = HoleFill_All\nINT opp_fill_period = 10\nREAL opp_al
           "BOOL opp_profile_all = false\n")
 CELLS = 7
 DATS = ["c_v1", "c_v3", "c_v16", "c_i2", "p_v"]
-MAPS = ["c2n", "p2c"]
+MAPS = ["c2n", "c2n1", "p2c"]
 P2C = [3, 0, 6, 6, 1]
 P_V = [1.5, -0.0, 0.0, -2.25e-300, 1e300, 3.0, -7.0, 0.1, 1.0 / 3.0, -1.0 / 3.0]
 need_seq = pytest.mark.skipif(not SEQ.exists(), reason="compiled reference not built (needs its sources)")
@@ -34,13 +34,18 @@ def inputs(seed: int = 0) -> dict:
             "c2n": rng.integers(0, 9, size=(CELLS, 4))}
 
 
-def write_inputs(d: Path, arrays: dict) -> None:
+def with_one_based(a: dict) -> dict:
+    """c2n1: c2n's entries plus 1, declared with OPP_maps_base_index = 1."""
+    return {**a, "c2n1": a["c2n"] + 1}
+
+
+def write_inputs(d: Path, arrays: dict, params: str = PARAMS) -> None:
     """The decl_*_txt files: a "rows dim" header, then one row of values a line (c_v3 holds one
     row more than the set, which the loader allows)."""
     (d / "in").mkdir(parents=True, exist_ok=True)
     (d / "files").mkdir(exist_ok=True)
-    (d / "params.txt").write_text(PARAMS)
-    for name, a in arrays.items():
+    (d / "params.txt").write_text(params)
+    for name, a in with_one_based(arrays).items():
         fmt = (lambda v: f"{float(v):.17g}") if a.dtype.kind == "f" else str
         rows = "".join(" ".join(fmt(v) for v in r) + "\n" for r in a)
         (d / "in" / f"{name}.txt").write_text(f"{a.shape[0]} {a.shape[1]}\n" + rows)
@@ -86,6 +91,7 @@ def test_reference_output_has_the_restated_format(tmp_path):
         assert f[n] == expected_file(a[n], CELLS, True), n
     assert f["c_i2"] == expected_file(a["c_i2"], CELLS, False)
     assert f["c2n"] == expected_file(a["c2n"], CELLS, False)
+    assert f["c2n1"] == f["c2n"]  # declared 1-based, held 0-based
     assert f["p2c"] == expected_file(np.array(P2C)[:, None], 5, False)
     pv = np.array(P_V).reshape(5, 2)
     assert f["p_v"] == expected_file(pv, 5, True)
@@ -132,8 +138,51 @@ def test_dropin_text_io_equals_reference(tmp_path, seed):
     for k in outs["seq"][0]:
         assert outs["dropin"][0][k] == outs["seq"][0][k], k
     assert outs["dropin"][1] == outs["seq"][1]
+    halo = [[ln for ln in outs[b][2].splitlines() if ln.startswith("halo ")] for b in ("seq", "dropin")]
+    assert halo[0] == halo[1] == ["halo 7 5"]  # one rank: the loop runs over the set's own elements
     fetch = [ln for ln in outs["dropin"][2].splitlines() if ln.startswith("fetch ")]
     assert fetch == [f"fetch 1 {CELLS} {format(float(a['c_v3'][1, 1]), '.17g')}"]
+
+
+GLOBAL_CASES = {
+    "defaults": (PARAMS, ()),
+    "periodic_no_period": (PARAMS.replace("HoleFill_All", "Sort_Periodic").replace("INT opp_fill_period = 10\n", ""),
+                           ()),
+    "periodic": (PARAMS.replace("HoleFill_All", "Shuffle_Periodic"), ()),
+    "args": (PARAMS, ("OPP_ALLOC_MULT=2.5", "OPP_MPI_ALLOC_MULT=3", "OPP_DH_DATA_DUMP=1")),
+}
+GLOBALS_EXPECTED = {"defaults": "globals 2 -1 1.1000000000000001 1 0",
+                    "periodic_no_period": "globals 2147483647 -1 1.1000000000000001 1 0",
+                    "periodic": "globals 10 -1 1.1000000000000001 1 0",
+                    # opp_set_args_core keeps 17 characters of "OPP_ALLOC_MULT=2.5": "2." reads as 2
+                    "args": "globals 2 -1 2 3 1"}
+
+
+def globals_line(out: str) -> str:
+    return next(ln for ln in out.splitlines() if ln.startswith("globals "))
+
+
+@need_seq
+@pytest.mark.parametrize("case", sorted(GLOBAL_CASES))
+def test_reference_globals(tmp_path, case):
+    params, args = GLOBAL_CASES[case]
+    write_inputs(tmp_path, inputs(), params)
+    r = run(SEQ, tmp_path, "-", *args)
+    assert r.returncode == 0, r.stdout[-2000:]
+    assert globals_line(r.stdout) == GLOBALS_EXPECTED[case]
+
+
+@pytest.mark.gpu
+@need_seq
+@pytest.mark.parametrize("case", sorted(GLOBAL_CASES))
+def test_dropin_globals_equal_reference(tmp_path, case):
+    """The fill period (a missing opp_fill_period of a periodic fill is INT_MAX, as there), the
+    allocation multiples, the direct-hop dump flag and moreX_hops (-1, never counted)."""
+    params, args = GLOBAL_CASES[case]
+    write_inputs(tmp_path, inputs(), params)
+    r = run(DROPIN, tmp_path, "-", *args)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert globals_line(r.stdout) == GLOBALS_EXPECTED[case]
 
 
 @pytest.mark.gpu
