@@ -194,8 +194,9 @@ class Profiler {
 };
 
 // Bounding box of the direct-hop grid (opp_lib/include/opp_direct_hop_core.h:41-177): the box of
-// the node positions widened by `expansion`, computed by oppb_dh_bounding_box exactly as the
-// reference does.  One unpartitioned mesh: the global box is the local one.  3-D only.
+// the node positions widened by `expansion`, computed by oppb_dh_bounding_box (3-D) or
+// oppb_dh_bounding_box_2d (2-D: z stays 0) exactly as the reference does.  One unpartitioned
+// mesh: the global box is the local one.
 class BoundingBox {
    public:
     BoundingBox(const opp_dat node_pos_dat, int dim, const opp_point expansion);
@@ -230,7 +231,7 @@ extern opp_fill_type OPP_fill_type;
 extern double OPP_part_alloc_mult;
 extern int OPP_iter_start;
 extern int OPP_iter_end;
-extern int OPP_move_max_hops;       // bound on cell visits per particle and move
+extern int OPP_move_max_hops;       // the parameter file's opp_move_max_hops, else -1 (unbounded there)
 // Communication and hop statistics the apps' logs print (opp_defs.h:428-439); one GPU has no
 // communication rounds, so they stay 0.
 extern int OPP_max_comm_iteration;
@@ -285,7 +286,9 @@ void opp_decl_const(int dim, T* data, const char* name) {
     opp_decl_const_impl(dim, sizeof(T), (char*)data, name);
 }
 // Value of a constant registered with opp_decl_const (abort if unknown).
-double opp_get_const(const char* name);
+// Element `index` of a constant declared by opp_decl_const (B200 extension: the generated loops
+// of this library read their constants here).
+double opp_get_const(const char* name, int index = 0);
 
 // ------------------------------------------------------------------- args
 opp_arg opp_arg_gbl(double* data, int dim, char const* typ, opp_access acc);
@@ -365,6 +368,51 @@ inline void opp_get_global_values(const int64_t value, int64_t& gbl_value, int64
     gbl_value = gbl_max = gbl_min = value;
 }
 
+// Particle initialisation helpers of opp_util.h:108-175, used by the apps' host set-up: the
+// same draws in the same order from the caller's engine, so a seeded set-up gives the
+// reference's particles.  Per dimension, N draws of N(mu, sigma).
+template <typename RNG>
+inline std::vector<std::vector<double>> get_normal_distribution(const int N, const int ndim, const double mu,
+                                                                const double sigma, RNG& rng) {
+    std::normal_distribution<> normal{mu, sigma};
+    std::vector<std::vector<double>> out(ndim, std::vector<double>(N));
+    for (int d = 0; d < ndim; d++)
+        for (int p = 0; p < N; p++) out[d][p] = normal(rng);
+    return out;
+}
+
+// Per dimension d, N draws of extents[d] * U[0, 1).
+template <typename RNG>
+inline std::vector<std::vector<double>> get_uniform_within_extents(const int N, const int ndim, const double* extents,
+                                                                   RNG& rng) {
+    std::uniform_real_distribution<double> unit(0.0, 1.0);
+    std::vector<std::vector<double>> out(ndim, std::vector<double>(N));
+    for (int d = 0; d < ndim; d++)
+        for (int p = 0; p < N; p++) out[d][p] = extents[d] * unit(rng);
+    return out;
+}
+
+// npart_per_cell particles in each cell c: cell c, position cell_pos_ll[c] plus a draw of
+// get_uniform_within_extents (cells in order).  The engine is taken by value, as there.
+template <typename T>
+inline void uniform_within_cartesian_cells(int ndim, const double* extents, const T* cell_pos_ll,
+                                           const int64_t cells_set_size, const int64_t npart_per_cell,
+                                           std::vector<std::vector<double>>& positions, std::vector<int>& cells,
+                                           std::mt19937 rng) {
+    const int64_t total = npart_per_cell * cells_set_size;
+    cells.resize(total);
+    positions.resize(ndim);
+    for (int d = 0; d < ndim; d++) positions[d] = std::vector<double>(total);
+    for (int64_t c = 0; c < cells_set_size; c++) {
+        const auto local = get_uniform_within_extents((int)npart_per_cell, ndim, extents, rng);
+        for (int64_t k = 0; k < npart_per_cell; k++) {
+            const int64_t p = c * npart_per_cell + k;
+            cells.at(p) = (int)c;
+            for (int d = 0; d < ndim; d++) positions.at(d).at(p) = cell_pos_ll[c * ndim + d] + local.at(d).at(k);
+        }
+    }
+}
+
 // printf-formatted value (opp_util.h:85).
 template <typename T>
 std::string str(T value, std::string format) {
@@ -377,6 +425,8 @@ std::string str(T value, std::string format) {
 // Device-resident packed mesh and scratch shared by the generated-loop entry points.
 namespace oppb_rt {
 cudaStream_t stream();
+// Bound on the cell visits of one particle's walk: OPP_move_max_hops when positive, else 4096.
+int max_hops();
 const oppb_tet_mesh& tet_mesh(opp_dat c_det, opp_dat c_volume, opp_map c2c, opp_map c2n, opp_dat c_ef);
 void* workspace(size_t bytes);
 oppb_move_status* move_status();

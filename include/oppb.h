@@ -305,6 +305,11 @@ int oppb_hole_fill(int32_t size, int32_t remove_count, const uint32_t* remove_bi
                    int32_t stride, int32_t n_dats, const oppb_dat* dats,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* remove_bits for oppb_hole_fill from the cells a move left: bit i of word i / 32 set where
+ * p2c[i] == OPPB_REMOVED_CELL, for i in [0, size) (ceil(size / 32) words written).  For moves
+ * that mark removed particles in p2c only (the advection move's global-move pre-pass). */
+int oppb_removal_bits(const int32_t* p2c, int32_t size, uint32_t* remove_bits, void* stream);
+
 /* Largest remove_count that oppb_hole_fill_static accepts. */
 #define OPPB_HOLE_FILL_STATIC_MAX_REMOVES 1048576
 

@@ -102,10 +102,20 @@ int oppb_advec_step(const oppb_advec_batch* batch, oppb_move_status* status, int
 
 /* The two loops separately, as the generated main calls them:
  * opp_par_loop_all__update_pos_kernel (apps_codegen/app_neso_advection_mdir_cg/cuda/update_pos_kernel_loop.hpp)
- * and opp_particle_move__move_kernel (.../cuda/move_kernel_loop.hpp). */
+ * and opp_particle_move__move_kernel (.../cuda/move_kernel_loop.hpp).  The update reads the
+ * batch's pos and vel only (mdir, p2c and cells may be NULL); the move reads pos, mdir, p2c and
+ * cells (vel may be NULL). */
 int oppb_advec_update_pos(const oppb_advec_batch* batch, void* stream);
 int oppb_advec_move(const oppb_advec_batch* batch, oppb_move_status* status, int32_t max_hops,
                     void* stream);
+
+/* verify_kernel of one instance (apps/app_neso_advection/kernels.h:115-151; the generated loop
+ * opp_par_loop_all__verify_kernel): adds to *incorrect (device int32) the number of particles
+ * i < n_parts whose position pos (SoA [2][stride]) lies outside the closed box
+ * [ix w, ix w + w] x [iy w, iy w + w] of their cell, (ix, iy) from the cell's global index
+ * g = c_gbl_idx[p2c[i]] as g mod nx, g div nx (a negative ix or iy counts as incorrect). */
+int oppb_advec_verify(const double* pos, int64_t stride, const int32_t* p2c, const int32_t* c_gbl_idx,
+                      int32_t n_parts, int32_t nx, double cell_width, int32_t* incorrect, void* stream);
 
 #ifdef __cplusplus
 }

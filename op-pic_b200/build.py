@@ -49,7 +49,8 @@ def _run(cmd: list[str]) -> None:
 CUDA_INC = "/usr/local/cuda/include"
 # Host sources of the C ABI library (set-up utilities) and of the C++ drop-in runtime.
 ABI_HOST = ("fempic_mesh.cpp", "fempic_field.cpp")
-RUNTIME_HOST = ("fempic_mesh.cpp", "fempic_field.cpp", "opp_runtime.cpp", "fempic_loops.cpp", "fempic_field_solver.cpp")
+RUNTIME_HOST = ("fempic_mesh.cpp", "fempic_field.cpp", "opp_runtime.cpp", "fempic_loops.cpp", "fempic_field_solver.cpp",
+                "advec_loops.cpp")
 
 
 def _objects(force: bool, names) -> list[Path]:

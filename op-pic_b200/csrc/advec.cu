@@ -341,17 +341,51 @@ void launch_seeded(const oppb_advec_batch* b, oppb_move_status* status, int32_t 
         launch_items<kMode, 2, kSeed>(b, status, max_hops, s);
 }
 
+// The pointers a launch reads or writes must be set: pos always, vel unless the launch only
+// moves, mdir, p2c and the 32-byte-aligned cells unless it only updates positions.
+template <int kMode>
 int check_batch(const oppb_advec_batch* b) {
     if (!b || b->n_instances <= 0 || b->n_work < 0 || !b->instances || !b->tile_prefix) return OPPB_ERR_ARG;
-    if (!b->pos || !b->vel || !b->mdir || !b->p2c || !b->cells || !aligned(b->cells, 32) || b->stride <= 0 ||
-        !b->work_counter)
-        return OPPB_ERR_ARG;
+    if (!b->pos || b->stride <= 0 || !b->work_counter) return OPPB_ERR_ARG;
+    if (kMode != kMoveOnly && !b->vel) return OPPB_ERR_ARG;
+    if (kMode != kUpdateOnly && (!b->mdir || !b->p2c || !b->cells || !aligned(b->cells, 32))) return OPPB_ERR_ARG;
     return OPPB_OK;
+}
+
+// verify_kernel (apps/app_neso_advection/kernels.h:115-151): a particle is incorrect when its
+// cell's global index g gives ix = g - (g / nx) nx < 0 or iy = g / nx < 0, or when its position
+// lies outside the closed box [ix w, ix w + w] x [iy w, iy w + w] (the products and sums rounded
+// on their own, as there; this file is compiled with -fmad=false).  Block counts are added
+// into *incorrect.
+__global__ void __launch_bounds__(256) advec_verify_kernel(const double* __restrict__ pos, int64_t stride,
+                                                           const int32_t* __restrict__ p2c,
+                                                           const int32_t* __restrict__ c_gbl_idx, int32_t n,
+                                                           int32_t nx, double w, int32_t* incorrect) {
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    int bad = 0;
+    if (i < n) {
+        const int32_t g = __ldg(c_gbl_idx + __ldg(p2c + i));
+        const int32_t iy = g / nx, ix = g - iy * nx;
+        if (ix < 0 || iy < 0) {
+            bad = 1;
+        } else {
+            const double llx = ix * w, lly = iy * w;
+            const double x = __ldg(pos + i), y = __ldg(pos + stride + i);
+            bad = (x < llx || x > llx + w || y < lly || y > lly + w) ? 1 : 0;
+        }
+    }
+    const int warp_bad = __popc(__ballot_sync(kFullMask, bad));
+    __shared__ int s_bad;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && warp_bad) atomicAdd(&s_bad, warp_bad);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_bad) atomicAdd(incorrect, s_bad);
 }
 
 template <int kMode>
 int launch_advec(const oppb_advec_batch* b, oppb_move_status* status, int32_t max_hops, void* stream) {
-    const int rc = check_batch(b);
+    const int rc = check_batch<kMode>(b);
     if (rc) return rc;
     if (kMode != kUpdateOnly && (!status || max_hops <= 0)) return OPPB_ERR_ARG;
     if (b->n_work == 0) return OPPB_OK;
@@ -409,4 +443,16 @@ extern "C" int oppb_advec_update_pos(const oppb_advec_batch* batch, void* stream
 extern "C" int oppb_advec_move(const oppb_advec_batch* batch, oppb_move_status* status, int32_t max_hops,
                                void* stream) {
     return oppb::launch_advec<oppb::kMoveOnly>(batch, status, max_hops, stream);
+}
+
+extern "C" int oppb_advec_verify(const double* pos, int64_t stride, const int32_t* p2c, const int32_t* c_gbl_idx,
+                                 int32_t n_parts, int32_t nx, double cell_width, int32_t* incorrect, void* stream) {
+    using namespace oppb;
+    if (n_parts < 0 || nx <= 0 || !incorrect || (n_parts > 0 && (!pos || !p2c || !c_gbl_idx || stride < n_parts)))
+        return OPPB_ERR_ARG;
+    if (n_parts == 0) return OPPB_OK;
+    advec_verify_kernel<<<ceil_div(n_parts, 256), 256, 0, as_stream(stream)>>>(pos, stride, p2c, c_gbl_idx, n_parts,
+                                                                              nx, cell_width, incorrect);
+    count_launches(1);
+    return launch_status();
 }

@@ -192,10 +192,29 @@ __global__ void step_end_kernel(oppb_set_count* cnt, int32_t pending, const oppb
     cnt->steps = step + 1;
 }
 
+// bits[w] bit b = (p2c[32 w + b] == removed) over [0, size); a warp writes one word, bits past
+// size are 0.
+__global__ void __launch_bounds__(256) removal_bits_kernel(const int32_t* __restrict__ p2c, int32_t size,
+                                                           uint32_t* __restrict__ bits) {
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    const bool gone = i < size && __ldg(p2c + i) == kRemoved;
+    const uint32_t w = __ballot_sync(kFullMask, gone);
+    if ((threadIdx.x & 31) == 0 && i < size) bits[i >> 5] = w;
+}
+
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 }  // namespace
 }  // namespace oppb
+
+extern "C" int oppb_removal_bits(const int32_t* p2c, int32_t size, uint32_t* remove_bits, void* stream) {
+    using namespace oppb;
+    if (size < 0 || (size > 0 && (!p2c || !remove_bits))) return OPPB_ERR_ARG;
+    if (size == 0) return OPPB_OK;
+    removal_bits_kernel<<<ceil_div(size, 256), 256, 0, as_stream(stream)>>>(p2c, size, remove_bits);
+    count_launches(1);
+    return launch_status();
+}
 
 extern "C" size_t oppb_hole_fill_workspace_bytes(int32_t size, int32_t remove_count) {
     using namespace oppb;

@@ -128,11 +128,11 @@ void opp_particle_move__move_kernel(opp_set set, opp_map c2c_map, opp_map p2c_ma
         oppb_move_options o{};
         o.precision = OPPB_PRECISION_F64;
         o.dh = &g_dh.grid;
-        check(oppb_move_ex(&mesh, &p, &o, nullptr, oppb_rt::move_status(), OPP_move_max_hops, nullptr, 0,
+        check(oppb_move_ex(&mesh, &p, &o, nullptr, oppb_rt::move_status(), oppb_rt::max_hops(), nullptr, 0,
                            oppb_rt::stream()),
               "oppb_move_ex");
     } else {
-        check(oppb_move_f64(&mesh, &p, oppb_rt::move_status(), OPP_move_max_hops, oppb_rt::stream()),
+        check(oppb_move_f64(&mesh, &p, oppb_rt::move_status(), oppb_rt::max_hops(), oppb_rt::stream()),
               "oppb_move_f64");
     }
     oppb_rt::mark_device_written(arg1.dat);
@@ -179,6 +179,7 @@ void opp_init_direct_hop_cg(double grid_spacing, const opp_dat c_gbl_id, const o
         for (int c = 0; c < cells->size; c++)
             if (id[c] != c) opp_abort("opp_init_direct_hop_cg: c_gbl_id must be the cell index on one GPU");
     }
+    if (b_box.getDim() != 3) opp_abort("opp_init_direct_hop_cg: the FemPIC grid is 3-D");
     opp_dat npos = b_box.nodePositions();
     if (!npos) opp_abort("opp_init_direct_hop_cg: the bounding box must come from the node positions");
     opp_map c2n = nullptr;  // the cell -> node map the binning reads

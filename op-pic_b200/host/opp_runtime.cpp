@@ -30,9 +30,10 @@ opp_fill_type OPP_fill_type = OPP_HoleFill_All;
 double OPP_part_alloc_mult = 1.0;
 int OPP_iter_start = 0;
 int OPP_iter_end = 0;
-// The reference's -1 leaves its walks unbounded; a kernel here stops a walk after this many
-// cell visits and reports OPPB_ERR_HOP_LIMIT (opp_move_max_hops in the parameter file sets it).
-int OPP_move_max_hops = 4096;
+// The reference's -1 leaves its walks unbounded; the kernels here stop a walk after
+// oppb_rt::max_hops() cell visits (this value when positive, set by opp_move_max_hops in the
+// parameter file, else 4096) and report OPPB_ERR_HOP_LIMIT.
+int OPP_move_max_hops = -1;
 double OPP_hybrid_balance = 1.0;
 int OPP_maps_base_index = 0;
 int OPP_auto_soa = 1;  // device dats are SoA, as the CUDA backend sets it in opp_init
@@ -514,10 +515,11 @@ void opp_decl_const_impl(int dim, int size, char* data, const char* name) {
     rt().consts[name] = v;
 }
 
-double opp_get_const(const char* name) {
+double opp_get_const(const char* name, int index) {
     auto it = rt().consts.find(name);
-    if (it == rt().consts.end() || it->second.empty()) opp_abort(std::string("unknown const ") + name);
-    return it->second[0];
+    if (it == rt().consts.end() || index < 0 || (size_t)index >= it->second.size())
+        opp_abort(std::string("unknown const ") + name);
+    return it->second[(size_t)index];
 }
 
 // -------------------------------------------------------------------- args
@@ -922,6 +924,8 @@ namespace oppb_rt {
 
 cudaStream_t stream() { return rt().stream; }
 
+int max_hops() { return OPP_move_max_hops > 0 ? OPP_move_max_hops : 4096; }
+
 void* workspace(size_t bytes) {
     auto& r = rt();
     if (bytes > r.ws_bytes) {
@@ -1024,20 +1028,22 @@ namespace opp {
 
 BoundingBox::BoundingBox(const opp_dat node_pos_dat, int dim, const opp_point expansion)
     : domain_expansion(expansion), dim_(dim), node_pos_(node_pos_dat) {
-    if (dim != 3) opp_abort("BoundingBox: the direct-hop grid of this backend is 3-D");
-    if (!node_pos_dat || node_pos_dat->dim != 3) opp_abort("BoundingBox: node positions must be a 3-component dat");
+    if (dim != 3 && dim != 2) opp_abort("For now, only 2D/3D BoundingBox is implemented");
+    if (!node_pos_dat || node_pos_dat->dim != dim)
+        opp_abort("BoundingBox: the positions must be a dat of `dim` components");
     opp_download_dat(node_pos_dat);
     const double e[3] = {expansion.x, expansion.y, expansion.z};
     double mn[3], mx[3];
-    if (oppb_dh_bounding_box(reinterpret_cast<const double*>(node_pos_dat->data), node_pos_dat->set->size, e, mn,
-                             mx) != OPPB_OK)
+    const double* p = reinterpret_cast<const double*>(node_pos_dat->data);
+    const int n = node_pos_dat->set->size;
+    if ((dim == 3 ? oppb_dh_bounding_box(p, n, e, mn, mx) : oppb_dh_bounding_box_2d(p, n, e, mn, mx)) != OPPB_OK)
         opp_abort("BoundingBox: no node positions");
     box_[0] = opp_point(mn[0], mn[1], mn[2]);
     box_[1] = opp_point(mx[0], mx[1], mx[2]);
 }
 
 BoundingBox::BoundingBox(int dim, opp_point min_coordinate, opp_point max_coordinate) : dim_(dim) {
-    if (dim != 3) opp_abort("BoundingBox: the direct-hop grid of this backend is 3-D");
+    if (dim != 3 && dim != 2) opp_abort("For now, only 2D/3D BoundingBox is implemented");
     box_[0] = min_coordinate;
     box_[1] = max_coordinate;
 }

@@ -198,6 +198,8 @@ _SIGS = {
     "oppb_advec_check_grid": (C.c_int, [c_vp, c_i32, c_i32, c_i32, C.c_double, c_vp, c_vp]),
     "oppb_advec_update_pos": (C.c_int, [P(AdvecBatch), c_vp]),
     "oppb_advec_move": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
+    "oppb_advec_verify": (C.c_int, [c_vp, c_i64, c_vp, c_vp, c_i32, c_i32, C.c_double, c_vp, c_vp]),
+    "oppb_removal_bits": (C.c_int, [c_vp, c_i32, c_vp, c_vp]),
     "oppb_dh_grid_init": (C.c_int, [c_vp, c_i32, C.c_double, c_vp, P(DhGrid)]),
     "oppb_dh_build": (C.c_int, [P(TetMesh), c_vp, P(DhGrid), c_vp, C.c_size_t, P(C.c_size_t), c_vp]),
     "oppb_dh_bounding_box_2d": (C.c_int, [c_vp, c_i32, c_vp, c_vp, c_vp]),

@@ -258,3 +258,45 @@ def test_reference_generated_main_runs_on_the_dropin(tmp_path, fill, period):
         assert abs(max_cef - max(0.0, float(m.c_ef.max()))) <= 1e-9 * max(1.0, abs(max_cef)), s
         assert abs(max_pot - float(np.abs(o.potential).max())) <= 1e-9 * max(1.0, abs(max_pot)), s
     assert removed > 0 and log[-1][1] > 50_000
+
+
+ADV_SEQ = REF_MAIN.parent / "advec_opp_seq"
+ADV_DROPIN = REF_MAIN.parent / "advec_opp_dropin"
+ADV_LOG = re.compile(r"^Main\[\d+\]\[\d+\] - ts: .*$")
+
+
+@pytest.mark.skipif(not (ADV_SEQ.exists() and ADV_DROPIN.exists()),
+                    reason="the NESO-advection generated main was not built (oracle/Makefile)")
+@pytest.mark.parametrize("global_move,nx,ny,ppc,steps", [(False, 128, 96, 50, 200), (True, 96, 64, 40, 120)])
+def test_reference_advection_main_runs_on_the_dropin(tmp_path, global_move, nx, ny, ppc, steps):
+    """The reference's generated NESO-advection main (apps_codegen/app_neso_advection_mdir_cg/
+    advec_opp.cpp), unmodified, built twice by oracle/Makefile: on the reference's seq backend with
+    its generated seq loops, and on include/ + libopp_b200.so.  Both with opp_exit wrapped to write
+    every particle dat (oracle/dump_at_exit.cpp).  Same parameter file: the app's own init_mesh,
+    its seeded init_particles, verify_particles every step, with and without the global move
+    (direct-hop grid built by the seq backend's all-cell search there, on the GPU here).  The
+    per-step log lines (errors, particle counts, hop bound) and the final particle dats (positions,
+    velocities, move directions, cells, indices) are equal byte for byte."""
+    params = (f"INT num_steps = {steps}\nINT nx = {nx}\nINT ny = {ny}\nREAL dt = 0.5\nREAL cell_width = 0.5\n"
+              f"INT npart_per_cell = {ppc}\nBOOL verify_particles = true\nREAL opp_allocation_multiple = 1.1\n"
+              "INT opp_threads_per_block = 512\nBOOL opp_profile_all = false\n"
+              f"BOOL opp_global_move = {'true' if global_move else 'false'}\nREAL grid_spacing = 0.5\n"
+              "BOOL opp_dh_data_generate = true\nSTRING opp_fill = HoleFill_All\nINT opp_fill_period = 4\n")
+    out = {}
+    for name, exe in (("seq", ADV_SEQ), ("cuda", ADV_DROPIN)):
+        d = tmp_path / name
+        (d / "files").mkdir(parents=True)
+        (d / "params.txt").write_text(params)
+        r = subprocess.run([str(exe), "params.txt"], capture_output=True, text=True, timeout=600, cwd=d)
+        assert r.returncode == 0, (name, r.stdout[-2000:], r.stderr[-2000:])
+        log = [ln for ln in r.stdout.splitlines() if ADV_LOG.match(ln)]
+        files = {p.name.replace(f"final_{name}_", ""): p.read_bytes() for p in (d / "files").iterdir()}
+        out[name] = (log, files)
+    log_seq, files_seq = out["seq"]
+    log_gpu, files_gpu = out["cuda"]
+    assert len(log_seq) == steps and all("errors: 0 |" in ln for ln in log_seq)
+    assert f"Gbl parts: {nx * ny * ppc} " in log_seq[-1]
+    assert log_gpu == log_seq
+    assert sorted(files_gpu) == sorted(files_seq) == ["p_index", "p_mesh_rel", "p_move_dir", "p_pos", "p_vel"]
+    for k in files_seq:
+        assert files_gpu[k] == files_seq[k], k
