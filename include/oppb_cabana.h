@@ -85,6 +85,53 @@ int oppb_cabana_move_deposit_mixed(const oppb_hex_mesh* mesh, const oppb_cabana_
                                    const oppb_cabana_consts* consts, double* acc, int32_t acc_stride,
                                    oppb_move_status* status, int32_t max_hops, void* stream);
 
+/* ------------------------------------------------------------ the mesh loops of the app
+ * The generated main's cell loops (apps_codegen/app_cabanapic_cg/cabana_opp.cpp:144-299; user
+ * kernels apps/app_cabanapic/kernels.h), one thread per cell of [0, n_cells), each value as the
+ * seq backend computes it.  Cell dats are SoA [dim][stride] (stride >= n_cells).  A neighbour
+ * argument is one column of a cell map's device copy (map + idx * stride): the cell each cell
+ * reads through that argument. */
+
+/* interpolate_mesh_fields_kernel: c_interp (18 values) of every cell with c_mask_ghost 0 from
+ * c_e at the cell and at nb_e = its xu_y_z, x_yu_z, x_y_zu, xu_yu_z, x_yu_zu, xu_y_zu neighbours,
+ * and c_b at the cell and at nb_b = its xu_y_z, x_yu_z, x_y_zu neighbours. */
+int oppb_cabana_interpolate(int32_t n_cells, int64_t stride, const double* c_e, const double* c_b,
+                            const int32_t* const nb_e[6], const int32_t* const nb_b[3], double* c_interp,
+                            const int32_t* c_mask_ghost, void* stream);
+
+/* accumulate_current_to_cells_kernel: c_j of every cell with c_mask_right 1 from c_acc at the
+ * cell and at nb_lower = its xd_y_z, x_yd_z, x_y_zd, xd_yd_z, x_yd_zd, xd_y_zd neighbours, times
+ * acc_coef (CONST_acc_coef). */
+int oppb_cabana_accumulate(int32_t n_cells, int64_t stride, double* c_j, const double* c_acc,
+                           const int32_t* const nb_lower[6], const int32_t* c_mask_right, const double acc_coef[3],
+                           void* stream);
+
+/* half_advance_b_kernel: c_b of every cell with c_mask_ghost 0 less half a step of curl c_e,
+ * c_e at nb_upper = its xu_y_z, x_yu_z, x_y_zu neighbours; p = CONST_p. */
+int oppb_cabana_half_advance_b(int32_t n_cells, int64_t stride, const int32_t* const nb_upper[3], const double* c_e,
+                               double* c_b, const int32_t* c_mask_ghost, const double p[3], void* stream);
+
+/* advance_e_kernel: c_e of every cell with c_mask_right 1 plus -dt_eps0 c_j + curl c_b, c_b at
+ * nb_lower = its xd_y_z, x_yd_z, x_y_zd neighbours; p = CONST_p, dt_eps0 = CONST_dt_eps0. */
+int oppb_cabana_advance_e(int32_t n_cells, int64_t stride, const int32_t* const nb_lower[3], const double* c_b,
+                          const double* c_j, double* c_e, const int32_t* c_mask_right, const double p[3],
+                          double dt_eps0, void* stream);
+
+/* update_ghosts_B_kernel (dim = -1: the three components of `from` at cell c copied to `to` at
+ * to_map[c]) and update_ghosts_kernel (dim 0..2: that component added there), for the cells c
+ * whose mask (a 6-component cell dat: c_mask_ugb or c_mask_ug) holds 1 at m_idx.  Cells written
+ * must not be read by the same call (the app's ghost maps pair interior and ghost cells). */
+int oppb_cabana_update_ghosts(int32_t n_cells, int64_t stride, const int32_t* mask, int32_t m_idx, const double* from,
+                              double* to, const int32_t* to_map, int32_t dim, void* stream);
+
+/* compute_energy_kernel: adds to *energy (device) the sum over the cells with c_mask_ghost 0 of
+ * fx fx + fy fy + fz fz.  The sum is taken in a fixed order (deterministic), not the seq
+ * backend's cell order, so it matches the reference's to rounding.  The workspace holds the
+ * block partials (oppb_cabana_energy_workspace_bytes, 8-byte aligned). */
+size_t oppb_cabana_energy_workspace_bytes(void);
+int oppb_cabana_energy(int32_t n_cells, int64_t stride, const int32_t* c_mask_ghost, const double* field,
+                       double* energy, void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,7 +27,8 @@ NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", f"
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", f"-I{INC}", "-Wall"]
 # Sources whose FP64 expressions must keep the reference's written order with one rounding
 # per operation: no FMA contraction anywhere in the file.
-PER_FILE_NVCC_FLAGS = {"cabana.cu": ["-fmad=false"], "advec.cu": ["-fmad=false"], "field.cu": ["-fmad=false"],
+PER_FILE_NVCC_FLAGS = {"cabana.cu": ["-fmad=false"], "cabana_field.cu": ["-fmad=false"], "advec.cu": ["-fmad=false"],
+                       "field.cu": ["-fmad=false"],
                        # the grid set-up loops of the direct-hop mapper run on the host
                        "dh.cu": ["-Xcompiler", "-ffp-contract=off"]}
 
@@ -50,7 +51,7 @@ CUDA_INC = "/usr/local/cuda/include"
 # Host sources of the C ABI library (set-up utilities) and of the C++ drop-in runtime.
 ABI_HOST = ("fempic_mesh.cpp", "fempic_field.cpp")
 RUNTIME_HOST = ("fempic_mesh.cpp", "fempic_field.cpp", "opp_runtime.cpp", "fempic_loops.cpp", "fempic_field_solver.cpp",
-                "advec_loops.cpp")
+                "advec_loops.cpp", "cabana_loops.cpp")
 
 
 def _objects(force: bool, names) -> list[Path]:

@@ -753,7 +753,7 @@ void opp_particle_sort(opp_set set) {
 void opp_reset_dat_impl(opp_dat dat, char* val, opp_reset) {
     oppb_rt::sync_host_to_device(dat);
     const int eb = elem_bytes(dat), stride = stride_of(dat->set);
-    const int n = dat->set->is_particle ? dat->set->size : dat->set->size;
+    const int n = dat->set->size;
     for (int c = 0; c < dat->dim; c++) {
         uint64_t pattern = 0;
         std::memcpy(&pattern, val + (size_t)c * eb, eb);

@@ -276,7 +276,7 @@ def test_reference_advection_main_runs_on_the_dropin(tmp_path, global_move, nx, 
     its seeded init_particles, verify_particles every step, with and without the global move
     (direct-hop grid built by the seq backend's all-cell search there, on the GPU here).  The
     per-step log lines (errors, particle counts, hop bound) and the final particle dats (positions,
-    velocities, move directions, cells, indices) are equal byte for byte."""
+    velocities, move directions, cells, indices), with the cell dats, are equal byte for byte."""
     params = (f"INT num_steps = {steps}\nINT nx = {nx}\nINT ny = {ny}\nREAL dt = 0.5\nREAL cell_width = 0.5\n"
               f"INT npart_per_cell = {ppc}\nBOOL verify_particles = true\nREAL opp_allocation_multiple = 1.1\n"
               "INT opp_threads_per_block = 512\nBOOL opp_profile_all = false\n"
@@ -297,6 +297,84 @@ def test_reference_advection_main_runs_on_the_dropin(tmp_path, global_move, nx, 
     assert len(log_seq) == steps and all("errors: 0 |" in ln for ln in log_seq)
     assert f"Gbl parts: {nx * ny * ppc} " in log_seq[-1]
     assert log_gpu == log_seq
-    assert sorted(files_gpu) == sorted(files_seq) == ["p_index", "p_mesh_rel", "p_move_dir", "p_pos", "p_vel"]
+    assert sorted(files_gpu) == sorted(files_seq)
+    assert {"p_index", "p_mesh_rel", "p_move_dir", "p_pos", "p_vel", "c_pos_ll"} <= set(files_seq)
     for k in files_seq:
         assert files_gpu[k] == files_seq[k], k
+
+
+CAB_SEQ = REF_MAIN.parent / "cabana_opp_seq"
+CAB_DROPIN = REF_MAIN.parent / "cabana_opp_dropin"
+CAB_LOG = re.compile(r"ts: (\d+)\s+e_energy: \s*(\S+) b_energy: \s*(\S+) max_jx: (\S+) max_ex: (\S+) max_bx: (\S+)")
+
+
+def read_dump(path: Path) -> np.ndarray:
+    """A file of opp_print_dat_to_txtfile: the header, one row of values per element, the two
+    marker lines."""
+    lines = path.read_text().splitlines()
+    size, dim = (int(v) for v in lines[0].split()[:2])
+    rows = [ln.split() for ln in lines[1:1 + size]]
+    assert all(len(r) == dim for r in rows) and lines[1 + size].startswith("import_exec_below")
+    return np.array(rows, dtype=np.float64).reshape(size, dim)
+
+
+@pytest.mark.skipif(not (CAB_SEQ.exists() and CAB_DROPIN.exists()),
+                    reason="the CabanaPIC generated main was not built (oracle/Makefile)")
+@pytest.mark.parametrize("nx,ny,nz,ppc,steps", [(8, 8, 24, 40, 25), (16, 16, 32, 60, 40)])
+def test_reference_cabana_main_runs_on_the_dropin(tmp_path, nx, ny, nz, ppc, steps):
+    """The reference's generated CabanaPIC main (apps_codegen/app_cabanapic_cg/cabana_opp.cpp),
+    unmodified, built on the reference's seq backend and on include/ + libopp_b200.so
+    (oracle/Makefile), opp_exit wrapped to write every dat (oracle/dump_at_exit.cpp): the app's own
+    mesh, its two-stream particles, the whole step (field interpolation, move + current deposit,
+    accumulation, the leapfrog B and E updates with their ghost copies) for `steps` steps.  The
+    masks, indices and cells equal; the fields, accumulators and particles, and the per-step energy
+    and maxima of the log and energy.csv, within 1e-9 of their largest values (B on E's scale):
+    the current deposit adds FP64 atomics in a different order than the seq loop, and the energy
+    is summed in a different order, so the two runs part at rounding level and the field
+    feedback carries that forward."""
+    params = (f"INT num_steps = {steps}\nREAL init_vel = 0.0866025403784439\nINT num_part_per_cell = {ppc}\n"
+              f"INT nx = {nx}\nINT ny = {ny}\nINT nz = {nz}\nREAL c = 1.0\nREAL qsp = -1.0\nREAL me = 1.0\n"
+              "REAL default_grid_len = 1.0\nREAL eps = 1.0\nSTRING part_enrich = two_stream\n"
+              "BOOL print_energy = true\nSTRING cluster = block\nREAL opp_allocation_multiple = 1.1\n"
+              "INT opp_threads_per_block = 256\nBOOL opp_profile_all = false\nBOOL print_final = true\n"
+              "STRING opp_fill = HoleFill_All\nINT opp_fill_period = 4\nBOOL opp_global_move = false\n"
+              "INT domain_expansion = 1\nREAL velX_mult_const = 1\nREAL velY_mult_const = 0.00\n"
+              "REAL velZ_mult_const = 0.00\n")
+    out = {}
+    for name, exe in (("seq", CAB_SEQ), ("cuda", CAB_DROPIN)):
+        d = tmp_path / name
+        (d / "files").mkdir(parents=True)
+        (d / "params.txt").write_text(params)
+        r = subprocess.run([str(exe), "params.txt"], capture_output=True, text=True, timeout=600, cwd=d)
+        assert r.returncode == 0, (name, r.stdout[-2000:], r.stderr[-2000:])
+        log = [m.groups() for m in map(CAB_LOG.search, r.stdout.splitlines()) if m]
+        energy = np.loadtxt(d / "energy.csv", delimiter=",", skiprows=1)
+        dats = {p.name.replace(f"final_{name}_", ""): read_dump(p) for p in (d / "files").iterdir()}
+        out[name] = (np.array(log, dtype=np.float64), energy, dats)
+    log_s, en_s, dats_s = out["seq"]
+    log_g, en_g, dats_g = out["cuda"]
+    assert log_s.shape == log_g.shape == (steps, 6) and en_s.shape == en_g.shape == (steps, 3)
+    np.testing.assert_array_equal(log_g[:, 0], np.arange(steps))
+    assert en_s[-1, 1] > 10 * en_s[0, 1] > 0  # the electric energy grows: the run is not trivial
+    assert sorted(dats_g) == sorted(dats_s)
+    assert {"p_pos", "p_vel", "p_streak_mid", "p_weight", "p2c_map", "c_e", "c_b", "c_j", "c_acc"} <= set(dats_s)
+    # E and B share their units (c = 1): B, which stays at rounding level in this workload, is
+    # compared on E's scale, and so is the magnetic energy on the electric energy's.
+    e_scale = np.abs(dats_s["c_e"]).max()
+    scale = {"c_b": e_scale, "c_e": e_scale, "c_interp": e_scale}
+    err = {}
+    for k in dats_s:
+        a, b = dats_g[k], dats_s[k]
+        assert a.shape == b.shape, k
+        if k.startswith("c_mask") or k in ("c_index", "c_colors", "p2c_map"):
+            np.testing.assert_array_equal(a, b, err_msg=k)
+        else:
+            err[k] = np.abs(a - b).max() / max(scale.get(k, np.abs(b).max()), 1e-300)
+    e_energy = np.abs(en_s[:, 1]).max()
+    err["e_energy"] = np.abs(en_g[:, 1] - en_s[:, 1]).max() / e_energy
+    err["b_energy"] = np.abs(en_g[:, 2] - en_s[:, 2]).max() / e_energy
+    # the logged maxima of jx, ex, bx, printed with 10, 10 and 16 decimals
+    err["max_jx"] = (np.abs(log_g[:, 3] - log_s[:, 3]).max() - 1e-10) / np.abs(log_s[:, 3]).max()
+    err["max_ex"] = (np.abs(log_g[:, 4] - log_s[:, 4]).max() - 1e-10) / e_scale
+    err["max_bx"] = (np.abs(log_g[:, 5] - log_s[:, 5]).max() - 1e-16) / e_scale
+    assert max(err.values()) <= 1e-9, err
