@@ -386,3 +386,61 @@ def test_check_grid_rejects_a_perturbed_mesh():
     with pytest.raises(L.OppbError):  # n_cells not a multiple of nx
         L.check("check", lib.oppb_advec_check_grid(cells.data_ptr(), 0, m2.n_cells, 7, m2.cell_width,
                                                    mism.data_ptr(), None))
+
+
+def test_verify_counts_particles_outside_their_cell():
+    """oppb_advec_verify (verify_kernel, apps/app_neso_advection/kernels.h:115-151) against the
+    same rule restated in numpy, on one instance after some steps with a few particles moved out
+    of their cell by hand: on the box's edges a particle counts as inside, one ulp beyond it
+    outside, and a cell whose global index is negative counts too."""
+    specs = [(48, 40, 0.5, 0.5, 30, 0.5)]
+    meshes, _, dev = _build(specs, seed0=77)
+    for _ in range(5):
+        dev.step()
+    m = meshes[0]
+    n = dev.counts[0]
+    rng = np.random.default_rng(5)
+    pos = dev.pos[:, :n].cpu().numpy().copy()
+    p2c = dev.p2c[:n].cpu().numpy()
+    w = m.cell_width
+    ix, iy = p2c % m.nx, p2c // m.nx
+    pick = rng.choice(n, 40, replace=False)
+    pos[0, pick[:10]] = ix[pick[:10]] * w                                   # on the lower x edge: inside
+    pos[1, pick[10:20]] = iy[pick[10:20]] * w + w                            # on the upper y edge: inside
+    pos[0, pick[20:30]] = np.nextafter(ix[pick[20:30]] * w + w, np.inf)      # one ulp beyond: outside
+    pos[1, pick[30:40]] = np.nextafter(iy[pick[30:40]] * w, -np.inf)         # one ulp below: outside
+    dev.pos[:, :n] = torch.from_numpy(pos).to(DEV)
+    gid = torch.arange(m.n_cells, dtype=torch.int32, device=DEV)
+    gid[int(p2c[pick[0]])] = -1  # a negative global index counts as incorrect
+    gidh = gid.cpu().numpy()
+    g = gidh[p2c]
+    giy, gix = g // m.nx, g - (g // m.nx) * m.nx
+    giy = np.where(g < 0, -((-g) // m.nx), giy)  # C division truncates toward zero
+    gix = g - giy * m.nx
+    llx, lly = gix * w, giy * w
+    bad = (gix < 0) | (giy < 0) | (pos[0] < llx) | (pos[0] > llx + w) | (pos[1] < lly) | (pos[1] > lly + w)
+    count = torch.zeros(1, dtype=torch.int32, device=DEV)
+    lib = L.load()
+    for rep in range(2):  # added into the count, as the OPP_INC global is
+        L.check("oppb_advec_verify", lib.oppb_advec_verify(dev.pos.data_ptr(), dev.capacity, dev.p2c.data_ptr(),
+                                                           gid.data_ptr(), n, m.nx, w, count.data_ptr(), None))
+        torch.cuda.synchronize()
+        assert int(count.item()) == (rep + 1) * int(bad.sum())
+    assert int(bad.sum()) >= 21  # the 20 moved out, and every particle of the cell with index -1
+
+
+@pytest.mark.parametrize("size", [1, 31, 32, 33, 100_003])
+def test_removal_bits_mark_removed_cells(size):
+    """oppb_removal_bits: bit i of word i/32 is set exactly where p2c[i] is the removed marker."""
+    rng = np.random.default_rng(size)
+    p2c = rng.integers(0, 1000, size).astype(np.int32)
+    p2c[rng.random(size) < 0.1] = L.REMOVED_CELL
+    words = (size + 31) // 32
+    bits = torch.full((words + 1,), -1, dtype=torch.int32, device=DEV)  # one guard word beyond
+    d = torch.from_numpy(p2c).to(DEV)
+    L.check("oppb_removal_bits", L.load().oppb_removal_bits(d.data_ptr(), size, bits.data_ptr(), None))
+    got = bits.cpu().numpy().view(np.uint32)
+    want = np.packbits((p2c == L.REMOVED_CELL).astype(np.uint8), bitorder="little")
+    want = np.pad(want, (0, 4 * words - len(want))).view("<u4")
+    np.testing.assert_array_equal(got[:words], want)
+    assert got[words] == 0xFFFFFFFF
