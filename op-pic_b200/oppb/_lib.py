@@ -199,6 +199,14 @@ _SIGS = {
     "oppb_advec_update_pos": (C.c_int, [P(AdvecBatch), c_vp]),
     "oppb_advec_move": (C.c_int, [P(AdvecBatch), c_vp, c_i32, c_vp]),
     "oppb_advec_verify": (C.c_int, [c_vp, c_i64, c_vp, c_vp, c_i32, c_i32, C.c_double, c_vp, c_vp]),
+    "oppb_cabana_interpolate": (C.c_int, [c_i32, c_i64, c_vp, c_vp, P(c_vp), P(c_vp), c_vp, c_vp, c_vp]),
+    "oppb_cabana_accumulate": (C.c_int, [c_i32, c_i64, c_vp, c_vp, P(c_vp), c_vp, P(C.c_double), c_vp]),
+    "oppb_cabana_half_advance_b": (C.c_int, [c_i32, c_i64, P(c_vp), c_vp, c_vp, c_vp, P(C.c_double), c_vp]),
+    "oppb_cabana_advance_e": (C.c_int, [c_i32, c_i64, P(c_vp), c_vp, c_vp, c_vp, c_vp, P(C.c_double), C.c_double,
+                                        c_vp]),
+    "oppb_cabana_update_ghosts": (C.c_int, [c_i32, c_i64, c_vp, c_i32, c_vp, c_vp, c_vp, c_i32, c_vp]),
+    "oppb_cabana_energy_workspace_bytes": (C.c_size_t, []),
+    "oppb_cabana_energy": (C.c_int, [c_i32, c_i64, c_vp, c_vp, c_vp, c_vp, C.c_size_t, c_vp]),
     "oppb_removal_bits": (C.c_int, [c_vp, c_i32, c_vp, c_vp]),
     "oppb_dh_grid_init": (C.c_int, [c_vp, c_i32, C.c_double, c_vp, P(DhGrid)]),
     "oppb_dh_build": (C.c_int, [P(TetMesh), c_vp, P(DhGrid), c_vp, C.c_size_t, P(C.c_size_t), c_vp]),
