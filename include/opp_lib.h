@@ -427,6 +427,10 @@ namespace oppb_rt {
 cudaStream_t stream();
 // Bound on the cell visits of one particle's walk: OPP_move_max_hops when positive, else 4096.
 int max_hops();
+// The number of opp_init calls so far: a cache keyed on a set, dat or map pointer also keeps the
+// generation it was made in, since after opp_exit and a new opp_init a new object may reuse an
+// old one's address.
+int generation();
 const oppb_tet_mesh& tet_mesh(opp_dat c_det, opp_dat c_volume, opp_map c2c, opp_map c2n, opp_dat c_ef);
 void* workspace(size_t bytes);
 oppb_move_status* move_status();

@@ -34,8 +34,9 @@ T* dev_alloc(size_t n) {
 }
 
 struct Advec {
-    opp_dat c_pos_ll = nullptr;  // the packed cells' source and its version
+    opp_dat c_pos_ll = nullptr;  // the packed cells' source, its version and the runtime's generation
     int c_pos_ll_version = -1;
+    int generation = -1;
     opp_map c2c = nullptr;
     int32_t n_cells = 0;
     int32_t grid_nx = 0;
@@ -46,6 +47,8 @@ struct Advec {
     int32_t* scratch = nullptr;    // grid-check mismatches, verify count
     oppb_advec_dh* dh = nullptr;   // the global move's grid (device, one entry) or nullptr
     int32_t* dh_map = nullptr;
+    oppb_advec_dh* dh_table = nullptr;  // device storage of `dh`
+    int dh_generation = -1;
 };
 
 Advec& adv() {
@@ -88,7 +91,9 @@ void upload_instance(opp_set set) {
 // against the periodic grid (one host read of the mismatch count).
 void pack_cells(opp_dat c_pos_ll, opp_map c2c) {
     Advec& a = adv();
-    if (a.c_pos_ll == c_pos_ll && a.c2c == c2c && a.c_pos_ll_version == c_pos_ll->version) return;
+    if (a.c_pos_ll == c_pos_ll && a.c2c == c2c && a.c_pos_ll_version == c_pos_ll->version &&
+        a.generation == oppb_rt::generation())
+        return;
     if (c_pos_ll->dim != 2 || c2c->dim != 4 || c2c->from != c_pos_ll->set)
         opp_abort("advection loops: c_pos_ll must be a 2-component cell dat and c_c_map a 4-entry cell map");
     oppb_rt::sync_host_to_device(c_pos_ll);
@@ -116,10 +121,12 @@ void pack_cells(opp_dat c_pos_ll, opp_map c2c) {
     a.c_pos_ll = c_pos_ll;
     a.c2c = c2c;
     a.c_pos_ll_version = c_pos_ll->version;
+    a.generation = oppb_rt::generation();
 }
 
 oppb_advec_batch batch_of(opp_set set, opp_dat pos, opp_dat vel, opp_dat mdir) {
     Advec& a = adv();
+    if (a.dh && a.dh_generation != oppb_rt::generation()) a.dh = nullptr;  // a grid of an earlier run
     oppb_advec_batch b{};
     b.n_instances = 1;
     b.n_work = (set->size + kWorkItem - 1) / kWorkItem;
@@ -174,7 +181,7 @@ void opp_particle_move__move_kernel(opp_set set, opp_map c2c_map, opp_map p2c_ma
     check_cuda(cudaMemsetAsync(st, 0, sizeof(oppb_move_status), s), "status reset");
     const oppb_advec_batch b = batch_of(set, pos, nullptr, mdir);
     check(oppb_advec_move(&b, st, oppb_rt::max_hops(), s), "oppb_advec_move");
-    if (adv().dh)  // only the global move's pre-pass removes particles
+    if (b.dh)  // only the global move's pre-pass removes particles
         check(oppb_removal_bits(b.p2c, set->size, oppb_rt::remove_bits(set), s), "oppb_removal_bits");
     oppb_rt::mark_device_written(mdir);
     oppb_rt::mark_device_written(set->mesh_relation_dat);
@@ -253,7 +260,9 @@ void opp_init_direct_hop_cg(double grid_spacing, const opp_dat c_gbl_id, const o
         d.inv_spacing = g.inv_spacing;
         d.dims[0] = g.dims[0];
         d.dims[1] = g.dims[1];
-        if (!a.dh) a.dh = dev_alloc<oppb_advec_dh>(1);
+        if (!a.dh_table) a.dh_table = dev_alloc<oppb_advec_dh>(1);
+        a.dh = a.dh_table;
+        a.dh_generation = oppb_rt::generation();
         check_cuda(cudaMemcpyAsync(a.dh, &d, sizeof d, cudaMemcpyHostToDevice, s), "dh upload");
         check_cuda(cudaStreamSynchronize(s), "dh sync");
     }

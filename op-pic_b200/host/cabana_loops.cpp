@@ -51,7 +51,8 @@ void finish(const char* name) {
 }
 
 struct HexMesh {
-    opp_map c2ngc = nullptr;
+    opp_map c2ngc = nullptr;  // the map packed into c2f, in the runtime generation `generation`
+    int generation = -1;
     int32_t n_cells = 0;
     int32_t* c2f = nullptr;
     double* interp = nullptr;
@@ -99,15 +100,18 @@ void opp_particle_move__move_deposit_kernel(opp_set set, opp_map c2c_map, opp_ma
     if (h.n_cells != n) {
         cudaFree(h.c2f);
         cudaFree(h.interp);
-        check_cuda(cudaMalloc(reinterpret_cast<void**>(&h.c2f), sizeof(int32_t) * 8 * (size_t)std::max(n, 1)), "cudaMalloc c2f");
-        check_cuda(cudaMalloc(reinterpret_cast<void**>(&h.interp), sizeof(double) * 20 * (size_t)std::max(n, 1)), "cudaMalloc interp");
+        const size_t cells_alloc = (size_t)std::max(n, 1);
+        check_cuda(cudaMalloc(reinterpret_cast<void**>(&h.c2f), sizeof(int32_t) * 8 * cells_alloc), "cudaMalloc c2f");
+        check_cuda(cudaMalloc(reinterpret_cast<void**>(&h.interp), sizeof(double) * 20 * cells_alloc),
+                   "cudaMalloc interp");
         h.n_cells = n;
         h.c2ngc = nullptr;
     }
     oppb_hex_mesh mesh{n, h.c2f, h.interp, nullptr};
-    check(oppb_hex_mesh_pack(&mesh, n, h.c2ngc == c2c_map ? nullptr : c2c_map->map_d, ddat(arg4), s),
-          "oppb_hex_mesh_pack");
+    const bool packed = h.c2ngc == c2c_map && h.generation == oppb_rt::generation();
+    check(oppb_hex_mesh_pack(&mesh, n, packed ? nullptr : c2c_map->map_d, ddat(arg4), s), "oppb_hex_mesh_pack");
     h.c2ngc = c2c_map;
+    h.generation = oppb_rt::generation();
     oppb_cabana_particles p{set->size,
                             std::max(set->set_capacity, 1),
                             ddat(arg1),

@@ -32,9 +32,11 @@ oppb_particles particles(opp_set set, opp_dat pos, opp_dat vel, opp_dat lc) {
 
 double charge_over_mass() { return opp_get_const("CONST_charge") / opp_get_const("CONST_mass"); }
 
-// The global move's structured grid, set up by opp_init_direct_hop_cg when opp_global_move is on.
+// The global move's structured grid, set up by opp_init_direct_hop_cg when opp_global_move is on,
+// for the run (the runtime generation) it was built in.
 struct DirectHop {
     bool on = false;
+    int generation = -1;
     oppb_dh_grid grid{};
 } g_dh;
 
@@ -124,7 +126,7 @@ void opp_particle_move__move_kernel(opp_set set, opp_map c2c_map, opp_map p2c_ma
     const oppb_tet_mesh& mesh = oppb_rt::tet_mesh(arg3.dat, arg2.dat, c2c_map, nullptr, nullptr);
     oppb_particles p = particles(set, arg0.dat, nullptr, arg1.dat);
     opp_profiler->start("move_kernel_only");
-    if (g_dh.on) {  // global move: the walks start from the structured grid's cells
+    if (g_dh.on && g_dh.generation == oppb_rt::generation()) {  // global move: the walks start from the grid's cells
         oppb_move_options o{};
         o.precision = OPPB_PRECISION_F64;
         o.dh = &g_dh.grid;
@@ -204,6 +206,7 @@ void opp_init_direct_hop_cg(double grid_spacing, const opp_dat c_gbl_id, const o
     check(rc, "oppb_dh_build");
     if (cudaStreamSynchronize(oppb_rt::stream()) != cudaSuccess) opp_abort("direct-hop grid build");
     g_dh.on = true;
+    g_dh.generation = oppb_rt::generation();
     opp_profiler->end("Setup_Mover");
 }
 

@@ -54,6 +54,8 @@ std::vector<opp_dat> opp_dats;
 
 namespace {
 
+int g_generation = 0;  // opp_init calls so far: caches keyed on sets, dats or maps check it
+
 struct Runtime {
     cudaStream_t stream = nullptr;
     std::map<std::string, std::vector<double>> consts;
@@ -302,6 +304,7 @@ void opp_init(int argc, char** argv) {
     OPP_gpu_shared_mem_per_block = prop.sharedMemPerBlock;
     check_cuda(cudaStreamCreateWithFlags(&rt().stream, cudaStreamNonBlocking), "stream");
     rt().status = reinterpret_cast<oppb_move_status*>(dev_alloc(sizeof(oppb_move_status)));
+    ++g_generation;
     rt().invalid = reinterpret_cast<int32_t*>(dev_alloc(sizeof(int32_t)));
 }
 
@@ -925,6 +928,8 @@ namespace oppb_rt {
 cudaStream_t stream() { return rt().stream; }
 
 int max_hops() { return OPP_move_max_hops > 0 ? OPP_move_max_hops : 4096; }
+
+int generation() { return g_generation; }
 
 void* workspace(size_t bytes) {
     auto& r = rt();
