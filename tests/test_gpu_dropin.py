@@ -200,14 +200,17 @@ LOG_LINE = re.compile(r"ts: (\d+)\s+np: (\d+) \((\d+) added, (\d+) removed\)\s+m
 
 
 @pytest.mark.skipif(not REF_MAIN.exists(), reason="the reference's generated main was not built (oracle/Makefile)")
-@pytest.mark.parametrize("fill,period", [("HoleFill_All", 10), ("Sort_Periodic", 5)])
-def test_reference_generated_main_runs_on_the_dropin(tmp_path, fill, period):
+@pytest.mark.parametrize("fill,period,global_move", [("HoleFill_All", 10, False), ("Sort_Periodic", 5, False),
+                                                     ("HoleFill_All", 10, True)])
+def test_reference_generated_main_runs_on_the_dropin(tmp_path, fill, period, global_move):
     """The reference's own generated FemPIC main, apps_codegen/app_fempic_cg/fempic_opp.cpp,
     compiled unmodified against include/ and linked with libopp_b200.so (oracle/Makefile): its
     mesh from the app's text files through its own load_mesh(), its injection from its own
     init_inject_distributions and rand_file, the field phase every step (FESolver on the GPU),
     the physical constants of fempic_defs.h.  Its per-step log (particles, added, removed, max
-    c_ef, max n_pot) against the oracle running the same step with the same field phase."""
+    c_ef, max n_pot) against the oracle running the same step with the same field phase.  With
+    opp_global_move on, the main's own BoundingBox and opp_init_direct_hop_cg build the grid (on
+    the GPU here) and every move starts from it, as the oracle's global move does."""
     from oracle import field as F
     from oracle import mesh as OM
 
@@ -224,7 +227,8 @@ def test_reference_generated_main_runs_on_the_dropin(tmp_path, fill, period):
         f"STRING global_mesh = {files['global_mesh']}\nSTRING inlet_mesh = {files['inlet_mesh']}\n"
         f"STRING wall_mesh = {files['wall_mesh']}\nSTRING rand_file = {tmp_path / 'rand.dat'}\n"
         f"STRING opp_fill = {fill}\nINT opp_fill_period = {period}\nREAL opp_allocation_multiple = 11\n"
-        "BOOL opp_global_move = false\nBOOL opp_profile_all = false\n")
+        f"BOOL opp_global_move = {'true' if global_move else 'false'}\nBOOL opp_dh_data_generate = true\n"
+        "BOOL opp_profile_all = false\n")
     r = subprocess.run([str(REF_MAIN), str(tmp_path / "params.txt")], capture_output=True, text=True, timeout=600,
                        cwd=tmp_path)
     assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
@@ -247,8 +251,9 @@ def test_reference_generated_main_runs_on_the_dropin(tmp_path, fill, period):
     bnd = np.where(m.n_type == OM.FIXED, -1.0 * wall, 0.0)  # init_boundary_pot_kernel
     fs = F.FieldSystem(m.n_pos, m.n_type, bnd, m.c2n)
     consts = F.FieldConsts(n0=n0, phi0=0.0, kte=kb * temp, qe=qe, eps0=eps0, max_iter=10000)
+    dh = O.DirectHop(m.n_pos, 0.1, (0.4, 0.4, 0.4), mesh=m) if global_move else None  # grid_spacing, 4 x it
     o = O.OracleFemPIC(m, dist, ion_velocity=vion, qm=(1 * qe) / (2 * amu), dt=dt, fill=fill, fill_period=period,
-                       field=(fs, consts, spwt, m.n_vol))
+                       field=(fs, consts, spwt, m.n_vol), dh=dh)
     removed = 0
     for s in range(steps):
         out = o.step(table)
